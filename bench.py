@@ -1,0 +1,344 @@
+#!/usr/bin/env python
+"""Throughput of the conserved semi-implicit PFC step on B200.
+
+Workload: 3D PFC on a 512^3 grid in FP32 -- random liquid psi0 = -0.18 +
+U(-0.05, 0.05) (numpy PCG64, seed 2024 + rank), eps = 0.3, dt = 0.25, dx = pi/4, no
+noise -- the grid and precision the headline metric is quoted on.  A step is one
+conserved semi-implicit step of the whole field (inverse FFT, cubic term, forward
+FFT, propagator).  The 539 MB state is larger than L2 (126 MB), so no L2 flush is
+needed between steps.
+
+Arms
+  default            this library's fused stepper (pfc_step through the C ABI)
+  --impl reference   the reference's own stock cuFFT step (copy, C2R, psi3_split,
+                     R2C, update_eom; cuda/kernels/eom.hpp etc.), compiled from the
+                     reference sources into oracle/_ref by oracle/Makefile
+
+Multi-GPU (torchrun, one process per GPU): every rank advances its own field
+(replicas only, no data-path collective); timing is the max over ranks and `value`
+counts the steps of all ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mcstar-libs_b200"))
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+WL = dict(nx=512, ny=512, nz=512, dx=math.pi / 4, dt=0.25, eps=0.3, psi0=-0.18, amp=0.05, seed=2024)
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=512, help="grid side (the headline workload is 512)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.dev)], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [ln.split(",") for ln in open(self.path).read().splitlines() if ln.strip()]
+        os.unlink(self.path)
+        mhz, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [v.strip() for v in r]
+            try:
+                mhz.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for i, nm in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        if not mhz:
+            return None
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kernel, size):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        d = json.load(open(p))
+        e = d[kernel]
+        return float(e["dram_bytes_per_launch"]) * (size / float(e.get("size", size))) ** 3
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def initial_field(shape, seed):
+    from mcstar_b200 import liquid_random
+    return liquid_random(shape, WL["psi0"], WL["amp"], seed)
+
+
+def cpu_baseline(n, steps_budget_s=20.0):
+    """The oracle (numpy/scipy restatement of the reference's step) in FP32 on the host
+    cores, a bounded number of steps of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pfc_oracle as O
+    cores = len(os.sched_getaffinity(0))
+    shape = (n, n, n)
+    psi = initial_field(shape, WL["seed"]).astype(np.float32)
+    lens = tuple(v * WL["dx"] for v in shape)
+    k = O.r2c(psi, workers=cores)
+    t0 = time.perf_counter()
+    k = O.step(k, 1, WL["dt"], WL["eps"], lens, shape, workers=cores, dtype=np.float32)
+    t1 = time.perf_counter()
+    extra = int(max(0, min(4, steps_budget_s / max(t1 - t0, 1e-3) - 1)))
+    if extra:
+        k = O.step(k, extra, WL["dt"], WL["eps"], lens, shape, workers=cores, dtype=np.float32)
+    t2 = time.perf_counter()
+    nsteps = 1 + extra
+    return {"value": nsteps / (t2 - t0), "unit": "steps/s", "cores": cores, "kind": "port",
+            "sample": f"{nsteps} step(s) of the {n}^3 fp32 workload, oracle/pfc_oracle.py with scipy.fft "
+                      f"workers={cores}"}
+
+
+# ---------------------------------------------------------------------------------------
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v):
+    if ws == 1:
+        return v
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_b200(args, ws, rank, local):
+    from mcstar_b200 import Stepper
+    n = args.size
+    shape = (n, n, n)
+    st = Stepper(shape, WL["dx"], WL["dt"], WL["eps"], dtype=np.float32)
+    st.set_real(initial_field(shape, WL["seed"] + rank))
+    ctx = st.ctx
+    S = ctx.state_bytes
+    # untimed warm-up
+    st.step(args.warmup)
+    torch.cuda.synchronize()
+    # ---- device-resident timed region --------------------------------------------------
+    clocks = Clocks(local)
+    ctx.profile_enable(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks.start()
+    e0.record()
+    st.step(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    prof = ctx.profile_read()
+    ctx.profile_enable(False)
+    ms_max = max_over_ranks(ws, ms)
+    # ---- end to end through the public API with host buffers ----------------------------------
+    host_in = torch.empty_like(st.kpsi, device="cpu").pin_memory()
+    host_in.copy_(st.kpsi)
+    host_out = torch.empty_like(host_in).pin_memory()
+    torch.cuda.synchronize()
+    barrier(ws)
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record()
+    st.kpsi.copy_(host_in, non_blocking=True)
+    st.step(args.steps)
+    host_out.copy_(st.kpsi, non_blocking=True)
+    e3.record()
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms_e2e = max_over_ranks(ws, e2.elapsed_time(e3))
+    if not np.isfinite(host_out.numpy()[:2]).all():
+        raise RuntimeError("non-finite state")
+
+    steps_total = ws * args.steps
+    value = steps_total / (ms_max / 1e3)
+    cells = n ** 3
+    # ---- roofline of the dominant kernel family -------------------------------------------------
+    peak, peak_kind = measured_peak()
+    fused = prof["xy_variant"] != 0
+    # algorithmic bytes per launch: the plane kernel reads and writes the state once
+    # (2S); the general xy part is three passes (6S per bracketed call); the z pass
+    # reads the carried state and the nonlinear term and writes the state (3S)
+    fam_bytes = {1: (2.0 * S if fused else 6.0 * S), 2: 3.0 * S}
+    fam_name = {1: ("k_plane_xy" if fused else "k_cols+k_rows_nonlin+k_cols"), 2: "k_zprop"}
+    fam = max((1, 2), key=lambda f: prof["ms"][f])
+    per_launch_ms = prof["ms"][fam] / max(1, prof["calls"][fam])
+    achieved = fam_bytes[fam] / (per_launch_ms / 1e3) / 1e9
+    step_bytes = (5.0 if fused else 9.0) * S
+    roof = {"bound": "hbm", "kernel": fam_name[fam], "achieved": round(achieved, 1), "peak": peak,
+            "peak_kind": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)", "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "algorithmic_bytes_per_launch": fam_bytes[fam],
+            "traffic": ncu_traffic(fam_name[fam], n),
+            "step_bytes_alg": step_bytes,
+            "step_frac": round(step_bytes * (value / ws) / 1e9 / peak, 4),
+            "family_ms_per_call": {k: round(prof["ms"][f] / max(1, prof["calls"][f]), 5)
+                                   for k, f in (("entry_exit", 0), ("xy", 1), ("z", 2))}}
+    out = {
+        "metric": "PFC steps/s (Gcell-upd/s in gcell_upd_per_s) at 512^3 fp32",
+        "value": round(value, 2), "unit": "steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded random liquid psi0=-0.18+U(-0.05,0.05) (numpy PCG64)",
+        "config": {"workload": f"pfc3d-conserved-semi-implicit {n}^3 fp32 liquid", "grid": [n, n, n],
+                   "dx": WL["dx"], "dt": WL["dt"], "eps": WL["eps"], "noise": False,
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                   "l2": "state (539 MB at 512^3) larger than L2; no flush"},
+        "gcell_upd_per_s": round(value * cells / 1e9, 2),
+        "e2e": {"value": round(steps_total / (ms_e2e / 1e3), 2), "unit": "steps/s",
+                "h2d_bytes_per_step": S / args.steps, "d2h_bytes_per_step": S / args.steps,
+                "note": "per K-step run: one pinned H2D of the initial half spectrum, K steps through "
+                        "pfc_step (C ABI), one D2H of the final half spectrum"},
+        "gpu_launches": prof["launches"],
+        "roofline": roof,
+        "clocks": clk,
+    }
+    return out
+
+
+def run_reference(args):
+    name = os.path.join(ROOT, "oracle", "_ref", "libref_pfc_f32.so")
+    if not torch.cuda.is_available():
+        return {"impl": "reference", "unavailable": "no CUDA device: the reference's step is CUDA/cuFFT code"}
+    if not os.path.exists(name):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libref_pfc_f32.so not built (make -C oracle)"}
+    L = ctypes.CDLL(name)
+    P, D, I = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
+    L.ref32_create.argtypes = [I, I, I, ctypes.c_ulonglong]
+    L.ref32_create.restype = P
+    L.ref32_destroy.argtypes = [P]
+    L.ref32_r2c.argtypes = [P, P, P]
+    L.ref32_set_kpsi.argtypes = [P, P]
+    L.ref32_step.argtypes = [P, I, D, D, D, D, D, D, D, I]
+    for f in (L.ref32_time_steps, L.ref32_time_e2e):
+        f.argtypes = [P, I, D, D, D, D, D, D, D, I]
+        f.restype = ctypes.c_float
+    n = args.size
+    shape = (n, n, n)
+    lens = tuple(v * WL["dx"] for v in shape)
+    psi = initial_field(shape, WL["seed"]).astype(np.float32)
+    h = L.ref32_create(n, n, n, 1234)
+    k = np.zeros((n, n, n // 2 + 1), dtype=np.complex64)
+    L.ref32_r2c(h, psi.ctypes.data, k.ctypes.data)
+    L.ref32_set_kpsi(h, k.ctypes.data)
+    L.ref32_step(h, args.warmup, 0.0, WL["dt"], WL["eps"], *lens, 0.0, 0)
+    clocks = Clocks(0)
+    clocks.start()
+    ms = L.ref32_time_steps(h, args.steps, 0.0, WL["dt"], WL["eps"], *lens, 0.0, 0)
+    clk = clocks.stop()
+    ms_e2e = L.ref32_time_e2e(h, args.steps, 0.0, WL["dt"], WL["eps"], *lens, 0.0, 0)
+    L.ref32_destroy(h)
+    S = (n // 2 + 1) * n * n * 8
+    value = args.steps / (ms / 1e3)
+    return {
+        "impl": "reference",
+        "metric": "PFC steps/s (Gcell-upd/s in gcell_upd_per_s) at 512^3 fp32",
+        "value": round(value, 2), "unit": "steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic: seeded random liquid psi0=-0.18+U(-0.05,0.05) (numpy PCG64)",
+        "config": {"workload": f"pfc3d-conserved-semi-implicit {n}^3 fp32 liquid", "grid": [n, n, n],
+                   "dx": WL["dx"], "dt": WL["dt"], "eps": WL["eps"], "noise": False,
+                   "parallelism": "single GPU", "l2": "state larger than L2; no flush"},
+        "gcell_upd_per_s": round(value * n ** 3 / 1e9, 2),
+        "e2e": {"value": round(args.steps / (ms_e2e / 1e3), 2), "unit": "steps/s",
+                "h2d_bytes_per_step": S / args.steps, "d2h_bytes_per_step": S / args.steps},
+        "cpu_baseline": {"value": round(value, 2), "unit": "steps/s", "cores": 1, "kind": "reference",
+                         "sample": "the reference has no CPU implementation of the step: this arm runs its "
+                                   "cuFFT path (oracle/_ref) on the GPU, driven by one host thread"},
+        "clocks": clk,
+    }
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)))
+        return
+    out = run_b200(args, ws, rank, local)
+    if rank == 0:
+        if ws == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(args.size)
+        print(json.dumps(out))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,166 @@
+/*
+ * pfc_b200.h -- C ABI of the B200-native conserved phase-field-crystal stepper.
+ *
+ * Every entry point replaces one host interface of mcstar-libs' header API (paths
+ * relative to the mcstar-libs root are cited beside each declaration).  The
+ * reference-name C++ headers shipped with this library (mcstar-libs_b200/shim/)
+ * forward to these functions, so a driver written against mcstar-libs compiles
+ * unchanged against this library; other languages bind the functions directly
+ * (plain pointers, sizes and scalars; no C++ or torch types).
+ *
+ * Conventions
+ *  - A context (pfc_ctx) is made for one grid shape (nx, ny, nz) and one precision.
+ *    It owns every workspace (FFT twiddles and scratch, reduction and peak scratch,
+ *    the FP64 k=0 slot of the fused stepper); no entry point allocates device
+ *    memory after pfc_create.  Field buffers belong to the caller.
+ *  - Layouts are the reference's (cuda/array_abstraction.hpp:37-70): x fastest,
+ *    real field F[nz][ny][nx], half spectrum {F re, F im}[nz][ny][nx/2+1].  All
+ *    field pointers are DEVICE pointers.  F = float (PFC_F32) or double (PFC_F64).
+ *  - Work is enqueued on the context's stream (pfc_set_stream; default the legacy
+ *    stream).  Entry points that return a host value synchronise that stream.
+ *  - Errors are returned as pfc_status; nothing calls exit() or aborts.  The
+ *    message of the last failure is pfc_last_error(ctx).  A context is not
+ *    thread-safe: use one per host thread.
+ */
+#ifndef PFC_B200_H
+#define PFC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pfc_status {
+    PFC_OK = 0,
+    PFC_ERR_INVALID = 1,      /* bad argument or shape                                */
+    PFC_ERR_UNSUPPORTED = 2,  /* valid but not implemented (e.g. a prime FFT length)  */
+    PFC_ERR_CUDA = 3,         /* a CUDA runtime error; see pfc_last_error            */
+    PFC_ERR_NOMEM = 4,        /* device allocation failed in pfc_create              */
+    PFC_ERR_CAPACITY = 5,     /* an output buffer was too small (count still set)    */
+    PFC_ERR_NONFINITE = 6     /* the stepper's watchdog saw NaN/Inf in the state     */
+} pfc_status;
+
+typedef enum pfc_dtype { PFC_F32 = 0, PFC_F64 = 1 } pfc_dtype;
+
+typedef struct pfc_desc {
+    int nx, ny, nz;   /* real extents; 2D fields have nz = 1, 1D fields ny = nz = 1 */
+    int dtype;        /* pfc_dtype                                                  */
+} pfc_desc;
+
+typedef struct pfc_ctx pfc_ctx;
+
+/* Replaces: the implicit set-up of the reference's typedef'd GPUArray/CufftPlan
+ * (cuda/array_abstraction.hpp:74-96, cuda/cufft_wrapper.hpp:68-77).  Lengths must
+ * factor into 2, 3, 5 (the reference's own restriction, cufft_unittest/main.cu:32-36). */
+pfc_status  pfc_create(const pfc_desc* desc, pfc_ctx** out);
+pfc_status  pfc_destroy(pfc_ctx* ctx);
+pfc_status  pfc_set_stream(pfc_ctx* ctx, void* cuda_stream);
+const char* pfc_last_error(const pfc_ctx* ctx);
+const char* pfc_status_string(pfc_status s);
+/* bytes of one half-spectrum buffer, (nx/2+1)*ny*nz*2*sizeof(F) -- Array::m_bytes,
+ * cuda/array_abstraction.hpp:53 */
+size_t      pfc_state_bytes(const pfc_ctx* ctx);
+size_t      pfc_workspace_bytes(const pfc_ctx* ctx);
+
+/* ---- FFT: replaces FFT::CufftPlan<F, R2C/C2R>::execute (cuda/cufft_wrapper.hpp:61-86).
+ * Unnormalised; a round trip multiplies by nx*ny*nz.  in and out must not alias;
+ * the input is preserved (cuFFT's C2R may overwrite its input; this one does not). */
+pfc_status pfc_fft_r2c(pfc_ctx* ctx, const void* real_in, void* cmpl_out);
+pfc_status pfc_fft_c2r(pfc_ctx* ctx, const void* cmpl_in, void* real_out);
+
+/* ---- pointwise kernels: replace the call_kernel_ functions of cuda/kernels/ ------------ */
+/* call_kernel_update_eom (cuda/kernels/eom.hpp:73-86); knoise may be NULL (eom.hpp:80) */
+pfc_status pfc_update_eom(pfc_ctx* ctx, void* kpsi, const void* knonlin, const void* knoise,
+                          double namp, double dt, double eps, double lx, double ly, double lz);
+/* call_kernel_update_eom_with_fen (eom.hpp:103-109): also overwrites knoise with L^psi^_old */
+pfc_status pfc_update_eom_with_fen(pfc_ctx* ctx, void* kpsi, const void* knonlin, void* knoise,
+                                   double namp, double dt, double eps, double lx, double ly, double lz);
+/* call_kernel_psi3_split (cuda/kernels/psi3_split.hpp:15-26); pot may be NULL */
+pfc_status pfc_psi3_split(pfc_ctx* ctx, void* arr, const void* pot, double mu, int norm);
+/* call_kernel_norm (cuda/kernels/norm.hpp:5-10) */
+pfc_status pfc_norm(pfc_ctx* ctx, void* arr);
+/* call_kernel_calc_fen (eom.hpp:130-141): writes the density f into lpsi like the
+ * reference and returns h^3 * sum(f) in *out, summed in FP64 in a fixed order
+ * (deterministic; the reference sums float atomics). */
+pfc_status pfc_calc_fen(pfc_ctx* ctx, const void* psi, void* lpsi,
+                        double hx, double hy, double hz, double* out);
+
+/* ---- noise: replaces NoiseHostApi<F> (cuda/noise.hpp:93-150) -------------------------
+ * Counter-based Philox4x32-10: (seed, counter) selects the draw, so a run resumes
+ * bit-exactly.  fill_kspace: complex normal, E|xi|^2 = 1, Hermitian on the i0 = 0 and
+ * i0 = nx/2 planes, self-conjugate modes real with unit variance (noise.hpp:110-142).
+ * fill: real N(0, sigma^2) per element (noise.hpp:108-109). */
+pfc_status pfc_noise_fill_kspace(pfc_ctx* ctx, void* arr, uint64_t seed, uint64_t counter);
+pfc_status pfc_noise_fill(pfc_ctx* ctx, void* arr, double sigma, uint64_t seed, uint64_t counter);
+
+/* ---- peaks: replaces call_kernel_findpeaks / call_kernel_findpeaks_2d
+ * (cuda/kernels/findpeaks.hpp:31-63, findpeaks_2d.hpp:29-56).  Cells strictly greater
+ * than all 26 (3D) or 8 (nz == 1) periodic neighbours and >= ths.  Output records
+ * have the layout of Maximum<F> (common/maximum_struct.hpp:3-6): {F i0, i1, i2; float
+ * field} -- 16 bytes for F32, 32 for F64 -- written to DEVICE memory, sorted by linear
+ * index (deterministic; the reference's order is that of racing atomics).
+ * *n_found receives the total count; if it exceeds capacity, capacity records are
+ * written and PFC_ERR_CAPACITY is returned. */
+pfc_status pfc_findpeaks(pfc_ctx* ctx, const void* psi, double ths,
+                         void* out_maxima, int capacity, int* n_found);
+
+/* ---- bond order: replaces bond_order_analysis<T> (bond-order-analysis/bond-order.hpp:4,
+ * bond-order.cpp:289-349) on the GPU.  Input: n device Maximum<F> records (as written
+ * by pfc_findpeaks).  Atoms with field > ths are kept; neighbours are atoms within
+ * rlim under the minimum image of a cubic box of side boxsize.  For every kept atom
+ * with at least one neighbour, one row of PFC_BOND_NCOL doubles is written to
+ * out_rows (device), in input order, with the columns
+ *   x y z nb xi q4 q6 q8 w4 q4b q6b q8b w4b w6
+ * (the reference's table, bond-order.cpp:333-338, plus w6).  *n_rows receives the
+ * row count; PFC_ERR_CAPACITY if it exceeds row_capacity. */
+#define PFC_BOND_NCOL 14
+pfc_status pfc_bond_order(pfc_ctx* ctx, const void* maxima, int n,
+                          double h0, double h1, double h2, double ths, double boxsize, double rlim,
+                          double* out_rows, int row_capacity, int* n_rows);
+
+/* ---- fused stepper (no reference counterpart as one call: it is the driver loop of
+ * copy, C2R, psi3_split(norm), R2C, [fill_kspace], update_eom that every mcstar-libs
+ * driver runs, eom.hpp:60-86 + psi3_split.hpp + cufft_wrapper.hpp).
+ * Advances kpsi (device, half spectrum, in place) by nsteps conserved semi-implicit
+ * steps  psi^ <- (psi^ - dt k^2 FFT((psi^3 - C psi - mu)) + dt namp sqrt(N) |k| xi^) /
+ *               (1 + dt k^2 ((1-k^2)^2 + C - eps)).
+ * C = 1 is the reference's split; the k = 0 mode is carried in FP64 and is invariant.
+ * Noise (namp != 0) of step t uses (seed, counter + t). */
+typedef struct pfc_step_params {
+    double dt, eps, mu, C;
+    double namp;
+    double lx, ly, lz;
+    uint64_t seed, counter;
+} pfc_step_params;
+pfc_status pfc_step(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params* params);
+
+/* Free energy F = h^3 sum 1/2 psi ((1+lap)^2 - eps) psi + 1/4 psi^4 of the state kpsi,
+ * computed as the reference does (eom.hpp:88-141: L^psi^, C2R, norm, calc_fen) with an
+ * FP64 deterministic sum.  Does not modify kpsi. */
+pfc_status pfc_free_energy(pfc_ctx* ctx, const void* kpsi, double eps,
+                           double lx, double ly, double lz,
+                           double hx, double hy, double hz, double* out);
+
+/* ---- tracing (the role of TimeAcc, cuda/cutiming.hpp:5-25, inside the library) ------
+ * While enabled, pfc_step brackets each kernel family with CUDA events on the
+ * context's stream and counts every kernel the library launches.  Families:
+ *   0 = entry/exit passes, 1 = the xy part of a step (one plane kernel, or the
+ *   y/x/y general passes), 2 = the z pass with the propagator.
+ * pfc_profile_read synchronises the stream and returns the totals since enabling. */
+#define PFC_PROFILE_FAMILIES 3
+typedef struct pfc_profile {
+    long long launches;                          /* kernels launched by the library  */
+    long long calls[PFC_PROFILE_FAMILIES];       /* bracketed launches per family    */
+    double ms[PFC_PROFILE_FAMILIES];             /* summed device time per family    */
+    int xy_variant;                              /* 0: general y/x/y passes; else the
+                                                    fused plane kernel in use        */
+} pfc_profile;
+pfc_status pfc_profile_enable(pfc_ctx* ctx, int on);
+pfc_status pfc_profile_read(pfc_ctx* ctx, pfc_profile* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PFC_B200_H */

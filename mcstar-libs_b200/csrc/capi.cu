@@ -1,0 +1,443 @@
+// extern "C" entry points of libpfc_b200 (declared in include/pfc_b200.h).
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+#include "pfc_ctx.h"
+
+using namespace pfc;
+
+namespace {
+
+bool factor_radices(int n, std::vector<int>& rs) {
+    rs.clear();
+    if (n < 1) return false;
+    while (n % 8 == 0) { rs.push_back(8); n /= 8; }
+    while (n % 4 == 0) { rs.push_back(4); n /= 4; }
+    while (n % 2 == 0) { rs.push_back(2); n /= 2; }
+    while (n % 3 == 0) { rs.push_back(3); n /= 3; }
+    while (n % 5 == 0) { rs.push_back(5); n /= 5; }
+    return n == 1 && (int)rs.size() <= kMaxStages;
+}
+
+// Appends the Stockham twiddles of an n-point plan to tab (forward sign, FP64).
+bool make_plan(int n, LinePlan& p, std::vector<std::complex<double>>& tab) {
+    std::vector<int> rs;
+    if (!factor_radices(n, rs)) return false;
+    std::memset(&p, 0, sizeof(p));
+    p.n = n;
+    p.nst = (int)rs.size();
+    int Ns = 1;
+    for (int s = 0; s < p.nst; ++s) {
+        const int R = rs[s];
+        p.radix[s] = R;
+        p.ns[s] = Ns;
+        p.twoff[s] = (int)tab.size();
+        for (int jj = 0; jj < Ns; ++jj)
+            for (int r = 1; r < R; ++r) {
+                const long long num = ((long long)r * jj) % ((long long)Ns * R);
+                const double ang = -2.0 * M_PI * (double)num / (double)(Ns * R);
+                tab.emplace_back(std::cos(ang), std::sin(ang));
+            }
+        Ns *= R;
+    }
+    return true;
+}
+
+int pow2_floor(size_t v, int cap) {
+    int t = 1;
+    while (t * 2 <= cap && (size_t)(t * 2) <= v) t *= 2;
+    return t;
+}
+
+pfc_status fail(pfc_ctx* c, pfc_status s, const std::string& msg) {
+    if (c) c->err = msg;
+    return s;
+}
+
+pfc_status cuda_fail(pfc_ctx* c, cudaError_t e, const char* where) {
+    return fail(c, PFC_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define PFC_CUDA(call, where)                       \
+    do {                                            \
+        cudaError_t e_ = (call);                    \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
+    } while (0)
+
+#define PFC_CHECK_CTX()                                                      \
+    do {                                                                     \
+        if (!ctx) return PFC_ERR_INVALID;                                    \
+    } while (0)
+
+void free_ctx(pfc_ctx* c) {
+    if (!c) return;
+    for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    void* ptrs[] = {c->tw, c->work, c->work2, c->red, c->k0, c->flag, c->peak_counts, c->peak_offsets, c->bond_scratch};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete c;
+}
+
+// Accumulates the device time of every bracketed launch recorded so far.
+cudaError_t prof_resolve(pfc_ctx* c) {
+    if (c->ev_pending.empty()) { c->ev_used = 0; return cudaSuccess; }
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e) return e;
+    for (auto& p : c->ev_pending) {
+        float ms = 0.f;
+        if ((e = cudaEventElapsedTime(&ms, c->ev_pool[p.second], c->ev_pool[p.second + 1]))) return e;
+        c->prof_ms[p.first] += ms;
+        c->prof_calls[p.first] += 1;
+    }
+    c->ev_pending.clear();
+    c->ev_used = 0;
+    return cudaSuccess;
+}
+
+// Runs launch() (which enqueues `n` kernels) bracketed by events when tracing is on.
+template <typename F>
+cudaError_t traced(pfc_ctx* c, int family, int n, F&& launch) {
+    c->launches += n;
+    if (!c->prof_on) return launch();
+    if (c->ev_used + 2 > c->ev_pool.size()) {
+        cudaError_t e = prof_resolve(c);
+        if (e) return e;
+    }
+    const size_t i = c->ev_used;
+    c->ev_used += 2;
+    cudaError_t e = cudaEventRecord(c->ev_pool[i], c->stream);
+    if (e) return e;
+    if ((e = launch())) return e;
+    if ((e = cudaEventRecord(c->ev_pool[i + 1], c->stream))) return e;
+    c->ev_pending.emplace_back(family, i);
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pfc_status_string(pfc_status s) {
+    switch (s) {
+        case PFC_OK: return "ok";
+        case PFC_ERR_INVALID: return "invalid argument";
+        case PFC_ERR_UNSUPPORTED: return "unsupported";
+        case PFC_ERR_CUDA: return "CUDA error";
+        case PFC_ERR_NOMEM: return "out of device memory";
+        case PFC_ERR_CAPACITY: return "output capacity exceeded";
+        case PFC_ERR_NONFINITE: return "non-finite value in the state";
+    }
+    return "unknown status";
+}
+
+const char* pfc_last_error(const pfc_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
+    if (!d || !out) return PFC_ERR_INVALID;
+    *out = nullptr;
+    if (d->nx < 1 || d->ny < 1 || d->nz < 1) return PFC_ERR_INVALID;
+    // the reference plans a 1D transform of the first row for (nx, 1, nz > 1)
+    // (technicalities.hpp:16-32 with cufft_wrapper.hpp:72-75); such shapes are refused.
+    if (d->ny == 1 && d->nz > 1) return PFC_ERR_INVALID;
+    if (d->dtype != PFC_F32 && d->dtype != PFC_F64) return PFC_ERR_INVALID;
+    pfc_ctx* c = new (std::nothrow) pfc_ctx();
+    if (!c) return PFC_ERR_NOMEM;
+    c->nx = d->nx; c->ny = d->ny; c->nz = d->nz;
+    c->nxh = d->nx / 2 + 1;
+    c->dtype = d->dtype;
+    c->fsize = d->dtype == PFC_F64 ? 8 : 4;
+    c->n_real = (size_t)d->nx * d->ny * d->nz;
+    c->n_cmpl = (size_t)c->nxh * d->ny * d->nz;
+    c->state_bytes = c->n_cmpl * 2 * c->fsize;
+    c->stream = 0;
+    const size_t csz = 2 * c->fsize;
+
+    std::vector<std::complex<double>> tab;
+    const bool even = (c->nx % 2) == 0;
+    const int lx = even ? c->nx / 2 : c->nx;
+    if (!make_plan(lx, c->px.plan, tab) || !make_plan(c->ny, c->py.plan, tab) || !make_plan(c->nz, c->pz.plan, tab)) {
+        free_ctx(c);
+        return PFC_ERR_UNSUPPORTED;
+    }
+    c->post_off = (int)tab.size();
+    for (int k = 0; k <= c->nx / 2; ++k) {
+        const double ang = -2.0 * M_PI * (double)k / (double)c->nx;
+        tab.emplace_back(std::cos(ang), std::sin(ang));
+    }
+    // tiles: two ping-pong buffers of `tile` lines per CTA
+    c->px.tile = pow2_floor((64 * 1024) / (2 * (size_t)lx * csz), 16);
+    c->px.smem = 2 * (size_t)c->px.tile * lx * csz;
+    c->py.tile = pow2_floor((64 * 1024) / (2 * (size_t)c->ny * csz), 16);
+    c->py.smem = 2 * (size_t)c->py.tile * c->ny * csz;
+    c->pz.tile = pow2_floor((64 * 1024) / (2 * (size_t)c->nz * csz), 16);
+    c->pz.smem = 2 * (size_t)c->pz.tile * c->nz * csz;
+    c->pzprop.tile = pow2_floor((96 * 1024) / (4 * (size_t)c->nz * csz), 8);
+    c->pzprop.smem = 4 * (size_t)c->pzprop.tile * c->nz * csz;
+    if (c->px.smem > kMaxDynSmem || c->py.smem > kMaxDynSmem || c->pz.smem > kMaxDynSmem ||
+        c->pzprop.smem > kMaxDynSmem) {
+        free_ctx(c);
+        return PFC_ERR_UNSUPPORTED;
+    }
+    c->n_peak_blocks = (int)((c->n_real + kPeakBlock - 1) / kPeakBlock);
+    c->max_atoms = (int)std::max<size_t>(4096, c->n_real / 512);
+    c->bond_scratch_bytes = bond_scratch_bytes(c->max_atoms);
+    c->fused_xy = fused_xy_variant(c->nx, c->ny, c->dtype);
+
+    cudaError_t e = cudaSuccess;
+    auto alloc = [&](void** p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+    };
+    alloc(&c->tw, tab.size() * csz);
+    alloc(&c->work, c->state_bytes);
+    alloc(&c->work2, c->state_bytes);
+    alloc((void**)&c->red, sizeof(double) * (kRedBlocks + 8));
+    alloc((void**)&c->k0, sizeof(double2));
+    alloc((void**)&c->flag, sizeof(int) * 4);
+    alloc((void**)&c->peak_counts, sizeof(int) * c->n_peak_blocks);
+    alloc((void**)&c->peak_offsets, sizeof(int) * (c->n_peak_blocks + 1));
+    alloc(&c->bond_scratch, c->bond_scratch_bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        free_ctx(c);
+        return e == cudaErrorMemoryAllocation ? PFC_ERR_NOMEM : PFC_ERR_CUDA;
+    }
+    if (c->dtype == PFC_F64) {
+        e = cudaMemcpy(c->tw, tab.data(), tab.size() * csz, cudaMemcpyHostToDevice);
+    } else {
+        std::vector<float2> t32(tab.size());
+        for (size_t i = 0; i < tab.size(); ++i) t32[i] = make_float2((float)tab[i].real(), (float)tab[i].imag());
+        e = cudaMemcpy(c->tw, t32.data(), tab.size() * csz, cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMemset(c->flag, 0, sizeof(int) * 4);
+    if (e == cudaSuccess) e = set_fft_attributes(c);
+    if (e == cudaSuccess && c->fused_xy) e = set_fused_attributes(c);
+    if (e != cudaSuccess) {
+        free_ctx(c);
+        return PFC_ERR_CUDA;
+    }
+    *out = c;
+    return PFC_OK;
+}
+
+pfc_status pfc_destroy(pfc_ctx* ctx) {
+    PFC_CHECK_CTX();
+    free_ctx(ctx);
+    return PFC_OK;
+}
+
+pfc_status pfc_set_stream(pfc_ctx* ctx, void* stream) {
+    PFC_CHECK_CTX();
+    ctx->stream = (cudaStream_t)stream;
+    return PFC_OK;
+}
+
+size_t pfc_state_bytes(const pfc_ctx* ctx) { return ctx ? ctx->state_bytes : 0; }
+
+size_t pfc_workspace_bytes(const pfc_ctx* ctx) {
+    if (!ctx) return 0;
+    return 2 * ctx->state_bytes + ctx->bond_scratch_bytes + sizeof(double) * (kRedBlocks + 8) +
+           sizeof(int) * (2 * ctx->n_peak_blocks + 1);
+}
+
+// ---- FFT ------------------------------------------------------------------------------
+pfc_status pfc_fft_r2c(pfc_ctx* ctx, const void* in, void* out) {
+    PFC_CHECK_CTX();
+    if (!in || !out) return fail(ctx, PFC_ERR_INVALID, "pfc_fft_r2c: null buffer");
+    PFC_CUDA(launch_rows_r2c(ctx, in, out), "pfc_fft_r2c rows");
+    if (ctx->ny > 1) PFC_CUDA(launch_cols(ctx, 1, -1, out, out, 1.0), "pfc_fft_r2c y");
+    if (ctx->nz > 1) PFC_CUDA(launch_cols(ctx, 2, -1, out, out, 1.0), "pfc_fft_r2c z");
+    return PFC_OK;
+}
+
+pfc_status pfc_fft_c2r(pfc_ctx* ctx, const void* in, void* out) {
+    PFC_CHECK_CTX();
+    if (!in || !out) return fail(ctx, PFC_ERR_INVALID, "pfc_fft_c2r: null buffer");
+    const void* src = in;
+    if (ctx->nz > 1) { PFC_CUDA(launch_cols(ctx, 2, 1, src, ctx->work, 1.0), "pfc_fft_c2r z"); src = ctx->work; }
+    if (ctx->ny > 1) { PFC_CUDA(launch_cols(ctx, 1, 1, src, ctx->work, 1.0), "pfc_fft_c2r y"); src = ctx->work; }
+    PFC_CUDA(launch_rows_c2r(ctx, src, out), "pfc_fft_c2r rows");
+    return PFC_OK;
+}
+
+// ---- pointwise ------------------------------------------------------------------------
+pfc_status pfc_update_eom(pfc_ctx* ctx, void* kpsi, const void* knl, const void* knoise, double namp, double dt,
+                          double eps, double lx, double ly, double lz) {
+    PFC_CHECK_CTX();
+    if (!kpsi || !knl) return fail(ctx, PFC_ERR_INVALID, "pfc_update_eom: null buffer");
+    PFC_CUDA(launch_update_eom(ctx, kpsi, knl, knoise, namp, dt, eps, lx, ly, lz, 0, 1.0), "pfc_update_eom");
+    return PFC_OK;
+}
+
+pfc_status pfc_update_eom_with_fen(pfc_ctx* ctx, void* kpsi, const void* knl, void* knoise, double namp, double dt,
+                                   double eps, double lx, double ly, double lz) {
+    PFC_CHECK_CTX();
+    if (!kpsi || !knl || !knoise) return fail(ctx, PFC_ERR_INVALID, "pfc_update_eom_with_fen: null buffer");
+    PFC_CUDA(launch_update_eom(ctx, kpsi, knl, knoise, namp, dt, eps, lx, ly, lz, 1, 1.0), "pfc_update_eom_with_fen");
+    return PFC_OK;
+}
+
+pfc_status pfc_psi3_split(pfc_ctx* ctx, void* arr, const void* pot, double mu, int norm) {
+    PFC_CHECK_CTX();
+    if (!arr) return fail(ctx, PFC_ERR_INVALID, "pfc_psi3_split: null buffer");
+    PFC_CUDA(launch_psi3(ctx, arr, pot, mu, norm, 1.0), "pfc_psi3_split");
+    return PFC_OK;
+}
+
+pfc_status pfc_norm(pfc_ctx* ctx, void* arr) {
+    PFC_CHECK_CTX();
+    if (!arr) return fail(ctx, PFC_ERR_INVALID, "pfc_norm: null buffer");
+    PFC_CUDA(launch_norm(ctx, arr), "pfc_norm");
+    return PFC_OK;
+}
+
+pfc_status pfc_calc_fen(pfc_ctx* ctx, const void* psi, void* lpsi, double hx, double hy, double hz, double* out) {
+    PFC_CHECK_CTX();
+    if (!psi || !lpsi || !out) return fail(ctx, PFC_ERR_INVALID, "pfc_calc_fen: null buffer");
+    PFC_CUDA(launch_calc_fen(ctx, psi, lpsi, hx * hy * hz), "pfc_calc_fen");
+    PFC_CUDA(cudaMemcpyAsync(out, ctx->red + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+             "pfc_calc_fen copy");
+    PFC_CUDA(cudaStreamSynchronize(ctx->stream), "pfc_calc_fen sync");
+    return PFC_OK;
+}
+
+pfc_status pfc_noise_fill_kspace(pfc_ctx* ctx, void* arr, uint64_t seed, uint64_t counter) {
+    PFC_CHECK_CTX();
+    if (!arr) return fail(ctx, PFC_ERR_INVALID, "pfc_noise_fill_kspace: null buffer");
+    PFC_CUDA(launch_noise_kspace(ctx, arr, seed, counter), "pfc_noise_fill_kspace");
+    return PFC_OK;
+}
+
+pfc_status pfc_noise_fill(pfc_ctx* ctx, void* arr, double sigma, uint64_t seed, uint64_t counter) {
+    PFC_CHECK_CTX();
+    if (!arr) return fail(ctx, PFC_ERR_INVALID, "pfc_noise_fill: null buffer");
+    PFC_CUDA(launch_noise_real(ctx, arr, sigma, seed, counter), "pfc_noise_fill");
+    return PFC_OK;
+}
+
+// ---- peaks and bond order ---------------------------------------------------------------
+pfc_status pfc_findpeaks(pfc_ctx* ctx, const void* psi, double ths, void* out, int capacity, int* n_found) {
+    PFC_CHECK_CTX();
+    if (!psi || !n_found || capacity < 0 || (capacity > 0 && !out))
+        return fail(ctx, PFC_ERR_INVALID, "pfc_findpeaks: bad arguments");
+    if (ctx->nz == 1 && !(ctx->nx > 1 && ctx->ny > 1))
+        return fail(ctx, PFC_ERR_INVALID, "pfc_findpeaks: input not a 2d array");
+    PFC_CUDA(launch_findpeaks(ctx, psi, ths, out, capacity), "pfc_findpeaks");
+    int total = 0;
+    PFC_CUDA(cudaMemcpyAsync(&total, ctx->peak_offsets + ctx->n_peak_blocks, sizeof(int), cudaMemcpyDeviceToHost,
+                             ctx->stream), "pfc_findpeaks copy");
+    PFC_CUDA(cudaStreamSynchronize(ctx->stream), "pfc_findpeaks sync");
+    *n_found = total;
+    if (total > capacity) return fail(ctx, PFC_ERR_CAPACITY, "pfc_findpeaks: more peaks than capacity");
+    return PFC_OK;
+}
+
+pfc_status pfc_bond_order(pfc_ctx* ctx, const void* maxima, int n, double h0, double h1, double h2, double ths,
+                          double boxsize, double rlim, double* out_rows, int row_capacity, int* n_rows) {
+    PFC_CHECK_CTX();
+    if (!n_rows || n < 0 || (n > 0 && !maxima) || row_capacity < 0 || (row_capacity > 0 && !out_rows) ||
+        !(boxsize > 0.0))
+        return fail(ctx, PFC_ERR_INVALID, "pfc_bond_order: bad arguments");
+    if (n > ctx->max_atoms) return fail(ctx, PFC_ERR_CAPACITY, "pfc_bond_order: more atoms than the context holds");
+    int rows = 0, overflow = 0;
+    PFC_CUDA(launch_bond_order(ctx, maxima, n, h0, h1, h2, ths, boxsize, rlim, out_rows, row_capacity, &rows,
+                               &overflow), "pfc_bond_order");
+    *n_rows = rows;
+    if (overflow) return fail(ctx, PFC_ERR_CAPACITY, "pfc_bond_order: an atom has more than 64 neighbours");
+    if (rows > row_capacity) return fail(ctx, PFC_ERR_CAPACITY, "pfc_bond_order: more rows than capacity");
+    return PFC_OK;
+}
+
+// ---- stepper ------------------------------------------------------------------------------
+pfc_status pfc_step(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params* p) {
+    PFC_CHECK_CTX();
+    if (!kpsi || !p || nsteps < 0) return fail(ctx, PFC_ERR_INVALID, "pfc_step: bad arguments");
+    if (nsteps == 0) return PFC_OK;
+    void* A = kpsi;
+    void* B = ctx->work;
+    const double mul = 1.0 / ((double)ctx->nx * (double)ctx->ny);
+    ZPropArgs za;
+    za.dt = p->dt; za.eps = p->eps; za.C = p->C;
+    za.namp_eff = p->namp * std::sqrt((double)ctx->n_real);
+    za.lx = p->lx; za.ly = p->ly; za.lz = p->lz;
+    za.seed = p->seed;
+    za.use_noise = p->namp != 0.0;
+    PFC_CUDA(cudaMemsetAsync(ctx->flag, 0, sizeof(int), ctx->stream), "pfc_step flag");
+    PFC_CUDA(traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
+                 cudaError_t e = launch_k0_save(ctx, kpsi);
+                 if (e || ctx->nz == 1) return e;
+                 return launch_cols(ctx, 2, 1, A, A, 1.0 / ctx->nz);
+             }), "pfc_step entry");
+    for (int t = 0; t < nsteps; ++t) {
+        if (ctx->fused_xy) {
+            PFC_CUDA(traced(ctx, 1, 1, [&] { return launch_fused_xy(ctx, A, B, nullptr, mul, p->C, p->mu); }),
+                     "pfc_step xy");
+        } else {
+            const int n = ctx->ny > 1 ? 3 : 1;
+            PFC_CUDA(traced(ctx, 1, n, [&] {
+                         cudaError_t e;
+                         if (ctx->ny > 1) e = launch_cols(ctx, 1, 1, A, B, 1.0);
+                         else e = cudaMemcpyAsync(B, A, ctx->state_bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+                         if (e) return e;
+                         if ((e = launch_rows_nonlin(ctx, B, nullptr, mul, p->C, p->mu))) return e;
+                         return ctx->ny > 1 ? launch_cols(ctx, 1, -1, B, B, 1.0) : cudaSuccess;
+                     }), "pfc_step xy");
+        }
+        za.counter = p->counter + (uint64_t)t;
+        za.final_step = (t == nsteps - 1);
+        PFC_CUDA(traced(ctx, 2, 1, [&] { return launch_zprop(ctx, A, B, za); }), "pfc_step z");
+    }
+    int flag = 0;
+    PFC_CUDA(cudaMemcpyAsync(&flag, ctx->flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "pfc_step copy flag");
+    PFC_CUDA(cudaStreamSynchronize(ctx->stream), "pfc_step sync");
+    if (flag) return fail(ctx, PFC_ERR_NONFINITE, "pfc_step: non-finite value in the state");
+    return PFC_OK;
+}
+
+pfc_status pfc_free_energy(pfc_ctx* ctx, const void* kpsi, double eps, double lx, double ly, double lz, double hx,
+                           double hy, double hz, double* out) {
+    PFC_CHECK_CTX();
+    if (!kpsi || !out) return fail(ctx, PFC_ERR_INVALID, "pfc_free_energy: bad arguments");
+    const double N = (double)ctx->n_real;
+    PFC_CUDA(launch_fen_spectral(ctx, kpsi, eps, lx, ly, lz), "pfc_free_energy spectral");
+    PFC_CUDA(launch_reduce_final(ctx, 1, 1.0), "pfc_free_energy reduce");
+    pfc_status s = pfc_fft_c2r(ctx, kpsi, ctx->work2);
+    if (s != PFC_OK) return s;
+    PFC_CUDA(launch_quartic_sum(ctx, ctx->work2, 1.0 / N), "pfc_free_energy quartic");
+    PFC_CUDA(launch_reduce_final(ctx, 2, 1.0), "pfc_free_energy reduce");
+    double h[2] = {0.0, 0.0};
+    PFC_CUDA(cudaMemcpyAsync(h, ctx->red + kRedBlocks + 1, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+             "pfc_free_energy copy");
+    PFC_CUDA(cudaStreamSynchronize(ctx->stream), "pfc_free_energy sync");
+    *out = hx * hy * hz * (h[0] / (2.0 * N) + 0.25 * h[1]);
+    return PFC_OK;
+}
+
+pfc_status pfc_profile_enable(pfc_ctx* ctx, int on) {
+    PFC_CHECK_CTX();
+    if (on && ctx->ev_pool.empty()) {
+        ctx->ev_pool.resize(4096);
+        for (auto& e : ctx->ev_pool) PFC_CUDA(cudaEventCreate(&e), "pfc_profile_enable");
+    }
+    ctx->ev_pending.clear();
+    ctx->ev_used = 0;
+    ctx->launches = 0;
+    for (int f = 0; f < PFC_PROFILE_FAMILIES; ++f) { ctx->prof_calls[f] = 0; ctx->prof_ms[f] = 0.0; }
+    ctx->prof_on = on != 0;
+    return PFC_OK;
+}
+
+pfc_status pfc_profile_read(pfc_ctx* ctx, pfc_profile* out) {
+    PFC_CHECK_CTX();
+    if (!out) return fail(ctx, PFC_ERR_INVALID, "pfc_profile_read: null output");
+    PFC_CUDA(prof_resolve(ctx), "pfc_profile_read");
+    out->launches = ctx->launches;
+    out->xy_variant = ctx->fused_xy;
+    for (int f = 0; f < PFC_PROFILE_FAMILIES; ++f) { out->calls[f] = ctx->prof_calls[f]; out->ms[f] = ctx->prof_ms[f]; }
+    return PFC_OK;
+}
+
+}  // extern "C"

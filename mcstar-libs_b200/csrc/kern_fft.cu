@@ -1,0 +1,363 @@
+// General-size FFT passes over the reference layout (x fastest; half spectrum of
+// nx/2+1 complex per row).  Each CTA stages a tile of whole lines in shared memory
+// and runs the Stockham engine of pfc_internal.cuh on them.  These kernels serve the
+// reference-shaped primitives (R2C, C2R) and the stepper for every grid the fused
+// plane kernels do not cover.
+#include "pfc_ctx.h"
+
+namespace pfc {
+namespace {
+
+// ---------------------------------------------------------------------------------
+// complex FFT along a strided axis: element (line o, inner i, position k) at
+// base + o*os + i + k*es.  A CTA owns `tile` consecutive inner lines of one o.
+// ---------------------------------------------------------------------------------
+template <typename T, int DIR>
+__global__ void __launch_bounds__(256) k_cols(const cx<T>* __restrict__ in, cx<T>* out, int ni, int64_t es,
+                                              int64_t os, LinePlan p, const cx<T>* __restrict__ tw, int tile,
+                                              T scale) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
+    const int n = p.n;
+    cx<T>* b1 = b0 + (size_t)tile * n;
+    const int i0 = blockIdx.x * tile;
+    const int nt = min(tile, ni - i0);
+    const int64_t base = (int64_t)blockIdx.y * os + i0;
+    for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
+        const int i = e % tile, k = e / tile;
+        if (i < nt) b0[i * n + k] = in[base + i + k * es];
+    }
+    __syncthreads();
+    cx<T>* r = stockham_lines<T, DIR>(b0, b1, nt, n, p, tw);
+    for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
+        const int i = e % tile, k = e / tile;
+        if (i < nt) out[base + i + k * es] = r[i * n + k] * scale;
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// rows: real <-> half spectrum along x.  Even nx packs x[2m], x[2m+1] into one
+// complex and runs an nx/2-point FFT with the split/merge twiddles W_nx^k; odd nx
+// runs the full nx-point complex FFT.
+// ---------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ cx<T> r2c_post(cx<T> zk, cx<T> zm, cx<T> w) {
+    // X[k] = 1/2 (Z[k] + conj Z[M-k]) - i/2 W^k (Z[k] - conj Z[M-k])
+    const cx<T> s = mkc<T>(zk.x + zm.x, zk.y - zm.y);
+    const cx<T> d = mkc<T>(zk.x - zm.x, zk.y + zm.y);
+    const cx<T> wd = cmul(w, d);
+    return mkc<T>(T(0.5) * (s.x + wd.y), T(0.5) * (s.y - wd.x));
+}
+template <typename T>
+__device__ __forceinline__ cx<T> c2r_pre(cx<T> xk, cx<T> xm, cx<T> w) {
+    // Z[k] = (X[k] + conj X[M-k]) + i W^-k (X[k] - conj X[M-k]); IFFT_M(Z) = nx * (x[2m] + i x[2m+1])
+    const cx<T> e = mkc<T>(xk.x + xm.x, xk.y - xm.y);
+    const cx<T> o = cmul(mkc<T>(xk.x - xm.x, xk.y + xm.y), cconj(w));
+    return mkc<T>(e.x - o.y, e.y + o.x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_rows_r2c(const T* __restrict__ in, cx<T>* __restrict__ out, int nrows,
+                                                  int nx, LinePlan p, const cx<T>* __restrict__ tw,
+                                                  const cx<T>* __restrict__ post, int rpc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
+    const int L = p.n;
+    cx<T>* b1 = b0 + (size_t)rpc * L;
+    const int row0 = blockIdx.x * rpc;
+    const int nr = min(rpc, nrows - row0);
+    const int nxh = nx / 2 + 1;
+    const bool even = (nx & 1) == 0;
+    for (int e = threadIdx.x; e < nr * L; e += blockDim.x) {
+        const int r = e / L, m = e - r * L;
+        const T* row = in + (int64_t)(row0 + r) * nx;
+        b0[e] = even ? reinterpret_cast<const cx<T>*>(row)[m] : mkc<T>(row[m], T(0));
+    }
+    __syncthreads();
+    cx<T>* z = stockham_lines<T, -1>(b0, b1, nr, L, p, tw);
+    for (int e = threadIdx.x; e < nr * nxh; e += blockDim.x) {
+        const int r = e / nxh, k = e - r * nxh;
+        const cx<T>* zr = z + (size_t)r * L;
+        cx<T> v;
+        if (even) v = r2c_post<T>(zr[k % L], zr[(L - k) % L], post[k]);
+        else v = zr[k];
+        out[(int64_t)(row0 + r) * nxh + k] = v;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_rows_c2r(const cx<T>* __restrict__ in, T* __restrict__ out, int nrows,
+                                                  int nx, LinePlan p, const cx<T>* __restrict__ tw,
+                                                  const cx<T>* __restrict__ post, int rpc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
+    const int L = p.n;
+    cx<T>* b1 = b0 + (size_t)rpc * L;
+    const int row0 = blockIdx.x * rpc;
+    const int nr = min(rpc, nrows - row0);
+    const int nxh = nx / 2 + 1;
+    const bool even = (nx & 1) == 0;
+    for (int e = threadIdx.x; e < nr * L; e += blockDim.x) {
+        const int r = e / L, k = e - r * L;
+        const cx<T>* row = in + (int64_t)(row0 + r) * nxh;
+        cx<T> v;
+        if (even) v = c2r_pre<T>(row[k], row[L - k], post[k]);
+        else v = k < nxh ? row[k] : cconj(row[nx - k]);
+        b0[e] = v;
+    }
+    __syncthreads();
+    cx<T>* z = stockham_lines<T, 1>(b0, b1, nr, L, p, tw);
+    for (int e = threadIdx.x; e < nr * L; e += blockDim.x) {
+        const int r = e / L, m = e - r * L;
+        T* row = out + (int64_t)(row0 + r) * nx;
+        if (even) reinterpret_cast<cx<T>*>(row)[m] = z[e];
+        else row[m] = z[e].x;
+    }
+}
+
+// The stepper's x pass: C2R, the cubic nonlinearity (psi3_split.hpp:8-13 with the
+// stabilisation constant C), R2C -- in place on rows of the mixed (kx, y, z) field.
+template <typename T>
+__device__ __forceinline__ T cubic(T v, T mul, T C, T mu) {
+    const T t = v * mul;
+    return t * t * t - C * t - mu;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_rows_nonlin(cx<T>* buf, const T* __restrict__ pot, int nrows, int nx,
+                                                     LinePlan p, const cx<T>* __restrict__ tw,
+                                                     const cx<T>* __restrict__ post, int rpc, T mul, T C, T mu) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
+    const int L = p.n;
+    cx<T>* b1 = b0 + (size_t)rpc * L;
+    const int row0 = blockIdx.x * rpc;
+    const int nr = min(rpc, nrows - row0);
+    const int nxh = nx / 2 + 1;
+    const bool even = (nx & 1) == 0;
+    for (int e = threadIdx.x; e < nr * L; e += blockDim.x) {
+        const int r = e / L, k = e - r * L;
+        const cx<T>* row = buf + (int64_t)(row0 + r) * nxh;
+        cx<T> v;
+        if (even) v = c2r_pre<T>(row[k], row[L - k], post[k]);
+        else v = k < nxh ? row[k] : cconj(row[nx - k]);
+        b0[e] = v;
+    }
+    __syncthreads();
+    cx<T>* z = stockham_lines<T, 1>(b0, b1, nr, L, p, tw);
+    cx<T>* other = (z == b0) ? b1 : b0;
+    for (int e = threadIdx.x; e < nr * L; e += blockDim.x) {
+        const int r = e / L, m = e - r * L;
+        const int64_t rowi = (int64_t)(row0 + r) * nx;
+        cx<T> v = z[e];
+        if (even) {
+            T a = cubic<T>(v.x, mul, C, mu), b = cubic<T>(v.y, mul, C, mu);
+            if (pot) { a += pot[rowi + 2 * m]; b += pot[rowi + 2 * m + 1]; }
+            v = mkc<T>(a, b);
+        } else {
+            T a = cubic<T>(v.x, mul, C, mu);
+            if (pot) a += pot[rowi + m];
+            v = mkc<T>(a, T(0));
+        }
+        z[e] = v;
+    }
+    __syncthreads();
+    cx<T>* y = stockham_lines<T, -1>(z, other, nr, L, p, tw);
+    for (int e = threadIdx.x; e < nr * nxh; e += blockDim.x) {
+        const int r = e / nxh, k = e - r * nxh;
+        const cx<T>* yr = y + (size_t)r * L;
+        cx<T> v;
+        if (even) v = r2c_post<T>(yr[k % L], yr[(L - k) % L], post[k]);
+        else v = yr[k];
+        buf[(int64_t)(row0 + r) * nxh + k] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// The stepper's z pass.  The state is carried as A = IFFT_z(psi^)/nz (k-space in x
+// and y, real space in z) and B = FFT_xy of the nonlinear term on the same mixed
+// grid.  Per tile of kx columns at one ky: FFT_z(A) = psi^, FFT_z(B) = N^, the
+// semi-implicit update (eom.hpp:60-72 with stabilisation C), conserved noise, the
+// FP64 k = 0 mode, then IFFT_z/nz back into A (or psi^ itself on the last step).
+// ---------------------------------------------------------------------------------
+template <typename T>
+struct ZArgsT {
+    T dt, eps, C, namp_eff, lx, ly, lz;
+    uint64_t seed, counter;
+    int use_noise, final_step;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict__ B, int nx, int ny, int nz,
+                                               LinePlan p, const cx<T>* __restrict__ tw, int tile, ZArgsT<T> a,
+                                               const double2* __restrict__ k0, int* flag) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int bad;
+    cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
+    const int n = nz;
+    cx<T>* b1 = b0 + (size_t)2 * tile * n;
+    const int nxh = nx / 2 + 1;
+    const int i0 = blockIdx.x * tile;
+    const int ky = blockIdx.y;
+    const int nt = min(tile, nxh - i0);
+    if (threadIdx.x == 0) bad = 0;
+    for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
+        const int i = e % tile, k = e / tile;
+        if (i < nt) {
+            const int64_t off = ((int64_t)k * ny + ky) * nxh + i0 + i;
+            b0[i * n + k] = A[off];
+            b0[(tile + i) * n + k] = B[off];
+        }
+    }
+    __syncthreads();
+    cx<T>* r = stockham_lines<T, -1>(b0, b1, 2 * tile, n, p, tw);
+    cx<T>* other = (r == b0) ? b1 : b0;
+    const T k1 = kwave<T>(ky, ny, a.ly);
+    const T deps = T(1) + a.C - a.eps;
+    for (int e = threadIdx.x; e < nt * n; e += blockDim.x) {
+        const int i = e / n, kz = e - i * n;
+        const int kx = i0 + i;
+        cx<T> psi = r[i * n + kz];
+        const cx<T> nl = r[(tile + i) * n + kz];
+        const T kk0 = kwave<T>(kx, nx, a.lx), kk2 = kwave<T>(kz, nz, a.lz);
+        const T dopx = -kk0 * kk0 - k1 * k1 - kk2 * kk2;
+        const T dopy = dopx * dopx;
+        const T denom = T(1) - a.dt * (deps * dopx + T(2) * dopy + dopx * dopy);
+        if (kx == 0 && ky == 0 && kz == 0) psi = mkc<T>((T)k0->x, (T)k0->y);
+        const T f = a.dt * dopx;
+        cx<T> num = mkc<T>(psi.x + f * nl.x, psi.y + f * nl.y);
+        if (a.use_noise) {
+            const T kabs = sqrt(-dopx);
+            const cx<T> xi = kspace_noise<T>(kx, ky, kz, nx, ny, nz, a.seed, a.counter);
+            const T g = a.dt * a.namp_eff * kabs;
+            num.x += g * xi.x;
+            num.y += g * xi.y;
+        }
+        const cx<T> v = mkc<T>(num.x / denom, num.y / denom);
+        if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
+        r[i * n + kz] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && bad) atomicOr(flag, 1);
+    cx<T>* outb = r;
+    T scale = T(1);
+    if (!a.final_step) {
+        outb = stockham_lines<T, 1>(r, other, nt, n, p, tw);
+        scale = T(1) / T(nz);
+    }
+    for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
+        const int i = e % tile, k = e / tile;
+        if (i < nt) A[((int64_t)k * ny + ky) * nxh + i0 + i] = outb[i * n + k] * scale;
+    }
+}
+
+template <typename T>
+cudaError_t set_attrs_T(const pfc_ctx* c) {
+    const int m = (int)kMaxDynSmem;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_cols<T, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
+    if ((e = cudaFuncSetAttribute(k_cols<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
+    if ((e = cudaFuncSetAttribute(k_rows_r2c<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
+    if ((e = cudaFuncSetAttribute(k_rows_c2r<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
+    if ((e = cudaFuncSetAttribute(k_rows_nonlin<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
+    if ((e = cudaFuncSetAttribute(k_zprop<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
+    (void)c;
+    return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t cols_T(const pfc_ctx* c, int axis, int dir, const void* in, void* out, double scale) {
+    const AxisPlan& ap = axis == 1 ? c->py : c->pz;
+    const int n = ap.plan.n;
+    if (n == 1 && in == out && scale == 1.0) return cudaSuccess;
+    int64_t es, os;
+    int no;
+    if (axis == 1) { es = c->nxh; os = (int64_t)c->ny * c->nxh; no = c->nz; }
+    else { es = (int64_t)c->ny * c->nxh; os = c->nxh; no = c->ny; }
+    dim3 grid((c->nxh + ap.tile - 1) / ap.tile, no);
+    const cx<T>* tw = reinterpret_cast<const cx<T>*>(c->tw);
+    if (dir < 0)
+        k_cols<T, -1><<<grid, 256, ap.smem, c->stream>>>((const cx<T>*)in, (cx<T>*)out, c->nxh, es, os, ap.plan, tw,
+                                                           ap.tile, (T)scale);
+    else
+        k_cols<T, 1><<<grid, 256, ap.smem, c->stream>>>((const cx<T>*)in, (cx<T>*)out, c->nxh, es, os, ap.plan, tw,
+                                                          ap.tile, (T)scale);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t set_fft_attributes(const pfc_ctx* c) {
+    return c->dtype == PFC_F64 ? set_attrs_T<double>(c) : set_attrs_T<float>(c);
+}
+
+cudaError_t launch_cols(const pfc_ctx* c, int axis, int dir, const void* in, void* out, double scale) {
+    return c->dtype == PFC_F64 ? cols_T<double>(c, axis, dir, in, out, scale)
+                               : cols_T<float>(c, axis, dir, in, out, scale);
+}
+
+cudaError_t launch_rows_r2c(const pfc_ctx* c, const void* in, void* out) {
+    const int nrows = c->ny * c->nz;
+    dim3 grid((nrows + c->px.tile - 1) / c->px.tile);
+    if (c->dtype == PFC_F64) {
+        const cx<double>* tw = (const cx<double>*)c->tw;
+        k_rows_r2c<double><<<grid, 256, c->px.smem, c->stream>>>((const double*)in, (cx<double>*)out, nrows, c->nx,
+                                                                  c->px.plan, tw, tw + c->post_off, c->px.tile);
+    } else {
+        const cx<float>* tw = (const cx<float>*)c->tw;
+        k_rows_r2c<float><<<grid, 256, c->px.smem, c->stream>>>((const float*)in, (cx<float>*)out, nrows, c->nx,
+                                                                 c->px.plan, tw, tw + c->post_off, c->px.tile);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rows_c2r(const pfc_ctx* c, const void* in, void* out) {
+    const int nrows = c->ny * c->nz;
+    dim3 grid((nrows + c->px.tile - 1) / c->px.tile);
+    if (c->dtype == PFC_F64) {
+        const cx<double>* tw = (const cx<double>*)c->tw;
+        k_rows_c2r<double><<<grid, 256, c->px.smem, c->stream>>>((const cx<double>*)in, (double*)out, nrows, c->nx,
+                                                                  c->px.plan, tw, tw + c->post_off, c->px.tile);
+    } else {
+        const cx<float>* tw = (const cx<float>*)c->tw;
+        k_rows_c2r<float><<<grid, 256, c->px.smem, c->stream>>>((const cx<float>*)in, (float*)out, nrows, c->nx,
+                                                                 c->px.plan, tw, tw + c->post_off, c->px.tile);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rows_nonlin(const pfc_ctx* c, void* buf, const void* pot, double mul, double C, double mu) {
+    const int nrows = c->ny * c->nz;
+    dim3 grid((nrows + c->px.tile - 1) / c->px.tile);
+    if (c->dtype == PFC_F64) {
+        const cx<double>* tw = (const cx<double>*)c->tw;
+        k_rows_nonlin<double><<<grid, 256, c->px.smem, c->stream>>>((cx<double>*)buf, (const double*)pot, nrows,
+                                                                     c->nx, c->px.plan, tw, tw + c->post_off,
+                                                                     c->px.tile, mul, C, mu);
+    } else {
+        const cx<float>* tw = (const cx<float>*)c->tw;
+        k_rows_nonlin<float><<<grid, 256, c->px.smem, c->stream>>>((cx<float>*)buf, (const float*)pot, nrows, c->nx,
+                                                                    c->px.plan, tw, tw + c->post_off, c->px.tile,
+                                                                    (float)mul, (float)C, (float)mu);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_zprop(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a) {
+    dim3 grid((c->nxh + c->pzprop.tile - 1) / c->pzprop.tile, c->ny);
+    if (c->dtype == PFC_F64) {
+        ZArgsT<double> t{a.dt, a.eps, a.C, a.namp_eff, a.lx, a.ly, a.lz, a.seed, a.counter, a.use_noise, a.final_step};
+        k_zprop<double><<<grid, 256, c->pzprop.smem, c->stream>>>((cx<double>*)A, (const cx<double>*)B, c->nx, c->ny,
+                                                                   c->nz, c->pz.plan, (const cx<double>*)c->tw,
+                                                                   c->pzprop.tile, t, c->k0, c->flag);
+    } else {
+        ZArgsT<float> t{(float)a.dt, (float)a.eps, (float)a.C, (float)a.namp_eff, (float)a.lx, (float)a.ly,
+                        (float)a.lz, a.seed, a.counter, a.use_noise, a.final_step};
+        k_zprop<float><<<grid, 256, c->pzprop.smem, c->stream>>>((cx<float>*)A, (const cx<float>*)B, c->nx, c->ny,
+                                                                  c->nz, c->pz.plan, (const cx<float>*)c->tw,
+                                                                  c->pzprop.tile, t, c->k0, c->flag);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace pfc

@@ -1,0 +1,123 @@
+// Local-maximum peak finding (cuda/kernels/findpeaks.hpp:7-29, findpeaks_2d.hpp:7-27).
+// A cell is a peak when it is strictly greater than all 26 (3D) or 8 (2D) periodic
+// neighbours and >= ths.  Deterministic compaction: pass 1 counts peaks per block of
+// kPeakBlock consecutive cells (__syncthreads_count), one block scans the counts,
+// pass 2 writes each peak at block offset + warp-ballot rank.  Blocks cover linear
+// index ranges in order, so the output is sorted by linear index.
+#include "pfc_ctx.h"
+
+namespace pfc {
+namespace {
+
+template <typename T> struct MaxRec;
+template <> struct MaxRec<float> { float i0, i1, i2; float field; };
+template <> struct MaxRec<double> { double i0, i1, i2; float field; };
+static_assert(sizeof(MaxRec<float>) == 16, "Maximum<float> layout");
+static_assert(sizeof(MaxRec<double>) == 32, "Maximum<double> layout");
+
+__device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+template <typename T>
+__device__ __forceinline__ bool peak_at(const T* __restrict__ psi, int64_t idx, int nx, int ny, int nz, bool d3,
+                                        T ths) {
+    const int i0 = (int)(idx % nx);
+    const int64_t r = idx / nx;
+    const int i1 = (int)(r % ny), i2 = (int)(r / ny);
+    const T v = psi[idx];
+    bool ok = true;
+    const int zlo = d3 ? -1 : 0, zhi = d3 ? 1 : 0;
+    for (int dz = zlo; dz <= zhi; ++dz) {
+        const int j2 = d3 ? wrapi(i2 + dz, nz) : i2;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int j1 = wrapi(i1 + dy, ny);
+            const int64_t rowb = ((int64_t)j2 * ny + j1) * nx;
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (dx == 0 && dy == 0 && dz == 0) continue;
+                ok &= (v > psi[rowb + wrapi(i0 + dx, nx)]);
+            }
+        }
+    }
+    return ok && (v >= ths);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kPeakBlock) k_peaks_count(const T* __restrict__ psi, int nx, int ny, int nz, int d3,
+                                                            T ths, int* __restrict__ counts) {
+    const int64_t n = (int64_t)nx * ny * nz;
+    const int64_t idx = (int64_t)blockIdx.x * kPeakBlock + threadIdx.x;
+    const bool f = idx < n && peak_at<T>(psi, idx, nx, ny, nz, d3 != 0, ths);
+    const int c = __syncthreads_count(f);
+    if (threadIdx.x == 0) counts[blockIdx.x] = c;
+}
+
+// Exclusive scan of nb counts by one block of 1024 threads; offsets[nb] = total.
+__global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ counts, int nb, int* __restrict__ offsets) {
+    __shared__ int part[1024];
+    const int chunk = (nb + 1023) / 1024;
+    const int b = threadIdx.x * chunk;
+    const int e = min(nb, b + chunk);
+    int s = 0;
+    for (int i = b; i < e; ++i) s += counts[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const int v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int run = part[threadIdx.x] - s;
+    for (int i = b; i < e; ++i) { offsets[i] = run; run += counts[i]; }
+    if (threadIdx.x == 1023) offsets[nb] = part[1023];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kPeakBlock) k_peaks_write(const T* __restrict__ psi, int nx, int ny, int nz, int d3,
+                                                            T ths, const int* __restrict__ offsets,
+                                                            MaxRec<T>* __restrict__ out, int capacity) {
+    __shared__ int wsum[kPeakBlock / 32];
+    const int64_t n = (int64_t)nx * ny * nz;
+    const int64_t idx = (int64_t)blockIdx.x * kPeakBlock + threadIdx.x;
+    const bool f = idx < n && peak_at<T>(psi, idx, nx, ny, nz, d3 != 0, ths);
+    const unsigned m = __ballot_sync(0xffffffffu, f);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) wsum[warp] = __popc(m);
+    __syncthreads();
+    if (!f) return;
+    int pos = offsets[blockIdx.x] + __popc(m & ((1u << lane) - 1u));
+    for (int w = 0; w < warp; ++w) pos += wsum[w];
+    if (pos >= capacity) return;
+    const int i0 = (int)(idx % nx);
+    const int64_t r = idx / nx;
+    MaxRec<T> rec;
+    rec.i0 = (T)i0;
+    rec.i1 = (T)(int)(r % ny);
+    rec.i2 = (T)(int)(r / ny);
+    rec.field = (float)psi[idx];
+    out[pos] = rec;
+}
+
+template <typename T>
+cudaError_t peaks_T(const pfc_ctx* c, const void* psi, double ths, void* out, int capacity) {
+    const int d3 = c->nz > 1 ? 1 : 0;
+    const int nb = c->n_peak_blocks;
+    k_peaks_count<T><<<nb, kPeakBlock, 0, c->stream>>>((const T*)psi, c->nx, c->ny, c->nz, d3, (T)ths, c->peak_counts);
+    cudaError_t e = cudaGetLastError();
+    if (e) return e;
+    k_scan<<<1, 1024, 0, c->stream>>>(c->peak_counts, nb, c->peak_offsets);
+    if ((e = cudaGetLastError())) return e;
+    if (capacity > 0 && out) {
+        k_peaks_write<T><<<nb, kPeakBlock, 0, c->stream>>>((const T*)psi, c->nx, c->ny, c->nz, d3, (T)ths,
+                                                           c->peak_offsets, (MaxRec<T>*)out, capacity);
+        if ((e = cudaGetLastError())) return e;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t launch_findpeaks(const pfc_ctx* c, const void* psi, double ths, void* out, int capacity) {
+    return c->dtype == PFC_F64 ? peaks_T<double>(c, psi, ths, out, capacity) : peaks_T<float>(c, psi, ths, out, capacity);
+}
+
+}  // namespace pfc

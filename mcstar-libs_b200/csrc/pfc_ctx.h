@@ -1,0 +1,113 @@
+// The context behind the C ABI and the host launchers of every kernel family.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <utility>
+#include <vector>
+#include "pfc_internal.cuh"
+#include "../../include/pfc_b200.h"
+
+namespace pfc {
+
+// Bytes of dynamic shared memory any general kernel may ask for (B200: 227 KB per CTA).
+constexpr size_t kMaxDynSmem = 200 * 1024;
+constexpr int kRedBlocks = 1184;        // 8 x 148 SMs: fixed grid of the FP64 reductions
+constexpr int kPeakBlock = 256;         // cells per block of the peak finder
+constexpr int kBondMaxNbr = 64;         // neighbour cap per atom of the bond-order kernels
+
+struct AxisPlan {
+    LinePlan plan;
+    int tile;          // lines per CTA (columns) or rows per CTA (x axis)
+    size_t smem;       // dynamic shared memory of the kernel using this plan
+};
+
+}  // namespace pfc
+
+struct pfc_ctx {
+    int nx, ny, nz, nxh;
+    int dtype;
+    size_t fsize;                 // sizeof(F)
+    size_t n_real, n_cmpl;        // element counts
+    size_t state_bytes;           // n_cmpl * 2 * fsize
+    cudaStream_t stream;
+    std::string err;
+
+    pfc::AxisPlan px;             // x: complex length nx/2 (even nx) or nx (odd nx)
+    pfc::AxisPlan py, pz;         // y, z: complex length ny, nz
+    pfc::AxisPlan pzprop;         // the stepper's z pass (two fields per tile)
+    pfc::AxisPlan pxnl;           // the stepper's fused x pass
+    int post_off;                 // twiddle offset of W_nx^k, k = 0..nx/2 (even nx)
+    void* tw;                     // device twiddles, cx<F>
+    void* work;                   // state_bytes: C2R scratch and the stepper's second field
+    void* work2;                  // state_bytes: free-energy real field
+    double* red;                  // kRedBlocks partial sums + 4 results
+    double2* k0;                  // FP64 k = 0 mode carried by the stepper
+    int* flag;                    // device status word of the stepper (non-finite watchdog)
+    int* peak_counts;             // per-block peak counts (kPeakBlock cells per block)
+    int* peak_offsets;            // exclusive scan of peak_counts (+ total)
+    int n_peak_blocks;
+    // bond order
+    int max_atoms;
+    void* bond_scratch;
+    size_t bond_scratch_bytes;
+    // fused plane kernels available for this shape
+    int fused_xy;                 // 0: general passes; otherwise the plane kernel variant id
+    // tracing (pfc_profile_enable / pfc_profile_read)
+    bool prof_on = false;
+    long long launches = 0;
+    long long prof_calls[PFC_PROFILE_FAMILIES] = {0, 0, 0};
+    double prof_ms[PFC_PROFILE_FAMILIES] = {0.0, 0.0, 0.0};
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<std::pair<int, size_t>> ev_pending;   // (family, index of the start event)
+};
+
+namespace pfc {
+
+// ---- general FFT passes (kern_fft.cu) ----
+cudaError_t set_fft_attributes(const pfc_ctx* c);
+// complex FFT along y or z of a half-spectrum-shaped buffer (in may equal out)
+cudaError_t launch_cols(const pfc_ctx* c, int axis, int dir, const void* in, void* out, double scale);
+cudaError_t launch_rows_r2c(const pfc_ctx* c, const void* in_real, void* out_cmpl);
+cudaError_t launch_rows_c2r(const pfc_ctx* c, const void* in_cmpl, void* out_real);
+cudaError_t launch_rows_nonlin(const pfc_ctx* c, void* buf, const void* pot, double mul, double C, double mu);
+struct ZPropArgs {
+    double dt, eps, C, namp_eff, lx, ly, lz;
+    uint64_t seed, counter;
+    int use_noise;
+    int final_step;
+};
+cudaError_t launch_zprop(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a);
+
+// ---- pointwise kernels, noise and reductions (kern_point.cu) ----
+cudaError_t launch_update_eom(const pfc_ctx* c, void* kpsi, const void* knl, const void* knoise,
+                              double namp, double dt, double eps, double lx, double ly, double lz,
+                              int with_fen, double C);
+cudaError_t launch_psi3(const pfc_ctx* c, void* arr, const void* pot, double mu, int norm, double C);
+cudaError_t launch_norm(const pfc_ctx* c, void* arr);
+cudaError_t launch_calc_fen(const pfc_ctx* c, const void* psi, void* lpsi, double scale);
+cudaError_t launch_fen_spectral(const pfc_ctx* c, const void* kpsi, double eps, double lx, double ly, double lz);
+cudaError_t launch_quartic_sum(const pfc_ctx* c, const void* psi_unnorm, double mul);
+cudaError_t launch_noise_kspace(const pfc_ctx* c, void* arr, uint64_t seed, uint64_t counter);
+cudaError_t launch_noise_real(const pfc_ctx* c, void* arr, double sigma, uint64_t seed, uint64_t counter);
+cudaError_t launch_k0_save(const pfc_ctx* c, const void* kpsi);
+// reduce the kRedBlocks partials in c->red into c->red[kRedBlocks + slot]
+cudaError_t launch_reduce_final(const pfc_ctx* c, int slot, double scale);
+
+// ---- peaks (kern_peaks.cu) ----
+cudaError_t launch_findpeaks(const pfc_ctx* c, const void* psi, double ths, void* out, int capacity);
+
+// ---- bond order (kern_bond.cu) ----
+size_t bond_scratch_bytes(int max_atoms);
+cudaError_t launch_bond_order(pfc_ctx* c, const void* maxima, int n, double h0, double h1, double h2,
+                              double ths, double boxsize, double rlim, double* out_rows, int row_capacity,
+                              int* n_rows_host, int* overflow_host);
+
+// ---- fused plane kernels (kern_fused.cu) ----
+int fused_xy_variant(int nx, int ny, int dtype);
+cudaError_t set_fused_attributes(const pfc_ctx* c);
+cudaError_t launch_fused_xy(const pfc_ctx* c, const void* A, void* B, const void* pot, double mul, double C,
+                            double mu);
+
+}  // namespace pfc

@@ -1,0 +1,242 @@
+// Internal building blocks of libpfc_b200: complex helpers, small-radix DFTs, the
+// shared-memory Stockham line FFT used by the general-size kernels, the wavenumber
+// of the reference, Philox4x32-10 and the noise draw.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+
+namespace pfc {
+
+template <typename T> struct CxOf;
+template <> struct CxOf<float> { using type = float2; };
+template <> struct CxOf<double> { using type = double2; };
+template <typename T> using cx = typename CxOf<T>::type;
+
+template <typename T> __host__ __device__ __forceinline__ cx<T> mkc(T a, T b) { cx<T> r; r.x = a; r.y = b; return r; }
+__host__ __device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 operator*(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 operator-(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 operator*(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+
+template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b) {
+    C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+template <typename C> __host__ __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
+// DIR * i * a  (DIR = -1 forward transform, +1 inverse)
+template <int DIR, typename C> __host__ __device__ __forceinline__ C rot(C a) {
+    C r;
+    if (DIR > 0) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; }
+    return r;
+}
+
+// ---------------------------------------------------------------------------------
+// small DFTs, X[k] = sum_n x[n] exp(DIR 2 pi i n k / R), in place, natural order.
+// Constants are the exact values of cos/sin at multiples of 2 pi / R.
+// ---------------------------------------------------------------------------------
+template <typename T, int DIR, int R> struct Dft;
+
+template <typename T, int DIR> struct Dft<T, DIR, 2> {
+    __device__ __forceinline__ static void run(cx<T>* v) {
+        cx<T> a = v[0], b = v[1]; v[0] = a + b; v[1] = a - b;
+    }
+};
+template <typename T, int DIR> struct Dft<T, DIR, 4> {
+    __device__ __forceinline__ static void run(cx<T>* v) {
+        cx<T> s02 = v[0] + v[2], d02 = v[0] - v[2], s13 = v[1] + v[3], d13 = rot<DIR>(v[1] - v[3]);
+        v[0] = s02 + s13; v[2] = s02 - s13; v[1] = d02 + d13; v[3] = d02 - d13;
+    }
+};
+template <typename T, int DIR> struct Dft<T, DIR, 8> {
+    __device__ __forceinline__ static void run(cx<T>* v) {
+        const T h = T(0.70710678118654752440);
+        cx<T> e[4] = {v[0], v[2], v[4], v[6]};
+        cx<T> o[4] = {v[1], v[3], v[5], v[7]};
+        Dft<T, DIR, 4>::run(e);
+        Dft<T, DIR, 4>::run(o);
+        // W8^1 = h (1 + DIR i), W8^2 = DIR i, W8^3 = h (-1 + DIR i)
+        cx<T> o1 = mkc<T>(h * (o[1].x - T(DIR) * o[1].y), h * (o[1].y + T(DIR) * o[1].x));
+        cx<T> o2 = rot<DIR>(o[2]);
+        cx<T> o3 = mkc<T>(h * (-o[3].x - T(DIR) * o[3].y), h * (-o[3].y + T(DIR) * o[3].x));
+        v[0] = e[0] + o[0]; v[4] = e[0] - o[0];
+        v[1] = e[1] + o1;   v[5] = e[1] - o1;
+        v[2] = e[2] + o2;   v[6] = e[2] - o2;
+        v[3] = e[3] + o3;   v[7] = e[3] - o3;
+    }
+};
+template <typename T, int DIR> struct Dft<T, DIR, 3> {
+    __device__ __forceinline__ static void run(cx<T>* v) {
+        const T s3 = T(0.86602540378443864676);
+        cx<T> t1 = v[1] + v[2];
+        cx<T> t2 = v[0] - t1 * T(0.5);
+        cx<T> t3 = rot<DIR>(v[1] - v[2]) * s3;
+        v[0] = v[0] + t1; v[1] = t2 + t3; v[2] = t2 - t3;
+    }
+};
+template <typename T, int DIR> struct Dft<T, DIR, 5> {
+    __device__ __forceinline__ static void run(cx<T>* v) {
+        const T c1 = T(0.30901699437494742410), c2 = T(-0.80901699437494742410);
+        const T s1 = T(0.95105651629515357212), s2 = T(0.58778525229247312917);
+        cx<T> a14 = v[1] + v[4], d14 = v[1] - v[4], a23 = v[2] + v[3], d23 = v[2] - v[3];
+        cx<T> A1 = v[0] + a14 * c1 + a23 * c2;
+        cx<T> A2 = v[0] + a14 * c2 + a23 * c1;
+        cx<T> B1 = rot<DIR>(d14 * s1 + d23 * s2);
+        cx<T> B2 = rot<DIR>(d14 * s2 - d23 * s1);
+        v[0] = v[0] + a14 + a23;
+        v[1] = A1 + B1; v[4] = A1 - B1; v[2] = A2 + B2; v[3] = A2 - B2;
+    }
+};
+
+// ---------------------------------------------------------------------------------
+// Stockham autosort FFT over lines held in shared memory (general 2^a 3^b 5^c).
+// Stage s has radix R_s and span Ns = R_0 ... R_{s-1}: butterfly j reads
+// x[j + r n/R], applies exp(DIR 2 pi i r (j mod Ns) / (Ns R)), runs the R-point DFT
+// and writes to (j - j mod Ns) R + j mod Ns + r Ns.  Twiddles are precomputed on
+// the host in FP64 (forward sign; the inverse uses their conjugates).
+// ---------------------------------------------------------------------------------
+constexpr int kMaxStages = 16;
+struct LinePlan {
+    int n;
+    int nst;
+    int radix[kMaxStages];
+    int ns[kMaxStages];
+    int twoff[kMaxStages];
+};
+
+template <typename T, int DIR, int R>
+__device__ __forceinline__ void stockham_bfly(const cx<T>* __restrict__ sl, cx<T>* __restrict__ dl,
+                                              int j, int m, int Ns, const cx<T>* __restrict__ tws) {
+    cx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = sl[j + r * m];
+    const int jj = j % Ns;
+    if (Ns > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+            cx<T> w = tws[jj * (R - 1) + r - 1];
+            if (DIR > 0) w.y = -w.y;
+            v[r] = cmul(v[r], w);
+        }
+    }
+    Dft<T, DIR, R>::run(v);
+    const int od = (j - jj) * R + jj;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dl[od + r * Ns] = v[r];
+}
+
+// FFT of nlines lines, line l at a[l*ld .. l*ld+n).  Ping-pongs between a and b and
+// returns the buffer holding the result.  All threads of the block must call it.
+template <typename T, int DIR>
+__device__ cx<T>* stockham_lines(cx<T>* a, cx<T>* b, int nlines, int ld, const LinePlan& p,
+                                 const cx<T>* __restrict__ tw) {
+    cx<T>* src = a;
+    cx<T>* dst = b;
+    for (int s = 0; s < p.nst; ++s) {
+        const int R = p.radix[s], Ns = p.ns[s], m = p.n / R;
+        const cx<T>* tws = tw + p.twoff[s];
+        const int total = nlines * m;
+        for (int e = threadIdx.x; e < total; e += blockDim.x) {
+            const int line = e / m, j = e - line * m;
+            const cx<T>* sl = src + (size_t)line * ld;
+            cx<T>* dl = dst + (size_t)line * ld;
+            switch (R) {
+                case 8: stockham_bfly<T, DIR, 8>(sl, dl, j, m, Ns, tws); break;
+                case 4: stockham_bfly<T, DIR, 4>(sl, dl, j, m, Ns, tws); break;
+                case 2: stockham_bfly<T, DIR, 2>(sl, dl, j, m, Ns, tws); break;
+                case 3: stockham_bfly<T, DIR, 3>(sl, dl, j, m, Ns, tws); break;
+                default: stockham_bfly<T, DIR, 5>(sl, dl, j, m, Ns, tws); break;
+            }
+        }
+        __syncthreads();
+        cx<T>* t = src; src = dst; dst = t;
+    }
+    return src;
+}
+
+// ---------------------------------------------------------------------------------
+// The reference's wavenumber, K(i, n, len) = (i < n/2+1 ? i : i-n) * 2pi / len
+// (cuda/kernels/common.hpp:27-28), evaluated in the field's precision.
+// ---------------------------------------------------------------------------------
+template <typename T> __device__ __forceinline__ T kwave(int i, int n, T len) {
+    return T(i < n / 2 + 1 ? i : i - n) * T(6.283185307179586232) / len;
+}
+
+// ---------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as
+// 1, 2, 3", SC'11): 10 rounds of two 32x32->64 multiplies with Weyl key bumps.
+// ---------------------------------------------------------------------------------
+struct U4 { uint32_t x, y, z, w; };
+__host__ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+        U4 n;
+        n.x = (uint32_t)(p1 >> 32) ^ c.y ^ k0;
+        n.y = (uint32_t)p1;
+        n.z = (uint32_t)(p0 >> 32) ^ c.w ^ k1;
+        n.w = (uint32_t)p0;
+        c = n;
+    }
+    return c;
+}
+
+constexpr uint32_t kKspaceDomain = 0x0u;
+constexpr uint32_t kRealDomain = 0x52454131u;
+
+// Two standard normals from counter (idx, counter) under key (seed, domain),
+// Box-Muller on uniforms strictly inside (0, 1) that are exact in T.
+template <typename T> __device__ __forceinline__ void philox_normal2(uint64_t idx, uint64_t seed, uint64_t counter,
+                                                                     uint32_t domain, T& g1, T& g2);
+template <> __device__ __forceinline__ void philox_normal2<float>(uint64_t idx, uint64_t seed, uint64_t counter,
+                                                                  uint32_t domain, float& g1, float& g2) {
+    U4 c{(uint32_t)idx, (uint32_t)(idx >> 32), (uint32_t)counter, (uint32_t)(counter >> 32)};
+    U4 r = philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32) ^ domain);
+    const float u1 = (float)((r.x >> 9) * 2u + 1u) * 5.9604644775390625e-08f;  // 2^-24
+    const float u2 = (float)((r.y >> 9) * 2u + 1u) * 5.9604644775390625e-08f;
+    const float rad = sqrtf(-2.0f * logf(u1));
+    float s, co;
+    sincospif(2.0f * u2, &s, &co);
+    g1 = rad * co; g2 = rad * s;
+}
+template <> __device__ __forceinline__ void philox_normal2<double>(uint64_t idx, uint64_t seed, uint64_t counter,
+                                                                   uint32_t domain, double& g1, double& g2) {
+    U4 c{(uint32_t)idx, (uint32_t)(idx >> 32), (uint32_t)counter, (uint32_t)(counter >> 32)};
+    U4 r = philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32) ^ domain);
+    const uint64_t a = ((((uint64_t)r.x << 32) | r.y) >> 12) * 2u + 1u;
+    const uint64_t b = ((((uint64_t)r.z << 32) | r.w) >> 12) * 2u + 1u;
+    const double u1 = (double)a * 1.1102230246251565404e-16;  // 2^-53
+    const double u2 = (double)b * 1.1102230246251565404e-16;
+    const double rad = sqrt(-2.0 * log(u1));
+    double s, co;
+    sincospi(2.0 * u2, &s, &co);
+    g1 = rad * co; g2 = rad * s;
+}
+
+// k-space noise of half-spectrum mode (i0, i1, i2): modes on the i0 = 0 and
+// i0 = nx/2 planes are keyed by the canonical (lower linear index) member of their
+// +-k pair and conjugated on the other member; self-conjugate modes are real.
+template <typename T>
+__device__ __forceinline__ cx<T> kspace_noise(int i0, int i1, int i2, int nx, int ny, int nz,
+                                              uint64_t seed, uint64_t counter) {
+    const int nxh = nx / 2 + 1;
+    const int64_t lin = ((int64_t)i2 * ny + i1) * nxh + i0;
+    int64_t canon = lin;
+    bool conj = false, selfc = false;
+    if (i0 == 0 || ((nx & 1) == 0 && i0 == nx / 2)) {
+        const int j1 = i1 == 0 ? 0 : ny - i1;
+        const int j2 = i2 == 0 ? 0 : nz - i2;
+        const int64_t part = ((int64_t)j2 * ny + j1) * nxh + i0;
+        if (part < lin) { canon = part; conj = true; }
+        selfc = (part == lin);
+    }
+    T g1, g2;
+    philox_normal2<T>((uint64_t)canon, seed, counter, kKspaceDomain, g1, g2);
+    const T s = T(0.70710678118654752440);
+    if (selfc) return mkc<T>(g1, T(0));
+    return mkc<T>(g1 * s, conj ? -g2 * s : g2 * s);
+}
+
+}  // namespace pfc

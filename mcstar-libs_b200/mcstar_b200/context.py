@@ -1,0 +1,174 @@
+"""Python face of one pfc_ctx: shape, precision, stream, and thin methods over the C ABI.
+
+Field buffers are torch CUDA tensors owned by the caller (flat, in the reference's
+complex-sized allocation, see ``array.GPUArray``); methods pass their device pointers
+and the current torch stream to the library.  Results that live on the host (sums,
+counts) come back as Python numbers.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import PfcDesc, PfcStepParams, check, lib
+
+_NP = {np.dtype(np.float32): _lib.PFC_F32, np.dtype(np.float64): _lib.PFC_F64}
+_TORCH = {_lib.PFC_F32: torch.float32, _lib.PFC_F64: torch.float64}
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("device tensor expected")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Context:
+    """One context per (shape, precision); owns the library's workspaces."""
+
+    def __init__(self, shape, dtype=np.float32):
+        nx, ny, nz = (int(v) for v in shape)
+        self.shape = (nx, ny, nz)
+        self.np_dtype = np.dtype(dtype)
+        if self.np_dtype not in _NP:
+            raise ValueError("dtype must be float32 or float64")
+        self.code = _NP[self.np_dtype]
+        self.torch_dtype = _TORCH[self.code]
+        if not torch.cuda.is_available():
+            raise RuntimeError("the pfc_b200 kernels need a CUDA device (B200, sm_100a)")
+        torch.cuda.init()
+        h = ctypes.c_void_p()
+        check(lib().pfc_create(ctypes.byref(PfcDesc(nx, ny, nz, self.code)), ctypes.byref(h)), None,
+              f"pfc_create{self.shape}")
+        self._h = h
+        self.nxh = nx // 2 + 1
+        self.n_real = nx * ny * nz
+        self.n_cmpl = self.nxh * ny * nz
+        self.state_bytes = int(lib().pfc_state_bytes(h))
+
+    # -- plumbing ---------------------------------------------------------------------
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pfc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _sync_stream(self):
+        s = torch.cuda.current_stream().cuda_stream
+        lib().pfc_set_stream(self._h, ctypes.c_void_p(s))
+
+    def _call(self, name, *args):
+        self._sync_stream()
+        check(getattr(lib(), name)(self._h, *args), self._h, name)
+
+    def empty_state(self):
+        """A device buffer of the reference's complex-sized allocation (2*n_cmpl F)."""
+        return torch.empty(2 * self.n_cmpl, dtype=self.torch_dtype, device="cuda")
+
+    # -- FFT ----------------------------------------------------------------------------
+    def r2c(self, real_in, cmpl_out):
+        self._call("pfc_fft_r2c", _ptr(real_in), _ptr(cmpl_out))
+
+    def c2r(self, cmpl_in, real_out):
+        self._call("pfc_fft_c2r", _ptr(cmpl_in), _ptr(real_out))
+
+    # -- pointwise ----------------------------------------------------------------------
+    def update_eom(self, kpsi, knl, knoise, namp, dt, eps, lens):
+        self._call("pfc_update_eom", _ptr(kpsi), _ptr(knl), _ptr(knoise), float(namp), float(dt), float(eps),
+                   *(float(v) for v in lens))
+
+    def update_eom_with_fen(self, kpsi, knl, knoise, namp, dt, eps, lens):
+        self._call("pfc_update_eom_with_fen", _ptr(kpsi), _ptr(knl), _ptr(knoise), float(namp), float(dt),
+                   float(eps), *(float(v) for v in lens))
+
+    def psi3_split(self, arr, pot=None, mu=0.0, norm=False):
+        self._call("pfc_psi3_split", _ptr(arr), _ptr(pot), float(mu), int(bool(norm)))
+
+    def norm(self, arr):
+        self._call("pfc_norm", _ptr(arr))
+
+    def calc_fen(self, psi, lpsi, hh):
+        out = ctypes.c_double()
+        self._call("pfc_calc_fen", _ptr(psi), _ptr(lpsi), *(float(v) for v in hh), ctypes.byref(out))
+        return out.value
+
+    def noise_kspace(self, arr, seed, counter):
+        self._call("pfc_noise_fill_kspace", _ptr(arr), ctypes.c_uint64(seed), ctypes.c_uint64(counter))
+
+    def noise_real(self, arr, sigma, seed, counter):
+        self._call("pfc_noise_fill", _ptr(arr), float(sigma), ctypes.c_uint64(seed), ctypes.c_uint64(counter))
+
+    # -- analysis -----------------------------------------------------------------------
+    def findpeaks(self, psi, ths, out=None, capacity=None):
+        """Returns (n_found, records) where records is a device uint8 tensor of
+        Maximum<F> structs (16 B for float, 32 B for double), sorted by linear index."""
+        rec = 16 if self.code == _lib.PFC_F32 else 32
+        if out is None:
+            capacity = max(1, self.n_real // 8) if capacity is None else capacity
+            out = torch.empty(capacity * rec, dtype=torch.uint8, device="cuda")
+        else:
+            capacity = out.numel() // rec if capacity is None else capacity
+        n = ctypes.c_int()
+        self._call("pfc_findpeaks", _ptr(psi), float(ths), _ptr(out), int(capacity), ctypes.byref(n))
+        return n.value, out[: n.value * rec]
+
+    def bond_order(self, maxima, n, h, ths, boxsize, rlim, capacity=None):
+        capacity = max(1, n) if capacity is None else capacity
+        rows = torch.empty(capacity * _lib.PFC_BOND_NCOL, dtype=torch.float64, device="cuda")
+        nr = ctypes.c_int()
+        self._call("pfc_bond_order", _ptr(maxima), int(n), *(float(v) for v in h), float(ths), float(boxsize),
+                   float(rlim), _ptr(rows), int(capacity), ctypes.byref(nr))
+        return rows[: nr.value * _lib.PFC_BOND_NCOL].view(nr.value, _lib.PFC_BOND_NCOL)
+
+    # -- stepper ------------------------------------------------------------------------
+    def step(self, kpsi, nsteps, dt, eps, lens, mu=0.0, C=1.0, namp=0.0, seed=0, counter=0):
+        p = PfcStepParams(float(dt), float(eps), float(mu), float(C), float(namp), float(lens[0]),
+                          float(lens[1]), float(lens[2]), int(seed), int(counter))
+        self._call("pfc_step", _ptr(kpsi), int(nsteps), ctypes.byref(p))
+
+    def profile_enable(self, on=True):
+        check(lib().pfc_profile_enable(self._h, int(bool(on))), self._h, "pfc_profile_enable")
+
+    def profile_read(self):
+        """{"launches": n, "calls": [3], "ms": [3]} since profile_enable (families:
+        0 entry/exit, 1 xy part of a step, 2 z pass)."""
+        self._sync_stream()
+        p = _lib.PfcProfile()
+        check(lib().pfc_profile_read(self._h, ctypes.byref(p)), self._h, "pfc_profile_read")
+        return {"launches": int(p.launches), "calls": [int(v) for v in p.calls], "ms": [float(v) for v in p.ms],
+                "xy_variant": int(p.xy_variant)}
+
+    def free_energy(self, kpsi, eps, lens, hh):
+        out = ctypes.c_double()
+        self._call("pfc_free_energy", _ptr(kpsi), float(eps), *(float(v) for v in lens), *(float(v) for v in hh),
+                   ctypes.byref(out))
+        return out.value
+
+
+_cache = threading.local()
+
+
+def get_context(shape, dtype):
+    """Per-thread cache of contexts keyed by (shape, dtype, device)."""
+    d = getattr(_cache, "d", None)
+    if d is None:
+        d = _cache.d = {}
+    key = (tuple(int(v) for v in shape), np.dtype(dtype).str, torch.cuda.current_device())
+    ctx = d.get(key)
+    if ctx is None:
+        ctx = d[key] = Context(shape, dtype)
+    return ctx

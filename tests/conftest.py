@@ -1,0 +1,55 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for p in (ROOT, os.path.join(ROOT, "mcstar-libs_b200"), os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built libpfc_b200.so")
+
+
+def pytest_collection_modifyitems(config, items):
+    import torch
+    if torch.cuda.is_available():
+        return
+    skip = pytest.mark.skip(reason="no CUDA device in this environment")
+    for it in items:
+        if "gpu" in it.keywords:
+            it.add_marker(skip)
+
+
+def ref_lib(dtype):
+    """The reference's own cuFFT path (oracle/_ref), or None when it was not built."""
+    import ctypes
+    import numpy as np
+    name = "libref_pfc_f32.so" if np.dtype(dtype) == np.float32 else "libref_pfc_f64.so"
+    path = os.path.join(REF_DIR, name)
+    if not os.path.exists(path):
+        return None
+    L = ctypes.CDLL(path)
+    pre = "ref32_" if np.dtype(dtype) == np.float32 else "ref64_"
+    P, D, I = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
+    sig = {
+        "create": ([I, I, I, ctypes.c_ulonglong], P), "destroy": ([P], None),
+        "set_kpsi": ([P, P], None), "get_kpsi": ([P, P], None), "r2c": ([P, P, P], None),
+        "c2r": ([P, P, P], None), "step": ([P, I, D, D, D, D, D, D, D, I], None),
+        "time_steps": ([P, I, D, D, D, D, D, D, D, I], ctypes.c_float), "get_psi": ([P, P], None),
+        "free_energy": ([P, D, D, D, D, D, D, D, P], ctypes.c_float),
+        "findpeaks": ([P, D, D, D, D, D, D, D, D, ctypes.c_char_p, ctypes.c_char_p], None),
+        "noise_kspace": ([P, P], None),
+    }
+    fns = {}
+    for k, (a, r) in sig.items():
+        f = getattr(L, pre + k)
+        f.argtypes = a
+        f.restype = r
+        fns[k] = f
+    return fns

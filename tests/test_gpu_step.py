@@ -1,0 +1,136 @@
+"""Parity of the fused conserved stepper (pfc_step through the C ABI) with the oracle
+and with the reference's own cuFFT step (oracle/_ref), plus the known answers derived
+from the reference's mathematics."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import pfc_oracle as O
+from conftest import ref_lib
+
+pytestmark = pytest.mark.gpu
+
+F32, F64 = np.float32, np.float64
+
+
+def stepper(shape, dtype, dx=math.pi / 4, dt=0.5, eps=0.3, namp=0.0, seed=0, C=1.0, mu=0.0):
+    from mcstar_b200 import Stepper
+    return Stepper(shape, dx, dt, eps, dtype=dtype, namp=namp, seed=seed, C=C, mu=mu)
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+CASES = [
+    ((16, 12, 10), F64, 0.0), ((16, 12, 10), F64, 0.05), ((15, 9, 7), F64, 0.0), ((24, 20, 1), F64, 0.0),
+    ((64, 1, 1), F64, 0.0), ((32, 32, 32), F32, 0.0), ((32, 32, 32), F32, 0.02), ((64, 64, 64), F32, 0.0),
+    ((128, 128, 128), F32, 0.0), ((256, 256, 1), F64, 0.0), ((48, 40, 30), F32, 0.0),
+]
+
+
+@pytest.mark.parametrize("shape,dtype,namp", CASES, ids=lambda v: str(v))
+def test_step_matches_oracle(shape, dtype, namp):
+    nx, ny, nz = shape
+    st = stepper(shape, dtype, namp=namp, seed=17)
+    psi = O.r2c(np.full((nz, ny, nx), -0.2) + 0.1 * np.random.default_rng(1).uniform(-1, 1, (nz, ny, nx)))
+    st.set_kspace(psi.astype(np.complex64 if dtype == F32 else np.complex128))
+    nsteps = 6
+    st.step(nsteps)
+    got = st.kspace()
+    want = O.step(psi, nsteps, st.dt, st.eps, st.lens, shape, namp=namp, seed=17, counter0=0)
+    tol = 2e-6 if dtype == F32 else 1e-12
+    assert rel_l2(got, want) < tol
+
+
+def test_step_stabilisation_constant_and_mu():
+    shape = (16, 16, 16)
+    st = stepper(shape, F64, C=0.0, mu=0.07, dt=0.1)
+    rng = np.random.default_rng(4)
+    psi = O.r2c(-0.2 + 0.1 * rng.uniform(-1, 1, (16, 16, 16)))
+    st.set_kspace(psi)
+    st.step(5)
+    want = O.step(psi, 5, 0.1, st.eps, st.lens, shape, mu=0.07, C=0.0)
+    assert rel_l2(st.kspace(), want) < 1e-12
+
+
+def test_k0_mode_bit_invariant_with_noise():
+    shape = (32, 32, 32)
+    st = stepper(shape, F32, namp=0.05, seed=3)
+    rng = np.random.default_rng(2)
+    st.set_real(-0.18 + 0.05 * rng.uniform(-1, 1, (32, 32, 32)))
+    k0 = st.kspace()[0, 0, 0]
+    for _ in range(4):
+        st.step(25)
+        assert st.kspace()[0, 0, 0] == k0
+
+
+def test_uniform_state_fixed_point():
+    shape = (32, 24, 16)
+    st = stepper(shape, F64)
+    st.set_real(np.full((16, 24, 32), -0.25))
+    k = st.kspace()
+    st.step(10)
+    np.testing.assert_allclose(st.kspace(), k, atol=1e-9)
+
+
+def test_resume_is_bit_exact():
+    shape = (32, 32, 32)
+    a = stepper(shape, F32, namp=0.05, seed=9)
+    b = stepper(shape, F32, namp=0.05, seed=9)
+    rng = np.random.default_rng(5)
+    psi = -0.2 + 0.05 * rng.uniform(-1, 1, (32, 32, 32))
+    a.set_real(psi)
+    b.set_real(psi)
+    a.step(10)
+    b.step(4)
+    b.step(6)
+    np.testing.assert_array_equal(a.kspace(), b.kspace())
+
+
+@pytest.mark.parametrize("dtype,shape,nsteps", [(F64, (64, 64, 1), 20), (F64, (16, 16, 16), 20),
+                                                 (F32, (64, 64, 64), 20), (F64, (36, 30, 20), 10)])
+def test_step_vs_reference_cufft(dtype, shape, nsteps):
+    ref = ref_lib(dtype)
+    if ref is None:
+        pytest.skip("oracle/_ref not built")
+    nx, ny, nz = shape
+    dx, dt, eps = math.pi / 4, 0.5, 0.25
+    lens = (nx * dx, ny * dx, nz * dx)
+    rng = np.random.default_rng(11)
+    psi = -0.25 + 0.01 * rng.uniform(-1, 1, (nz, ny, nx))
+    k = O.r2c(psi).astype(np.complex64 if dtype == F32 else np.complex128)
+    h = ref["create"](nx, ny, nz, 1)
+    ref["set_kpsi"](h, k.ctypes.data)
+    ref["step"](h, nsteps, 0.0, dt, eps, *lens, 0.0, 0)
+    want = np.zeros_like(k)
+    ref["get_kpsi"](h, want.ctypes.data)
+    ref["destroy"](h)
+    st = stepper(shape, dtype, dx=dx, dt=dt, eps=eps)
+    st.set_kspace(k)
+    st.step(nsteps)
+    tol = 1e-5 if dtype == F32 else 1e-12
+    assert rel_l2(st.kspace(), want) < tol
+
+
+def test_free_energy_and_peaks_of_stepper_match_reference():
+    ref = ref_lib(F64)
+    if ref is None:
+        pytest.skip("oracle/_ref not built")
+    from mcstar_b200 import bcc_sphere
+    shape = (32, 32, 32)
+    dx = math.pi / 4
+    psi = bcc_sphere(shape, dx, -0.2, 0.2, 9.0)
+    k = O.r2c(psi)
+    h = ref["create"](32, 32, 32, 1)
+    ref["set_kpsi"](h, k.ctypes.data)
+    ref["step"](h, 10, 0.0, 0.5, 0.3, 32 * dx, 32 * dx, 32 * dx, 0.0, 0)
+    f_ref = ref["free_energy"](h, 0.3, 32 * dx, 32 * dx, 32 * dx, dx, dx, dx, None)
+    ref["destroy"](h)
+    st = stepper(shape, F64, dx=dx)
+    st.set_kspace(k)
+    st.step(10)
+    # the reference returns a float summed with float atomics (eom.hpp:126)
+    assert abs(st.free_energy() - f_ref) / abs(f_ref) < 1e-5
