@@ -52,8 +52,9 @@ typedef struct pfc_desc {
 typedef struct pfc_ctx pfc_ctx;
 
 /* Replaces: the implicit set-up of the reference's typedef'd GPUArray/CufftPlan
- * (cuda/array_abstraction.hpp:74-96, cuda/cufft_wrapper.hpp:68-77).  Lengths must
- * factor into 2, 3, 5 (the reference's own restriction, cufft_unittest/main.cu:32-36). */
+ * (cuda/array_abstraction.hpp:74-96, cuda/cufft_wrapper.hpp:68-77).  Every length
+ * must have prime factors <= 31 (PFC_ERR_UNSUPPORTED otherwise); the reference's own
+ * drivers keep to 2, 3, 5 (cufft_unittest/main.cu:32-36, cuda/math.hpp:125-149). */
 pfc_status  pfc_create(const pfc_desc* desc, pfc_ctx** out);
 pfc_status  pfc_destroy(pfc_ctx* ctx);
 pfc_status  pfc_set_stream(pfc_ctx* ctx, void* cuda_stream);

@@ -20,6 +20,12 @@ bool factor_radices(int n, std::vector<int>& rs) {
     while (n % 2 == 0) { rs.push_back(2); n /= 2; }
     while (n % 3 == 0) { rs.push_back(3); n /= 3; }
     while (n % 5 == 0) { rs.push_back(5); n /= 5; }
+    for (int p = 7; p <= kMaxOddRadix; p += 2) {
+        bool prime = true;
+        for (int d = 3; d * d <= p; d += 2) prime = prime && (p % d != 0);
+        if (!prime) continue;
+        while (n % p == 0) { rs.push_back(p); n /= p; }
+    }
     return n == 1 && (int)rs.size() <= kMaxStages;
 }
 
@@ -40,6 +46,12 @@ bool make_plan(int n, LinePlan& p, std::vector<std::complex<double>>& tab) {
             for (int r = 1; r < R; ++r) {
                 const long long num = ((long long)r * jj) % ((long long)Ns * R);
                 const double ang = -2.0 * M_PI * (double)num / (double)(Ns * R);
+                tab.emplace_back(std::cos(ang), std::sin(ang));
+            }
+        p.rtoff[s] = (int)tab.size();
+        if (R > 5)
+            for (int q = 0; q < R; ++q) {
+                const double ang = -2.0 * M_PI * (double)q / (double)R;
                 tab.emplace_back(std::cos(ang), std::sin(ang));
             }
         Ns *= R;
@@ -168,6 +180,45 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
         const double ang = -2.0 * M_PI * (double)k / (double)c->nx;
         tab.emplace_back(std::cos(ang), std::sin(ang));
     }
+    c->fused_xy = fused_xy_variant(c->nx, c->ny, c->dtype);
+    c->plane_tw_off = (int)tab.size();
+    if (c->fused_xy) {
+        const int lens[3] = {c->ny, c->nx / 2, c->nx};
+        const int cnt[3] = {c->ny, c->nx / 2, c->nx / 2 + 1};
+        for (int a = 0; a < 3; ++a)
+            for (int m = 0; m < cnt[a]; ++m) {
+                const double ang = -2.0 * M_PI * (double)m / (double)lens[a];
+                tab.emplace_back(std::cos(ang), std::sin(ang));
+            }
+    }
+    auto roots = [&](int n, int count) {
+        for (int m = 0; m < count; ++m) {
+            const double ang = -2.0 * M_PI * (double)m / (double)n;
+            tab.emplace_back(std::cos(ang), std::sin(ang));
+        }
+    };
+    c->fused_z = fused_z_variant(c->nx, c->nz, c->dtype);
+    c->zcol_tw_off = (int)tab.size();
+    if (c->fused_z) roots(c->nz, c->nz);
+    c->fused_y = fused_y_variant(c->ny, c->dtype);
+    c->fused_x = fused_x_variant(c->nx, c->dtype);
+    if (!(c->fused_y && c->fused_x)) c->fused_y = c->fused_x = 0;
+    c->ypass_tw_off = (int)tab.size();
+    if (c->fused_y) roots(c->ny, c->ny);
+    c->xpass_tw_off = (int)tab.size();
+    if (c->fused_x) {
+        roots(c->nx / 2, c->nx / 2);
+        roots(c->nx, c->nx / 2 + 1);
+    }
+    // xy part of a step: register passes where available, else the cluster plane kernel,
+    // else the general passes; PFC_XY_MODE=0|1|2 overrides (for measurements).
+    c->xy_mode = c->fused_y ? 2 : (c->fused_xy ? 1 : 0);
+    if (const char* m = getenv("PFC_XY_MODE")) {
+        const int w = atoi(m);
+        if ((w == 1 && c->fused_xy) || (w == 2 && c->fused_y) || w == 0) c->xy_mode = w;
+    }
+    c->slab = 0;
+    if (const char* s = getenv("PFC_SLAB")) c->slab = std::max(0, atoi(s));
     // tiles: two ping-pong buffers of `tile` lines per CTA
     c->px.tile = pow2_floor((64 * 1024) / (2 * (size_t)lx * csz), 16);
     c->px.smem = 2 * (size_t)c->px.tile * lx * csz;
@@ -185,7 +236,6 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
     c->n_peak_blocks = (int)((c->n_real + kPeakBlock - 1) / kPeakBlock);
     c->max_atoms = (int)std::max<size_t>(4096, c->n_real / 512);
     c->bond_scratch_bytes = bond_scratch_bytes(c->max_atoms);
-    c->fused_xy = fused_xy_variant(c->nx, c->ny, c->dtype);
 
     cudaError_t e = cudaSuccess;
     auto alloc = [&](void** p, size_t bytes) {
@@ -215,6 +265,8 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
     if (e == cudaSuccess) e = cudaMemset(c->flag, 0, sizeof(int) * 4);
     if (e == cudaSuccess) e = set_fft_attributes(c);
     if (e == cudaSuccess && c->fused_xy) e = set_fused_attributes(c);
+    if (e == cudaSuccess && c->fused_z) e = set_zcol_attributes(c);
+    if (e == cudaSuccess && c->fused_y) e = set_pass_attributes(c);
     if (e != cudaSuccess) {
         free_ctx(c);
         return PFC_ERR_CUDA;
@@ -372,9 +424,28 @@ pfc_status pfc_step(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params*
                  return launch_cols(ctx, 2, 1, A, A, 1.0 / ctx->nz);
              }), "pfc_step entry");
     for (int t = 0; t < nsteps; ++t) {
-        if (ctx->fused_xy) {
+        if (ctx->xy_mode == 1) {
             PFC_CUDA(traced(ctx, 1, 1, [&] { return launch_fused_xy(ctx, A, B, nullptr, mul, p->C, p->mu); }),
                      "pfc_step xy");
+        } else if (ctx->xy_mode == 2) {
+            // y-inverse, x (C2R, cubic, R2C), y-forward; with slabs the intermediate of
+            // each slab of z-planes lives in one reused slab-sized buffer (L2-resident)
+            const int slab = (ctx->slab > 0 && ctx->slab < ctx->nz) ? ctx->slab : ctx->nz;
+            const int nslab = (ctx->nz + slab - 1) / slab;
+            const int64_t pe = (int64_t)ctx->ny * ctx->nxh;  // complex elements per plane
+            PFC_CUDA(traced(ctx, 1, 3 * nslab, [&] {
+                         cudaError_t e = cudaSuccess;
+                         for (int z0 = 0; z0 < ctx->nz && !e; z0 += slab) {
+                             const int nzs = std::min(slab, ctx->nz - z0);
+                             const float2* a = (const float2*)A + z0 * pe;
+                             float2* b = (float2*)B + z0 * pe;
+                             float2* s = slab < ctx->nz ? (float2*)ctx->work2 : b;
+                             if ((e = launch_ypass(ctx, 1, a, s, 1.0, nzs))) break;
+                             if ((e = launch_xpass(ctx, s, nullptr, mul, p->C, p->mu, nzs))) break;
+                             e = launch_ypass(ctx, -1, s, b, 1.0, nzs);
+                         }
+                         return e;
+                     }), "pfc_step xy");
         } else {
             const int n = ctx->ny > 1 ? 3 : 1;
             PFC_CUDA(traced(ctx, 1, n, [&] {
@@ -388,7 +459,10 @@ pfc_status pfc_step(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params*
         }
         za.counter = p->counter + (uint64_t)t;
         za.final_step = (t == nsteps - 1);
-        PFC_CUDA(traced(ctx, 2, 1, [&] { return launch_zprop(ctx, A, B, za); }), "pfc_step z");
+        if (ctx->fused_z)
+            PFC_CUDA(traced(ctx, 2, 1, [&] { return launch_zcol(ctx, A, B, za); }), "pfc_step z");
+        else
+            PFC_CUDA(traced(ctx, 2, 1, [&] { return launch_zprop(ctx, A, B, za); }), "pfc_step z");
     }
     int flag = 0;
     PFC_CUDA(cudaMemcpyAsync(&flag, ctx->flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "pfc_step copy flag");

@@ -190,16 +190,16 @@ struct ZArgsT {
 template <typename T>
 __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict__ B, int nx, int ny, int nz,
                                                LinePlan p, const cx<T>* __restrict__ tw, int tile, ZArgsT<T> a,
-                                               const double2* __restrict__ k0, int* flag) {
+                                               const double2* __restrict__ k0, int* flag, int col0, int col_end) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int bad;
     cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
     const int n = nz;
     cx<T>* b1 = b0 + (size_t)2 * tile * n;
     const int nxh = nx / 2 + 1;
-    const int i0 = blockIdx.x * tile;
+    const int i0 = col0 + blockIdx.x * tile;
     const int ky = blockIdx.y;
-    const int nt = min(tile, nxh - i0);
+    const int nt = min(tile, col_end - i0);
     if (threadIdx.x == 0) bad = 0;
     for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
         const int i = e % tile, k = e / tile;
@@ -343,21 +343,27 @@ cudaError_t launch_rows_nonlin(const pfc_ctx* c, void* buf, const void* pot, dou
     return cudaGetLastError();
 }
 
-cudaError_t launch_zprop(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a) {
-    dim3 grid((c->nxh + c->pzprop.tile - 1) / c->pzprop.tile, c->ny);
+cudaError_t launch_zprop_cols(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int col0, int ncols) {
+    const int tile = c->pzprop.tile;
+    dim3 grid((ncols + tile - 1) / tile, c->ny);
+    const int col_end = col0 + ncols;
     if (c->dtype == PFC_F64) {
         ZArgsT<double> t{a.dt, a.eps, a.C, a.namp_eff, a.lx, a.ly, a.lz, a.seed, a.counter, a.use_noise, a.final_step};
         k_zprop<double><<<grid, 256, c->pzprop.smem, c->stream>>>((cx<double>*)A, (const cx<double>*)B, c->nx, c->ny,
-                                                                   c->nz, c->pz.plan, (const cx<double>*)c->tw,
-                                                                   c->pzprop.tile, t, c->k0, c->flag);
+                                                                   c->nz, c->pz.plan, (const cx<double>*)c->tw, tile,
+                                                                   t, c->k0, c->flag, col0, col_end);
     } else {
         ZArgsT<float> t{(float)a.dt, (float)a.eps, (float)a.C, (float)a.namp_eff, (float)a.lx, (float)a.ly,
                         (float)a.lz, a.seed, a.counter, a.use_noise, a.final_step};
         k_zprop<float><<<grid, 256, c->pzprop.smem, c->stream>>>((cx<float>*)A, (const cx<float>*)B, c->nx, c->ny,
-                                                                  c->nz, c->pz.plan, (const cx<float>*)c->tw,
-                                                                  c->pzprop.tile, t, c->k0, c->flag);
+                                                                  c->nz, c->pz.plan, (const cx<float>*)c->tw, tile, t,
+                                                                  c->k0, c->flag, col0, col_end);
     }
     return cudaGetLastError();
+}
+
+cudaError_t launch_zprop(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a) {
+    return launch_zprop_cols(c, A, B, a, 0, c->nxh);
 }
 
 }  // namespace pfc

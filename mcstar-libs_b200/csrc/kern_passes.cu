@@ -1,0 +1,223 @@
+// Register-resident single-dimension passes of the FP32 stepper (power-of-two grids).
+//
+//  k_ycol  complex FFT along y (either direction, optional scale) of a tile of TX
+//          consecutive kx columns of one z-plane; in place or out of place.
+//  k_xrow  the x pass on R consecutive rows of the mixed (kx, y, z) field: inverse real
+//          FFT (nx/2-point complex FFT with the split/merge twiddles), the cubic term
+//          of psi3_split.hpp:8-13 with stabilisation C (and the optional potential of
+//          psi3_split.hpp:1-6), forward real FFT -- in place, one read and one write.
+//
+// A y pass, the x pass and a y pass replace the general y/x/y passes of the step;
+// they stream whole tiles (contiguous rows for x, 64-byte column segments for y)
+// and keep every FFT in registers with one shared-memory transpose per transform.
+#include "pfc_ctx.h"
+#include "regfft.cuh"
+
+namespace pfc {
+namespace {
+
+constexpr int cmaxi(int a, int b) { return a > b ? a : b; }
+
+template <int NY_, int E_, int TX_>
+struct YCfg {
+    static constexpr int NY = NY_, E = E_, TX = TX_;
+    static constexpr int P = NY / E, U = E / P, T = TX * P;
+    static constexpr int PADG = TX < 32 ? TX / U : 0;
+    static constexpr int XB = E * (P * TX + PADG);
+    static constexpr size_t SMEM = (size_t)(XB + NY) * sizeof(float2);
+    static constexpr int MINB = T <= 128 ? 4 : 2;
+    static_assert(P * E == NY && U * P == E && (TX >= 32 || (32 % TX == 0 && TX % U == 0)), "shape");
+};
+
+template <class Y, int DIR>
+__global__ void __launch_bounds__(Y::T, Y::MINB)
+    k_ycol(const float2* in, float2* out, int nxh, const float2* __restrict__ twg, float scale) {
+    constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P, U = Y::U;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* xb = sm;
+    float2* tw = sm + Y::XB;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < NY; i += Y::T) tw[i] = twg[i];
+    const int c = tid % TX, t = tid / TX;
+    const int kx = blockIdx.x * TX + c;
+    const bool valid = kx < nxh;
+    const int64_t base = (int64_t)blockIdx.y * NY * nxh + kx;
+    float2 v[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = valid ? in[base + (int64_t)(t + P * j) * nxh] : make_float2(0.f, 0.f);
+    __syncthreads();
+    fft_d1_to_d2<NY, E, TX, DIR, BarCta, Y::PADG>(v, t, c, xb, tw);
+    if (valid) {
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int k2 = 0; k2 < P; ++k2) {
+                const float2 w = v[u * P + k2];
+                out[base + (int64_t)((t * U + u) + E * k2) * nxh] = make_float2(w.x * scale, w.y * scale);
+            }
+    }
+}
+
+template <int NX_, int E_, int T_>
+struct XCfg {
+    static constexpr int NX = NX_, M = NX / 2, NXH = M + 1, E = E_, T = T_;
+    static constexpr int P = M / E, U = E / P, R = T / P;
+    static constexpr int LDR = NXH;  // odd: a warp over 32 rows at one k is conflict-free
+    static constexpr int BUF = cmaxi(R * LDR, E * P * R);
+    static constexpr size_t SMEM = (size_t)(BUF + M + M + 1) * sizeof(float2);
+    static_assert(P * E == M && U * P == E && R >= 32 && R * P == T, "shape");
+};
+
+template <class X>
+__global__ void __launch_bounds__(X::T, 2)
+    k_xrow(float2* buf, const float* __restrict__ pot, int nrows, const float2* __restrict__ twg, float mul, float Cc,
+           float mu) {
+    constexpr int NX = X::NX, M = X::M, NXH = X::NXH, E = X::E, P = X::P, U = X::U, R = X::R, LDR = X::LDR;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* rb = sm;
+    float2* twM = sm + X::BUF;  // W_M^m, m < M
+    float2* twP = twM + M;      // W_NX^k, k <= M
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 2 * M + 1; i += X::T) twM[i] = twg[i];
+    const int r = tid % R, t = tid / R;
+    const int row0 = blockIdx.x * R;
+    const int nr = min(R, nrows - row0);
+    const int64_t g0 = (int64_t)row0 * NXH;
+    for (int i = tid; i < nr * NXH; i += X::T) rb[i] = buf[g0 + i];
+    __syncthreads();
+    float2 v[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+        const int k = t + P * j;
+        v[j] = c2r_pre_f(rb[r * LDR + k], rb[r * LDR + M - k], twP[k]);
+    }
+    fft_d1_to_d2<M, E, R, 1>(v, t, r, rb, twM);
+    const int64_t prow = (int64_t)(row0 + r) * NX;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int k2 = 0; k2 < P; ++k2) {
+            const int n = (t * U + u) + E * k2;
+            const float2 x = v[u * P + k2];
+            const float a = x.x * mul, b = x.y * mul;
+            float2 o = make_float2(a * a * a - Cc * a - mu, b * b * b - Cc * b - mu);
+            if (pot && r < nr) {
+                const float2 pp = *reinterpret_cast<const float2*>(pot + prow + 2 * n);
+                o.x += pp.x;
+                o.y += pp.y;
+            }
+            v[u * P + k2] = o;
+        }
+    fft_d2_to_d1<M, E, R, -1>(v, t, r, rb, twM);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < E; ++j) rb[r * LDR + t + P * j] = v[j];
+    __syncthreads();
+    float2 xm_last = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+        const int k = t + P * j;
+        const float2 yk = v[j];
+        if (k == 0) xm_last = make_float2(yk.x - yk.y, 0.f);  // X[nx/2]
+        v[j] = r2c_post_f(yk, rb[r * LDR + ((M - k) & (M - 1))], twP[k]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < E; ++j) rb[r * LDR + t + P * j] = v[j];
+    if (t == 0) rb[r * LDR + M] = xm_last;
+    __syncthreads();
+    for (int i = tid; i < nr * NXH; i += X::T) buf[g0 + i] = rb[i];
+}
+
+using Y512 = YCfg<512, 32, 8>;
+using Y256 = YCfg<256, 16, 8>;
+using Y128 = YCfg<128, 16, 8>;
+using Y64 = YCfg<64, 8, 8>;
+using X512 = XCfg<512, 32, 256>;
+using X256 = XCfg<256, 16, 256>;
+using X128 = XCfg<128, 16, 128>;
+using X64 = XCfg<64, 8, 128>;
+
+template <class Y>
+cudaError_t yattr() {
+    cudaError_t e = cudaFuncSetAttribute(k_ycol<Y, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Y::SMEM);
+    if (e) return e;
+    return cudaFuncSetAttribute(k_ycol<Y, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Y::SMEM);
+}
+template <class X>
+cudaError_t xattr() {
+    return cudaFuncSetAttribute(k_xrow<X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)X::SMEM);
+}
+
+template <class Y>
+cudaError_t ylaunch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs) {
+    dim3 grid((c->nxh + Y::TX - 1) / Y::TX, nzs);
+    const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->ypass_tw_off;
+    if (dir > 0)
+        k_ycol<Y, 1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, tw, (float)scale);
+    else
+        k_ycol<Y, -1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, tw, (float)scale);
+    return cudaGetLastError();
+}
+template <class X>
+cudaError_t xlaunch(const pfc_ctx* c, void* b, const void* pot, double mul, double C, double mu, int nzs) {
+    const int nrows = nzs * c->ny;
+    dim3 grid((nrows + X::R - 1) / X::R);
+    const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->xpass_tw_off;
+    k_xrow<X><<<grid, X::T, X::SMEM, c->stream>>>((float2*)b, (const float*)pot, nrows, tw, (float)mul, (float)C,
+                                                 (float)mu);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+int fused_y_variant(int ny, int dtype) {
+    if (dtype != PFC_F32) return 0;
+    switch (ny) { case 512: return 1; case 256: return 2; case 128: return 3; case 64: return 4; }
+    return 0;
+}
+int fused_x_variant(int nx, int dtype) {
+    if (dtype != PFC_F32) return 0;
+    switch (nx) { case 512: return 1; case 256: return 2; case 128: return 3; case 64: return 4; }
+    return 0;
+}
+
+cudaError_t set_pass_attributes(const pfc_ctx* c) {
+    cudaError_t e = cudaSuccess;
+    switch (c->fused_y) {
+        case 1: e = yattr<Y512>(); break;
+        case 2: e = yattr<Y256>(); break;
+        case 3: e = yattr<Y128>(); break;
+        case 4: e = yattr<Y64>(); break;
+    }
+    if (e) return e;
+    switch (c->fused_x) {
+        case 1: e = xattr<X512>(); break;
+        case 2: e = xattr<X256>(); break;
+        case 3: e = xattr<X128>(); break;
+        case 4: e = xattr<X64>(); break;
+    }
+    return e;
+}
+
+cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs) {
+    switch (c->fused_y) {
+        case 1: return ylaunch<Y512>(c, dir, in, out, scale, nzs);
+        case 2: return ylaunch<Y256>(c, dir, in, out, scale, nzs);
+        case 3: return ylaunch<Y128>(c, dir, in, out, scale, nzs);
+        case 4: return ylaunch<Y64>(c, dir, in, out, scale, nzs);
+    }
+    return cudaErrorNotSupported;
+}
+
+cudaError_t launch_xpass(const pfc_ctx* c, void* b, const void* pot, double mul, double C, double mu, int nzs) {
+    switch (c->fused_x) {
+        case 1: return xlaunch<X512>(c, b, pot, mul, C, mu, nzs);
+        case 2: return xlaunch<X256>(c, b, pot, mul, C, mu, nzs);
+        case 3: return xlaunch<X128>(c, b, pot, mul, C, mu, nzs);
+        case 4: return xlaunch<X64>(c, b, pot, mul, C, mu, nzs);
+    }
+    return cudaErrorNotSupported;
+}
+
+}  // namespace pfc

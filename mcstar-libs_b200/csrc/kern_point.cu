@@ -12,6 +12,10 @@ inline int grid_for(size_t n, int block) {
     return (int)(g < cap ? (g ? g : 1) : cap);
 }
 
+// |k| as the reference evaluates it, sqrtf(-dop.x) (eom.hpp:68): single precision even
+// when Float is double.
+template <typename T> __device__ __forceinline__ T ref_sqrtf(T x) { return (T)sqrtf((float)x); }
+
 // kernel_update_eom / kernel_update_eom_with_fen (eom.hpp:60-72, 88-102), with the
 // stabilisation constant C (C = 1 is the reference: (1 + C - eps) = (2 - eps)).
 template <typename T>
@@ -31,7 +35,7 @@ __global__ void k_update_eom(cx<T>* __restrict__ kpsi, const cx<T>* __restrict__
         const T k0 = kwave<T>(i0, nx, lx), k1 = kwave<T>(i1, ny, ly), k2 = kwave<T>(i2, nz, lz);
         const T dopx = -k0 * k0 - k1 * k1 - k2 * k2;
         const T dopy = dopx * dopx;
-        const T k = sqrt(-dopx);
+        const T k = ref_sqrtf<T>(-dopx);
         T denom;
         if (with_fen) {
             const T lk = (T(2) - eps) + T(2) * dopx + dopy;

@@ -53,6 +53,14 @@ struct pfc_ctx {
     size_t bond_scratch_bytes;
     // fused plane kernels available for this shape
     int fused_xy;                 // 0: general passes; otherwise the plane kernel variant id
+    int plane_tw_off;             // twiddles of the plane kernel: W_ny^m, W_{nx/2}^m, W_nx^k (k <= nx/2)
+    int fused_z;                  // 0: general z pass; otherwise the register z kernel variant id
+    int zcol_tw_off;              // twiddles of the register z kernel: W_nz^m
+    int fused_y, fused_x;         // register y / x pass variants (0: none)
+    int ypass_tw_off;             // W_ny^m
+    int xpass_tw_off;             // W_{nx/2}^m, then W_nx^k (k <= nx/2)
+    int xy_mode;                  // 0 general passes, 1 cluster plane kernel, 2 register y/x/y passes
+    int slab;                     // z-planes per slab of the register xy passes (0: whole field)
     // tracing (pfc_profile_enable / pfc_profile_read)
     bool prof_on = false;
     long long launches = 0;
@@ -79,6 +87,23 @@ struct ZPropArgs {
     int final_step;
 };
 cudaError_t launch_zprop(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a);
+// the general z pass over the kx columns [col0, col0 + ncols)
+cudaError_t launch_zprop_cols(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int col0, int ncols);
+
+// ---- register-resident y and x passes (kern_passes.cu) ----
+int fused_y_variant(int ny, int dtype);
+int fused_x_variant(int nx, int dtype);
+cudaError_t set_pass_attributes(const pfc_ctx* c);
+// y FFT of nzs consecutive planes starting at in / out (in may equal out)
+cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs);
+// C2R, cubic term, R2C on the rows of nzs consecutive planes starting at b, in place;
+// pot (real field, or null) starts at the same first plane
+cudaError_t launch_xpass(const pfc_ctx* c, void* b, const void* pot, double mul, double C, double mu, int nzs);
+
+// ---- register-resident z pass (kern_zcol.cu) ----
+int fused_z_variant(int nx, int nz, int dtype);
+cudaError_t set_zcol_attributes(const pfc_ctx* c);
+cudaError_t launch_zcol(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a);
 
 // ---- pointwise kernels, noise and reductions (kern_point.cu) ----
 cudaError_t launch_update_eom(const pfc_ctx* c, void* kpsi, const void* knl, const void* knoise,

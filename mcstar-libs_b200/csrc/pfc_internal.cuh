@@ -97,13 +97,49 @@ template <typename T, int DIR> struct Dft<T, DIR, 5> {
 // the host in FP64 (forward sign; the inverse uses their conjugates).
 // ---------------------------------------------------------------------------------
 constexpr int kMaxStages = 16;
+constexpr int kMaxOddRadix = 31;  // largest prime radix of the general stage
 struct LinePlan {
     int n;
     int nst;
     int radix[kMaxStages];
     int ns[kMaxStages];
     int twoff[kMaxStages];
+    int rtoff[kMaxStages];  // W_R^q, q < R, for radices without a hand-written DFT
 };
+
+// Stage of a prime radix R (7 <= R <= kMaxOddRadix): direct R-point DFT with the
+// roots of unity W_R^q from the plan's table.
+template <typename T, int DIR>
+__device__ __forceinline__ void stockham_bfly_gen(const cx<T>* __restrict__ sl, cx<T>* __restrict__ dl, int j,
+                                                  int m, int Ns, int R, const cx<T>* __restrict__ tws,
+                                                  const cx<T>* __restrict__ wr) {
+    cx<T> v[kMaxOddRadix];
+    const int jj = j % Ns;
+    for (int r = 0; r < R; ++r) {
+        cx<T> a = sl[j + r * m];
+        if (Ns > 1 && r > 0) {
+            cx<T> w = tws[jj * (R - 1) + r - 1];
+            if (DIR > 0) w.y = -w.y;
+            a = cmul(a, w);
+        }
+        v[r] = a;
+    }
+    const int od = (j - jj) * R + jj;
+    for (int k = 0; k < R; ++k) {
+        cx<T> acc = v[0];
+        int q = 0;
+        for (int r = 1; r < R; ++r) {
+            q += k;
+            if (q >= R) q -= R;
+            cx<T> w = wr[q];
+            if (DIR > 0) w.y = -w.y;
+            const cx<T> p = cmul(v[r], w);
+            acc.x += p.x;
+            acc.y += p.y;
+        }
+        dl[od + k * Ns] = acc;
+    }
+}
 
 template <typename T, int DIR, int R>
 __device__ __forceinline__ void stockham_bfly(const cx<T>* __restrict__ sl, cx<T>* __restrict__ dl,
@@ -146,7 +182,8 @@ __device__ cx<T>* stockham_lines(cx<T>* a, cx<T>* b, int nlines, int ld, const L
                 case 4: stockham_bfly<T, DIR, 4>(sl, dl, j, m, Ns, tws); break;
                 case 2: stockham_bfly<T, DIR, 2>(sl, dl, j, m, Ns, tws); break;
                 case 3: stockham_bfly<T, DIR, 3>(sl, dl, j, m, Ns, tws); break;
-                default: stockham_bfly<T, DIR, 5>(sl, dl, j, m, Ns, tws); break;
+                case 5: stockham_bfly<T, DIR, 5>(sl, dl, j, m, Ns, tws); break;
+                default: stockham_bfly_gen<T, DIR>(sl, dl, j, m, Ns, R, tws, tw + p.rtoff[s]); break;
             }
         }
         __syncthreads();

@@ -1,0 +1,205 @@
+// Register-resident FFT building blocks of the fused plane and column kernels.
+//
+//  RF<N, DIR>::run(v)     N-point DFT (N a power of two <= 64) of v[0..N) held in
+//                         registers, natural order in and out: radix-4 decimation in
+//                         time down to 8/4/2-point kernels; every twiddle is a
+//                         compile-time constant (trivial ones cost nothing).
+//  fft_d1_to_d2 / fft_d2_to_d1
+//                         an N-point FFT spread over P = N/E threads holding E values
+//                         each (the four-step algorithm: E-point DFTs in registers,
+//                         twiddles W_N^{ab}, one transpose through shared memory,
+//                         P-point DFTs).  Distribution D1: thread t holds x[t + P j];
+//                         distribution D2: thread t holds x[(t E/P + u) + E k2] at
+//                         register u P + k2.  d1_to_d2 maps D1 input to D2 output,
+//                         d2_to_d1 the converse, so an inverse FFT, a pointwise map and
+//                         a forward FFT chain with no extra exchange.
+#pragma once
+#include <type_traits>
+#include "pfc_internal.cuh"
+
+namespace pfc {
+namespace ct {
+constexpr double kPi = 3.14159265358979323846264338327950288;
+// Taylor series on |r| <= pi/4 (error < 1e-19), after reduction by quadrant.
+constexpr double sin_s(double x) {
+    double t = x, s = x;
+    for (int n = 1; n < 14; ++n) { t *= -x * x / ((2.0 * n) * (2.0 * n + 1.0)); s += t; }
+    return s;
+}
+constexpr double cos_s(double x) {
+    double t = 1.0, s = 1.0;
+    for (int n = 1; n < 14; ++n) { t *= -x * x / ((2.0 * n - 1.0) * (2.0 * n)); s += t; }
+    return s;
+}
+constexpr double cos2pi(long k, long n) {
+    k %= n;
+    if (k < 0) k += n;
+    const long q = (8 * k + n) / (2 * n);
+    const double r = 2.0 * kPi * ((double)(4 * k - q * n) / (double)(4 * n));
+    const double c = cos_s(r), s = sin_s(r);
+    switch (q & 3) { case 0: return c; case 1: return -s; case 2: return -c; default: return s; }
+}
+constexpr double sin2pi(long k, long n) {
+    k %= n;
+    if (k < 0) k += n;
+    const long q = (8 * k + n) / (2 * n);
+    const double r = 2.0 * kPi * ((double)(4 * k - q * n) / (double)(4 * n));
+    const double c = cos_s(r), s = sin_s(r);
+    switch (q & 3) { case 0: return s; case 1: return c; case 2: return -s; default: return -c; }
+}
+}  // namespace ct
+
+template <int N, int K, int DIR> struct Tw {  // exp(DIR 2 pi i K / N)
+    static constexpr float re = (float)ct::cos2pi(K, N);
+    static constexpr float im = (float)(DIR * ct::sin2pi(K, N));
+};
+
+template <int I, int N, class F> __device__ __forceinline__ void sfor(F&& f) {
+    if constexpr (I < N) {
+        f(std::integral_constant<int, I>{});
+        sfor<I + 1, N>(f);
+    }
+}
+
+// a * exp(DIR 2 pi i K / N) with the trivial angles special-cased at compile time
+template <int N, int K, int DIR> __device__ __forceinline__ float2 twmul(float2 a) {
+    constexpr int k = ((K % N) + N) % N;
+    if constexpr (k == 0) {
+        return a;
+    } else if constexpr (4 * k == N) {
+        return rot<DIR>(a);
+    } else if constexpr (2 * k == N) {
+        return make_float2(-a.x, -a.y);
+    } else if constexpr (4 * k == 3 * N) {
+        return rot<-DIR>(a);
+    } else {
+        constexpr float c = Tw<N, k, DIR>::re, s = Tw<N, k, DIR>::im;
+        return make_float2(a.x * c - a.y * s, a.x * s + a.y * c);
+    }
+}
+
+template <int N, int DIR> struct RF;
+template <int DIR> struct RF<1, DIR> { __device__ __forceinline__ static void run(float2*) {} };
+template <int DIR> struct RF<2, DIR> { __device__ __forceinline__ static void run(float2* v) { Dft<float, DIR, 2>::run(v); } };
+template <int DIR> struct RF<4, DIR> { __device__ __forceinline__ static void run(float2* v) { Dft<float, DIR, 4>::run(v); } };
+template <int DIR> struct RF<8, DIR> { __device__ __forceinline__ static void run(float2* v) { Dft<float, DIR, 8>::run(v); } };
+template <int N, int DIR> struct RF {
+    static_assert(N % 4 == 0 && N >= 16, "power of two");
+    __device__ __forceinline__ static void run(float2* v) {
+        constexpr int Q = N / 4;
+        float2 s0[Q], s1[Q], s2[Q], s3[Q];
+#pragma unroll
+        for (int m = 0; m < Q; ++m) { s0[m] = v[4 * m]; s1[m] = v[4 * m + 1]; s2[m] = v[4 * m + 2]; s3[m] = v[4 * m + 3]; }
+        RF<Q, DIR>::run(s0);
+        RF<Q, DIR>::run(s1);
+        RF<Q, DIR>::run(s2);
+        RF<Q, DIR>::run(s3);
+        sfor<0, Q>([&](auto kk) {
+            constexpr int k = decltype(kk)::value;
+            const float2 a0 = s0[k];
+            const float2 a1 = twmul<N, k, DIR>(s1[k]);
+            const float2 a2 = twmul<N, 2 * k, DIR>(s2[k]);
+            const float2 a3 = twmul<N, 3 * k, DIR>(s3[k]);
+            const float2 t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, t3 = rot<DIR>(a1 - a3);
+            v[k] = t0 + t2;
+            v[k + 2 * Q] = t0 - t2;
+            v[k + Q] = t1 + t3;
+            v[k + 3 * Q] = t1 - t3;
+        });
+    }
+};
+
+// Barrier policies of the exchanges: the whole CTA, or a named barrier over the
+// first COUNT threads (used when half of a CTA runs a transform alone).
+struct BarCta {
+    __device__ __forceinline__ static void sync() { __syncthreads(); }
+};
+template <int ID, int COUNT> struct BarNamed {
+    __device__ __forceinline__ static void sync() { asm volatile("bar.sync %0, %1;" ::"n"(ID), "n"(COUNT) : "memory"); }
+};
+
+// Distributed shared memory: the 32-bit shared::cluster address of `local` in CTA
+// `rank` of this cluster, and an 8-byte store to it.
+__device__ __forceinline__ uint32_t dsmem_addr(const void* local, uint32_t rank) {
+    uint32_t a = (uint32_t)__cvta_generic_to_shared(local), r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void dsmem_st(uint32_t addr, float2 v) {
+    asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
+}
+
+// Exchange slots: group g of NG interleaved groups, logical index (a, b) of an
+// E x P matrix -> (a P + b) NG + a PADG + g.  Warps run over consecutive g (and, when
+// NG < 32, over 32/NG consecutive t); PADG shifts successive blocks of P rows so that
+// the t-groups of a warp land in different banks.  Buffer: E (P NG + PADG) float2.
+template <int N, int E, int NG, int PADG>
+__device__ __forceinline__ int xslot(int a, int b, int g) {
+    return (a * (N / E) + b) * NG + a * PADG + g;
+}
+
+template <int N, int E, int NG, int DIR, class Bar = BarCta, int PADG = 0>
+__device__ __forceinline__ void fft_d1_to_d2(float2 (&v)[E], int t, int g, float2* xb, const float2* twN) {
+    constexpr int P = N / E, U = E / P;
+    static_assert(P * E == N && U * P == E, "four-step shape");
+    RF<E, DIR>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < E; ++k1) {
+        float2 w = twN[(t * k1) & (N - 1)];
+        if (DIR > 0) w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+    }
+    Bar::sync();
+#pragma unroll
+    for (int k1 = 0; k1 < E; ++k1) xb[xslot<N, E, NG, PADG>(k1, t, g)] = v[k1];
+    Bar::sync();
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int tt = 0; tt < P; ++tt) v[u * P + tt] = xb[xslot<N, E, NG, PADG>(t * U + u, tt, g)];
+#pragma unroll
+    for (int u = 0; u < U; ++u) RF<P, DIR>::run(&v[u * P]);
+}
+
+template <int N, int E, int NG, int DIR, class Bar = BarCta, int PADG = 0>
+__device__ __forceinline__ void fft_d2_to_d1(float2 (&v)[E], int t, int g, float2* xb, const float2* twN) {
+    constexpr int P = N / E, U = E / P;
+    static_assert(P * E == N && U * P == E, "four-step shape");
+#pragma unroll
+    for (int u = 0; u < U; ++u) RF<P, DIR>::run(&v[u * P]);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int n1 = t * U + u;
+#pragma unroll
+        for (int k2 = 1; k2 < P; ++k2) {
+            float2 w = twN[(n1 * k2) & (N - 1)];
+            if (DIR > 0) w.y = -w.y;
+            v[u * P + k2] = cmul(v[u * P + k2], w);
+        }
+    }
+    Bar::sync();
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int k2 = 0; k2 < P; ++k2) xb[xslot<N, E, NG, PADG>(t * U + u, k2, g)] = v[u * P + k2];
+    Bar::sync();
+#pragma unroll
+    for (int n1 = 0; n1 < E; ++n1) v[n1] = xb[xslot<N, E, NG, PADG>(n1, t, g)];
+    RF<E, DIR>::run(v);
+}
+
+// Split / merge of a real FFT of length 2M done as an M-point complex FFT
+// (z[m] = x[2m] + i x[2m+1]); w = W_2M^k = exp(-2 pi i k / 2M).
+__device__ __forceinline__ float2 r2c_post_f(float2 zk, float2 zm, float2 w) {
+    const float2 s = make_float2(zk.x + zm.x, zk.y - zm.y);
+    const float2 d = make_float2(zk.x - zm.x, zk.y + zm.y);
+    const float2 wd = cmul(w, d);
+    return make_float2(0.5f * (s.x + wd.y), 0.5f * (s.y - wd.x));
+}
+__device__ __forceinline__ float2 c2r_pre_f(float2 xk, float2 xm, float2 w) {
+    const float2 e = make_float2(xk.x + xm.x, xk.y - xm.y);
+    const float2 o = cmul(make_float2(xk.x - xm.x, xk.y + xm.y), cconj(w));
+    return make_float2(e.x - o.y, e.y + o.x);
+}
+
+}  // namespace pfc

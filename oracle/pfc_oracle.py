@@ -105,19 +105,25 @@ def c2r(cmpl, shape_xyz, workers=None):
 # ----------------------------------------------------------------------------------
 # pointwise kernels
 # ----------------------------------------------------------------------------------
-def update_eom(kpsi, knl, knoise, namp, dt, eps, lens, shape_xyz, C=1.0):
+def update_eom(kpsi, knl, knoise, namp, dt, eps, lens, shape_xyz, C=1.0, ref_float_sqrt=True):
     """psi^ <- (psi^ - dt k^2 N^ + dt namp sqrt(N) |k| xi^) / (1 + dt k^2 ((1-k^2)^2 + C - eps)).
 
     C = 1 is the reference (eom.hpp:62-71: denom = 1 - dt((2-eps)(-k^2) + 2k^4 - k^6));
     C is the stabilisation constant of the split, matching psi3_split's  - C psi.
+    ref_float_sqrt: the reference takes sqrt(N) and |k| with sqrtf (eom.hpp:62,68), i.e. in
+    single precision even for double fields; False evaluates both in full precision.
     """
     nx, ny, nz = shape_xyz
     k2 = kgrid(shape_xyz, lens)
     dopx = -k2
     dopy = k2 * k2
-    k = np.sqrt(k2)
+    if ref_float_sqrt:
+        k = np.sqrt(k2.astype(np.float32)).astype(np.float64)
+        namp_eff = namp * float(np.sqrt(np.float32(nx * ny * nz)))
+    else:
+        k = np.sqrt(k2)
+        namp_eff = namp * math.sqrt(nx * ny * nz)
     denom = 1.0 - dt * ((1.0 + C - eps) * dopx + 2.0 * dopy + dopx * dopy)
-    namp_eff = namp * math.sqrt(nx * ny * nz)
     num = kpsi.astype(np.complex128) + dt * dopx * knl
     if knoise is not None:
         num = num + dt * namp_eff * k * knoise
@@ -260,11 +266,15 @@ def fill_real(n, sigma, seed, counter, dtype=np.float32):
 # the step
 # ----------------------------------------------------------------------------------
 def step(kpsi, nsteps, dt, eps, lens, shape_xyz, mu=0.0, C=1.0, namp=0.0,
-         seed=0, counter0=0, workers=None, dtype=np.float64):
+         seed=0, counter0=0, workers=None, dtype=np.float64, noise_dtype=None, ref_float_sqrt=False):
     """nsteps conserved semi-implicit steps: the driver loop of the reference
-    (copy, C2R, psi3_split(norm=True), R2C, [fill_kspace], update_eom)."""
+    (copy, C2R, psi3_split(norm=True), R2C, [fill_kspace], update_eom).
+    noise_dtype selects the precision of the Philox draw (that of the field being
+    compared); the fused stepper evaluates sqrt(N) and |k| in full precision, hence
+    ref_float_sqrt=False by default here."""
     real_t = np.dtype(dtype)
     cmpl_t = np.complex128 if real_t == np.float64 else np.complex64
+    noise_t = real_t if noise_dtype is None else np.dtype(noise_dtype)
     kpsi = kpsi.astype(cmpl_t)
     for t in range(nsteps):
         psi = c2r(kpsi, shape_xyz, workers=workers).astype(real_t)
@@ -272,8 +282,9 @@ def step(kpsi, nsteps, dt, eps, lens, shape_xyz, mu=0.0, C=1.0, namp=0.0,
         knl = r2c(nl, workers=workers).astype(cmpl_t)
         knoise = None
         if namp != 0.0:
-            knoise = fill_kspace(shape_xyz, seed, counter0 + t, dtype=real_t)
-        kpsi = update_eom(kpsi, knl, knoise, namp, dt, eps, lens, shape_xyz, C=C).astype(cmpl_t)
+            knoise = fill_kspace(shape_xyz, seed, counter0 + t, dtype=noise_t)
+        kpsi = update_eom(kpsi, knl, knoise, namp, dt, eps, lens, shape_xyz, C=C,
+                          ref_float_sqrt=ref_float_sqrt).astype(cmpl_t)
     return kpsi
 
 

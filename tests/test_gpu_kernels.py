@@ -23,7 +23,8 @@ def mk(shape, dtype):
 
 def up_c(ctx, X):
     b = ctx.empty_state()
-    b.copy_(torch.from_numpy(np.ascontiguousarray(X).view(ctx.np_dtype).ravel()))
+    ct = np.complex64 if ctx.np_dtype == F32 else np.complex128
+    b.copy_(torch.from_numpy(np.ascontiguousarray(X, dtype=ct).view(ctx.np_dtype).ravel()))
     return b
 
 

@@ -28,6 +28,9 @@ CASES = [
     ((16, 12, 10), F64, 0.0), ((16, 12, 10), F64, 0.05), ((15, 9, 7), F64, 0.0), ((24, 20, 1), F64, 0.0),
     ((64, 1, 1), F64, 0.0), ((32, 32, 32), F32, 0.0), ((32, 32, 32), F32, 0.02), ((64, 64, 64), F32, 0.0),
     ((128, 128, 128), F32, 0.0), ((256, 256, 1), F64, 0.0), ((48, 40, 30), F32, 0.0),
+    # every fused plane-kernel variant (FP32, nx = ny in {64, 128, 256, 512})
+    ((64, 64, 16), F32, 0.05), ((128, 128, 8), F32, 0.0), ((256, 256, 12), F32, 0.02), ((512, 512, 6), F32, 0.0),
+    ((512, 512, 1), F32, 0.0),
 ]
 
 
@@ -40,7 +43,7 @@ def test_step_matches_oracle(shape, dtype, namp):
     nsteps = 6
     st.step(nsteps)
     got = st.kspace()
-    want = O.step(psi, nsteps, st.dt, st.eps, st.lens, shape, namp=namp, seed=17, counter0=0)
+    want = O.step(psi, nsteps, st.dt, st.eps, st.lens, shape, namp=namp, seed=17, counter0=0, noise_dtype=dtype)
     tol = 2e-6 if dtype == F32 else 1e-12
     assert rel_l2(got, want) < tol
 
