@@ -27,7 +27,7 @@ struct ZCfg {
 };
 
 struct ZArgsF {
-    float dt, eps, C, namp_eff, lx, ly, lz;
+    float dt, eps, C, namp_eff, ckx, cky, ckz;  // ck = 2 pi / L per axis
     uint64_t seed, counter;
     int use_noise, final_step;
 };
@@ -70,10 +70,11 @@ __global__ void __launch_bounds__(Z::T, 2) k_zcol(float2* A, const float2* __res
     __syncthreads();
     if (half != 0) return;
 
-    const float k0x = kwave<float>(kx, nx, a.lx), k1y = kwave<float>(ky, ny, a.ly);
+    // wavenumbers K(i) = i' * 2 pi / L (common.hpp:27-28) with 2 pi / L precomputed
+    const float k0x = (float)kx * a.ckx;
+    const float k1y = (float)(ky < ny / 2 + 1 ? ky : ky - ny) * a.cky;
     const float kxy = k0x * k0x + k1y * k1y;
     const float deps = 1.0f + a.C - a.eps;
-    bool bad = false;
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
@@ -81,23 +82,43 @@ __global__ void __launch_bounds__(Z::T, 2) k_zcol(float2* A, const float2* __res
             const int kz = (t * U + u) + E * k2;
             float2 psi = v[u * P + k2];
             const float2 nl = regB[kz * TX + c];
-            const float k2z = kwave<float>(kz, NZ, a.lz);
+            const float k2z = (float)(kz < NZ / 2 + 1 ? kz : kz - NZ) * a.ckz;
             const float dopx = -kxy - k2z * k2z;
             const float dopy = dopx * dopx;
-            const float denom = 1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy);
+            const float inv = __frcp_rn(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
             if (kx == 0 && ky == 0 && kz == 0) psi = make_float2((float)k0->x, (float)k0->y);
             const float f = a.dt * dopx;
-            float2 num = make_float2(psi.x + f * nl.x, psi.y + f * nl.y);
-            if (a.use_noise) {
-                const float2 xi = kspace_noise<float>(kx, ky, kz, nx, ny, NZ, a.seed, a.counter);
-                const float g = a.dt * a.namp_eff * sqrtf(-dopx);
-                num.x += g * xi.x;
-                num.y += g * xi.y;
-            }
-            const float2 w = make_float2(num.x / denom, num.y / denom);
-            bad |= !isfinite(w.x) || !isfinite(w.y);
-            v[u * P + k2] = w;
+            v[u * P + k2] = make_float2((psi.x + f * nl.x) * inv, (psi.y + f * nl.y) * inv);
         }
+    if (a.use_noise) {
+        // conserved k-space noise, dt namp sqrt(N) |k| xi / D(k): a compact loop over this
+        // thread's modes, staged through its own N^ slots (kept out of the unrolled body)
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int k2 = 0; k2 < P; ++k2) regB[((t * U + u) + E * k2) * TX + c] = v[u * P + k2];
+#pragma unroll 1
+        for (int m = 0; m < E; ++m) {
+            const int kz = (t * U + m / P) + E * (m % P);
+            const float k2z = (float)(kz < NZ / 2 + 1 ? kz : kz - NZ) * a.ckz;
+            const float dopx = -kxy - k2z * k2z;
+            const float dopy = dopx * dopx;
+            const float inv = __frcp_rn(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
+            const float2 xi = kspace_noise<float>(kx, ky, kz, nx, ny, NZ, a.seed, a.counter);
+            const float g = a.dt * a.namp_eff * sqrtf(-dopx) * inv;
+            float2 w = regB[kz * TX + c];
+            w.x += g * xi.x;
+            w.y += g * xi.y;
+            regB[kz * TX + c] = w;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int k2 = 0; k2 < P; ++k2) v[u * P + k2] = regB[((t * U + u) + E * k2) * TX + c];
+    }
+    bool bad = false;
+#pragma unroll
+    for (int j = 0; j < E; ++j) bad |= !isfinite(v[j].x) || !isfinite(v[j].y);
     if (bad && valid) atomicOr(flag, 1);
     if (a.final_step) {
         if (valid)
@@ -126,8 +147,9 @@ cudaError_t zattr() {
 
 template <class Z>
 cudaError_t zlaunch(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& p) {
-    ZArgsF a{(float)p.dt, (float)p.eps, (float)p.C, (float)p.namp_eff, (float)p.lx, (float)p.ly, (float)p.lz,
-             p.seed, p.counter, p.use_noise, p.final_step};
+    const double tp = 6.283185307179586232;
+    ZArgsF a{(float)p.dt, (float)p.eps, (float)p.C, (float)p.namp_eff, (float)(tp / p.lx), (float)(tp / p.ly),
+             (float)(tp / p.lz), p.seed, p.counter, p.use_noise, p.final_step};
     dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
     k_zcol<Z><<<grid, Z::T, Z::SMEM, c->stream>>>((float2*)A, (const float2*)B, c->nx, c->ny, a, c->k0, c->flag, tw);

@@ -31,6 +31,10 @@ CASES = [
     # every fused plane-kernel variant (FP32, nx = ny in {64, 128, 256, 512})
     ((64, 64, 16), F32, 0.05), ((128, 128, 8), F32, 0.0), ((256, 256, 12), F32, 0.02), ((512, 512, 6), F32, 0.0),
     ((512, 512, 1), F32, 0.0),
+    # every register z-kernel variant (nz in {64, 128, 256, 512}), with and without noise,
+    # including a partial last tile of kx columns (nx/2 + 1 = 17)
+    ((16, 16, 512), F32, 0.03), ((16, 8, 512), F32, 0.0), ((32, 32, 256), F32, 0.02), ((32, 16, 128), F32, 0.05),
+    ((64, 64, 64), F32, 0.02),
 ]
 
 
