@@ -107,6 +107,20 @@ pfc_status pfc_noise_fill(pfc_ctx* ctx, void* arr, double sigma, uint64_t seed, 
 pfc_status pfc_findpeaks(pfc_ctx* ctx, const void* psi, double ths,
                          void* out_maxima, int capacity, int* n_found);
 
+/* The same peak finder for callers that must not allocate device memory -- no
+ * counterpart in mcstar-libs.  A simulation whose device memory is reserved up front
+ * by its own pool, or a driver that cannot afford the device-wide synchronisation a
+ * cudaMalloc may bring, cannot create a context (pfc_create allocates workspaces).
+ * This entry point takes the shape, precision and stream directly, allocates
+ * nothing, and keeps its scratch (block counts and their scan) in a static device
+ * array of 4 MiB that every GPU loading the library holds until exit; grids of more
+ * than 2^27 cells (512^3) are refused with PFC_ERR_CAPACITY and a message on stderr.
+ * The first call on a device looks up the array's address (make that first call
+ * before any stream capture).  All calls share the array: calls whose work overlaps
+ * on the GPU race.  Output, ordering, counts and errors as pfc_findpeaks. */
+pfc_status pfc_findpeaks_static(const void* psi, int nx, int ny, int nz, int dtype, double ths,
+                                void* out_maxima, int capacity, int* n_found, void* cuda_stream);
+
 /* ---- bond order: replaces bond_order_analysis<T> (bond-order-analysis/bond-order.hpp:4,
  * bond-order.cpp:289-349) on the GPU.  Input: n device Maximum<F> records (as written
  * by pfc_findpeaks).  Atoms with field > ths are kept; neighbours are atoms within

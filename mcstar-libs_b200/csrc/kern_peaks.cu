@@ -4,6 +4,8 @@
 // kPeakBlock consecutive cells (__syncthreads_count), one block scans the counts,
 // pass 2 writes each peak at block offset + warp-ballot rank.  Blocks cover linear
 // index ranges in order, so the output is sorted by linear index.
+#include <cstdio>
+#include <mutex>
 #include "pfc_ctx.h"
 
 namespace pfc {
@@ -11,7 +13,7 @@ namespace {
 
 template <typename T> struct MaxRec;
 template <> struct MaxRec<float> { float i0, i1, i2; float field; };
-template <> struct MaxRec<double> { double i0, i1, i2; float field; };
+template <> struct MaxRec<double> { double i0, i1, i2; float field; float pad; };  // pad written as 0
 static_assert(sizeof(MaxRec<float>) == 16, "Maximum<float> layout");
 static_assert(sizeof(MaxRec<double>) == 32, "Maximum<double> layout");
 
@@ -89,7 +91,7 @@ __global__ void __launch_bounds__(kPeakBlock) k_peaks_write(const T* __restrict_
     if (pos >= capacity) return;
     const int i0 = (int)(idx % nx);
     const int64_t r = idx / nx;
-    MaxRec<T> rec;
+    MaxRec<T> rec = {};
     rec.i0 = (T)i0;
     rec.i1 = (T)(int)(r % ny);
     rec.i2 = (T)(int)(r / ny);
@@ -97,18 +99,20 @@ __global__ void __launch_bounds__(kPeakBlock) k_peaks_write(const T* __restrict_
     out[pos] = rec;
 }
 
+// counts: one int per kPeakBlock cells; offsets: their exclusive scan plus the total
 template <typename T>
-cudaError_t peaks_T(const pfc_ctx* c, const void* psi, double ths, void* out, int capacity) {
-    const int d3 = c->nz > 1 ? 1 : 0;
-    const int nb = c->n_peak_blocks;
-    k_peaks_count<T><<<nb, kPeakBlock, 0, c->stream>>>((const T*)psi, c->nx, c->ny, c->nz, d3, (T)ths, c->peak_counts);
+cudaError_t peaks_raw(const void* psi, int nx, int ny, int nz, double ths, int* counts, int* offsets, void* out,
+                      int capacity, cudaStream_t st) {
+    const int d3 = nz > 1 ? 1 : 0;
+    const int nb = (int)(((int64_t)nx * ny * nz + kPeakBlock - 1) / kPeakBlock);
+    k_peaks_count<T><<<nb, kPeakBlock, 0, st>>>((const T*)psi, nx, ny, nz, d3, (T)ths, counts);
     cudaError_t e = cudaGetLastError();
     if (e) return e;
-    k_scan<<<1, 1024, 0, c->stream>>>(c->peak_counts, nb, c->peak_offsets);
+    k_scan<<<1, 1024, 0, st>>>(counts, nb, offsets);
     if ((e = cudaGetLastError())) return e;
     if (capacity > 0 && out) {
-        k_peaks_write<T><<<nb, kPeakBlock, 0, c->stream>>>((const T*)psi, c->nx, c->ny, c->nz, d3, (T)ths,
-                                                           c->peak_offsets, (MaxRec<T>*)out, capacity);
+        k_peaks_write<T><<<nb, kPeakBlock, 0, st>>>((const T*)psi, nx, ny, nz, d3, (T)ths, offsets, (MaxRec<T>*)out,
+                                                    capacity);
         if ((e = cudaGetLastError())) return e;
     }
     return cudaSuccess;
@@ -117,7 +121,69 @@ cudaError_t peaks_T(const pfc_ctx* c, const void* psi, double ths, void* out, in
 }  // namespace
 
 cudaError_t launch_findpeaks(const pfc_ctx* c, const void* psi, double ths, void* out, int capacity) {
-    return c->dtype == PFC_F64 ? peaks_T<double>(c, psi, ths, out, capacity) : peaks_T<float>(c, psi, ths, out, capacity);
+    return c->dtype == PFC_F64
+               ? peaks_raw<double>(psi, c->nx, c->ny, c->nz, ths, c->peak_counts, c->peak_offsets, out, capacity,
+                                   c->stream)
+               : peaks_raw<float>(psi, c->nx, c->ny, c->nz, ths, c->peak_counts, c->peak_offsets, out, capacity,
+                                  c->stream);
 }
 
 }  // namespace pfc
+
+// ---------------------------------------------------------------------------------------
+// Peak finding that allocates nothing.  Its scratch -- the per-block counts of the
+// compaction and their scan -- lives in this file-scope device array, sized for grids of
+// at most kStaticPeakCells cells (512^3); every GPU that loads the library holds it
+// (4 MiB) until the process exits.  Host code must not pass the array's name to a
+// kernel: on the host it is only a stand-in for the symbol.  The device address is
+// looked up once per device, by the first call on that device, with that device
+// current (cudaGetSymbolAddress) and cached.
+// ---------------------------------------------------------------------------------------
+namespace {
+constexpr int64_t kStaticPeakCells = (int64_t)1 << 27;
+constexpr int kStaticPeakBlocks = (int)(kStaticPeakCells / pfc::kPeakBlock);
+static __device__ __align__(256) int g_peak_scratch[2 * kStaticPeakBlocks + 1];
+constexpr int kMaxDevices = 64;
+int* g_peak_scratch_dev[kMaxDevices];
+std::mutex g_peak_scratch_mutex;
+}  // namespace
+
+extern "C" pfc_status pfc_findpeaks_static(const void* psi, int nx, int ny, int nz, int dtype, double ths,
+                                           void* out_maxima, int capacity, int* n_found, void* cuda_stream) {
+    if (!psi || !n_found || nx < 1 || ny < 1 || nz < 1 || capacity < 0 || (capacity > 0 && !out_maxima) ||
+        (dtype != PFC_F32 && dtype != PFC_F64) || (nz == 1 && !(nx > 1 && ny > 1)))
+        return PFC_ERR_INVALID;
+    const int64_t cells = (int64_t)nx * ny * nz;
+    if (cells > kStaticPeakCells) {
+        fprintf(stderr, "pfc_findpeaks_static: %lld cells exceed the static scratch maximum of %lld cells (512^3)\n",
+                (long long)cells, (long long)kStaticPeakCells);
+        return PFC_ERR_CAPACITY;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PFC_ERR_CUDA;
+    int* scratch;
+    {
+        std::lock_guard<std::mutex> lock(g_peak_scratch_mutex);
+        if (!g_peak_scratch_dev[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_peak_scratch) != cudaSuccess || !p) return PFC_ERR_CUDA;
+            g_peak_scratch_dev[dev] = (int*)p;
+        }
+        scratch = g_peak_scratch_dev[dev];
+    }
+    // counts and offsets are rewritten in full by every call: nothing needs clearing
+    int* counts = scratch;
+    int* offsets = scratch + kStaticPeakBlocks;
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    cudaError_t e = dtype == PFC_F64
+                        ? pfc::peaks_raw<double>(psi, nx, ny, nz, ths, counts, offsets, out_maxima, capacity, st)
+                        : pfc::peaks_raw<float>(psi, nx, ny, nz, ths, counts, offsets, out_maxima, capacity, st);
+    if (e != cudaSuccess) return PFC_ERR_CUDA;
+    const int nb = (int)((cells + pfc::kPeakBlock - 1) / pfc::kPeakBlock);
+    int total = 0;
+    if (cudaMemcpyAsync(&total, offsets + nb, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return PFC_ERR_CUDA;
+    *n_found = total;
+    return total > capacity ? PFC_ERR_CAPACITY : PFC_OK;
+}
