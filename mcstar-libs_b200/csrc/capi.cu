@@ -219,6 +219,15 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
     }
     c->slab = 0;
     if (const char* s = getenv("PFC_SLAB")) c->slab = std::max(0, atoi(s));
+    c->z_pipe = 0;
+    if (const char* s = getenv("PFC_Z_PIPE")) c->z_pipe = atoi(s) != 0;
+    {
+        int dev = 0;
+        c->num_sms = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess)
+            cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaGetLastError();
+    }
     // tiles: two ping-pong buffers of `tile` lines per CTA
     c->px.tile = pow2_floor((64 * 1024) / (2 * (size_t)lx * csz), 16);
     c->px.smem = 2 * (size_t)c->px.tile * lx * csz;

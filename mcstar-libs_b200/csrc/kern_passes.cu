@@ -10,6 +10,7 @@
 // A y pass, the x pass and a y pass replace the general y/x/y passes of the step;
 // they stream whole tiles (contiguous rows for x, 64-byte column segments for y)
 // and keep every FFT in registers with one shared-memory transpose per transform.
+#include <cstdlib>
 #include "pfc_ctx.h"
 #include "regfft.cuh"
 
@@ -65,11 +66,12 @@ struct XCfg {
     static constexpr int LDR = NXH;  // odd: a warp over 32 rows at one k is conflict-free
     static constexpr int BUF = cmaxi(R * LDR, E * P * R);
     static constexpr size_t SMEM = (size_t)(BUF + M + M + 1) * sizeof(float2);
-    static_assert(P * E == M && U * P == E && R >= 32 && R * P == T, "shape");
+    static constexpr int MINB = E <= 16 ? 3 : 2;
+    static_assert(P * E == M && U * P == E && (R % 32 == 0 || R == 16) && R * P == T, "shape");
 };
 
 template <class X>
-__global__ void __launch_bounds__(X::T, 2)
+__global__ void __launch_bounds__(X::T, X::MINB)
     k_xrow(float2* buf, const float* __restrict__ pot, int nrows, const float2* __restrict__ twg, float mul, float Cc,
            float mu) {
     constexpr int NX = X::NX, M = X::M, NXH = X::NXH, E = X::E, P = X::P, U = X::U, R = X::R, LDR = X::LDR;
@@ -130,10 +132,12 @@ __global__ void __launch_bounds__(X::T, 2)
 }
 
 using Y512 = YCfg<512, 32, 8>;
+using Y512w = YCfg<512, 32, 16>;  // 128-byte column segments, 256 threads
 using Y256 = YCfg<256, 16, 8>;
 using Y128 = YCfg<128, 16, 8>;
 using Y64 = YCfg<64, 8, 8>;
 using X512 = XCfg<512, 32, 256>;
+using X512h = XCfg<512, 16, 256>;  // 16 rows per CTA, 16 values per thread: three CTAs per SM
 using X256 = XCfg<256, 16, 256>;
 using X128 = XCfg<128, 16, 128>;
 using X64 = XCfg<64, 8, 128>;
@@ -171,14 +175,32 @@ cudaError_t xlaunch(const pfc_ctx* c, void* b, const void* pot, double mul, doub
 
 }  // namespace
 
+// 512-point variants, measured against each other: the x pass defaults to 16 values per
+// thread (three CTAs per SM; PFC_X_VARIANT=1 selects 32), the y pass to 64-byte column
+// segments (PFC_Y_VARIANT=5 selects 128-byte segments).
+static int env_choice(const char* name) {
+    const char* s = getenv(name);
+    return s ? atoi(s) : 0;
+}
+
 int fused_y_variant(int ny, int dtype) {
     if (dtype != PFC_F32) return 0;
-    switch (ny) { case 512: return 1; case 256: return 2; case 128: return 3; case 64: return 4; }
+    switch (ny) {
+        case 512: return env_choice("PFC_Y_VARIANT") == 5 ? 5 : 1;
+        case 256: return 2;
+        case 128: return 3;
+        case 64: return 4;
+    }
     return 0;
 }
 int fused_x_variant(int nx, int dtype) {
     if (dtype != PFC_F32) return 0;
-    switch (nx) { case 512: return 1; case 256: return 2; case 128: return 3; case 64: return 4; }
+    switch (nx) {
+        case 512: return env_choice("PFC_X_VARIANT") == 1 ? 1 : 5;
+        case 256: return 2;
+        case 128: return 3;
+        case 64: return 4;
+    }
     return 0;
 }
 
@@ -189,6 +211,7 @@ cudaError_t set_pass_attributes(const pfc_ctx* c) {
         case 2: e = yattr<Y256>(); break;
         case 3: e = yattr<Y128>(); break;
         case 4: e = yattr<Y64>(); break;
+        case 5: e = yattr<Y512w>(); break;
     }
     if (e) return e;
     switch (c->fused_x) {
@@ -196,6 +219,7 @@ cudaError_t set_pass_attributes(const pfc_ctx* c) {
         case 2: e = xattr<X256>(); break;
         case 3: e = xattr<X128>(); break;
         case 4: e = xattr<X64>(); break;
+        case 5: e = xattr<X512h>(); break;
     }
     return e;
 }
@@ -206,6 +230,7 @@ cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, d
         case 2: return ylaunch<Y256>(c, dir, in, out, scale, nzs);
         case 3: return ylaunch<Y128>(c, dir, in, out, scale, nzs);
         case 4: return ylaunch<Y64>(c, dir, in, out, scale, nzs);
+        case 5: return ylaunch<Y512w>(c, dir, in, out, scale, nzs);
     }
     return cudaErrorNotSupported;
 }
@@ -216,6 +241,7 @@ cudaError_t launch_xpass(const pfc_ctx* c, void* b, const void* pot, double mul,
         case 2: return xlaunch<X256>(c, b, pot, mul, C, mu, nzs);
         case 3: return xlaunch<X128>(c, b, pot, mul, C, mu, nzs);
         case 4: return xlaunch<X64>(c, b, pot, mul, C, mu, nzs);
+        case 5: return xlaunch<X512h>(c, b, pot, mul, C, mu, nzs);
     }
     return cudaErrorNotSupported;
 }

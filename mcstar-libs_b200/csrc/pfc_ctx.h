@@ -55,6 +55,8 @@ struct pfc_ctx {
     int fused_xy;                 // 0: general passes; otherwise the plane kernel variant id
     int plane_tw_off;             // twiddles of the plane kernel: W_ny^m, W_{nx/2}^m, W_nx^k (k <= nx/2)
     int fused_z;                  // 0: general z pass; otherwise the register z kernel variant id
+    int z_pipe;                   // register z pass as the persistent pipelined kernel (1) or one tile per CTA (0)
+    int num_sms;                  // multiprocessors of the device the context was made on
     int zcol_tw_off;              // twiddles of the register z kernel: W_nz^m
     int fused_y, fused_x;         // register y / x pass variants (0: none)
     int ypass_tw_off;             // W_ny^m

@@ -52,6 +52,48 @@ def test_step_matches_oracle(shape, dtype, namp):
     assert rel_l2(got, want) < tol
 
 
+_VARIANT_SCRIPT = r"""
+import sys, json, math
+import numpy as np
+sys.path[:0] = [{pkg!r}, {orc!r}]
+import pfc_oracle as O
+from mcstar_b200 import Stepper
+out = {{}}
+for shape, namp in [((64, 64, 64), 0.02), ((128, 128, 16), 0.0), ((32, 16, 128), 0.05), ((256, 256, 8), 0.0),
+                    ((512, 512, 4), 0.0)]:
+    nx, ny, nz = shape
+    st = Stepper(shape, math.pi / 4, 0.5, 0.3, dtype=np.float32, namp=namp, seed=5)
+    rng = np.random.default_rng(3)
+    k = O.r2c(-0.2 + 0.1 * rng.uniform(-1, 1, (nz, ny, nx)))
+    st.set_kspace(k.astype(np.complex64))
+    st.step(4)
+    want = O.step(k, 4, 0.5, 0.3, st.lens, shape, namp=namp, seed=5, noise_dtype=np.float32)
+    got = st.kspace()
+    out[str(shape)] = float(np.linalg.norm(got - want) / np.linalg.norm(want))
+print(json.dumps(out))
+"""
+
+
+@pytest.mark.parametrize("env", [{"PFC_Z_PIPE": "1"}, {"PFC_XY_MODE": "1"}, {"PFC_XY_MODE": "0"},
+                                 {"PFC_XY_MODE": "2", "PFC_SLAB": "3"}, {"PFC_X_VARIANT": "1", "PFC_Y_VARIANT": "5"}],
+                         ids=lambda e: ",".join(f"{k}={v}" for k, v in e.items()))
+def test_step_kernel_variants_match_oracle(env):
+    """The kernel variants chosen per context from the environment: the one-tile-per-CTA
+    z kernel, the cluster plane kernel, the general passes, slabbed register passes."""
+    import json
+    import os
+    import subprocess
+    import sys
+    from conftest import ROOT
+    code = _VARIANT_SCRIPT.format(pkg=os.path.join(ROOT, "mcstar-libs_b200"), orc=os.path.join(ROOT, "oracle"))
+    res = subprocess.run([sys.executable, "-c", code], env={**os.environ, **env}, capture_output=True, text=True,
+                         timeout=600)
+    assert res.returncode == 0, res.stderr[-2000:]
+    errs = json.loads(res.stdout.strip().splitlines()[-1])
+    for shape, e in errs.items():
+        assert e < 2e-6, (shape, e)
+
+
 def test_step_stabilisation_constant_and_mu():
     shape = (16, 16, 16)
     st = stepper(shape, F64, C=0.0, mu=0.07, dt=0.1)
