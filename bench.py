@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", type=int, default=512, help="grid side (the headline workload is 512)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="pfc512", choices=["pfc512", "ensemble"],
+                    help="pfc512: the headline 512^3 field (default); ensemble: 64 mixed-size replicas")
     return ap.parse_args()
 
 
@@ -152,31 +154,75 @@ def cpu_baseline(n, steps_budget_s=20.0):
 
 # ---------------------------------------------------------------------------------------
 def dist_setup(args):
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from mcstar_b200 import dist
+    ws, rank, local = dist.env_world()
     if torch.cuda.is_available():
         torch.cuda.set_device(local)
     if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init("nccl", timeout_s=300)
     return ws, rank, local
 
 
 def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from mcstar_b200 import dist
+    dist.barrier(ws)
 
 
 def max_over_ranks(ws, v):
+    from mcstar_b200 import dist
+    return dist.reduce_scalars(ws, [v], "max")[0]
+
+
+def run_ensemble(args, ws, rank, local):
+    """The batched workload: 48 2D + 16 3D FP32 fields of mixed sizes, eps, psi0, seeds,
+    noise T = 1e-3, one graph launch per step on each GPU (members dealt out by cost);
+    against the same members stepped one at a time through pfc_step."""
+    from mcstar_b200 import Ensemble, Stepper, ensemble_members, partition
+    members = ensemble_members(seed=4)
+    mine = partition(members, ws)[rank]
+    ens = Ensemble([members[i] for i in mine], steps_per_graph=1)
+    ens.run(args.warmup)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks.start()
+    e0.record()
+    ens.run(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    ms = max_over_ranks(ws, e0.elapsed_time(e1))
+    cells = sum(int(np.prod(m["shape"])) for m in members)
+    value = cells * args.steps / (ms / 1e3) / 1e9
+    out = {
+        "metric": "ensemble Gcell-upd/s (48 2D + 16 3D mixed-size fp32 replicas, one graph launch per step)",
+        "value": round(value, 2), "unit": "Gcell-upd/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic: seeded random liquids (numpy PCG64)",
+        "config": {"workload": "ensemble of 64 replicas", "members": len(members), "members_this_rank": len(mine),
+                   "steps_per_graph": 1, "noise_T": 1e-3, "parallelism": f"members dealt by cost over {ws} GPU(s)"},
+        "clocks": clk,
+    }
     if ws == 1:
-        return v
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+        # the same members one after another, each through pfc_step
+        seq_ms = 0.0
+        for m in members:
+            st = Stepper(m["shape"], m["dx"], m["dt"], m["eps"], dtype=np.float32, namp=m["namp"], seed=m["seed"])
+            st.set_real(initial_field(m["shape"], m["seed"]))
+            st.step(2)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            st.step(args.steps)
+            b.record()
+            torch.cuda.synchronize()
+            seq_ms += a.elapsed_time(b)
+        out["sequential"] = {"value": round(cells * args.steps / (seq_ms / 1e3) / 1e9, 2), "unit": "Gcell-upd/s",
+                             "ms_per_step": round(seq_ms / args.steps, 4)}
+    return out
 
 
 def run_b200(args, ws, rank, local):
@@ -326,18 +372,21 @@ def run_reference(args):
 def main():
     args = parse()
     ws, rank, local = dist_setup(args)
+    from mcstar_b200 import dist
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)))
+        dist.shutdown(ws)
         return
-    out = run_b200(args, ws, rank, local)
-    if rank == 0:
-        if ws == 1 and not args.no_cpu_baseline:
+    if args.workload == "ensemble":
+        out = run_ensemble(args, ws, rank, local)
+    else:
+        out = run_b200(args, ws, rank, local)
+        if rank == 0 and ws == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(args.size)
+    if rank == 0:
         print(json.dumps(out))
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    dist.shutdown(ws)
 
 
 if __name__ == "__main__":

@@ -151,6 +151,23 @@ typedef struct pfc_step_params {
 } pfc_step_params;
 pfc_status pfc_step(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params* params);
 
+/* ---- ensembles (no counterpart in mcstar-libs, whose drivers run one field per process):
+ * n independent fields, each with its own context (contexts and buffers must not be
+ * shared between members), shape, precision and parameters, advanced together.
+ * pfc_ensemble_create captures steps_per_graph steps of every member into one CUDA graph
+ * (one branch per member, so members of different sizes run concurrently);
+ * pfc_ensemble_run(e, nsteps, stream) converts every member into the stepper's carried
+ * form, replays the graph nsteps / steps_per_graph times (nsteps must be a multiple) and
+ * converts back, then checks every member's non-finite watchdog.  Each member's noise
+ * counter lives on the device and advances by one per step, so replays draw fresh noise
+ * and a run resumes exactly where the last one stopped. */
+typedef struct pfc_ensemble pfc_ensemble;
+pfc_status  pfc_ensemble_create(int n, pfc_ctx* const* ctxs, void* const* kpsis, const pfc_step_params* params,
+                                int steps_per_graph, pfc_ensemble** out);
+pfc_status  pfc_ensemble_run(pfc_ensemble* e, int nsteps, void* cuda_stream);
+pfc_status  pfc_ensemble_destroy(pfc_ensemble* e);
+const char* pfc_ensemble_last_error(const pfc_ensemble* e);
+
 /* Free energy F = h^3 sum 1/2 psi ((1+lap)^2 - eps) psi + 1/4 psi^4 of the state kpsi,
  * computed as the reference does (eom.hpp:88-141: L^psi^, C2R, norm, calc_fen) with an
  * FP64 deterministic sum.  Does not modify kpsi. */

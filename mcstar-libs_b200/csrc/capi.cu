@@ -129,6 +129,109 @@ cudaError_t traced(pfc_ctx* c, int family, int n, F&& launch) {
     return cudaSuccess;
 }
 
+// ---- the pieces of a step (enqueue only; capturable in a CUDA graph) -----------------------
+ZPropArgs zargs(const pfc_ctx* c, const pfc_step_params* p) {
+    ZPropArgs za;
+    za.dt = p->dt; za.eps = p->eps; za.C = p->C;
+    za.namp_eff = p->namp * std::sqrt((double)c->n_real);
+    za.lx = p->lx; za.ly = p->ly; za.lz = p->lz;
+    za.seed = p->seed;
+    za.counter = p->counter;
+    za.dev_counter = nullptr;
+    za.use_noise = p->namp != 0.0;
+    za.final_step = 0;
+    return za;
+}
+
+// psi^ -> A = IFFT_z(psi^)/nz in place; the k = 0 mode is kept in FP64
+cudaError_t step_entry(pfc_ctx* ctx, void* kpsi) {
+    return traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
+        cudaError_t e = launch_k0_save(ctx, kpsi);
+        if (e || ctx->nz == 1) return e;
+        return launch_cols(ctx, 2, 1, kpsi, kpsi, 1.0 / ctx->nz);
+    });
+}
+
+// A -> psi^ = FFT_z(A) in place, with the k = 0 mode restored from FP64
+cudaError_t step_exit(pfc_ctx* ctx, void* A) {
+    return traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
+        cudaError_t e = ctx->nz > 1 ? launch_cols(ctx, 2, -1, A, A, 1.0) : cudaSuccess;
+        if (e) return e;
+        return launch_k0_restore(ctx, A);
+    });
+}
+
+// B = FFT_xy(cubic term of IFFT_xy(A)) on the mixed grid
+cudaError_t step_xy(pfc_ctx* ctx, const void* A, void* B, const pfc_step_params* p) {
+    const double mul = 1.0 / ((double)ctx->nx * (double)ctx->ny);
+    if (ctx->xy_mode == 1)
+        return traced(ctx, 1, 1, [&] { return launch_fused_xy(ctx, A, B, nullptr, mul, p->C, p->mu); });
+    if (ctx->xy_mode == 2) {
+        // y-inverse, x (C2R, cubic, R2C), y-forward; with slabs the intermediate of each
+        // slab of z-planes lives in one reused slab-sized buffer (L2-resident)
+        const int slab = (ctx->slab > 0 && ctx->slab < ctx->nz) ? ctx->slab : ctx->nz;
+        const int nslab = (ctx->nz + slab - 1) / slab;
+        const int64_t pe = (int64_t)ctx->ny * ctx->nxh;  // complex elements per plane
+        return traced(ctx, 1, 3 * nslab, [&] {
+            cudaError_t e = cudaSuccess;
+            for (int z0 = 0; z0 < ctx->nz && !e; z0 += slab) {
+                const int nzs = std::min(slab, ctx->nz - z0);
+                const float2* a = (const float2*)A + z0 * pe;
+                float2* b = (float2*)B + z0 * pe;
+                float2* s = slab < ctx->nz ? (float2*)ctx->work2 : b;
+                if ((e = launch_ypass(ctx, 1, a, s, 1.0, nzs))) break;
+                if ((e = launch_xpass(ctx, s, nullptr, mul, p->C, p->mu, nzs))) break;
+                e = launch_ypass(ctx, -1, s, b, 1.0, nzs);
+            }
+            return e;
+        });
+    }
+    return traced(ctx, 1, ctx->ny > 1 ? 3 : 1, [&] {
+        cudaError_t e;
+        if (ctx->ny > 1) e = launch_cols(ctx, 1, 1, A, B, 1.0);
+        else e = cudaMemcpyAsync(B, A, ctx->state_bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e) return e;
+        if ((e = launch_rows_nonlin(ctx, B, nullptr, mul, p->C, p->mu))) return e;
+        return ctx->ny > 1 ? launch_cols(ctx, 1, -1, B, B, 1.0) : cudaSuccess;
+    });
+}
+
+// the z pass with the semi-implicit update
+cudaError_t step_z(pfc_ctx* ctx, void* A, const void* B, const ZPropArgs& za) {
+    if (ctx->fused_z) return traced(ctx, 2, 1, [&] { return launch_zcol(ctx, A, B, za); });
+    return traced(ctx, 2, 1, [&] { return launch_zprop(ctx, A, B, za); });
+}
+
+}  // namespace
+
+// ---- ensembles: many independent fields advanced by one CUDA graph launch -------------------
+struct pfc_ensemble {
+    std::vector<pfc_ctx*> ctx;
+    std::vector<void*> kpsi;
+    std::vector<pfc_step_params> p;
+    std::vector<cudaStream_t> st;
+    std::vector<cudaEvent_t> join;
+    cudaEvent_t fork = nullptr;
+    unsigned long long* ctr = nullptr;  // device noise counters, one per member
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int steps_per_graph = 1;
+    std::string err;
+};
+
+namespace {
+void free_ensemble(pfc_ensemble* e) {
+    if (!e) return;
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    for (cudaEvent_t v : e->join)
+        if (v) cudaEventDestroy(v);
+    if (e->fork) cudaEventDestroy(e->fork);
+    for (cudaStream_t s : e->st)
+        if (s) cudaStreamDestroy(s);
+    if (e->ctr) cudaFree(e->ctr);
+    delete e;
+}
 }  // namespace
 
 extern "C" {
@@ -419,59 +522,14 @@ pfc_status pfc_step(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params*
     if (nsteps == 0) return PFC_OK;
     void* A = kpsi;
     void* B = ctx->work;
-    const double mul = 1.0 / ((double)ctx->nx * (double)ctx->ny);
-    ZPropArgs za;
-    za.dt = p->dt; za.eps = p->eps; za.C = p->C;
-    za.namp_eff = p->namp * std::sqrt((double)ctx->n_real);
-    za.lx = p->lx; za.ly = p->ly; za.lz = p->lz;
-    za.seed = p->seed;
-    za.use_noise = p->namp != 0.0;
+    ZPropArgs za = zargs(ctx, p);
     PFC_CUDA(cudaMemsetAsync(ctx->flag, 0, sizeof(int), ctx->stream), "pfc_step flag");
-    PFC_CUDA(traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
-                 cudaError_t e = launch_k0_save(ctx, kpsi);
-                 if (e || ctx->nz == 1) return e;
-                 return launch_cols(ctx, 2, 1, A, A, 1.0 / ctx->nz);
-             }), "pfc_step entry");
+    PFC_CUDA(step_entry(ctx, kpsi), "pfc_step entry");
     for (int t = 0; t < nsteps; ++t) {
-        if (ctx->xy_mode == 1) {
-            PFC_CUDA(traced(ctx, 1, 1, [&] { return launch_fused_xy(ctx, A, B, nullptr, mul, p->C, p->mu); }),
-                     "pfc_step xy");
-        } else if (ctx->xy_mode == 2) {
-            // y-inverse, x (C2R, cubic, R2C), y-forward; with slabs the intermediate of
-            // each slab of z-planes lives in one reused slab-sized buffer (L2-resident)
-            const int slab = (ctx->slab > 0 && ctx->slab < ctx->nz) ? ctx->slab : ctx->nz;
-            const int nslab = (ctx->nz + slab - 1) / slab;
-            const int64_t pe = (int64_t)ctx->ny * ctx->nxh;  // complex elements per plane
-            PFC_CUDA(traced(ctx, 1, 3 * nslab, [&] {
-                         cudaError_t e = cudaSuccess;
-                         for (int z0 = 0; z0 < ctx->nz && !e; z0 += slab) {
-                             const int nzs = std::min(slab, ctx->nz - z0);
-                             const float2* a = (const float2*)A + z0 * pe;
-                             float2* b = (float2*)B + z0 * pe;
-                             float2* s = slab < ctx->nz ? (float2*)ctx->work2 : b;
-                             if ((e = launch_ypass(ctx, 1, a, s, 1.0, nzs))) break;
-                             if ((e = launch_xpass(ctx, s, nullptr, mul, p->C, p->mu, nzs))) break;
-                             e = launch_ypass(ctx, -1, s, b, 1.0, nzs);
-                         }
-                         return e;
-                     }), "pfc_step xy");
-        } else {
-            const int n = ctx->ny > 1 ? 3 : 1;
-            PFC_CUDA(traced(ctx, 1, n, [&] {
-                         cudaError_t e;
-                         if (ctx->ny > 1) e = launch_cols(ctx, 1, 1, A, B, 1.0);
-                         else e = cudaMemcpyAsync(B, A, ctx->state_bytes, cudaMemcpyDeviceToDevice, ctx->stream);
-                         if (e) return e;
-                         if ((e = launch_rows_nonlin(ctx, B, nullptr, mul, p->C, p->mu))) return e;
-                         return ctx->ny > 1 ? launch_cols(ctx, 1, -1, B, B, 1.0) : cudaSuccess;
-                     }), "pfc_step xy");
-        }
+        PFC_CUDA(step_xy(ctx, A, B, p), "pfc_step xy");
         za.counter = p->counter + (uint64_t)t;
         za.final_step = (t == nsteps - 1);
-        if (ctx->fused_z)
-            PFC_CUDA(traced(ctx, 2, 1, [&] { return launch_zcol(ctx, A, B, za); }), "pfc_step z");
-        else
-            PFC_CUDA(traced(ctx, 2, 1, [&] { return launch_zprop(ctx, A, B, za); }), "pfc_step z");
+        PFC_CUDA(step_z(ctx, A, B, za), "pfc_step z");
     }
     int flag = 0;
     PFC_CUDA(cudaMemcpyAsync(&flag, ctx->flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "pfc_step copy flag");
@@ -498,6 +556,121 @@ pfc_status pfc_free_energy(pfc_ctx* ctx, const void* kpsi, double eps, double lx
     *out = hx * hy * hz * (h[0] / (2.0 * N) + 0.25 * h[1]);
     return PFC_OK;
 }
+
+pfc_status pfc_ensemble_create(int n, pfc_ctx* const* ctxs, void* const* kpsis, const pfc_step_params* params,
+                                int steps_per_graph, pfc_ensemble** out) {
+    if (!out || n < 1 || !ctxs || !kpsis || !params || steps_per_graph < 1) return PFC_ERR_INVALID;
+    *out = nullptr;
+    for (int i = 0; i < n; ++i) {
+        if (!ctxs[i] || !kpsis[i]) return PFC_ERR_INVALID;
+        for (int j = 0; j < i; ++j)
+            if (ctxs[j] == ctxs[i] || kpsis[j] == kpsis[i]) return PFC_ERR_INVALID;  // members run concurrently
+    }
+    pfc_ensemble* e = new (std::nothrow) pfc_ensemble();
+    if (!e) return PFC_ERR_NOMEM;
+    e->ctx.assign(ctxs, ctxs + n);
+    e->kpsi.assign(kpsis, kpsis + n);
+    e->p.assign(params, params + n);
+    e->steps_per_graph = steps_per_graph;
+    e->st.assign(n, nullptr);
+    e->join.assign(n, nullptr);
+    cudaError_t ce = cudaMalloc(&e->ctr, sizeof(unsigned long long) * n);
+    for (int i = 0; i < n && !ce; ++i) {
+        ce = cudaStreamCreateWithFlags(&e->st[i], cudaStreamNonBlocking);
+        if (!ce) ce = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming);
+    }
+    if (!ce) ce = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+    cudaStream_t cap = nullptr;
+    if (!ce) ce = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+    std::vector<cudaStream_t> saved(n);
+    std::vector<bool> prof(n);
+    for (int i = 0; i < n; ++i) {
+        saved[i] = e->ctx[i]->stream;
+        prof[i] = e->ctx[i]->prof_on;
+        e->ctx[i]->prof_on = false;  // no event brackets inside the graph
+    }
+    // One graph: a fork, steps_per_graph steps of every member on its own branch, a join.
+    if (!ce) ce = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (!ce) {
+        cudaError_t ie = cudaEventRecord(e->fork, cap);
+        for (int i = 0; i < n && !ie; ++i) {
+            pfc_ctx* c = e->ctx[i];
+            c->stream = e->st[i];
+            ie = cudaStreamWaitEvent(e->st[i], e->fork, 0);
+            ZPropArgs za = zargs(c, &e->p[i]);
+            za.dev_counter = e->ctr + i;
+            for (int s = 0; s < steps_per_graph && !ie; ++s) {
+                ie = step_xy(c, e->kpsi[i], c->work, &e->p[i]);
+                if (!ie) ie = step_z(c, e->kpsi[i], c->work, za);
+                if (!ie) ie = launch_counter(e->st[i], e->ctr + i, 0, 0);
+            }
+            if (!ie) ie = cudaEventRecord(e->join[i], e->st[i]);
+            if (!ie) ie = cudaStreamWaitEvent(cap, e->join[i], 0);
+        }
+        ce = cudaStreamEndCapture(cap, &e->graph);
+        if (!ce) ce = ie;
+    }
+    if (!ce) ce = cudaGraphInstantiate(&e->exec, e->graph, 0);
+    for (int i = 0; i < n; ++i) {
+        e->ctx[i]->stream = saved[i];
+        e->ctx[i]->prof_on = prof[i];
+    }
+    if (cap) cudaStreamDestroy(cap);
+    if (ce) {
+        cudaGetLastError();
+        free_ensemble(e);
+        return ce == cudaErrorMemoryAllocation ? PFC_ERR_NOMEM : PFC_ERR_CUDA;
+    }
+    *out = e;
+    return PFC_OK;
+}
+
+pfc_status pfc_ensemble_run(pfc_ensemble* e, int nsteps, void* stream) {
+    if (!e) return PFC_ERR_INVALID;
+    if (nsteps < 0 || nsteps % e->steps_per_graph) {
+        e->err = "pfc_ensemble_run: nsteps must be a multiple of steps_per_graph";
+        return PFC_ERR_INVALID;
+    }
+    if (nsteps == 0) return PFC_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int n = (int)e->ctx.size();
+    std::vector<cudaStream_t> saved(n);
+    cudaError_t ce = cudaSuccess;
+    for (int i = 0; i < n && !ce; ++i) {
+        pfc_ctx* c = e->ctx[i];
+        saved[i] = c->stream;
+        c->stream = st;
+        ce = cudaMemsetAsync(c->flag, 0, sizeof(int), st);
+        if (!ce) ce = launch_counter(st, e->ctr + i, e->p[i].counter, 1);
+        if (!ce) ce = step_entry(c, e->kpsi[i]);
+    }
+    for (int r = 0; r < nsteps / e->steps_per_graph && !ce; ++r) ce = cudaGraphLaunch(e->exec, st);
+    for (int i = 0; i < n && !ce; ++i) ce = step_exit(e->ctx[i], e->kpsi[i]);
+    std::vector<int> flags(n, 0);
+    for (int i = 0; i < n && !ce; ++i)
+        ce = cudaMemcpyAsync(&flags[i], e->ctx[i]->flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (!ce) ce = cudaStreamSynchronize(st);
+    for (int i = 0; i < n; ++i) e->ctx[i]->stream = saved[i];
+    if (ce) {
+        e->err = std::string("pfc_ensemble_run: ") + cudaGetErrorString(ce);
+        return PFC_ERR_CUDA;
+    }
+    for (int i = 0; i < n; ++i) e->p[i].counter += (uint64_t)nsteps;
+    for (int i = 0; i < n; ++i)
+        if (flags[i]) {
+            e->err = "pfc_ensemble_run: non-finite value in member " + std::to_string(i);
+            return PFC_ERR_NONFINITE;
+        }
+    return PFC_OK;
+}
+
+pfc_status pfc_ensemble_destroy(pfc_ensemble* e) {
+    if (!e) return PFC_ERR_INVALID;
+    free_ensemble(e);
+    return PFC_OK;
+}
+
+const char* pfc_ensemble_last_error(const pfc_ensemble* e) { return e ? e->err.c_str() : "null ensemble"; }
 
 pfc_status pfc_profile_enable(pfc_ctx* ctx, int on) {
     PFC_CHECK_CTX();

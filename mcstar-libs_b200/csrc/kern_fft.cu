@@ -184,6 +184,7 @@ template <typename T>
 struct ZArgsT {
     T dt, eps, C, namp_eff, lx, ly, lz;
     uint64_t seed, counter;
+    const unsigned long long* dev_counter;  // read instead of counter when set
     int use_noise, final_step;
 };
 
@@ -228,7 +229,8 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
         cx<T> num = mkc<T>(psi.x + f * nl.x, psi.y + f * nl.y);
         if (a.use_noise) {
             const T kabs = sqrt(-dopx);
-            const cx<T> xi = kspace_noise<T>(kx, ky, kz, nx, ny, nz, a.seed, a.counter);
+            const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
+            const cx<T> xi = kspace_noise<T>(kx, ky, kz, nx, ny, nz, a.seed, ctr);
             const T g = a.dt * a.namp_eff * kabs;
             num.x += g * xi.x;
             num.y += g * xi.y;
@@ -348,13 +350,14 @@ cudaError_t launch_zprop_cols(const pfc_ctx* c, void* A, const void* B, const ZP
     dim3 grid((ncols + tile - 1) / tile, c->ny);
     const int col_end = col0 + ncols;
     if (c->dtype == PFC_F64) {
-        ZArgsT<double> t{a.dt, a.eps, a.C, a.namp_eff, a.lx, a.ly, a.lz, a.seed, a.counter, a.use_noise, a.final_step};
+        ZArgsT<double> t{a.dt,   a.eps,     a.C,         a.namp_eff, a.lx,        a.ly,
+                         a.lz,   a.seed,    a.counter,   a.dev_counter, a.use_noise, a.final_step};
         k_zprop<double><<<grid, 256, c->pzprop.smem, c->stream>>>((cx<double>*)A, (const cx<double>*)B, c->nx, c->ny,
                                                                    c->nz, c->pz.plan, (const cx<double>*)c->tw, tile,
                                                                    t, c->k0, c->flag, col0, col_end);
     } else {
         ZArgsT<float> t{(float)a.dt, (float)a.eps, (float)a.C, (float)a.namp_eff, (float)a.lx, (float)a.ly,
-                        (float)a.lz, a.seed, a.counter, a.use_noise, a.final_step};
+                        (float)a.lz, a.seed, a.counter, a.dev_counter, a.use_noise, a.final_step};
         k_zprop<float><<<grid, 256, c->pzprop.smem, c->stream>>>((cx<float>*)A, (const cx<float>*)B, c->nx, c->ny,
                                                                   c->nz, c->pz.plan, (const cx<float>*)c->tw, tile, t,
                                                                   c->k0, c->flag, col0, col_end);

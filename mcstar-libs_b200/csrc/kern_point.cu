@@ -176,7 +176,28 @@ __global__ void k_k0_save(const cx<T>* __restrict__ kpsi, double2* k0) {
     *k0 = make_double2((double)kpsi[0].x, (double)kpsi[0].y);
 }
 
+template <typename T>
+__global__ void k_k0_restore(cx<T>* __restrict__ kpsi, const double2* k0) {
+    kpsi[0] = mkc<T>((T)k0->x, (T)k0->y);
+}
+
+__global__ void k_counter(unsigned long long* ctr, unsigned long long value, int set) {
+    if (set) *ctr = value;
+    else *ctr += 1ull;
+}
+
 }  // namespace
+
+cudaError_t launch_k0_restore(const pfc_ctx* c, void* kpsi) {
+    if (c->dtype == PFC_F64) k_k0_restore<double><<<1, 1, 0, c->stream>>>((cx<double>*)kpsi, c->k0);
+    else k_k0_restore<float><<<1, 1, 0, c->stream>>>((cx<float>*)kpsi, c->k0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_counter(cudaStream_t st, unsigned long long* ctr, unsigned long long value, int set) {
+    k_counter<<<1, 1, 0, st>>>(ctr, value, set);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_update_eom(const pfc_ctx* c, void* kpsi, const void* knl, const void* knoise, double namp,
                               double dt, double eps, double lx, double ly, double lz, int with_fen, double C) {

@@ -22,6 +22,7 @@ namespace {
 struct ZArgsF {
     float dt, eps, C, namp_eff, ckx, cky, ckz;  // ck = 2 pi / L per axis
     uint64_t seed, counter;
+    const unsigned long long* dev_counter;      // read instead of counter when set
     int use_noise, final_step;
 };
 
@@ -75,6 +76,7 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], NL nl, float2* scra
         // conserved k-space noise, dt namp sqrt(N) |k| xi / D(k): a compact loop over this
         // thread's modes, staged through its own slots (kept out of the unrolled body)
         Bar::sync();
+        const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
@@ -86,7 +88,7 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], NL nl, float2* scra
             const float dopx = -kxy - k2z * k2z;
             const float dopy = dopx * dopx;
             const float inv = __frcp_rn(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
-            const float2 xi = kspace_noise<float>(kx, ky, kz, nx, ny, NZ, a.seed, a.counter);
+            const float2 xi = kspace_noise<float>(kx, ky, kz, nx, ny, NZ, a.seed, ctr);
             const float g = a.dt * a.namp_eff * sqrtf(-dopx) * inv;
             float2 w = scratch[kz * TX + c];
             w.x += g * xi.x;
@@ -267,7 +269,7 @@ template <class Z>
 cudaError_t zlaunch(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& p) {
     const double tp = 6.283185307179586232;
     ZArgsF a{(float)p.dt, (float)p.eps, (float)p.C, (float)p.namp_eff, (float)(tp / p.lx), (float)(tp / p.ly),
-             (float)(tp / p.lz), p.seed, p.counter, p.use_noise, p.final_step};
+             (float)(tp / p.lz), p.seed, p.counter, p.dev_counter, p.use_noise, p.final_step};
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
     const int ntx = (c->nxh + Z::TX - 1) / Z::TX;
     if (c->z_pipe) {

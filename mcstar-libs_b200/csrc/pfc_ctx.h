@@ -85,6 +85,9 @@ cudaError_t launch_rows_nonlin(const pfc_ctx* c, void* buf, const void* pot, dou
 struct ZPropArgs {
     double dt, eps, C, namp_eff, lx, ly, lz;
     uint64_t seed, counter;
+    // when set, the noise counter is read from device memory (graph-replayed steps, whose
+    // kernel arguments are fixed at capture, advance it on the device)
+    const unsigned long long* dev_counter;
     int use_noise;
     int final_step;
 };
@@ -119,6 +122,9 @@ cudaError_t launch_quartic_sum(const pfc_ctx* c, const void* psi_unnorm, double 
 cudaError_t launch_noise_kspace(const pfc_ctx* c, void* arr, uint64_t seed, uint64_t counter);
 cudaError_t launch_noise_real(const pfc_ctx* c, void* arr, double sigma, uint64_t seed, uint64_t counter);
 cudaError_t launch_k0_save(const pfc_ctx* c, const void* kpsi);
+cudaError_t launch_k0_restore(const pfc_ctx* c, void* kpsi);
+// set (set != 0) or increment a device-side step counter
+cudaError_t launch_counter(cudaStream_t st, unsigned long long* ctr, unsigned long long value, int set);
 // reduce the kRedBlocks partials in c->red into c->red[kRedBlocks + slot]
 cudaError_t launch_reduce_final(const pfc_ctx* c, int slot, double scale);
 

@@ -24,7 +24,8 @@ EXPORTED = (
     "pfc_state_bytes", "pfc_workspace_bytes", "pfc_fft_r2c", "pfc_fft_c2r", "pfc_update_eom",
     "pfc_update_eom_with_fen", "pfc_psi3_split", "pfc_norm", "pfc_calc_fen", "pfc_noise_fill_kspace",
     "pfc_noise_fill", "pfc_findpeaks", "pfc_bond_order", "pfc_step", "pfc_free_energy",
-    "pfc_profile_enable", "pfc_profile_read", "pfc_findpeaks_static",
+    "pfc_profile_enable", "pfc_profile_read", "pfc_findpeaks_static", "pfc_ensemble_create",
+    "pfc_ensemble_run", "pfc_ensemble_destroy", "pfc_ensemble_last_error",
 )
 
 
@@ -82,6 +83,11 @@ _SIGS = {
     "pfc_profile_enable": ([_P, _I], _I),
     "pfc_profile_read": ([_P, ctypes.POINTER(PfcProfile)], _I),
     "pfc_findpeaks_static": ([_P, _I, _I, _I, _I, _D, _P, _I, ctypes.POINTER(_I), _P], _I),
+    "pfc_ensemble_create": ([_I, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(PfcStepParams), _I,
+                             ctypes.POINTER(_P)], _I),
+    "pfc_ensemble_run": ([_P, _I, _P], _I),
+    "pfc_ensemble_destroy": ([_P], _I),
+    "pfc_ensemble_last_error": ([_P], ctypes.c_char_p),
 }
 
 
