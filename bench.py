@@ -124,6 +124,36 @@ def ncu_traffic(kernel, size):
         return None
 
 
+def kernel_table(prof, S, steps):
+    """Per-kernel device time of the timed region (the library's CUDA-event brackets on
+    its stream) with the algorithmic HBM bytes of one launch, S = bytes of one
+    half-spectrum field: every pass reads each input field once and writes each output
+    field once."""
+    t = {}
+
+    def add(name, fam, bytes_per_launch):
+        calls = prof["calls"][fam]
+        if calls:
+            t[name] = {"ms_total": prof["ms"][fam], "launches": calls, "ms_per_launch": prof["ms"][fam] / calls,
+                       "bytes_per_launch": bytes_per_launch}
+
+    if prof["xy_mode"] == 2 and prof["calls"][3]:
+        add("k_ycol", 3, 2.0 * S)  # y-inverse A -> B, y-forward B -> B
+        add("k_xrow", 4, 2.0 * S)  # C2R, cubic term, R2C of every row, in place
+    elif prof["xy_mode"] == 2:
+        add("k_ycol+k_xrow+k_ycol (z slabs)", 1, 6.0 * S)
+    elif prof["xy_mode"] == 1:
+        add("k_plane_xy", 1, 2.0 * S)
+    else:
+        add("k_cols+k_rows_nonlin+k_cols", 1, 6.0 * S)
+    if prof["z_mode"] == 2:
+        # psi^ and B read, psi^' and A' written; the last step of a run writes psi^' only
+        add("k_zcarry", 2, (4.0 * (steps - 1) + 3.0) / steps * S)
+    else:
+        add("k_zcol" if prof["z_mode"] == 1 else "k_zprop", 2, 3.0 * S)
+    return t
+
+
 def initial_field(shape, seed):
     from mcstar_b200 import liquid_random
     return liquid_random(shape, WL["psi0"], WL["amp"], seed)
@@ -276,24 +306,24 @@ def run_b200(args, ws, rank, local):
     cells = n ** 3
     # ---- roofline of the dominant kernel family -------------------------------------------------
     peak, peak_kind = measured_peak()
-    fused = prof["xy_variant"] != 0
-    # algorithmic bytes per launch: the plane kernel reads and writes the state once
-    # (2S); the general xy part is three passes (6S per bracketed call); the z pass
-    # reads the carried state and the nonlinear term and writes the state (3S)
-    fam_bytes = {1: (2.0 * S if fused else 6.0 * S), 2: 3.0 * S}
-    fam_name = {1: ("k_plane_xy" if fused else "k_cols+k_rows_nonlin+k_cols"), 2: "k_zprop"}
-    fam = max((1, 2), key=lambda f: prof["ms"][f])
-    per_launch_ms = prof["ms"][fam] / max(1, prof["calls"][fam])
-    achieved = fam_bytes[fam] / (per_launch_ms / 1e3) / 1e9
-    step_bytes = (5.0 if fused else 9.0) * S
-    roof = {"bound": "hbm", "kernel": fam_name[fam], "achieved": round(achieved, 1), "peak": peak,
+    kern = kernel_table(prof, S, args.steps)
+    dom = max(kern, key=lambda k: kern[k]["ms_total"])
+    d = kern[dom]
+    achieved = d["bytes_per_launch"] / (d["ms_per_launch"] / 1e3) / 1e9
+    step_bytes = sum(k["bytes_per_launch"] * k["launches"] for k in kern.values()) / args.steps
+    roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
             "peak_kind": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)", "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "algorithmic_bytes_per_launch": fam_bytes[fam],
-            "traffic": ncu_traffic(fam_name[fam], n),
+            "frac": round(achieved / peak, 4), "algorithmic_bytes_per_launch": d["bytes_per_launch"],
+            "ms_per_launch": round(d["ms_per_launch"], 5),
+            "traffic": ncu_traffic(dom, n),
             "step_bytes_alg": step_bytes,
             "step_frac": round(step_bytes * (value / ws) / 1e9 / peak, 4),
-            "family_ms_per_call": {k: round(prof["ms"][f] / max(1, prof["calls"][f]), 5)
-                                   for k, f in (("entry_exit", 0), ("xy", 1), ("z", 2))}}
+            "kernels": {k: {"ms_per_launch": round(v["ms_per_launch"], 5), "launches": v["launches"],
+                            "share": round(v["ms_total"] / max(1e-9, prof["ms"][1] + prof["ms"][2]), 4),
+                            "alg_bytes_per_launch": v["bytes_per_launch"],
+                            "frac": round(v["bytes_per_launch"] / (v["ms_per_launch"] / 1e3) / 1e9 / peak, 4)}
+                        for k, v in kern.items()},
+            "entry_exit_ms_per_run": round(prof["ms"][0], 5)}
     out = {
         "metric": "PFC steps/s (Gcell-upd/s in gcell_upd_per_s) at 512^3 fp32",
         "value": round(value, 2), "unit": "steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,

@@ -179,15 +179,22 @@ pfc_status pfc_free_energy(pfc_ctx* ctx, const void* kpsi, double eps,
  * While enabled, pfc_step brackets each kernel family with CUDA events on the
  * context's stream and counts every kernel the library launches.  Families:
  *   0 = entry/exit passes, 1 = the xy part of a step (one plane kernel, or the
- *   y/x/y general passes), 2 = the z pass with the propagator.
+ *   y/x/y passes), 2 = the z pass with the propagator, 3 = each register y pass and
+ *   4 = the register x pass (3 and 4 only when those passes run on the whole field;
+ *   their time is also inside family 1).
  * pfc_profile_read synchronises the stream and returns the totals since enabling. */
-#define PFC_PROFILE_FAMILIES 3
+#define PFC_PROFILE_FAMILIES 5
 typedef struct pfc_profile {
     long long launches;                          /* kernels launched by the library  */
     long long calls[PFC_PROFILE_FAMILIES];       /* bracketed launches per family    */
     double ms[PFC_PROFILE_FAMILIES];             /* summed device time per family    */
     int xy_variant;                              /* 0: general y/x/y passes; else the
                                                     fused plane kernel in use        */
+    int xy_mode;                                 /* 0 general passes, 1 cluster plane
+                                                    kernel, 2 register y/x/y passes  */
+    int z_mode;                                  /* 0 general z pass, 1 register z pass
+                                                    carrying A = IFFT_z(psi^)/nz, 2
+                                                    register z pass carrying psi^    */
 } pfc_profile;
 pfc_status pfc_profile_enable(pfc_ctx* ctx, int on);
 pfc_status pfc_profile_read(pfc_ctx* ctx, pfc_profile* out);

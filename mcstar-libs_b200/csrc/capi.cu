@@ -101,9 +101,9 @@ cudaError_t prof_resolve(pfc_ctx* c) {
     if (e) return e;
     for (auto& p : c->ev_pending) {
         float ms = 0.f;
-        if ((e = cudaEventElapsedTime(&ms, c->ev_pool[p.second], c->ev_pool[p.second + 1]))) return e;
-        c->prof_ms[p.first] += ms;
-        c->prof_calls[p.first] += 1;
+        if ((e = cudaEventElapsedTime(&ms, c->ev_pool[p.from], c->ev_pool[p.to]))) return e;
+        c->prof_ms[p.family] += ms;
+        c->prof_calls[p.family] += 1;
     }
     c->ev_pending.clear();
     c->ev_used = 0;
@@ -125,7 +125,37 @@ cudaError_t traced(pfc_ctx* c, int family, int n, F&& launch) {
     if (e) return e;
     if ((e = launch())) return e;
     if ((e = cudaEventRecord(c->ev_pool[i + 1], c->stream))) return e;
-    c->ev_pending.emplace_back(family, i);
+    c->ev_pending.push_back({family, i, i + 1});
+    return cudaSuccess;
+}
+
+// The register xy part (y-inverse, x, y-forward passes) with each pass bracketed too:
+// family 1 gets the whole part, 3 each y pass and 4 the x pass.
+template <typename FY1, typename FX, typename FY2>
+cudaError_t traced_xy3(pfc_ctx* c, FY1&& y1, FX&& x, FY2&& y2) {
+    c->launches += 3;
+    if (!c->prof_on) {
+        cudaError_t e = y1();
+        if (!e) e = x();
+        if (!e) e = y2();
+        return e;
+    }
+    if (c->ev_used + 4 > c->ev_pool.size()) {
+        cudaError_t e = prof_resolve(c);
+        if (e) return e;
+    }
+    const size_t i = c->ev_used;
+    c->ev_used += 4;
+    cudaError_t e;
+    if ((e = cudaEventRecord(c->ev_pool[i], c->stream)) || (e = y1()) ||
+        (e = cudaEventRecord(c->ev_pool[i + 1], c->stream)) || (e = x()) ||
+        (e = cudaEventRecord(c->ev_pool[i + 2], c->stream)) || (e = y2()) ||
+        (e = cudaEventRecord(c->ev_pool[i + 3], c->stream)))
+        return e;
+    c->ev_pending.push_back({1, i, i + 3});
+    c->ev_pending.push_back({3, i, i + 1});
+    c->ev_pending.push_back({4, i + 1, i + 2});
+    c->ev_pending.push_back({3, i + 2, i + 3});
     return cudaSuccess;
 }
 
@@ -143,26 +173,34 @@ ZPropArgs zargs(const pfc_ctx* c, const pfc_step_params* p) {
     return za;
 }
 
-// psi^ -> A = IFFT_z(psi^)/nz in place; the k = 0 mode is kept in FP64
+// Where the stepper's mixed-grid field A = IFFT_z(psi^)/nz lives: beside the carried
+// psi^ (z_carry), or in place of it.
+void* carried_A(pfc_ctx* ctx, void* kpsi) { return ctx->z_carry ? ctx->work2 : kpsi; }
+
+// psi^ -> A = IFFT_z(psi^)/nz; the k = 0 mode is kept in FP64
 cudaError_t step_entry(pfc_ctx* ctx, void* kpsi) {
     return traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
         cudaError_t e = launch_k0_save(ctx, kpsi);
         if (e || ctx->nz == 1) return e;
-        return launch_cols(ctx, 2, 1, kpsi, kpsi, 1.0 / ctx->nz);
+        return launch_cols(ctx, 2, 1, kpsi, carried_A(ctx, kpsi), 1.0 / ctx->nz);
     });
 }
 
-// A -> psi^ = FFT_z(A) in place, with the k = 0 mode restored from FP64
-cudaError_t step_exit(pfc_ctx* ctx, void* A) {
+// back to psi^ after non-final steps: FFT_z(A) with the k = 0 mode restored from FP64
+// (nothing to do when psi^ is carried)
+cudaError_t step_exit(pfc_ctx* ctx, void* kpsi) {
+    if (ctx->z_carry) return cudaSuccess;
     return traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
-        cudaError_t e = ctx->nz > 1 ? launch_cols(ctx, 2, -1, A, A, 1.0) : cudaSuccess;
+        cudaError_t e = ctx->nz > 1 ? launch_cols(ctx, 2, -1, kpsi, kpsi, 1.0) : cudaSuccess;
         if (e) return e;
-        return launch_k0_restore(ctx, A);
+        return launch_k0_restore(ctx, kpsi);
     });
 }
 
 // B = FFT_xy(cubic term of IFFT_xy(A)) on the mixed grid
-cudaError_t step_xy(pfc_ctx* ctx, const void* A, void* B, const pfc_step_params* p) {
+cudaError_t step_xy(pfc_ctx* ctx, void* kpsi, const pfc_step_params* p) {
+    const void* A = carried_A(ctx, kpsi);
+    void* B = ctx->work;
     const double mul = 1.0 / ((double)ctx->nx * (double)ctx->ny);
     if (ctx->xy_mode == 1)
         return traced(ctx, 1, 1, [&] { return launch_fused_xy(ctx, A, B, nullptr, mul, p->C, p->mu); });
@@ -172,6 +210,11 @@ cudaError_t step_xy(pfc_ctx* ctx, const void* A, void* B, const pfc_step_params*
         const int slab = (ctx->slab > 0 && ctx->slab < ctx->nz) ? ctx->slab : ctx->nz;
         const int nslab = (ctx->nz + slab - 1) / slab;
         const int64_t pe = (int64_t)ctx->ny * ctx->nxh;  // complex elements per plane
+        if (nslab == 1)
+            return traced_xy3(
+                ctx, [&] { return launch_ypass(ctx, 1, A, B, 1.0, ctx->nz); },
+                [&] { return launch_xpass(ctx, B, nullptr, mul, p->C, p->mu, ctx->nz); },
+                [&] { return launch_ypass(ctx, -1, B, B, 1.0, ctx->nz); });
         return traced(ctx, 1, 3 * nslab, [&] {
             cudaError_t e = cudaSuccess;
             for (int z0 = 0; z0 < ctx->nz && !e; z0 += slab) {
@@ -197,9 +240,11 @@ cudaError_t step_xy(pfc_ctx* ctx, const void* A, void* B, const pfc_step_params*
 }
 
 // the z pass with the semi-implicit update
-cudaError_t step_z(pfc_ctx* ctx, void* A, const void* B, const ZPropArgs& za) {
-    if (ctx->fused_z) return traced(ctx, 2, 1, [&] { return launch_zcol(ctx, A, B, za); });
-    return traced(ctx, 2, 1, [&] { return launch_zprop(ctx, A, B, za); });
+cudaError_t step_z(pfc_ctx* ctx, void* kpsi, const ZPropArgs& za) {
+    void* B = ctx->work;
+    if (ctx->z_carry) return traced(ctx, 2, 1, [&] { return launch_zcarry(ctx, kpsi, ctx->work2, B, za); });
+    if (ctx->fused_z) return traced(ctx, 2, 1, [&] { return launch_zcol(ctx, kpsi, B, za); });
+    return traced(ctx, 2, 1, [&] { return launch_zprop(ctx, kpsi, B, za); });
 }
 
 }  // namespace
@@ -324,6 +369,15 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
     if (const char* s = getenv("PFC_SLAB")) c->slab = std::max(0, atoi(s));
     c->z_pipe = 0;
     if (const char* s = getenv("PFC_Z_PIPE")) c->z_pipe = atoi(s) != 0;
+    // the register z pass carries A = IFFT_z(psi^)/nz (three z transforms, three field
+    // sweeps; measured faster); PFC_Z_CARRY=1 carries psi^ itself (two transforms, four
+    // sweeps).  The slabbed xy passes and the pipelined z kernel need work2 / carry A.
+    c->z_carry = 0;
+    if (const char* s = getenv("PFC_Z_CARRY")) c->z_carry = c->fused_z && atoi(s) != 0;
+    if (c->slab > 0 || c->z_pipe) c->z_carry = 0;
+    // L2 prefetch of the register passes, in waves of CTAs ahead (PFC_PREFETCH)
+    c->pf_waves = 0.f;
+    if (const char* s = getenv("PFC_PREFETCH")) c->pf_waves = std::max(0.f, (float)atof(s));
     {
         int dev = 0;
         c->num_sms = 148;
@@ -520,16 +574,14 @@ pfc_status pfc_step(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params*
     PFC_CHECK_CTX();
     if (!kpsi || !p || nsteps < 0) return fail(ctx, PFC_ERR_INVALID, "pfc_step: bad arguments");
     if (nsteps == 0) return PFC_OK;
-    void* A = kpsi;
-    void* B = ctx->work;
     ZPropArgs za = zargs(ctx, p);
     PFC_CUDA(cudaMemsetAsync(ctx->flag, 0, sizeof(int), ctx->stream), "pfc_step flag");
     PFC_CUDA(step_entry(ctx, kpsi), "pfc_step entry");
     for (int t = 0; t < nsteps; ++t) {
-        PFC_CUDA(step_xy(ctx, A, B, p), "pfc_step xy");
+        PFC_CUDA(step_xy(ctx, kpsi, p), "pfc_step xy");
         za.counter = p->counter + (uint64_t)t;
-        za.final_step = (t == nsteps - 1);
-        PFC_CUDA(step_z(ctx, A, B, za), "pfc_step z");
+        za.final_step = (t == nsteps - 1);  // the last step writes psi^ itself
+        PFC_CUDA(step_z(ctx, kpsi, za), "pfc_step z");
     }
     int flag = 0;
     PFC_CUDA(cudaMemcpyAsync(&flag, ctx->flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "pfc_step copy flag");
@@ -600,8 +652,8 @@ pfc_status pfc_ensemble_create(int n, pfc_ctx* const* ctxs, void* const* kpsis, 
             ZPropArgs za = zargs(c, &e->p[i]);
             za.dev_counter = e->ctr + i;
             for (int s = 0; s < steps_per_graph && !ie; ++s) {
-                ie = step_xy(c, e->kpsi[i], c->work, &e->p[i]);
-                if (!ie) ie = step_z(c, e->kpsi[i], c->work, za);
+                ie = step_xy(c, e->kpsi[i], &e->p[i]);
+                if (!ie) ie = step_z(c, e->kpsi[i], za);
                 if (!ie) ie = launch_counter(e->st[i], e->ctr + i, 0, 0);
             }
             if (!ie) ie = cudaEventRecord(e->join[i], e->st[i]);
@@ -691,7 +743,9 @@ pfc_status pfc_profile_read(pfc_ctx* ctx, pfc_profile* out) {
     if (!out) return fail(ctx, PFC_ERR_INVALID, "pfc_profile_read: null output");
     PFC_CUDA(prof_resolve(ctx), "pfc_profile_read");
     out->launches = ctx->launches;
-    out->xy_variant = ctx->fused_xy;
+    out->xy_variant = ctx->xy_mode == 1 ? ctx->fused_xy : 0;
+    out->xy_mode = ctx->xy_mode;
+    out->z_mode = ctx->z_carry ? 2 : (ctx->fused_z ? 1 : 0);
     for (int f = 0; f < PFC_PROFILE_FAMILIES; ++f) { out->calls[f] = ctx->prof_calls[f]; out->ms[f] = ctx->prof_ms[f]; }
     return PFC_OK;
 }

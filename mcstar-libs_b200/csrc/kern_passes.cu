@@ -32,7 +32,7 @@ struct YCfg {
 
 template <class Y, int DIR>
 __global__ void __launch_bounds__(Y::T, Y::MINB)
-    k_ycol(const float2* in, float2* out, int nxh, const float2* __restrict__ twg, float scale) {
+    k_ycol(const float2* in, float2* out, int nxh, const float2* __restrict__ twg, float scale, int pf) {
     constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P, U = Y::U;
     extern __shared__ __align__(16) float2 sm[];
     float2* xb = sm;
@@ -46,6 +46,17 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
     float2 v[E];
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = valid ? in[base + (int64_t)(t + P * j) * nxh] : make_float2(0.f, 0.f);
+    if (pf) {
+        // L2 prefetch of the tile pf tiles ahead in launch order: its column segment of every y row
+        const int ntx = (int)gridDim.x;
+        const int tgt = (int)(blockIdx.y * gridDim.x + blockIdx.x) + pf;
+        if (tgt < ntx * (int)gridDim.y) {
+            const int kx0 = (tgt % ntx) * TX;
+            const float2* f = in + (int64_t)(tgt / ntx) * NY * nxh + kx0;
+            const unsigned bytes = (unsigned)(min(TX, nxh - kx0) * sizeof(float2));
+            for (int y = tid; y < NY; y += Y::T) l2_prefetch(f + (int64_t)y * nxh, bytes);
+        }
+    }
     __syncthreads();
     fft_d1_to_d2<NY, E, TX, DIR, BarCta, Y::PADG>(v, t, c, xb, tw);
     if (valid) {
@@ -73,7 +84,7 @@ struct XCfg {
 template <class X>
 __global__ void __launch_bounds__(X::T, X::MINB)
     k_xrow(float2* buf, const float* __restrict__ pot, int nrows, const float2* __restrict__ twg, float mul, float Cc,
-           float mu) {
+           float mu, int pf) {
     constexpr int NX = X::NX, M = X::M, NXH = X::NXH, E = X::E, P = X::P, U = X::U, R = X::R, LDR = X::LDR;
     extern __shared__ __align__(16) float2 sm[];
     float2* rb = sm;
@@ -86,6 +97,17 @@ __global__ void __launch_bounds__(X::T, X::MINB)
     const int nr = min(R, nrows - row0);
     const int64_t g0 = (int64_t)row0 * NXH;
     for (int i = tid; i < nr * NXH; i += X::T) rb[i] = buf[g0 + i];
+    if (pf) {
+        // L2 prefetch of the rows of the CTA pf CTAs ahead, in 4 KB pieces
+        const int row1 = (blockIdx.x + pf) * R;
+        if (row1 < nrows) {
+            const int64_t e0 = (int64_t)row1 * NXH;
+            const int64_t n = (int64_t)min(R, nrows - row1) * NXH;
+            constexpr int kPiece = 512;  // float2
+            for (int64_t i = (int64_t)tid * kPiece; i < n; i += (int64_t)X::T * kPiece)
+                l2_prefetch(buf + e0 + i, (unsigned)(min((int64_t)kPiece, n - i) * sizeof(float2)));
+        }
+    }
     __syncthreads();
     float2 v[E];
 #pragma unroll
@@ -157,10 +179,13 @@ template <class Y>
 cudaError_t ylaunch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs) {
     dim3 grid((c->nxh + Y::TX - 1) / Y::TX, nzs);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->ypass_tw_off;
+    static const int per_sm = resident_ctas(k_ycol<Y, 1>, Y::T, Y::SMEM);
+    const int pf = prefetch_ahead(c, per_sm, in);
     if (dir > 0)
-        k_ycol<Y, 1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, tw, (float)scale);
+        k_ycol<Y, 1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, tw, (float)scale, pf);
     else
-        k_ycol<Y, -1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, tw, (float)scale);
+        k_ycol<Y, -1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, tw, (float)scale,
+                                                          pf);
     return cudaGetLastError();
 }
 template <class X>
@@ -168,8 +193,9 @@ cudaError_t xlaunch(const pfc_ctx* c, void* b, const void* pot, double mul, doub
     const int nrows = nzs * c->ny;
     dim3 grid((nrows + X::R - 1) / X::R);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->xpass_tw_off;
+    static const int per_sm = resident_ctas(k_xrow<X>, X::T, X::SMEM);
     k_xrow<X><<<grid, X::T, X::SMEM, c->stream>>>((float2*)b, (const float*)pot, nrows, tw, (float)mul, (float)C,
-                                                 (float)mu);
+                                                 (float)mu, prefetch_ahead(c, per_sm, b));
     return cudaGetLastError();
 }
 

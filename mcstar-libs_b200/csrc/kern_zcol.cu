@@ -40,18 +40,24 @@ struct ZCfg {
     static constexpr int STG = NZ * TX;  // staging of one field tile, [z][c]
     static constexpr size_t SMEM = (size_t)(2 * REG + NZ) * sizeof(float2);
     static constexpr size_t SMEM_PIPE = (size_t)(2 * STG + 2 * REG + NHS + NZ) * sizeof(float2);
+    static constexpr size_t SMEM_CARRY = (size_t)(REG + STG + NZ) * sizeof(float2);  // TH threads, one field
+    // resident CTAs of k_zcarry the shared memory allows (228 KB per SM): its register cap
+    static constexpr int CMINB = 4 * (SMEM_CARRY + 1024) <= 228 * 1024 ? 4 : 3;
     static_assert(TH % 32 == 0 && U * P == E && TX % U == 0 && 32 % TX == 0, "shape");
 };
 
 template <class Z> __device__ __forceinline__ int nh_slot(int kz, int c) { return kz * Z::TX + c + (kz / Z::U) * 8; }
 
-// The update of the thread's modes kz = (t U + u) + E k2 of column kx at ky.  nl(kz)
-// returns N^; scratch (this thread's own slots kz * TX + c) stages the noise pass, after
-// a barrier of the half (Bar) so that no thread of the half still reads its exchange.
-template <class Z, class Bar, class NL>
-__device__ __forceinline__ void propagate(float2 (&v)[Z::E], NL nl, float2* scratch, int kx, int ky, int t, int c,
-                                          int nx, int ny, bool valid, const ZArgsF& a, const double2* k0, int* flag) {
-    constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, U = Z::U;
+// The update of the thread's modes kz = (t U + u) + E k2 of column kx at ky; the result
+// replaces v.  kPsiInV: v holds psi^ and other(kz) returns N^; otherwise v holds N^ and
+// other(kz) returns psi^.  The noise pass is staged through the thread's own slots
+// scratch[slot(kz)]; kSync puts a barrier of the transforming threads (Bar) first, for
+// a scratch that is an exchange buffer other threads may still be reading.
+template <class Z, class Bar, bool kPsiInV, bool kSync, class OTHER, class SLOT>
+__device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2* scratch, SLOT slot, int kx, int ky,
+                                          int t, int nx, int ny, bool valid, const ZArgsF& a, const double2* k0,
+                                          int* flag) {
+    constexpr int NZ = Z::NZ, E = Z::E, P = Z::P, U = Z::U;
     // wavenumbers K(i) = i' * 2 pi / L (common.hpp:27-28) with 2 pi / L precomputed
     const float k0x = (float)kx * a.ckx;
     const float k1y = (float)(ky < ny / 2 + 1 ? ky : ky - ny) * a.cky;
@@ -62,8 +68,8 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], NL nl, float2* scra
 #pragma unroll
         for (int k2 = 0; k2 < P; ++k2) {
             const int kz = (t * U + u) + E * k2;
-            float2 psi = v[u * P + k2];
-            const float2 n = nl(kz);
+            float2 psi = kPsiInV ? v[u * P + k2] : other(kz);
+            const float2 n = kPsiInV ? other(kz) : v[u * P + k2];
             const float k2z = (float)(kz < NZ / 2 + 1 ? kz : kz - NZ) * a.ckz;
             const float dopx = -kxy - k2z * k2z;
             const float dopy = dopx * dopx;
@@ -75,12 +81,12 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], NL nl, float2* scra
     if (a.use_noise) {
         // conserved k-space noise, dt namp sqrt(N) |k| xi / D(k): a compact loop over this
         // thread's modes, staged through its own slots (kept out of the unrolled body)
-        Bar::sync();
+        if (kSync) Bar::sync();
         const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int k2 = 0; k2 < P; ++k2) scratch[((t * U + u) + E * k2) * TX + c] = v[u * P + k2];
+            for (int k2 = 0; k2 < P; ++k2) scratch[slot((t * U + u) + E * k2)] = v[u * P + k2];
 #pragma unroll 1
         for (int m = 0; m < E; ++m) {
             const int kz = (t * U + m / P) + E * (m % P);
@@ -90,15 +96,15 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], NL nl, float2* scra
             const float inv = __frcp_rn(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
             const float2 xi = kspace_noise<float>(kx, ky, kz, nx, ny, NZ, a.seed, ctr);
             const float g = a.dt * a.namp_eff * sqrtf(-dopx) * inv;
-            float2 w = scratch[kz * TX + c];
+            float2 w = scratch[slot(kz)];
             w.x += g * xi.x;
             w.y += g * xi.y;
-            scratch[kz * TX + c] = w;
+            scratch[slot(kz)] = w;
         }
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int k2 = 0; k2 < P; ++k2) v[u * P + k2] = scratch[((t * U + u) + E * k2) * TX + c];
+            for (int k2 = 0; k2 < P; ++k2) v[u * P + k2] = scratch[slot((t * U + u) + E * k2)];
     }
     bool bad = false;
 #pragma unroll
@@ -124,10 +130,28 @@ __device__ __forceinline__ void store_state(float2 (&v)[Z::E], float2* A, int64_
     }
 }
 
+// L2 prefetch of the tile `ahead` tiles after this CTA's in launch order (grid x: kx
+// tiles of TX columns, grid y: ky): the column segment of every z row of the fields
+// f0 and f1, spread over the CTA's threads.
+template <int NZ, int TX>
+__device__ __forceinline__ void prefetch_ztile(const float2* f0, const float2* f1, int ahead, int nxh, int64_t zs,
+                                               int tid, int nthreads) {
+    const int ntx = (int)gridDim.x;
+    const int tgt = (int)(blockIdx.y * gridDim.x + blockIdx.x) + ahead;
+    if (tgt >= ntx * (int)gridDim.y) return;
+    const int kx0 = (tgt % ntx) * TX;
+    const int64_t off = (int64_t)(tgt / ntx) * nxh + kx0;
+    const unsigned bytes = (unsigned)(min(TX, nxh - kx0) * sizeof(float2));
+    for (int i = tid; i < 2 * NZ; i += nthreads) {
+        const int z = i < NZ ? i : i - NZ;
+        l2_prefetch((i < NZ ? f0 : f1) + off + (int64_t)z * zs, bytes);
+    }
+}
+
 template <class Z>
 __global__ void __launch_bounds__(Z::T, 2) k_zcol(float2* A, const float2* __restrict__ B, int nx, int ny, ZArgsF a,
                                                    const double2* __restrict__ k0, int* flag,
-                                                   const float2* __restrict__ twg) {
+                                                   const float2* __restrict__ twg, int pf) {
     constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, U = Z::U, TH = Z::TH;
     extern __shared__ __align__(16) float2 sm[];
     float2* regA = sm;
@@ -148,6 +172,7 @@ __global__ void __launch_bounds__(Z::T, 2) k_zcol(float2* A, const float2* __res
     float2 v[E];
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = valid ? src[base + (int64_t)(t + P * j) * zs] : make_float2(0.f, 0.f);
+    if (pf) prefetch_ztile<NZ, TX>(A, B, pf, nxh, zs, tid, Z::T);
     __syncthreads();
     if (half == 0) {
         fft_d1_to_d2<NZ, E, TX, -1, BarNamed<1, TH>, Z::PADG>(v, t, c, regA, tw);
@@ -161,8 +186,9 @@ __global__ void __launch_bounds__(Z::T, 2) k_zcol(float2* A, const float2* __res
     }
     __syncthreads();
     if (half != 0) return;
-    propagate<Z, BarNamed<1, TH>>(v, [&](int kz) { return regB[kz * TX + c]; }, regB, kx, ky, t, c, nx, ny, valid, a,
-                                  k0, flag);
+    auto own = [&](int kz) { return kz * TX + c; };
+    propagate<Z, BarNamed<1, TH>, true, true>(v, [&](int kz) { return regB[own(kz)]; }, regB, own, kx, ky, t, nx, ny,
+                                              valid, a, k0, flag);
     if (!a.final_step) fft_d2_to_d1<NZ, E, TX, 1, BarNamed<1, TH>, Z::PADG>(v, t, c, regA, tw);
     store_state<Z>(v, A, base, zs, t, valid, a.final_step);
 }
@@ -173,6 +199,69 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Row of mode kz in the psi^ staging tile ([row][c], TX = 8 float2 per row).  A warp
+// reads the modes kz = t U + u + E k2 of four consecutive t at once; with U = 2 those
+// rows all have the parity of u, so rows are swapped in pairs for odd t, which puts two
+// t-groups in each half of the 32 banks (two wavefronts, the minimum for 8-byte reads).
+template <class Z> __device__ __forceinline__ int stg_row(int kz) {
+    if constexpr (Z::U == 2) return kz ^ ((kz >> 1) & 1);
+    else return kz;
+}
+
+// The z pass when the state psi^ itself is carried (k-space, reference layout) and
+// A = IFFT_z(psi^)/nz is only the input of the next xy part.  The whole CTA works on
+// one field: psi^ of the tile is copied into a shared staging tile with cp.async while
+// every thread loads and transforms B (N^ = FFT_z(B)); the update then reads psi^ from
+// the staging tile (no transform), writes psi^' and, unless this is the last step,
+// A' = IFFT_z(psi^')/nz.  Two z transforms per column instead of k_zcol's three, no FP32
+// round trip of the state per step (its rounding matches the reference's k-space
+// update), and one more read and write of the state.
+template <class Z>
+__global__ void __launch_bounds__(Z::TH, Z::CMINB) k_zcarry(float2* kpsi, float2* A, const float2* __restrict__ B, int nx,
+                                                      int ny, ZArgsF a, const double2* __restrict__ k0, int* flag,
+                                                      const float2* __restrict__ twg, int pf) {
+    constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, TH = Z::TH;
+    static_assert(TX == 8 && (Z::U == 1 || Z::U == 2), "staging swizzle assumes 8 columns per tile");
+    extern __shared__ __align__(16) float2 sm[];
+    float2* xb = sm;
+    float2* stg = sm + Z::REG;
+    float2* tw = stg + Z::STG;
+    const int tid = threadIdx.x;
+    const int c = tid % TX, t = tid / TX;
+    const int kx = blockIdx.x * TX + c;
+    const int ky = blockIdx.y;
+    const int nxh = nx / 2 + 1;
+    const bool valid = kx < nxh;  // the last tile holds only the kx = nx/2 column
+    const int64_t zs = (int64_t)ny * nxh;
+    const int64_t base = (int64_t)ky * nxh + kx;
+    if (valid) {
+#pragma unroll 4
+        for (int j = 0; j < E; ++j) {
+            const int z = t + P * j;
+            cp_async8(&stg[stg_row<Z>(z) * TX + c], kpsi + base + (int64_t)z * zs);
+        }
+    }
+    cp_commit();
+    for (int i = tid; i < NZ; i += TH) tw[i] = twg[i];
+    float2 v[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = valid ? B[base + (int64_t)(t + P * j) * zs] : make_float2(0.f, 0.f);
+    if (pf) prefetch_ztile<NZ, TX>(kpsi, B, pf, nxh, zs, tid, TH);
+    __syncthreads();
+    fft_d1_to_d2<NZ, E, TX, -1, BarCta, Z::PADG>(v, t, c, xb, tw);
+    cp_wait_all();
+    __syncthreads();  // psi^ staged by the other threads of the column is visible
+    // the noise pass stages through the thread's own psi^ slots, read only by itself
+    auto own = [&](int kz) { return stg_row<Z>(kz) * TX + c; };
+    propagate<Z, BarCta, false, false>(v, [&](int kz) { return stg[own(kz)]; }, stg, own, kx, ky, t, nx, ny, valid, a,
+                                       k0, flag);
+    store_state<Z>(v, kpsi, base, zs, t, valid, true);
+    if (a.final_step) return;
+    fft_d2_to_d1<NZ, E, TX, 1, BarCta, Z::PADG>(v, t, c, xb, tw);
+    store_state<Z>(v, A, base, zs, t, valid, false);
+}
+
 __device__ __forceinline__ void bar_arrive(int id, int count) {
     asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
@@ -242,8 +331,9 @@ __global__ void __launch_bounds__(Z::T, 1) k_zpipe(float2* A, const float2* __re
         } else {
             fft_d1_to_d2<NZ, E, TX, -1, BarNamed<1, TH>, Z::PADG>(v, t, c, regA, tw);
             bar_sync(3, T);
-            propagate<Z, BarNamed<1, TH>>(v, [&](int kz) { return nh[nh_slot<Z>(kz, c)]; }, regA, kx, ky, t, c, nx,
-                                          ny, valid, a, k0, flag);
+            auto own = [&](int kz) { return kz * TX + c; };
+            propagate<Z, BarNamed<1, TH>, true, true>(v, [&](int kz) { return nh[nh_slot<Z>(kz, c)]; }, regA, own, kx,
+                                                      ky, t, nx, ny, valid, a, k0, flag);
             if (has_next) bar_arrive(4, T);  // N^ slots free for the next tile
             if (!a.final_step) fft_d2_to_d1<NZ, E, TX, 1, BarNamed<1, TH>, Z::PADG>(v, t, c, regA, tw);
             store_state<Z>(v, A, base, zs, t, valid, a.final_step);
@@ -262,14 +352,31 @@ template <class Z>
 cudaError_t zattr() {
     cudaError_t e = cudaFuncSetAttribute(k_zcol<Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Z::SMEM);
     if (e) return e;
+    if ((e = cudaFuncSetAttribute(k_zcarry<Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Z::SMEM_CARRY)))
+        return e;
     return cudaFuncSetAttribute(k_zpipe<Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Z::SMEM_PIPE);
+}
+
+ZArgsF zargs_f(const ZPropArgs& p) {
+    const double tp = 6.283185307179586232;
+    return ZArgsF{(float)p.dt, (float)p.eps, (float)p.C, (float)p.namp_eff, (float)(tp / p.lx), (float)(tp / p.ly),
+                  (float)(tp / p.lz), p.seed, p.counter, p.dev_counter, p.use_noise, p.final_step};
+}
+
+template <class Z>
+cudaError_t zlaunch_carry(const pfc_ctx* c, void* kpsi, void* A, const void* B, const ZPropArgs& p) {
+    const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
+    static const int per_sm = resident_ctas(k_zcarry<Z>, Z::TH, Z::SMEM_CARRY);
+    dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny);
+    k_zcarry<Z><<<grid, Z::TH, Z::SMEM_CARRY, c->stream>>>((float2*)kpsi, (float2*)A, (const float2*)B, c->nx, c->ny,
+                                                           zargs_f(p), c->k0, c->flag, tw,
+                                                           prefetch_ahead(c, per_sm, kpsi, B));
+    return cudaGetLastError();
 }
 
 template <class Z>
 cudaError_t zlaunch(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& p) {
-    const double tp = 6.283185307179586232;
-    ZArgsF a{(float)p.dt, (float)p.eps, (float)p.C, (float)p.namp_eff, (float)(tp / p.lx), (float)(tp / p.ly),
-             (float)(tp / p.lz), p.seed, p.counter, p.dev_counter, p.use_noise, p.final_step};
+    const ZArgsF a = zargs_f(p);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
     const int ntx = (c->nxh + Z::TX - 1) / Z::TX;
     if (c->z_pipe) {
@@ -278,9 +385,10 @@ cudaError_t zlaunch(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& p
         k_zpipe<Z><<<grid, Z::T, Z::SMEM_PIPE, c->stream>>>((float2*)A, (const float2*)B, c->nx, c->ny, a, c->k0,
                                                              c->flag, tw);
     } else {
+        static const int per_sm = resident_ctas(k_zcol<Z>, Z::T, Z::SMEM);
         dim3 grid(ntx, c->ny);
         k_zcol<Z><<<grid, Z::T, Z::SMEM, c->stream>>>((float2*)A, (const float2*)B, c->nx, c->ny, a, c->k0, c->flag,
-                                                       tw);
+                                                       tw, prefetch_ahead(c, per_sm, A, B));
     }
     return cudaGetLastError();
 }
@@ -306,6 +414,16 @@ cudaError_t set_zcol_attributes(const pfc_ctx* c) {
         case 4: return zattr<Z64>();
     }
     return cudaSuccess;
+}
+
+cudaError_t launch_zcarry(const pfc_ctx* c, void* kpsi, void* A, const void* B, const ZPropArgs& a) {
+    switch (c->fused_z) {
+        case 1: return zlaunch_carry<Z512>(c, kpsi, A, B, a);
+        case 2: return zlaunch_carry<Z256>(c, kpsi, A, B, a);
+        case 3: return zlaunch_carry<Z128>(c, kpsi, A, B, a);
+        case 4: return zlaunch_carry<Z64>(c, kpsi, A, B, a);
+    }
+    return cudaErrorNotSupported;
 }
 
 cudaError_t launch_zcol(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a) {

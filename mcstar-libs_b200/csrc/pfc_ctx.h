@@ -56,6 +56,7 @@ struct pfc_ctx {
     int plane_tw_off;             // twiddles of the plane kernel: W_ny^m, W_{nx/2}^m, W_nx^k (k <= nx/2)
     int fused_z;                  // 0: general z pass; otherwise the register z kernel variant id
     int z_pipe;                   // register z pass as the persistent pipelined kernel (1) or one tile per CTA (0)
+    int z_carry;                  // carry psi^ itself (A = IFFT_z(psi^)/nz lives in work2) instead of A
     int num_sms;                  // multiprocessors of the device the context was made on
     int zcol_tw_off;              // twiddles of the register z kernel: W_nz^m
     int fused_y, fused_x;         // register y / x pass variants (0: none)
@@ -63,17 +64,39 @@ struct pfc_ctx {
     int xpass_tw_off;             // W_{nx/2}^m, then W_nx^k (k <= nx/2)
     int xy_mode;                  // 0 general passes, 1 cluster plane kernel, 2 register y/x/y passes
     int slab;                     // z-planes per slab of the register xy passes (0: whole field)
+    float pf_waves;               // L2 prefetch distance of the register passes, in waves of CTAs (0: off)
     // tracing (pfc_profile_enable / pfc_profile_read)
     bool prof_on = false;
     long long launches = 0;
-    long long prof_calls[PFC_PROFILE_FAMILIES] = {0, 0, 0};
-    double prof_ms[PFC_PROFILE_FAMILIES] = {0.0, 0.0, 0.0};
+    long long prof_calls[PFC_PROFILE_FAMILIES] = {};
+    double prof_ms[PFC_PROFILE_FAMILIES] = {};
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
-    std::vector<std::pair<int, size_t>> ev_pending;   // (family, index of the start event)
+    struct Span { int family; size_t from, to; };     // elapsed time between two pool events
+    std::vector<Span> ev_pending;
 };
 
 namespace pfc {
+
+// Resident CTAs per SM of a kernel launch shape (at least 1).
+template <class K>
+int resident_ctas(K kernel, int threads, size_t smem) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess) {
+        (void)cudaGetLastError();
+        n = 1;
+    }
+    return n > 0 ? n : 1;
+}
+
+// Tiles ahead of the L2 prefetch of a register pass whose CTAs run `per_sm` to an SM:
+// pf_waves full waves; 0 (off) unless every prefetched field starts on a 16-byte boundary
+// (field sizes are multiples of 16 bytes for every shape the register passes take).
+inline int prefetch_ahead(const pfc_ctx* c, int per_sm, const void* f0, const void* f1 = nullptr) {
+    if (c->pf_waves <= 0.f) return 0;
+    if (((uintptr_t)f0 & 15) || ((uintptr_t)f1 & 15)) return 0;
+    return (int)(c->pf_waves * (float)(c->num_sms * per_sm) + 0.5f);
+}
 
 // ---- general FFT passes (kern_fft.cu) ----
 cudaError_t set_fft_attributes(const pfc_ctx* c);
@@ -109,6 +132,8 @@ cudaError_t launch_xpass(const pfc_ctx* c, void* b, const void* pot, double mul,
 int fused_z_variant(int nx, int nz, int dtype);
 cudaError_t set_zcol_attributes(const pfc_ctx* c);
 cudaError_t launch_zcol(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a);
+// the z pass that carries psi^: reads psi^ (kpsi) and B, writes psi^' and (unless last) A'
+cudaError_t launch_zcarry(const pfc_ctx* c, void* kpsi, void* A, const void* B, const ZPropArgs& a);
 
 // ---- pointwise kernels, noise and reductions (kern_point.cu) ----
 cudaError_t launch_update_eom(const pfc_ctx* c, void* kpsi, const void* knl, const void* knoise,

@@ -129,6 +129,15 @@ __device__ __forceinline__ void dsmem_st(uint32_t addr, float2 v) {
     asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
 }
 
+// L2 prefetch of the bytes [p, p + n), widened to 16-byte bounds: the buffer holding
+// them must start on a 16-byte boundary and span a multiple of 16 bytes, so that the
+// widened range stays inside it.  A hint: nothing waits on it.
+__device__ __forceinline__ void l2_prefetch(const void* p, unsigned n) {
+    const uintptr_t a = (uintptr_t)p & ~(uintptr_t)15;
+    const uintptr_t e = ((uintptr_t)p + n + 15) & ~(uintptr_t)15;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
+}
+
 // Exchange slots: group g of NG interleaved groups, logical index (a, b) of an
 // E x P matrix -> (a P + b) NG + a PADG + g.  Warps run over consecutive g (and, when
 // NG < 32, over 32/NG consecutive t); PADG shifts successive blocks of P rows so that

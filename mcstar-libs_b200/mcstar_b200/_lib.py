@@ -47,9 +47,13 @@ class PfcStepParams(ctypes.Structure):
                 ("lz", ctypes.c_double), ("seed", ctypes.c_uint64), ("counter", ctypes.c_uint64)]
 
 
+PROFILE_FAMILIES = 5  # PFC_PROFILE_FAMILIES
+
+
 class PfcProfile(ctypes.Structure):
-    _fields_ = [("launches", ctypes.c_longlong), ("calls", ctypes.c_longlong * 3), ("ms", ctypes.c_double * 3),
-                ("xy_variant", ctypes.c_int)]
+    _fields_ = [("launches", ctypes.c_longlong), ("calls", ctypes.c_longlong * PROFILE_FAMILIES),
+                ("ms", ctypes.c_double * PROFILE_FAMILIES), ("xy_variant", ctypes.c_int), ("xy_mode", ctypes.c_int),
+                ("z_mode", ctypes.c_int)]
 
 
 _lib = None

@@ -144,13 +144,14 @@ class Context:
         check(lib().pfc_profile_enable(self._h, int(bool(on))), self._h, "pfc_profile_enable")
 
     def profile_read(self):
-        """{"launches": n, "calls": [3], "ms": [3]} since profile_enable (families:
-        0 entry/exit, 1 xy part of a step, 2 z pass)."""
+        """{"launches": n, "calls": [5], "ms": [5]} since profile_enable (families:
+        0 entry/exit, 1 xy part of a step, 2 z pass, 3 register y passes, 4 register x
+        pass; 3 and 4 are also counted inside 1)."""
         self._sync_stream()
         p = _lib.PfcProfile()
         check(lib().pfc_profile_read(self._h, ctypes.byref(p)), self._h, "pfc_profile_read")
         return {"launches": int(p.launches), "calls": [int(v) for v in p.calls], "ms": [float(v) for v in p.ms],
-                "xy_variant": int(p.xy_variant)}
+                "xy_variant": int(p.xy_variant), "xy_mode": int(p.xy_mode), "z_mode": int(p.z_mode)}
 
     def free_energy(self, kpsi, eps, lens, hh):
         out = ctypes.c_double()
