@@ -178,11 +178,23 @@ ZPropArgs zargs(const pfc_ctx* c, const pfc_step_params* p) {
 void* carried_A(pfc_ctx* ctx, void* kpsi) { return ctx->z_carry ? ctx->work2 : kpsi; }
 
 // psi^ -> A = IFFT_z(psi^)/nz; the k = 0 mode is kept in FP64
+// complex FFT along z of a half-spectrum field: the register column kernel where the
+// length has one, else the general column pass
+cudaError_t zcols(const pfc_ctx* ctx, int dir, const void* in, void* out, double scale) {
+    if (ctx->fused_zfft) return launch_zfft(ctx, dir, in, out, scale);
+    return launch_cols(ctx, 2, dir, in, out, scale);
+}
+// the same along y (register kernel only together with the register x rows)
+cudaError_t ycols(const pfc_ctx* ctx, int dir, const void* in, void* out) {
+    if (ctx->fused_y && ctx->fused_x) return launch_ypass(ctx, dir, in, out, 1.0, ctx->nz);
+    return launch_cols(ctx, 1, dir, in, out, 1.0);
+}
+
 cudaError_t step_entry(pfc_ctx* ctx, void* kpsi) {
     return traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
         cudaError_t e = launch_k0_save(ctx, kpsi);
         if (e || ctx->nz == 1) return e;
-        return launch_cols(ctx, 2, 1, kpsi, carried_A(ctx, kpsi), 1.0 / ctx->nz);
+        return zcols(ctx, 1, kpsi, carried_A(ctx, kpsi), 1.0 / ctx->nz);
     });
 }
 
@@ -191,7 +203,7 @@ cudaError_t step_entry(pfc_ctx* ctx, void* kpsi) {
 cudaError_t step_exit(pfc_ctx* ctx, void* kpsi) {
     if (ctx->z_carry) return cudaSuccess;
     return traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
-        cudaError_t e = ctx->nz > 1 ? launch_cols(ctx, 2, -1, kpsi, kpsi, 1.0) : cudaSuccess;
+        cudaError_t e = ctx->nz > 1 ? zcols(ctx, -1, kpsi, kpsi, 1.0) : cudaSuccess;
         if (e) return e;
         return launch_k0_restore(ctx, kpsi);
     });
@@ -358,6 +370,10 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
         roots(c->nx / 2, c->nx / 2);
         roots(c->nx, c->nx / 2 + 1);
     }
+    // (its line stride ny (nx/2+1) is a 32-bit int)
+    c->fused_zfft = c->nz > 1 && c->n_cmpl < (1ull << 31) ? fused_zfft_variant(c->nz, c->dtype) : 0;
+    c->zfft_tw_off = (int)tab.size();
+    if (c->fused_zfft) roots(c->nz, c->nz);
     // xy part of a step: register passes where available, else the cluster plane kernel,
     // else the general passes; PFC_XY_MODE=0|1|2 overrides (for measurements).
     c->xy_mode = c->fused_y ? 2 : (c->fused_xy ? 1 : 0);
@@ -433,6 +449,7 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
     if (e == cudaSuccess && c->fused_xy) e = set_fused_attributes(c);
     if (e == cudaSuccess && c->fused_z) e = set_zcol_attributes(c);
     if (e == cudaSuccess && c->fused_y) e = set_pass_attributes(c);
+    if (e == cudaSuccess && c->fused_zfft) e = set_zfft_attributes(c);
     if (e != cudaSuccess) {
         free_ctx(c);
         return PFC_ERR_CUDA;
@@ -465,19 +482,24 @@ size_t pfc_workspace_bytes(const pfc_ctx* ctx) {
 pfc_status pfc_fft_r2c(pfc_ctx* ctx, const void* in, void* out) {
     PFC_CHECK_CTX();
     if (!in || !out) return fail(ctx, PFC_ERR_INVALID, "pfc_fft_r2c: null buffer");
-    PFC_CUDA(launch_rows_r2c(ctx, in, out), "pfc_fft_r2c rows");
-    if (ctx->ny > 1) PFC_CUDA(launch_cols(ctx, 1, -1, out, out, 1.0), "pfc_fft_r2c y");
-    if (ctx->nz > 1) PFC_CUDA(launch_cols(ctx, 2, -1, out, out, 1.0), "pfc_fft_r2c z");
+    const bool reg_xy = ctx->fused_x && ctx->fused_y;
+    if (reg_xy) PFC_CUDA(launch_xrows_r2c(ctx, in, out), "pfc_fft_r2c rows");
+    else PFC_CUDA(launch_rows_r2c(ctx, in, out), "pfc_fft_r2c rows");
+    if (ctx->ny > 1) PFC_CUDA(ycols(ctx, -1, out, out), "pfc_fft_r2c y");
+    if (ctx->nz > 1) PFC_CUDA(zcols(ctx, -1, out, out, 1.0), "pfc_fft_r2c z");
+    ctx->launches += 1 + (ctx->ny > 1) + (ctx->nz > 1);
     return PFC_OK;
 }
 
 pfc_status pfc_fft_c2r(pfc_ctx* ctx, const void* in, void* out) {
     PFC_CHECK_CTX();
     if (!in || !out) return fail(ctx, PFC_ERR_INVALID, "pfc_fft_c2r: null buffer");
-    const void* src = in;
-    if (ctx->nz > 1) { PFC_CUDA(launch_cols(ctx, 2, 1, src, ctx->work, 1.0), "pfc_fft_c2r z"); src = ctx->work; }
-    if (ctx->ny > 1) { PFC_CUDA(launch_cols(ctx, 1, 1, src, ctx->work, 1.0), "pfc_fft_c2r y"); src = ctx->work; }
-    PFC_CUDA(launch_rows_c2r(ctx, src, out), "pfc_fft_c2r rows");
+    const void* src = in;  // the input is left unchanged: the passes run in the workspace
+    if (ctx->nz > 1) { PFC_CUDA(zcols(ctx, 1, src, ctx->work, 1.0), "pfc_fft_c2r z"); src = ctx->work; }
+    if (ctx->ny > 1) { PFC_CUDA(ycols(ctx, 1, src, ctx->work), "pfc_fft_c2r y"); src = ctx->work; }
+    if (ctx->fused_x && ctx->fused_y) PFC_CUDA(launch_xrows_c2r(ctx, src, out), "pfc_fft_c2r rows");
+    else PFC_CUDA(launch_rows_c2r(ctx, src, out), "pfc_fft_c2r rows");
+    ctx->launches += 1 + (ctx->ny > 1) + (ctx->nz > 1);
     return PFC_OK;
 }
 

@@ -32,7 +32,10 @@ struct YCfg {
 
 template <class Y, int DIR>
 __global__ void __launch_bounds__(Y::T, Y::MINB)
-    k_ycol(const float2* in, float2* out, int nxh, const float2* __restrict__ twg, float scale, int pf) {
+    k_ycol(const float2* in, float2* out, int nxh, int64_t ps, int ls, const float2* __restrict__ twg, float scale,
+           int pf) {
+    // columns of NY elements ls apart, starting at kx + blockIdx.y * ps: y columns of one
+    // z-plane (ps = ny nxh, ls = nxh) or z columns at one ky (ps = nxh, ls = ny nxh)
     constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P, U = Y::U;
     extern __shared__ __align__(16) float2 sm[];
     float2* xb = sm;
@@ -42,19 +45,19 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
     const int c = tid % TX, t = tid / TX;
     const int kx = blockIdx.x * TX + c;
     const bool valid = kx < nxh;
-    const int64_t base = (int64_t)blockIdx.y * NY * nxh + kx;
+    const int64_t base = (int64_t)blockIdx.y * ps + kx;
     float2 v[E];
 #pragma unroll
-    for (int j = 0; j < E; ++j) v[j] = valid ? in[base + (int64_t)(t + P * j) * nxh] : make_float2(0.f, 0.f);
+    for (int j = 0; j < E; ++j) v[j] = valid ? in[base + (int64_t)(t + P * j) * ls] : make_float2(0.f, 0.f);
     if (pf) {
-        // L2 prefetch of the tile pf tiles ahead in launch order: its column segment of every y row
+        // L2 prefetch of the tile pf tiles ahead in launch order: its segment of every line
         const int ntx = (int)gridDim.x;
         const int tgt = (int)(blockIdx.y * gridDim.x + blockIdx.x) + pf;
         if (tgt < ntx * (int)gridDim.y) {
             const int kx0 = (tgt % ntx) * TX;
-            const float2* f = in + (int64_t)(tgt / ntx) * NY * nxh + kx0;
+            const float2* f = in + (int64_t)(tgt / ntx) * ps + kx0;
             const unsigned bytes = (unsigned)(min(TX, nxh - kx0) * sizeof(float2));
-            for (int y = tid; y < NY; y += Y::T) l2_prefetch(f + (int64_t)y * nxh, bytes);
+            for (int y = tid; y < NY; y += Y::T) l2_prefetch(f + (int64_t)y * ls, bytes);
         }
     }
     __syncthreads();
@@ -65,7 +68,7 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
 #pragma unroll
             for (int k2 = 0; k2 < P; ++k2) {
                 const float2 w = v[u * P + k2];
-                out[base + (int64_t)((t * U + u) + E * k2) * nxh] = make_float2(w.x * scale, w.y * scale);
+                out[base + (int64_t)((t * U + u) + E * k2) * ls] = make_float2(w.x * scale, w.y * scale);
             }
     }
 }
@@ -81,11 +84,16 @@ struct XCfg {
     static_assert(P * E == M && U * P == E && (R % 32 == 0 || R == 16) && R * P == T, "shape");
 };
 
-template <class X>
+// MODE 0: the step's x pass, in place (in == out).  MODE 1: R2C of real rows (in: rows
+// of M float2 pairs x[2m] + i x[2m+1]) into half-spectrum rows (out: rows of NXH).
+// MODE 2: C2R of half-spectrum rows (in) into real rows (out, M pairs per row).  The
+// transforms are unnormalised, as cufft_wrapper.hpp:61-86.
+template <class X, int MODE>
 __global__ void __launch_bounds__(X::T, X::MINB)
-    k_xrow(float2* buf, const float* __restrict__ pot, int nrows, const float2* __restrict__ twg, float mul, float Cc,
-           float mu, int pf) {
+    k_xrow(const float2* in, float2* out, const float* __restrict__ pot, int nrows, const float2* __restrict__ twg,
+           float mul, float Cc, float mu, int pf) {
     constexpr int NX = X::NX, M = X::M, NXH = X::NXH, E = X::E, P = X::P, U = X::U, R = X::R, LDR = X::LDR;
+    constexpr int LIN = MODE == 1 ? M : NXH;  // input row length (float2)
     extern __shared__ __align__(16) float2 sm[];
     float2* rb = sm;
     float2* twM = sm + X::BUF;  // W_M^m, m < M
@@ -95,43 +103,67 @@ __global__ void __launch_bounds__(X::T, X::MINB)
     const int r = tid % R, t = tid / R;
     const int row0 = blockIdx.x * R;
     const int nr = min(R, nrows - row0);
-    const int64_t g0 = (int64_t)row0 * NXH;
-    for (int i = tid; i < nr * NXH; i += X::T) rb[i] = buf[g0 + i];
+    const int64_t g0 = (int64_t)row0 * LIN;
+    if constexpr (LIN == LDR) {
+        for (int i = tid; i < nr * LIN; i += X::T) rb[i] = in[g0 + i];
+    } else {
+        for (int i = tid; i < nr * LIN; i += X::T) rb[(i / LIN) * LDR + i % LIN] = in[g0 + i];
+    }
     if (pf) {
         // L2 prefetch of the rows of the CTA pf CTAs ahead, in 4 KB pieces
         const int row1 = (blockIdx.x + pf) * R;
         if (row1 < nrows) {
-            const int64_t e0 = (int64_t)row1 * NXH;
-            const int64_t n = (int64_t)min(R, nrows - row1) * NXH;
+            const int64_t e0 = (int64_t)row1 * LIN;
+            const int64_t n = (int64_t)min(R, nrows - row1) * LIN;
             constexpr int kPiece = 512;  // float2
             for (int64_t i = (int64_t)tid * kPiece; i < n; i += (int64_t)X::T * kPiece)
-                l2_prefetch(buf + e0 + i, (unsigned)(min((int64_t)kPiece, n - i) * sizeof(float2)));
+                l2_prefetch(in + e0 + i, (unsigned)(min((int64_t)kPiece, n - i) * sizeof(float2)));
         }
     }
     __syncthreads();
     float2 v[E];
+    if constexpr (MODE != 1) {
 #pragma unroll
-    for (int j = 0; j < E; ++j) {
-        const int k = t + P * j;
-        v[j] = c2r_pre_f(rb[r * LDR + k], rb[r * LDR + M - k], twP[k]);
-    }
-    fft_d1_to_d2<M, E, R, 1>(v, t, r, rb, twM);
-    const int64_t prow = (int64_t)(row0 + r) * NX;
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-#pragma unroll
-        for (int k2 = 0; k2 < P; ++k2) {
-            const int n = (t * U + u) + E * k2;
-            const float2 x = v[u * P + k2];
-            const float a = x.x * mul, b = x.y * mul;
-            float2 o = make_float2(a * a * a - Cc * a - mu, b * b * b - Cc * b - mu);
-            if (pot && r < nr) {
-                const float2 pp = *reinterpret_cast<const float2*>(pot + prow + 2 * n);
-                o.x += pp.x;
-                o.y += pp.y;
-            }
-            v[u * P + k2] = o;
+        for (int j = 0; j < E; ++j) {
+            const int k = t + P * j;
+            v[j] = c2r_pre_f(rb[r * LDR + k], rb[r * LDR + M - k], twP[k]);
         }
+        fft_d1_to_d2<M, E, R, 1>(v, t, r, rb, twM);
+    }
+    if constexpr (MODE == 2) {
+        // real pairs out through shared memory, so that rows are stored contiguously
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int k2 = 0; k2 < P; ++k2) rb[r * LDR + (t * U + u) + E * k2] = v[u * P + k2];
+        __syncthreads();
+        for (int i = tid; i < nr * M; i += X::T) out[(int64_t)row0 * M + i] = rb[(i / M) * LDR + i % M];
+        return;
+    }
+    if constexpr (MODE == 1) {
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int k2 = 0; k2 < P; ++k2) v[u * P + k2] = rb[r * LDR + (t * U + u) + E * k2];
+    } else {
+        const int64_t prow = (int64_t)(row0 + r) * NX;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int k2 = 0; k2 < P; ++k2) {
+                const int n = (t * U + u) + E * k2;
+                const float2 x = v[u * P + k2];
+                const float a = x.x * mul, b = x.y * mul;
+                float2 o = make_float2(a * a * a - Cc * a - mu, b * b * b - Cc * b - mu);
+                if (pot && r < nr) {
+                    const float2 pp = *reinterpret_cast<const float2*>(pot + prow + 2 * n);
+                    o.x += pp.x;
+                    o.y += pp.y;
+                }
+                v[u * P + k2] = o;
+            }
+    }
     fft_d2_to_d1<M, E, R, -1>(v, t, r, rb, twM);
     __syncthreads();
 #pragma unroll
@@ -150,7 +182,8 @@ __global__ void __launch_bounds__(X::T, X::MINB)
     for (int j = 0; j < E; ++j) rb[r * LDR + t + P * j] = v[j];
     if (t == 0) rb[r * LDR + M] = xm_last;
     __syncthreads();
-    for (int i = tid; i < nr * NXH; i += X::T) buf[g0 + i] = rb[i];
+    const int64_t o0 = (int64_t)row0 * NXH;
+    for (int i = tid; i < nr * NXH; i += X::T) out[o0 + i] = rb[i];
 }
 
 using Y512 = YCfg<512, 32, 8>;
@@ -172,30 +205,47 @@ cudaError_t yattr() {
 }
 template <class X>
 cudaError_t xattr() {
-    return cudaFuncSetAttribute(k_xrow<X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)X::SMEM);
+    cudaError_t e = cudaFuncSetAttribute(k_xrow<X, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)X::SMEM);
+    if (!e) e = cudaFuncSetAttribute(k_xrow<X, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)X::SMEM);
+    if (!e) e = cudaFuncSetAttribute(k_xrow<X, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)X::SMEM);
+    return e;
 }
 
+// complex FFTs of the columns (lines of Y::NY elements ls apart) of the kx tiles of
+// `planes` planes ps apart; twiddles W_NY^m at tw_off
 template <class Y>
-cudaError_t ylaunch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs) {
-    dim3 grid((c->nxh + Y::TX - 1) / Y::TX, nzs);
-    const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->ypass_tw_off;
+cudaError_t collaunch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int planes, int64_t ps,
+                      int ls, int tw_off) {
+    dim3 grid((c->nxh + Y::TX - 1) / Y::TX, planes);
+    const float2* tw = reinterpret_cast<const float2*>(c->tw) + tw_off;
     static const int per_sm = resident_ctas(k_ycol<Y, 1>, Y::T, Y::SMEM);
     const int pf = prefetch_ahead(c, per_sm, in);
     if (dir > 0)
-        k_ycol<Y, 1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, tw, (float)scale, pf);
+        k_ycol<Y, 1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, ps, ls, tw,
+                                                         (float)scale, pf);
     else
-        k_ycol<Y, -1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, tw, (float)scale,
-                                                          pf);
+        k_ycol<Y, -1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, ps, ls, tw,
+                                                          (float)scale, pf);
     return cudaGetLastError();
 }
-template <class X>
-cudaError_t xlaunch(const pfc_ctx* c, void* b, const void* pot, double mul, double C, double mu, int nzs) {
-    const int nrows = nzs * c->ny;
+template <class Y>
+cudaError_t ylaunch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs) {
+    return collaunch<Y>(c, dir, in, out, scale, nzs, (int64_t)c->ny * c->nxh, c->nxh, c->ypass_tw_off);
+}
+template <class Y>
+cudaError_t zlaunch_fft(const pfc_ctx* c, int dir, const void* in, void* out, double scale) {
+    // z line stride ny nxh: an int for every shape with fewer than 2^31 complex modes
+    return collaunch<Y>(c, dir, in, out, scale, c->ny, c->nxh, c->ny * c->nxh, c->zfft_tw_off);
+}
+template <class X, int MODE>
+cudaError_t xlaunch(const pfc_ctx* c, const void* in, void* out, const void* pot, double mul, double C, double mu,
+                    int nrows) {
     dim3 grid((nrows + X::R - 1) / X::R);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->xpass_tw_off;
-    static const int per_sm = resident_ctas(k_xrow<X>, X::T, X::SMEM);
-    k_xrow<X><<<grid, X::T, X::SMEM, c->stream>>>((float2*)b, (const float*)pot, nrows, tw, (float)mul, (float)C,
-                                                 (float)mu, prefetch_ahead(c, per_sm, b));
+    static const int per_sm = resident_ctas(k_xrow<X, MODE>, X::T, X::SMEM);
+    k_xrow<X, MODE><<<grid, X::T, X::SMEM, c->stream>>>((const float2*)in, (float2*)out, (const float*)pot, nrows, tw,
+                                                        (float)mul, (float)C, (float)mu,
+                                                        prefetch_ahead(c, per_sm, in));
     return cudaGetLastError();
 }
 
@@ -261,13 +311,54 @@ cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, d
     return cudaErrorNotSupported;
 }
 
-cudaError_t launch_xpass(const pfc_ctx* c, void* b, const void* pot, double mul, double C, double mu, int nzs) {
+template <int MODE>
+cudaError_t xdispatch(const pfc_ctx* c, const void* in, void* out, const void* pot, double mul, double C, double mu,
+                      int nrows) {
     switch (c->fused_x) {
-        case 1: return xlaunch<X512>(c, b, pot, mul, C, mu, nzs);
-        case 2: return xlaunch<X256>(c, b, pot, mul, C, mu, nzs);
-        case 3: return xlaunch<X128>(c, b, pot, mul, C, mu, nzs);
-        case 4: return xlaunch<X64>(c, b, pot, mul, C, mu, nzs);
-        case 5: return xlaunch<X512h>(c, b, pot, mul, C, mu, nzs);
+        case 1: return xlaunch<X512, MODE>(c, in, out, pot, mul, C, mu, nrows);
+        case 2: return xlaunch<X256, MODE>(c, in, out, pot, mul, C, mu, nrows);
+        case 3: return xlaunch<X128, MODE>(c, in, out, pot, mul, C, mu, nrows);
+        case 4: return xlaunch<X64, MODE>(c, in, out, pot, mul, C, mu, nrows);
+        case 5: return xlaunch<X512h, MODE>(c, in, out, pot, mul, C, mu, nrows);
+    }
+    return cudaErrorNotSupported;
+}
+
+cudaError_t launch_xpass(const pfc_ctx* c, void* b, const void* pot, double mul, double C, double mu, int nzs) {
+    return xdispatch<0>(c, b, b, pot, mul, C, mu, nzs * c->ny);
+}
+cudaError_t launch_xrows_r2c(const pfc_ctx* c, const void* in_real, void* out_cmpl) {
+    return xdispatch<1>(c, in_real, out_cmpl, nullptr, 1.0, 0.0, 0.0, c->ny * c->nz);
+}
+cudaError_t launch_xrows_c2r(const pfc_ctx* c, const void* in_cmpl, void* out_real) {
+    return xdispatch<2>(c, in_cmpl, out_real, nullptr, 1.0, 0.0, 0.0, c->ny * c->nz);
+}
+
+int fused_zfft_variant(int nz, int dtype) {
+    if (dtype != PFC_F32) return 0;
+    switch (nz) {
+        case 512: return 1;
+        case 256: return 2;
+        case 128: return 3;
+        case 64: return 4;
+    }
+    return 0;
+}
+cudaError_t set_zfft_attributes(const pfc_ctx* c) {
+    switch (c->fused_zfft) {
+        case 1: return yattr<Y512>();
+        case 2: return yattr<Y256>();
+        case 3: return yattr<Y128>();
+        case 4: return yattr<Y64>();
+    }
+    return cudaSuccess;
+}
+cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, double scale) {
+    switch (c->fused_zfft) {
+        case 1: return zlaunch_fft<Y512>(c, dir, in, out, scale);
+        case 2: return zlaunch_fft<Y256>(c, dir, in, out, scale);
+        case 3: return zlaunch_fft<Y128>(c, dir, in, out, scale);
+        case 4: return zlaunch_fft<Y64>(c, dir, in, out, scale);
     }
     return cudaErrorNotSupported;
 }

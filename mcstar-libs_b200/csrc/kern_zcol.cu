@@ -48,15 +48,25 @@ struct ZCfg {
 
 template <class Z> __device__ __forceinline__ int nh_slot(int kz, int c) { return kz * Z::TX + c + (kz / Z::U) * 8; }
 
+// Row of mode kz in a [row][c] tile of modes (TX = 8 float2 per row: the N^ hand-over
+// and the psi^ staging).  A warp touches the modes kz = t U + u + E k2 of four
+// consecutive t at once; with U = 2 those rows all have the parity of u, so rows are
+// swapped in pairs for odd t, which puts two t-groups in each half of the 32 banks (two
+// wavefronts, the minimum for 8-byte accesses).  A permutation of the rows: no padding.
+template <class Z> __device__ __forceinline__ int stg_row(int kz) {
+    if constexpr (Z::U == 2) return kz ^ ((kz >> 1) & 1);
+    else return kz;
+}
+
 // The update of the thread's modes kz = (t U + u) + E k2 of column kx at ky; the result
 // replaces v.  kPsiInV: v holds psi^ and other(kz) returns N^; otherwise v holds N^ and
 // other(kz) returns psi^.  The noise pass is staged through the thread's own slots
-// scratch[slot(kz)]; kSync puts a barrier of the transforming threads (Bar) first, for
+// scratch[slot(kz)]; kSync puts a barrier of the transforming threads (bar) first, for
 // a scratch that is an exchange buffer other threads may still be reading.
-template <class Z, class Bar, bool kPsiInV, bool kSync, class OTHER, class SLOT>
-__device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2* scratch, SLOT slot, int kx, int ky,
-                                          int t, int nx, int ny, bool valid, const ZArgsF& a, const double2* k0,
-                                          int* flag) {
+template <class Z, bool kPsiInV, bool kSync, class Bar, class OTHER, class SLOT>
+__device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2* scratch, SLOT slot, const Bar& bar,
+                                          int kx, int ky, int t, int nx, int ny, bool valid, const ZArgsF& a,
+                                          const double2* k0, int* flag) {
     constexpr int NZ = Z::NZ, E = Z::E, P = Z::P, U = Z::U;
     // wavenumbers K(i) = i' * 2 pi / L (common.hpp:27-28) with 2 pi / L precomputed
     const float k0x = (float)kx * a.ckx;
@@ -81,7 +91,7 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2
     if (a.use_noise) {
         // conserved k-space noise, dt namp sqrt(N) |k| xi / D(k): a compact loop over this
         // thread's modes, staged through its own slots (kept out of the unrolled body)
-        if (kSync) Bar::sync();
+        if (kSync) bar.sync();
         const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
 #pragma unroll
         for (int u = 0; u < U; ++u)
@@ -174,22 +184,22 @@ __global__ void __launch_bounds__(Z::T, 2) k_zcol(float2* A, const float2* __res
     for (int j = 0; j < E; ++j) v[j] = valid ? src[base + (int64_t)(t + P * j) * zs] : make_float2(0.f, 0.f);
     if (pf) prefetch_ztile<NZ, TX>(A, B, pf, nxh, zs, tid, Z::T);
     __syncthreads();
-    if (half == 0) {
-        fft_d1_to_d2<NZ, E, TX, -1, BarNamed<1, TH>, Z::PADG>(v, t, c, regA, tw);
-    } else {
-        fft_d1_to_d2<NZ, E, TX, -1, BarNamed<2, TH>, Z::PADG>(v, t, c, regB, tw);
-        BarNamed<2, TH>::sync();
+    // both halves run one copy of the forward transform, each on its own named barrier
+    const BarDyn bar{1 + half, TH};
+    fft_d1_to_d2<NZ, E, TX, -1, BarDyn, Z::PADG>(v, t, c, half ? regB : regA, tw, bar);
+    auto own = [&](int kz) { return stg_row<Z>(kz) * TX + c; };  // N^ hand-over slots, conflict-free
+    if (half != 0) {
+        bar.sync();
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int k2 = 0; k2 < P; ++k2) regB[((t * U + u) + E * k2) * TX + c] = v[u * P + k2];
+            for (int k2 = 0; k2 < P; ++k2) regB[own((t * U + u) + E * k2)] = v[u * P + k2];
     }
     __syncthreads();
     if (half != 0) return;
-    auto own = [&](int kz) { return kz * TX + c; };
-    propagate<Z, BarNamed<1, TH>, true, true>(v, [&](int kz) { return regB[own(kz)]; }, regB, own, kx, ky, t, nx, ny,
-                                              valid, a, k0, flag);
-    if (!a.final_step) fft_d2_to_d1<NZ, E, TX, 1, BarNamed<1, TH>, Z::PADG>(v, t, c, regA, tw);
+    propagate<Z, true, true>(v, [&](int kz) { return regB[own(kz)]; }, regB, own, bar, kx, ky, t, nx, ny, valid, a,
+                             k0, flag);
+    if (!a.final_step) fft_d2_to_d1<NZ, E, TX, 1, BarDyn, Z::PADG>(v, t, c, regA, tw, bar);
     store_state<Z>(v, A, base, zs, t, valid, a.final_step);
 }
 
@@ -200,14 +210,6 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// Row of mode kz in the psi^ staging tile ([row][c], TX = 8 float2 per row).  A warp
-// reads the modes kz = t U + u + E k2 of four consecutive t at once; with U = 2 those
-// rows all have the parity of u, so rows are swapped in pairs for odd t, which puts two
-// t-groups in each half of the 32 banks (two wavefronts, the minimum for 8-byte reads).
-template <class Z> __device__ __forceinline__ int stg_row(int kz) {
-    if constexpr (Z::U == 2) return kz ^ ((kz >> 1) & 1);
-    else return kz;
-}
 
 // The z pass when the state psi^ itself is carried (k-space, reference layout) and
 // A = IFFT_z(psi^)/nz is only the input of the next xy part.  The whole CTA works on
@@ -254,8 +256,8 @@ __global__ void __launch_bounds__(Z::TH, Z::CMINB) k_zcarry(float2* kpsi, float2
     __syncthreads();  // psi^ staged by the other threads of the column is visible
     // the noise pass stages through the thread's own psi^ slots, read only by itself
     auto own = [&](int kz) { return stg_row<Z>(kz) * TX + c; };
-    propagate<Z, BarCta, false, false>(v, [&](int kz) { return stg[own(kz)]; }, stg, own, kx, ky, t, nx, ny, valid, a,
-                                       k0, flag);
+    propagate<Z, false, false>(v, [&](int kz) { return stg[own(kz)]; }, stg, own, BarCta{}, kx, ky, t, nx, ny, valid,
+                               a, k0, flag);
     store_state<Z>(v, kpsi, base, zs, t, valid, true);
     if (a.final_step) return;
     fft_d2_to_d1<NZ, E, TX, 1, BarCta, Z::PADG>(v, t, c, xb, tw);
@@ -332,8 +334,8 @@ __global__ void __launch_bounds__(Z::T, 1) k_zpipe(float2* A, const float2* __re
             fft_d1_to_d2<NZ, E, TX, -1, BarNamed<1, TH>, Z::PADG>(v, t, c, regA, tw);
             bar_sync(3, T);
             auto own = [&](int kz) { return kz * TX + c; };
-            propagate<Z, BarNamed<1, TH>, true, true>(v, [&](int kz) { return nh[nh_slot<Z>(kz, c)]; }, regA, own, kx,
-                                                      ky, t, nx, ny, valid, a, k0, flag);
+            propagate<Z, true, true>(v, [&](int kz) { return nh[nh_slot<Z>(kz, c)]; }, regA, own, BarNamed<1, TH>{},
+                                     kx, ky, t, nx, ny, valid, a, k0, flag);
             if (has_next) bar_arrive(4, T);  // N^ slots free for the next tile
             if (!a.final_step) fft_d2_to_d1<NZ, E, TX, 1, BarNamed<1, TH>, Z::PADG>(v, t, c, regA, tw);
             store_state<Z>(v, A, base, zs, t, valid, a.final_step);

@@ -60,6 +60,8 @@ struct pfc_ctx {
     int num_sms;                  // multiprocessors of the device the context was made on
     int zcol_tw_off;              // twiddles of the register z kernel: W_nz^m
     int fused_y, fused_x;         // register y / x pass variants (0: none)
+    int fused_zfft;               // register column kernel variant for plain z transforms (0: none)
+    int zfft_tw_off;              // W_nz^m of the plain z transforms
     int ypass_tw_off;             // W_ny^m
     int xpass_tw_off;             // W_{nx/2}^m, then W_nx^k (k <= nx/2)
     int xy_mode;                  // 0 general passes, 1 cluster plane kernel, 2 register y/x/y passes
@@ -127,6 +129,13 @@ cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, d
 // C2R, cubic term, R2C on the rows of nzs consecutive planes starting at b, in place;
 // pot (real field, or null) starts at the same first plane
 cudaError_t launch_xpass(const pfc_ctx* c, void* b, const void* pot, double mul, double C, double mu, int nzs);
+// unnormalised real transforms of every x row (register kernels; out of place)
+cudaError_t launch_xrows_r2c(const pfc_ctx* c, const void* in_real, void* out_cmpl);
+cudaError_t launch_xrows_c2r(const pfc_ctx* c, const void* in_cmpl, void* out_real);
+// complex FFT along z of a half-spectrum-shaped field with the register column kernel
+int fused_zfft_variant(int nz, int dtype);
+cudaError_t set_zfft_attributes(const pfc_ctx* c);
+cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, double scale);
 
 // ---- register-resident z pass (kern_zcol.cu) ----
 int fused_z_variant(int nx, int nz, int dtype);

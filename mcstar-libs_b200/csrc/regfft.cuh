@@ -117,6 +117,12 @@ struct BarCta {
 template <int ID, int COUNT> struct BarNamed {
     __device__ __forceinline__ static void sync() { asm volatile("bar.sync %0, %1;" ::"n"(ID), "n"(COUNT) : "memory"); }
 };
+// A named barrier whose id is chosen at run time: the thread groups of a CTA that run the
+// same transform on different data share one copy of its code.
+struct BarDyn {
+    int id, count;
+    __device__ __forceinline__ void sync() const { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory"); }
+};
 
 // Distributed shared memory: the 32-bit shared::cluster address of `local` in CTA
 // `rank` of this cluster, and an 8-byte store to it.
@@ -148,7 +154,8 @@ __device__ __forceinline__ int xslot(int a, int b, int g) {
 }
 
 template <int N, int E, int NG, int DIR, class Bar = BarCta, int PADG = 0>
-__device__ __forceinline__ void fft_d1_to_d2(float2 (&v)[E], int t, int g, float2* xb, const float2* twN) {
+__device__ __forceinline__ void fft_d1_to_d2(float2 (&v)[E], int t, int g, float2* xb, const float2* twN,
+                                             const Bar& bar = Bar{}) {
     constexpr int P = N / E, U = E / P;
     static_assert(P * E == N && U * P == E, "four-step shape");
     RF<E, DIR>::run(v);
@@ -158,10 +165,10 @@ __device__ __forceinline__ void fft_d1_to_d2(float2 (&v)[E], int t, int g, float
         if (DIR > 0) w.y = -w.y;
         v[k1] = cmul(v[k1], w);
     }
-    Bar::sync();
+    bar.sync();
 #pragma unroll
     for (int k1 = 0; k1 < E; ++k1) xb[xslot<N, E, NG, PADG>(k1, t, g)] = v[k1];
-    Bar::sync();
+    bar.sync();
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
@@ -171,7 +178,8 @@ __device__ __forceinline__ void fft_d1_to_d2(float2 (&v)[E], int t, int g, float
 }
 
 template <int N, int E, int NG, int DIR, class Bar = BarCta, int PADG = 0>
-__device__ __forceinline__ void fft_d2_to_d1(float2 (&v)[E], int t, int g, float2* xb, const float2* twN) {
+__device__ __forceinline__ void fft_d2_to_d1(float2 (&v)[E], int t, int g, float2* xb, const float2* twN,
+                                             const Bar& bar = Bar{}) {
     constexpr int P = N / E, U = E / P;
     static_assert(P * E == N && U * P == E, "four-step shape");
 #pragma unroll
@@ -186,12 +194,12 @@ __device__ __forceinline__ void fft_d2_to_d1(float2 (&v)[E], int t, int g, float
             v[u * P + k2] = cmul(v[u * P + k2], w);
         }
     }
-    Bar::sync();
+    bar.sync();
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
         for (int k2 = 0; k2 < P; ++k2) xb[xslot<N, E, NG, PADG>(t * U + u, k2, g)] = v[u * P + k2];
-    Bar::sync();
+    bar.sync();
 #pragma unroll
     for (int n1 = 0; n1 < E; ++n1) v[n1] = xb[xslot<N, E, NG, PADG>(n1, t, g)];
     RF<E, DIR>::run(v);

@@ -96,6 +96,21 @@ def test_small_and_odd_shapes(nshape):
     np.testing.assert_allclose(y / x.size, x, atol=1e-13)
 
 
+@pytest.mark.parametrize("nshape", [(64, 64, 64), (128, 64, 256), (512, 64, 128), (8, 512, 512), (64, 32, 64),
+                                    (256, 128, 512), (3, 256, 64)], ids=lambda s: "x".join(map(str, s)))
+def test_register_transform_paths_fp32(nshape):
+    """Power-of-two FP32 shapes: register x rows + y columns where nx and ny are in
+    {64, .., 512}, register z columns where nz is, general passes for the other axes."""
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal(nshape).astype(np.float32)
+    want = np.fft.rfftn(x.astype(np.float64))
+    got = r2c_gpu(x)
+    s = math.sqrt(x.size)
+    assert np.max(np.abs(got - want)) / s <= TOL[np.float32]
+    y = c2r_gpu(want.astype(np.complex64), nshape, np.float32)
+    assert np.max(np.abs(y / x.size - x.astype(np.float64))) <= 1e-5
+
+
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_r2c_c2r_vs_reference_cufft(dtype):
     ref = ref_lib(dtype)
