@@ -390,7 +390,8 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
     // sweeps).  The slabbed xy passes and the pipelined z kernel need work2 / carry A.
     c->z_carry = 0;
     if (const char* s = getenv("PFC_Z_CARRY")) c->z_carry = c->fused_z && atoi(s) != 0;
-    if (c->slab > 0 || c->z_pipe) c->z_carry = 0;
+    if (c->fused_z == 5) c->z_pipe = 0;  // the 16-column z variant exists as k_zcol only
+    if (c->slab > 0 || c->z_pipe || c->fused_z == 5) c->z_carry = 0;
     // L2 prefetch of the register passes, in waves of CTAs ahead (PFC_PREFETCH)
     c->pf_waves = 0.f;
     if (const char* s = getenv("PFC_PREFETCH")) c->pf_waves = std::max(0.f, (float)atof(s));

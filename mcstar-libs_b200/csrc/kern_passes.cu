@@ -30,13 +30,16 @@ struct YCfg {
     static_assert(P * E == NY && U * P == E && (TX >= 32 || (32 % TX == 0 && TX % U == 0)), "shape");
 };
 
-template <class Y, int DIR>
+template <class Y, int DIR, bool kZ>
 __global__ void __launch_bounds__(Y::T, Y::MINB)
-    k_ycol(const float2* in, float2* out, int nxh, int64_t ps, int ls, const float2* __restrict__ twg, float scale,
-           int pf) {
+    k_ycol(const float2* in, float2* out, int nxh, int64_t ps_z, int ls_z, const float2* __restrict__ twg,
+           float scale, int pf) {
     // columns of NY elements ls apart, starting at kx + blockIdx.y * ps: y columns of one
-    // z-plane (ps = ny nxh, ls = nxh) or z columns at one ky (ps = nxh, ls = ny nxh)
+    // z-plane (kZ false: ps = ny nxh, ls = nxh) or z columns at one ky (kZ: the strides
+    // passed, ps = nxh, ls = ny nxh)
     constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P, U = Y::U;
+    const int64_t ps = kZ ? ps_z : (int64_t)NY * nxh;
+    const int ls = kZ ? ls_z : nxh;
     extern __shared__ __align__(16) float2 sm[];
     float2* xb = sm;
     float2* tw = sm + Y::XB;
@@ -197,11 +200,12 @@ using X256 = XCfg<256, 16, 256>;
 using X128 = XCfg<128, 16, 128>;
 using X64 = XCfg<64, 8, 128>;
 
-template <class Y>
+template <class Y, bool kZ>
 cudaError_t yattr() {
-    cudaError_t e = cudaFuncSetAttribute(k_ycol<Y, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Y::SMEM);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_ycol<Y, 1, kZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Y::SMEM);
     if (e) return e;
-    return cudaFuncSetAttribute(k_ycol<Y, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Y::SMEM);
+    return cudaFuncSetAttribute(k_ycol<Y, -1, kZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Y::SMEM);
 }
 template <class X>
 cudaError_t xattr() {
@@ -212,30 +216,30 @@ cudaError_t xattr() {
 }
 
 // complex FFTs of the columns (lines of Y::NY elements ls apart) of the kx tiles of
-// `planes` planes ps apart; twiddles W_NY^m at tw_off
-template <class Y>
+// `planes` planes ps apart (kZ; y columns of z-planes otherwise); twiddles W_NY^m at tw_off
+template <class Y, bool kZ>
 cudaError_t collaunch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int planes, int64_t ps,
                       int ls, int tw_off) {
     dim3 grid((c->nxh + Y::TX - 1) / Y::TX, planes);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + tw_off;
-    static const int per_sm = resident_ctas(k_ycol<Y, 1>, Y::T, Y::SMEM);
+    static const int per_sm = resident_ctas(k_ycol<Y, 1, kZ>, Y::T, Y::SMEM);
     const int pf = prefetch_ahead(c, per_sm, in);
     if (dir > 0)
-        k_ycol<Y, 1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, ps, ls, tw,
-                                                         (float)scale, pf);
+        k_ycol<Y, 1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, ps, ls, tw,
+                                                             (float)scale, pf);
     else
-        k_ycol<Y, -1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, ps, ls, tw,
-                                                          (float)scale, pf);
+        k_ycol<Y, -1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, ps, ls, tw,
+                                                              (float)scale, pf);
     return cudaGetLastError();
 }
 template <class Y>
 cudaError_t ylaunch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs) {
-    return collaunch<Y>(c, dir, in, out, scale, nzs, (int64_t)c->ny * c->nxh, c->nxh, c->ypass_tw_off);
+    return collaunch<Y, false>(c, dir, in, out, scale, nzs, 0, 0, c->ypass_tw_off);
 }
 template <class Y>
 cudaError_t zlaunch_fft(const pfc_ctx* c, int dir, const void* in, void* out, double scale) {
     // z line stride ny nxh: an int for every shape with fewer than 2^31 complex modes
-    return collaunch<Y>(c, dir, in, out, scale, c->ny, c->nxh, c->ny * c->nxh, c->zfft_tw_off);
+    return collaunch<Y, true>(c, dir, in, out, scale, c->ny, c->nxh, c->ny * c->nxh, c->zfft_tw_off);
 }
 template <class X, int MODE>
 cudaError_t xlaunch(const pfc_ctx* c, const void* in, void* out, const void* pot, double mul, double C, double mu,
@@ -283,11 +287,11 @@ int fused_x_variant(int nx, int dtype) {
 cudaError_t set_pass_attributes(const pfc_ctx* c) {
     cudaError_t e = cudaSuccess;
     switch (c->fused_y) {
-        case 1: e = yattr<Y512>(); break;
-        case 2: e = yattr<Y256>(); break;
-        case 3: e = yattr<Y128>(); break;
-        case 4: e = yattr<Y64>(); break;
-        case 5: e = yattr<Y512w>(); break;
+        case 1: e = yattr<Y512, false>(); break;
+        case 2: e = yattr<Y256, false>(); break;
+        case 3: e = yattr<Y128, false>(); break;
+        case 4: e = yattr<Y64, false>(); break;
+        case 5: e = yattr<Y512w, false>(); break;
     }
     if (e) return e;
     switch (c->fused_x) {
@@ -346,10 +350,10 @@ int fused_zfft_variant(int nz, int dtype) {
 }
 cudaError_t set_zfft_attributes(const pfc_ctx* c) {
     switch (c->fused_zfft) {
-        case 1: return yattr<Y512>();
-        case 2: return yattr<Y256>();
-        case 3: return yattr<Y128>();
-        case 4: return yattr<Y64>();
+        case 1: return yattr<Y512, true>();
+        case 2: return yattr<Y256, true>();
+        case 3: return yattr<Y128, true>();
+        case 4: return yattr<Y64, true>();
     }
     return cudaSuccess;
 }

@@ -32,6 +32,7 @@ struct ZCfg {
     static constexpr int P = NZ / E, U = E / P;
     static constexpr int TH = TX * P;  // threads per field
     static constexpr int T = 2 * TH;
+    static constexpr int MINB = T <= 256 ? 2 : 1;  // k_zcol CTAs per SM its register cap allows
     static constexpr int PADG = TX / U;  // exchange padding: the 32/TX t-groups of a warp hit distinct banks
     static constexpr int REG = E * (P * TX + PADG);
     // N^ slots of the pipelined kernel, skewed by 8 per U modes so that a warp's four
@@ -159,7 +160,7 @@ __device__ __forceinline__ void prefetch_ztile(const float2* f0, const float2* f
 }
 
 template <class Z>
-__global__ void __launch_bounds__(Z::T, 2) k_zcol(float2* A, const float2* __restrict__ B, int nx, int ny, ZArgsF a,
+__global__ void __launch_bounds__(Z::T, Z::MINB) k_zcol(float2* A, const float2* __restrict__ B, int nx, int ny, ZArgsF a,
                                                    const double2* __restrict__ k0, int* flag,
                                                    const float2* __restrict__ twg, int pf) {
     constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, U = Z::U, TH = Z::TH;
@@ -346,6 +347,7 @@ __global__ void __launch_bounds__(Z::T, 1) k_zpipe(float2* A, const float2* __re
 }
 
 using Z512 = ZCfg<512, 32, 8>;
+using Z512w = ZCfg<512, 32, 16>;  // 128-byte column segments, one 512-thread CTA per SM (k_zcol only)
 using Z256 = ZCfg<256, 16, 8>;
 using Z128 = ZCfg<128, 16, 8>;
 using Z64 = ZCfg<64, 8, 8>;
@@ -400,7 +402,10 @@ cudaError_t zlaunch(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& p
 int fused_z_variant(int nx, int nz, int dtype) {
     if (dtype != PFC_F32 || nx < 16 || (nx / 2) % 8 != 0 || nx % 2 != 0) return 0;
     switch (nz) {
-        case 512: return 1;
+        case 512: {
+            const char* s = getenv("PFC_Z_VARIANT");  // 5: 16-column tiles (measurement variant)
+            return s && atoi(s) == 5 ? 5 : 1;
+        }
         case 256: return 2;
         case 128: return 3;
         case 64: return 4;
@@ -414,6 +419,9 @@ cudaError_t set_zcol_attributes(const pfc_ctx* c) {
         case 2: return zattr<Z256>();
         case 3: return zattr<Z128>();
         case 4: return zattr<Z64>();
+        case 5:
+            return cudaFuncSetAttribute(k_zcol<Z512w>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)Z512w::SMEM);
     }
     return cudaSuccess;
 }
@@ -430,6 +438,15 @@ cudaError_t launch_zcarry(const pfc_ctx* c, void* kpsi, void* A, const void* B, 
 
 cudaError_t launch_zcol(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a) {
     switch (c->fused_z) {
+        case 5: {
+            using Z = Z512w;
+            static const int per_sm = resident_ctas(k_zcol<Z>, Z::T, Z::SMEM);
+            const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
+            dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny);
+            k_zcol<Z><<<grid, Z::T, Z::SMEM, c->stream>>>((float2*)A, (const float2*)B, c->nx, c->ny, zargs_f(a), c->k0,
+                                                           c->flag, tw, prefetch_ahead(c, per_sm, A, B));
+            return cudaGetLastError();
+        }
         case 1: return zlaunch<Z512>(c, A, B, a);
         case 2: return zlaunch<Z256>(c, A, B, a);
         case 3: return zlaunch<Z128>(c, A, B, a);
