@@ -175,6 +175,26 @@ pfc_status pfc_free_energy(pfc_ctx* ctx, const void* kpsi, double eps,
                            double lx, double ly, double lz,
                            double hx, double hy, double hz, double* out);
 
+/* ---- reverse mode of pfc_step (no counterpart in mcstar-libs) ------------------------
+ * The step maps psi^ -> psi^' = D^-1 (psi^ - dt k^2 F[psi^3 - C psi - mu]) + D^-1 noise,
+ * D = 1 + dt k^2 (C - eps + (1 - k^2)^2), on the real field psi = C2R(psi^)/N.  The
+ * adjoint variable lam is a REAL field in a state-sized buffer: lam = dL/dpsi.
+ *
+ * pfc_sf_loss: L = sum over the full spectrum of (|psi^_k|^2 / N - s_k)^2, s given on
+ *   the half spectrum (n_cmpl reals of the context's precision, even in k); writes
+ *   lam_T = dL/dpsi to lam_out and L (FP64 sum) to *loss.
+ * pfc_adjoint_step: from lam_{n+1} (in lam) and the states psi^_n, psi^_{n+1} of that
+ *   step (p: the step's dt, eps, C, lengths; noise and mu do not enter), writes
+ *   lam_n = dL/dpsi_n to lam and adds the step's dL/deps to *deps (may be NULL).
+ *   workspace: pfc_adjoint_workspace_bytes(ctx) bytes of device memory (2 states).
+ * A whole run: forward with checkpoints, then adjoint steps from the last step back,
+ * recomputing the states between checkpoints (mcstar_b200.adjoint).  dL/dpsi0 of the
+ * initial mean density is the sum of lam_0. */
+size_t     pfc_adjoint_workspace_bytes(const pfc_ctx* ctx);
+pfc_status pfc_sf_loss(pfc_ctx* ctx, const void* kpsi, const void* s_target, void* lam_out, double* loss);
+pfc_status pfc_adjoint_step(pfc_ctx* ctx, const void* kpsi_n, const void* kpsi_np1, void* lam,
+                            const pfc_step_params* p, void* workspace, double* deps);
+
 /* ---- tracing (the role of TimeAcc, cuda/cutiming.hpp:5-25, inside the library) ------
  * While enabled, pfc_step brackets each kernel family with CUDA events on the
  * context's stream and counts every kernel the library launches.  Families:

@@ -632,6 +632,50 @@ pfc_status pfc_free_energy(pfc_ctx* ctx, const void* kpsi, double eps, double lx
     return PFC_OK;
 }
 
+// ---- reverse mode ------------------------------------------------------------------------
+size_t pfc_adjoint_workspace_bytes(const pfc_ctx* ctx) { return ctx ? 2 * ctx->state_bytes : 0; }
+
+pfc_status pfc_sf_loss(pfc_ctx* ctx, const void* kpsi, const void* s_target, void* lam_out, double* loss) {
+    PFC_CHECK_CTX();
+    if (!kpsi || !s_target || !lam_out || !loss) return fail(ctx, PFC_ERR_INVALID, "pfc_sf_loss: null argument");
+    // (4/N) r psi^ into work2, then its C2R (which runs in work) into lam_out
+    PFC_CUDA(launch_sf_loss(ctx, kpsi, s_target, ctx->work2), "pfc_sf_loss");
+    PFC_CUDA(cudaMemcpyAsync(loss, ctx->red + kRedBlocks + 3, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+             "pfc_sf_loss copy");
+    PFC_CUDA(cudaStreamSynchronize(ctx->stream), "pfc_sf_loss sync");
+    return pfc_fft_c2r(ctx, ctx->work2, lam_out);
+}
+
+pfc_status pfc_adjoint_step(pfc_ctx* ctx, const void* kpsi_n, const void* kpsi_np1, void* lam,
+                            const pfc_step_params* p, void* workspace, double* deps) {
+    PFC_CHECK_CTX();
+    if (!kpsi_n || !kpsi_np1 || !lam || !p || !workspace)
+        return fail(ctx, PFC_ERR_INVALID, "pfc_adjoint_step: null argument");
+    // w1: lam^ then D^-1 lam^; w2 (work2): (dt k^2/D) lam^ then psi_n; w3: B.  The
+    // transforms use work for their intermediates.
+    void* w1 = workspace;
+    void* w3 = (char*)workspace + ctx->state_bytes;
+    void* w2 = ctx->work2;
+    pfc_status s = pfc_fft_r2c(ctx, lam, w1);
+    if (s != PFC_OK) return s;
+    if (deps) {
+        PFC_CUDA(launch_adj_eps(ctx, w1, kpsi_np1, p), "pfc_adjoint_step eps");
+        double v = 0.0;
+        PFC_CUDA(cudaMemcpyAsync(&v, ctx->red + kRedBlocks + 3, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+                 "pfc_adjoint_step copy");
+        PFC_CUDA(cudaStreamSynchronize(ctx->stream), "pfc_adjoint_step sync");
+        *deps += v;
+    }
+    PFC_CUDA(launch_adj_mul(ctx, w1, w2, p, 1), "pfc_adjoint_step K");
+    if ((s = pfc_fft_c2r(ctx, w2, w3)) != PFC_OK) return s;
+    PFC_CUDA(launch_adj_mul(ctx, w1, w1, p, 0), "pfc_adjoint_step M");
+    if ((s = pfc_fft_c2r(ctx, w1, lam)) != PFC_OK) return s;
+    if ((s = pfc_fft_c2r(ctx, kpsi_n, w2)) != PFC_OK) return s;
+    PFC_CUDA(launch_adj_combine(ctx, lam, w2, w3, p->C), "pfc_adjoint_step combine");
+    ctx->launches += 4;
+    return PFC_OK;
+}
+
 pfc_status pfc_ensemble_create(int n, pfc_ctx* const* ctxs, void* const* kpsis, const pfc_step_params* params,
                                 int steps_per_graph, pfc_ensemble** out) {
     if (!out || n < 1 || !ctxs || !kpsis || !params || steps_per_graph < 1) return PFC_ERR_INVALID;

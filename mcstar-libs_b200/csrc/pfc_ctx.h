@@ -171,6 +171,12 @@ cudaError_t launch_bond_order(pfc_ctx* c, const void* maxima, int n, double h0, 
                               double ths, double boxsize, double rlim, double* out_rows, int row_capacity,
                               int* n_rows_host, int* overflow_host);
 
+// ---- adjoint of the step (kern_adjoint.cu); the sums land in red slot 3 ----
+cudaError_t launch_adj_mul(const pfc_ctx* c, const void* in, void* out, const pfc_step_params* p, int mode);
+cudaError_t launch_adj_eps(const pfc_ctx* c, const void* lam_hat, const void* kpsi_np1, const pfc_step_params* p);
+cudaError_t launch_adj_combine(const pfc_ctx* c, void* lam, const void* psi_u, const void* b, double C);
+cudaError_t launch_sf_loss(const pfc_ctx* c, const void* kpsi, const void* s_target, void* out);
+
 // ---- fused plane kernels (kern_fused.cu) ----
 int fused_xy_variant(int nx, int ny, int dtype);
 cudaError_t set_fused_attributes(const pfc_ctx* c);

@@ -13,6 +13,7 @@ from .kernels import (CufftPlan, R2C, C2R, NoiseHostApi, call_kernel_update_eom,
                       mu, omega, init_pot_line, TimeAcc, BOND_COLUMNS, findpeaks_device, records_to_host)
 from .stepper import Stepper, liquid_random, bcc_sphere, namp_from_temperature, BCC_Q
 from .ensemble import Ensemble, ensemble_members, partition, member_cost
+from .adjoint import AdjointRun, SFLoss, structure_factor
 from . import dist
 
 __all__ = [n for n in dir() if not n.startswith("_")]

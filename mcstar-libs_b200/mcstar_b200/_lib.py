@@ -25,7 +25,8 @@ EXPORTED = (
     "pfc_update_eom_with_fen", "pfc_psi3_split", "pfc_norm", "pfc_calc_fen", "pfc_noise_fill_kspace",
     "pfc_noise_fill", "pfc_findpeaks", "pfc_bond_order", "pfc_step", "pfc_free_energy",
     "pfc_profile_enable", "pfc_profile_read", "pfc_findpeaks_static", "pfc_ensemble_create",
-    "pfc_ensemble_run", "pfc_ensemble_destroy", "pfc_ensemble_last_error",
+    "pfc_ensemble_run", "pfc_ensemble_destroy", "pfc_ensemble_last_error", "pfc_adjoint_workspace_bytes",
+    "pfc_sf_loss", "pfc_adjoint_step",
 )
 
 
@@ -92,6 +93,9 @@ _SIGS = {
     "pfc_ensemble_run": ([_P, _I, _P], _I),
     "pfc_ensemble_destroy": ([_P], _I),
     "pfc_ensemble_last_error": ([_P], ctypes.c_char_p),
+    "pfc_adjoint_workspace_bytes": ([_P], ctypes.c_size_t),
+    "pfc_sf_loss": ([_P, _P, _P, _P, ctypes.POINTER(_D)], _I),
+    "pfc_adjoint_step": ([_P, _P, _P, _P, ctypes.POINTER(PfcStepParams), _P, ctypes.POINTER(_D)], _I),
 }
 
 

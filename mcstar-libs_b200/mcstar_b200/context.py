@@ -140,6 +140,28 @@ class Context:
                           float(lens[1]), float(lens[2]), int(seed), int(counter))
         self._call("pfc_step", _ptr(kpsi), int(nsteps), ctypes.byref(p))
 
+    # -- reverse mode --------------------------------------------------------------------
+    def adjoint_workspace(self):
+        """Device workspace of pfc_adjoint_step (two states)."""
+        n = int(lib().pfc_adjoint_workspace_bytes(self._h)) // self.torch_dtype.itemsize
+        return torch.empty(n, dtype=self.torch_dtype, device="cuda")
+
+    def sf_loss(self, kpsi, s_target, lam_out):
+        """L = sum_k (|psi^_k|^2/N - s_k)^2 over the full spectrum; lam_out <- dL/dpsi (real)."""
+        out = ctypes.c_double()
+        self._call("pfc_sf_loss", _ptr(kpsi), _ptr(s_target), _ptr(lam_out), ctypes.byref(out))
+        return out.value
+
+    def adjoint_step(self, kpsi_n, kpsi_np1, lam, dt, eps, lens, C=1.0, workspace=None, with_eps=True):
+        """lam <- dL/dpsi_n from dL/dpsi_{n+1}; returns this step's dL/deps (0 if not with_eps)."""
+        p = PfcStepParams(float(dt), float(eps), 0.0, float(C), 0.0, float(lens[0]), float(lens[1]), float(lens[2]),
+                          0, 0)
+        ws = self.adjoint_workspace() if workspace is None else workspace
+        d = ctypes.c_double(0.0)
+        self._call("pfc_adjoint_step", _ptr(kpsi_n), _ptr(kpsi_np1), _ptr(lam), ctypes.byref(p), _ptr(ws),
+                   ctypes.byref(d) if with_eps else None)
+        return d.value
+
     def profile_enable(self, on=True):
         check(lib().pfc_profile_enable(self._h, int(bool(on))), self._h, "pfc_profile_enable")
 

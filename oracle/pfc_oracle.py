@@ -174,6 +174,57 @@ def free_energy(kpsi, eps, lens, hh, shape_xyz):
 
 
 # ----------------------------------------------------------------------------------
+# reverse mode of the step (no reference counterpart; pinned by finite differences of
+# step() in the tests)
+# ----------------------------------------------------------------------------------
+def half_weights(shape_xyz):
+    """w_k on the half spectrum: 2 for 0 < i0 < nx/2 (the mode and its mirror), else 1."""
+    nx, ny, nz = shape_xyz
+    i0 = np.arange(nx // 2 + 1)
+    w = np.where((i0 == 0) | ((nx % 2 == 0) & (i0 == nx // 2)), 1.0, 2.0)
+    return np.broadcast_to(w[None, None, :], cmpl_shape(shape_xyz))
+
+
+def sf_loss(kpsi, s_target, shape_xyz):
+    """L = sum over the full spectrum of (|psi^|^2/N - s)^2 and lam_T = dL/dpsi_T =
+    (4/N) C2R(r psi^), r = |psi^|^2/N - s (unnormalised C2R)."""
+    n = float(np.prod(shape_xyz))
+    k = kpsi.astype(np.complex128)
+    r = (k.real ** 2 + k.imag ** 2) / n - s_target
+    loss = float(np.sum(half_weights(shape_xyz) * r * r))
+    return loss, c2r((4.0 / n) * r * k, shape_xyz)
+
+
+def adjoint_step(kpsi_n, kpsi_np1, lam, dt, eps, lens, shape_xyz, C=1.0):
+    """lam_n = M lam_{n+1} - (3 psi_n^2 - C) K lam_{n+1}, M = F^-1 D^-1 F,
+    K = F^-1 (dt k^2 / D) F, and this step's dL/deps = (1/N) sum_k w_k
+    Re(conj(lam^_{n+1}) (dt k^2 / D) psi^_{n+1}); D as in update_eom."""
+    n = float(np.prod(shape_xyz))
+    k2 = kgrid(shape_xyz, lens)
+    D = 1.0 + dt * k2 * (C - eps + (1.0 - k2) ** 2)
+    kf = dt * k2 / D
+    lh = r2c(lam.astype(np.float64))
+    deps = float(np.sum(half_weights(shape_xyz) * np.real(np.conj(lh) * kf * kpsi_np1))) / n
+    A = c2r(lh / D, shape_xyz) / n
+    B = c2r(kf * lh, shape_xyz) / n
+    psi = c2r(kpsi_n.astype(np.complex128), shape_xyz) / n
+    return A - (3.0 * psi * psi - C) * B, deps
+
+
+def sf_loss_grads(psi_init, nsteps, s_target, dt, eps, lens, shape_xyz, C=1.0, mu=0.0):
+    """(L, dL/dpsi_init, dL/deps) of nsteps of step() in FP64, storing every state."""
+    states = [r2c(psi_init.astype(np.float64))]
+    for _ in range(nsteps):
+        states.append(step(states[-1], 1, dt, eps, lens, shape_xyz, mu=mu, C=C))
+    loss, lam = sf_loss(states[-1], s_target, shape_xyz)
+    deps = 0.0
+    for t in range(nsteps - 1, -1, -1):
+        lam, d = adjoint_step(states[t], states[t + 1], lam, dt, eps, lens, shape_xyz, C=C)
+        deps += d
+    return loss, lam, deps
+
+
+# ----------------------------------------------------------------------------------
 # Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as easy as
 # 1, 2, 3", SC'11) -- vectorised over numpy uint64 lanes holding 32-bit words.
 # ----------------------------------------------------------------------------------
