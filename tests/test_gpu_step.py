@@ -96,6 +96,28 @@ def test_step_kernel_variants_match_oracle(env):
         assert e < 2e-6, (shape, e)
 
 
+@pytest.mark.parametrize("shape,dtype", [((64, 64, 64), F32), ((32, 32, 32), F32), ((16, 12, 10), F64)],
+                         ids=["register-z", "register-z-32", "general-z"])
+def test_nonfinite_state_is_reported_and_context_stays_usable(shape, dtype):
+    """A NaN planted in psi^ on the host reaches every mode after one transform; the z
+    pass's watchdog flags it and pfc_step returns PFC_ERR_NONFINITE.  The next run on a
+    clean state works."""
+    from mcstar_b200 import PfcError
+    from mcstar_b200._lib import PFC_ERR_NONFINITE
+    nx, ny, nz = shape
+    psi = -0.2 + 0.05 * np.random.default_rng(2).uniform(-1, 1, (nz, ny, nx))
+    st = stepper(shape, dtype)
+    st.set_real(psi)
+    st.kpsi[10] = float("nan")
+    with pytest.raises(PfcError) as err:
+        st.step(2)
+    assert err.value.status == PFC_ERR_NONFINITE
+    st.set_real(psi)
+    st.step(2)
+    want = O.step(O.r2c(psi), 2, st.dt, st.eps, st.lens, shape)
+    assert rel_l2(st.kspace(), want) < (2e-6 if dtype == F32 else 1e-12)
+
+
 def test_step_stabilisation_constant_and_mu():
     shape = (16, 16, 16)
     st = stepper(shape, F64, C=0.0, mu=0.07, dt=0.1)
