@@ -36,6 +36,28 @@ inline void call_kernel_update_eom_with_fen(GPUArray& arr_kpsi, GPUArray& arr_kn
     PFC_SHIM_SYNC();
 }
 
+// the update with the polynomial kernel P(k^2) (eom.hpp:143-180)
+inline void call_kernel_update_eom_py(GPUArray& arr_kpsi, GPUArray& arr_knonlin, GPUArray& arr_knoise, Float namp,
+                                      Float dt, Float eps, Float3 lens) {
+    pfc_ctx* c = pfc_shim::context<Float>(arr_kpsi.real_vext());
+    PFC_SHIM_CHECK(pfc_update_eom_py(c, arr_kpsi.ptr_void(), arr_knonlin.ptr_void(), arr_knoise.ptr_void(), namp, dt,
+                                     eps, lens.x, lens.y, lens.z),
+                   c);
+    PFC_SHIM_SYNC();
+}
+
+// the 2D update with anisotropic noise from three noise fields (eom.hpp:16-58)
+inline void call_kernel_update_eom_hpfcnoise(GPUArray& arr_kpsi, GPUArray& arr_knonlin, GPUArray& arr_knoise1,
+                                             GPUArray& arr_knoise2, GPUArray& arr_knoise3, Float namp, Float dt,
+                                             Float eps, Float3 lens) {
+    pfc_ctx* c = pfc_shim::context<Float>(arr_kpsi.real_vext());
+    PFC_SHIM_CHECK(pfc_update_eom_hpfcnoise(c, arr_kpsi.ptr_void(), arr_knonlin.ptr_void(), arr_knoise1.ptr_void(),
+                                            arr_knoise2.ptr_void(), arr_knoise3.ptr_void(), namp, dt, eps, lens.x,
+                                            lens.y, lens.z),
+                   c);
+    PFC_SHIM_SYNC();
+}
+
 // writes f = psi (L psi - psi + psi^3 / 2) / 2 into arr_lpsi; returns h^3 sum(f)
 inline float call_kernel_calc_fen(GPUArray& arr_psi, GPUArray& arr_lpsi, Float3 hh) {
     pfc_ctx* c = pfc_shim::context<Float>(arr_psi.real_vext());

@@ -88,6 +88,35 @@ pfc_status pfc_norm(pfc_ctx* ctx, void* arr);
 pfc_status pfc_calc_fen(pfc_ctx* ctx, const void* psi, void* lpsi,
                         double hx, double hy, double hz, double* out);
 
+/* ---- the reference's other propagators, pointwise on the half spectrum ---------------
+ * pfc_init_eom_op: kop = {exp(-L dt), (exp(-L dt) - 1)/L}, L = k^2 ((1 - k^2)^2 + 1 - eps)
+ *   (-dt where L = 0) -- kernel_init_eom_op, cuda/kernels/eom-exp.hpp:3-16.
+ * pfc_update_eom_exp(_with_fen): psi^ <- kop.x psi^ + k^2 kop.y N^ - namp sqrt(N) |k| kop.y xi^
+ *   (knoise may be NULL; _with_fen also writes L^ psi^_old into knoise) -- eom-exp.hpp:18-60.
+ * pfc_update_el: non-conserved relaxation psi^ <- (psi^ - dt N^)/(1 + dt((1-k^2)^2 + 1 - eps)),
+ *   *max_change = max_k |psi^'_k - psi^_k| -- el.hpp:3-45.
+ * pfc_init_el_op / pfc_update_el_exp: its exponential form, kop = {exp(-L dt), (exp(-L dt)-1)/L},
+ *   L = (1-k^2)^2 + 1 - eps; psi^ <- kop.x psi^ + kop.y N^ -- el-exp.hpp:3-60.
+ * pfc_update_eom_py: the conserved update with the polynomial P(k^2) of eom.hpp:143-180,
+ *   denominator 1 + dt k^2 (1 - eps - P(k^2)).
+ * pfc_update_eom_hpfcnoise: the 2D conserved update with the anisotropic noise built from
+ *   three noise fields, cut off above |k| = 0.25 -- eom.hpp:16-58; PFC_ERR_INVALID on 3D grids
+ *   (the reference exits). */
+pfc_status pfc_init_eom_op(pfc_ctx* ctx, void* kop, double dt, double eps, double lx, double ly, double lz);
+pfc_status pfc_update_eom_exp(pfc_ctx* ctx, const void* kop, void* kpsi, const void* knonlin, const void* knoise,
+                              double namp, double eps, double lx, double ly, double lz);
+pfc_status pfc_update_eom_exp_with_fen(pfc_ctx* ctx, const void* kop, void* kpsi, const void* knonlin, void* knoise,
+                                       double namp, double eps, double lx, double ly, double lz);
+pfc_status pfc_update_el(pfc_ctx* ctx, void* kpsi, const void* knonlin, double dt, double eps,
+                         double lx, double ly, double lz, double* max_change);
+pfc_status pfc_init_el_op(pfc_ctx* ctx, void* kop, double dt, double eps, double lx, double ly, double lz);
+pfc_status pfc_update_el_exp(pfc_ctx* ctx, const void* kop, void* kpsi, const void* knonlin, double* max_change);
+pfc_status pfc_update_eom_py(pfc_ctx* ctx, void* kpsi, const void* knonlin, const void* knoise,
+                             double namp, double dt, double eps, double lx, double ly, double lz);
+pfc_status pfc_update_eom_hpfcnoise(pfc_ctx* ctx, void* kpsi, const void* knonlin, const void* knoise1,
+                                    const void* knoise2, const void* knoise3, double namp, double dt, double eps,
+                                    double lx, double ly, double lz);
+
 /* ---- noise: replaces NoiseHostApi<F> (cuda/noise.hpp:93-150) -------------------------
  * Counter-based Philox4x32-10: (seed, counter) selects the draw, so a run resumes
  * bit-exactly.  fill_kspace: complex normal, E|xi|^2 = 1, Hermitian on the i0 = 0 and

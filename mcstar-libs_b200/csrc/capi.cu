@@ -632,6 +632,76 @@ pfc_status pfc_free_energy(pfc_ctx* ctx, const void* kpsi, double eps, double lx
     return PFC_OK;
 }
 
+// ---- the reference's other propagators ------------------------------------------------------
+pfc_status pfc_init_eom_op(pfc_ctx* ctx, void* kop, double dt, double eps, double lx, double ly, double lz) {
+    PFC_CHECK_CTX();
+    if (!kop) return fail(ctx, PFC_ERR_INVALID, "pfc_init_eom_op: null buffer");
+    PFC_CUDA(launch_init_eom_op(ctx, kop, dt, eps, lx, ly, lz), "pfc_init_eom_op");
+    return PFC_OK;
+}
+
+pfc_status pfc_update_eom_exp(pfc_ctx* ctx, const void* kop, void* kpsi, const void* knonlin, const void* knoise,
+                              double namp, double eps, double lx, double ly, double lz) {
+    PFC_CHECK_CTX();
+    if (!kop || !kpsi || !knonlin) return fail(ctx, PFC_ERR_INVALID, "pfc_update_eom_exp: null buffer");
+    PFC_CUDA(launch_update_eom_exp(ctx, kop, kpsi, knonlin, const_cast<void*>(knoise), namp, eps, lx, ly, lz, 0),
+             "pfc_update_eom_exp");
+    return PFC_OK;
+}
+
+pfc_status pfc_update_eom_exp_with_fen(pfc_ctx* ctx, const void* kop, void* kpsi, const void* knonlin, void* knoise,
+                                       double namp, double eps, double lx, double ly, double lz) {
+    PFC_CHECK_CTX();
+    if (!kop || !kpsi || !knonlin || !knoise)
+        return fail(ctx, PFC_ERR_INVALID, "pfc_update_eom_exp_with_fen: null buffer");
+    PFC_CUDA(launch_update_eom_exp(ctx, kop, kpsi, knonlin, knoise, namp, eps, lx, ly, lz, 1),
+             "pfc_update_eom_exp_with_fen");
+    return PFC_OK;
+}
+
+pfc_status pfc_update_el(pfc_ctx* ctx, void* kpsi, const void* knonlin, double dt, double eps, double lx, double ly,
+                         double lz, double* max_change) {
+    PFC_CHECK_CTX();
+    if (!kpsi || !knonlin || !max_change) return fail(ctx, PFC_ERR_INVALID, "pfc_update_el: null argument");
+    PFC_CUDA(launch_update_el(ctx, nullptr, kpsi, knonlin, dt, eps, lx, ly, lz, max_change), "pfc_update_el");
+    return PFC_OK;
+}
+
+pfc_status pfc_init_el_op(pfc_ctx* ctx, void* kop, double dt, double eps, double lx, double ly, double lz) {
+    PFC_CHECK_CTX();
+    if (!kop) return fail(ctx, PFC_ERR_INVALID, "pfc_init_el_op: null buffer");
+    PFC_CUDA(launch_init_el_op(ctx, kop, dt, eps, lx, ly, lz), "pfc_init_el_op");
+    return PFC_OK;
+}
+
+pfc_status pfc_update_el_exp(pfc_ctx* ctx, const void* kop, void* kpsi, const void* knonlin, double* max_change) {
+    PFC_CHECK_CTX();
+    if (!kop || !kpsi || !knonlin || !max_change)
+        return fail(ctx, PFC_ERR_INVALID, "pfc_update_el_exp: null argument");
+    PFC_CUDA(launch_update_el(ctx, kop, kpsi, knonlin, 0.0, 0.0, 1.0, 1.0, 1.0, max_change), "pfc_update_el_exp");
+    return PFC_OK;
+}
+
+pfc_status pfc_update_eom_py(pfc_ctx* ctx, void* kpsi, const void* knonlin, const void* knoise, double namp,
+                             double dt, double eps, double lx, double ly, double lz) {
+    PFC_CHECK_CTX();
+    if (!kpsi || !knonlin) return fail(ctx, PFC_ERR_INVALID, "pfc_update_eom_py: null buffer");
+    PFC_CUDA(launch_update_eom_py(ctx, kpsi, knonlin, knoise, namp, dt, eps, lx, ly, lz), "pfc_update_eom_py");
+    return PFC_OK;
+}
+
+pfc_status pfc_update_eom_hpfcnoise(pfc_ctx* ctx, void* kpsi, const void* knonlin, const void* knoise1,
+                                    const void* knoise2, const void* knoise3, double namp, double dt, double eps,
+                                    double lx, double ly, double lz) {
+    PFC_CHECK_CTX();
+    if (!kpsi || !knonlin || !knoise1 || !knoise2 || !knoise3)
+        return fail(ctx, PFC_ERR_INVALID, "pfc_update_eom_hpfcnoise: null buffer");
+    if (ctx->nz != 1) return fail(ctx, PFC_ERR_INVALID, "pfc_update_eom_hpfcnoise: 2D grids only (nz = 1)");
+    PFC_CUDA(launch_update_eom_hpfcnoise(ctx, kpsi, knonlin, knoise1, knoise2, knoise3, namp, dt, eps, lx, ly, lz),
+             "pfc_update_eom_hpfcnoise");
+    return PFC_OK;
+}
+
 // ---- reverse mode ------------------------------------------------------------------------
 size_t pfc_adjoint_workspace_bytes(const pfc_ctx* ctx) { return ctx ? 2 * ctx->state_bytes : 0; }
 

@@ -171,6 +171,19 @@ cudaError_t launch_bond_order(pfc_ctx* c, const void* maxima, int n, double h0, 
                               double ths, double boxsize, double rlim, double* out_rows, int row_capacity,
                               int* n_rows_host, int* overflow_host);
 
+// ---- the reference's other propagators (kern_variants.cu) ----
+cudaError_t launch_init_eom_op(const pfc_ctx* c, void* kop, double dt, double eps, double lx, double ly, double lz);
+cudaError_t launch_update_eom_exp(const pfc_ctx* c, const void* kop, void* kpsi, const void* knl, void* knoise,
+                                  double namp, double eps, double lx, double ly, double lz, int with_fen);
+cudaError_t launch_init_el_op(const pfc_ctx* c, void* kop, double dt, double eps, double lx, double ly, double lz);
+cudaError_t launch_update_el(const pfc_ctx* c, const void* kop, void* kpsi, const void* knl, double dt, double eps,
+                             double lx, double ly, double lz, double* max_change);
+cudaError_t launch_update_eom_py(const pfc_ctx* c, void* kpsi, const void* knl, const void* knoise, double namp,
+                                 double dt, double eps, double lx, double ly, double lz);
+cudaError_t launch_update_eom_hpfcnoise(const pfc_ctx* c, void* kpsi, const void* knl, const void* n1, const void* n2,
+                                        const void* n3, double namp, double dt, double eps, double lx, double ly,
+                                        double lz);
+
 // ---- adjoint of the step (kern_adjoint.cu); the sums land in red slot 3 ----
 cudaError_t launch_adj_mul(const pfc_ctx* c, const void* in, void* out, const pfc_step_params* p, int mode);
 cudaError_t launch_adj_eps(const pfc_ctx* c, const void* lam_hat, const void* kpsi_np1, const pfc_step_params* p);

@@ -26,7 +26,8 @@ EXPORTED = (
     "pfc_noise_fill", "pfc_findpeaks", "pfc_bond_order", "pfc_step", "pfc_free_energy",
     "pfc_profile_enable", "pfc_profile_read", "pfc_findpeaks_static", "pfc_ensemble_create",
     "pfc_ensemble_run", "pfc_ensemble_destroy", "pfc_ensemble_last_error", "pfc_adjoint_workspace_bytes",
-    "pfc_sf_loss", "pfc_adjoint_step",
+    "pfc_sf_loss", "pfc_adjoint_step", "pfc_init_eom_op", "pfc_update_eom_exp", "pfc_update_eom_exp_with_fen",
+    "pfc_update_el", "pfc_init_el_op", "pfc_update_el_exp", "pfc_update_eom_py", "pfc_update_eom_hpfcnoise",
 )
 
 
@@ -96,6 +97,14 @@ _SIGS = {
     "pfc_adjoint_workspace_bytes": ([_P], ctypes.c_size_t),
     "pfc_sf_loss": ([_P, _P, _P, _P, ctypes.POINTER(_D)], _I),
     "pfc_adjoint_step": ([_P, _P, _P, _P, ctypes.POINTER(PfcStepParams), _P, ctypes.POINTER(_D)], _I),
+    "pfc_init_eom_op": ([_P, _P, _D, _D, _D, _D, _D], _I),
+    "pfc_update_eom_exp": ([_P, _P, _P, _P, _P, _D, _D, _D, _D, _D], _I),
+    "pfc_update_eom_exp_with_fen": ([_P, _P, _P, _P, _P, _D, _D, _D, _D, _D], _I),
+    "pfc_update_el": ([_P, _P, _P, _D, _D, _D, _D, _D, ctypes.POINTER(_D)], _I),
+    "pfc_init_el_op": ([_P, _P, _D, _D, _D, _D, _D], _I),
+    "pfc_update_el_exp": ([_P, _P, _P, _P, ctypes.POINTER(_D)], _I),
+    "pfc_update_eom_py": ([_P, _P, _P, _P, _D, _D, _D, _D, _D, _D], _I),
+    "pfc_update_eom_hpfcnoise": ([_P, _P, _P, _P, _P, _P, _D, _D, _D, _D, _D, _D], _I),
 }
 
 

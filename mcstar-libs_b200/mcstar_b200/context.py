@@ -112,6 +112,38 @@ class Context:
     def noise_real(self, arr, sigma, seed, counter):
         self._call("pfc_noise_fill", _ptr(arr), float(sigma), ctypes.c_uint64(seed), ctypes.c_uint64(counter))
 
+    # -- the reference's other propagators (eom-exp.hpp, el.hpp, el-exp.hpp, eom.hpp) -----------
+    def init_eom_op(self, kop, dt, eps, lens):
+        self._call("pfc_init_eom_op", _ptr(kop), float(dt), float(eps), *(float(v) for v in lens))
+
+    def update_eom_exp(self, kop, kpsi, knl, knoise, namp, eps, lens, with_fen=False):
+        name = "pfc_update_eom_exp_with_fen" if with_fen else "pfc_update_eom_exp"
+        self._call(name, _ptr(kop), _ptr(kpsi), _ptr(knl), _ptr(knoise), float(namp), float(eps),
+                   *(float(v) for v in lens))
+
+    def update_el(self, kpsi, knl, dt, eps, lens):
+        """Non-conserved relaxation step; returns max_k |psi^'_k - psi^_k|."""
+        out = ctypes.c_double()
+        self._call("pfc_update_el", _ptr(kpsi), _ptr(knl), float(dt), float(eps), *(float(v) for v in lens),
+                   ctypes.byref(out))
+        return out.value
+
+    def init_el_op(self, kop, dt, eps, lens):
+        self._call("pfc_init_el_op", _ptr(kop), float(dt), float(eps), *(float(v) for v in lens))
+
+    def update_el_exp(self, kop, kpsi, knl):
+        out = ctypes.c_double()
+        self._call("pfc_update_el_exp", _ptr(kop), _ptr(kpsi), _ptr(knl), ctypes.byref(out))
+        return out.value
+
+    def update_eom_py(self, kpsi, knl, knoise, namp, dt, eps, lens):
+        self._call("pfc_update_eom_py", _ptr(kpsi), _ptr(knl), _ptr(knoise), float(namp), float(dt), float(eps),
+                   *(float(v) for v in lens))
+
+    def update_eom_hpfcnoise(self, kpsi, knl, n1, n2, n3, namp, dt, eps, lens):
+        self._call("pfc_update_eom_hpfcnoise", _ptr(kpsi), _ptr(knl), _ptr(n1), _ptr(n2), _ptr(n3), float(namp),
+                   float(dt), float(eps), *(float(v) for v in lens))
+
     # -- analysis -----------------------------------------------------------------------
     def findpeaks(self, psi, ths, out=None, capacity=None):
         """Returns (n_found, records) where records is a device uint8 tensor of

@@ -174,6 +174,107 @@ def free_energy(kpsi, eps, lens, hh, shape_xyz):
 
 
 # ----------------------------------------------------------------------------------
+# the reference's other propagators (FP64 restatements; exp and sqrt in single
+# precision where the reference calls expf / sqrtf)
+# ----------------------------------------------------------------------------------
+def _f32(fn, x):
+    return fn(np.asarray(x, dtype=np.float64).astype(np.float32)).astype(np.float64)
+
+
+def _dops(shape_xyz, lens):
+    k2 = kgrid(shape_xyz, lens)
+    return -k2, k2 * k2
+
+
+def init_eom_op(shape_xyz, lens, dt, eps):
+    """kernel_init_eom_op (eom-exp.hpp:3-10): kop = exp(-L dt) + i (exp(-L dt) - 1)/L,
+    L = -dop.x ((2 - eps) + 2 dop.x + dop.y); -dt where L = 0 (the 0/0 at k = 0)."""
+    dx, dy = _dops(shape_xyz, lens)
+    lin = -dx * ((2.0 - eps) + 2.0 * dx + dy)
+    e = _f32(np.exp, -lin * dt)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        second = (e - 1.0) / lin
+    return e + 1j * np.where(np.isnan(second), -dt, second)
+
+
+def update_eom_exp(kop, kpsi, knl, knoise, namp, eps, lens, shape_xyz, with_fen=False):
+    """kernel_update_eom(_with_fen) of eom-exp.hpp:18-60: kop.x psi^ - dop.x kop.y N^ -
+    namp sqrt(N) |k| kop.y xi^; with_fen also returns L^ psi^_old."""
+    nx, ny, nz = shape_xyz
+    dx, dy = _dops(shape_xyz, lens)
+    k = _f32(np.sqrt, -dx)
+    ne = namp * float(np.sqrt(np.float32(nx * ny * nz)))
+    a, b = kop.real, kop.imag
+    new = kpsi * a - dx * knl * b
+    if knoise is not None:
+        new = new - ne * k * knoise * b
+    if with_fen:
+        return new, ((2.0 - eps) + 2.0 * dx + dy) * kpsi
+    return new
+
+
+def update_el(kpsi, knl, dt, eps, lens, shape_xyz):
+    """kernel_update_el (el.hpp:3-25): (psi^ - dt N^)/(1 + dt((2 - eps) + 2 dop.x + dop.y)),
+    and max_k |psi^' - psi^| (call_kernel_update_el, el.hpp:26-45)."""
+    dx, dy = _dops(shape_xyz, lens)
+    new = (kpsi - dt * knl) / (1.0 + dt * ((2.0 - eps) + 2.0 * dx + dy))
+    return new, float(np.max(np.abs(kpsi - new)))
+
+
+def init_el_op(shape_xyz, lens, dt, eps):
+    """kernel_init_el_op (el-exp.hpp:3-9): exp(-L dt) + i (exp(-L dt) - 1)/L, L = (2-eps) + 2 dop.x + dop.y."""
+    dx, dy = _dops(shape_xyz, lens)
+    lin = (2.0 - eps) + 2.0 * dx + dy
+    e = _f32(np.exp, -lin * dt)
+    return e + 1j * (e - 1.0) / lin
+
+
+def update_el_exp(kop, kpsi, knl):
+    """kernel_update_el of el-exp.hpp:17-40: kop.x psi^ + kop.y N^, and the largest change."""
+    new = kpsi * kop.real + knl * kop.imag
+    return new, float(np.max(np.abs(kpsi - new)))
+
+
+PY_COEFFS = (-57.94636917114257, 164.4074088310241, -181.1481995196213, 100.6942650417575,
+             -30.20985042718309, 4.678065276755401, -0.293423255328944)  # c0, c2, ..., c12 (eom.hpp:143-149)
+
+
+def update_eom_py(kpsi, knl, knoise, namp, dt, eps, lens, shape_xyz):
+    """kernel_update_eom_py (eom.hpp:151-176): denominator 1 - dt dop.x (1 - eps - P(k^2))."""
+    nx, ny, nz = shape_xyz
+    dx, _ = _dops(shape_xyz, lens)
+    k2 = -dx
+    p = np.full_like(k2, PY_COEFFS[-1])
+    for c in PY_COEFFS[-2::-1]:
+        p = p * k2 + c
+    denom = 1.0 - dt * dx * (1.0 - eps - p)
+    ne = namp * float(np.sqrt(np.float32(nx * ny * nz)))
+    num = kpsi + dt * dx * knl
+    if knoise is not None:
+        num = num + dt * ne * _f32(np.sqrt, k2) * knoise
+    return num / denom
+
+
+def update_eom_hpfcnoise(kpsi, knl, n1, n2, n3, namp, dt, eps, lens, shape_xyz):
+    """kernel_update_eom_hpfcnoise (eom.hpp:16-44), 2D: the noise
+    (c1 kx^2 + c2 ky^2) xi1 + (c2 kx^2 + c1 ky^2) xi2 + 2 kx ky xi3 for |k| <= 0.25, kappa = 4/3,
+    c2 = sqrt(1 + kappa/2 + sqrt(1 + kappa)), c1 = kappa / (2 c2)."""
+    nx, ny, nz = shape_xyz
+    kappa = np.float32(4.0) / np.float32(3.0)
+    c2 = float(np.sqrt(np.float32(1.0) + kappa / np.float32(2.0) + np.sqrt(np.float32(1.0) + kappa)))
+    c1 = float(kappa) / c2 / 2.0
+    k0 = wavenumbers(nx, lens[0], half=True)[None, None, :]
+    k1 = wavenumbers(ny, lens[1])[None, :, None]
+    dx, dy = _dops(shape_xyz, lens)
+    k = _f32(np.sqrt, -dx)
+    denom = 1.0 - dt * ((2.0 - eps) * dx + 2.0 * dy + dx * dy)
+    noise = (c1 * k0 * k0 + c2 * k1 * k1) * n1 + (c2 * k0 * k0 + c1 * k1 * k1) * n2 + 2.0 * k0 * k1 * n3
+    noise = np.where(k <= 0.25, noise, 0.0)
+    ne = namp * float(np.sqrt(np.float32(nx * ny * nz)))
+    return (kpsi + dt * dx * knl + dt * ne * noise) / denom
+
+
+# ----------------------------------------------------------------------------------
 # reverse mode of the step (no reference counterpart; pinned by finite differences of
 # step() in the tests)
 # ----------------------------------------------------------------------------------

@@ -230,4 +230,40 @@ void REFP(noise_kspace)(void* h, void* cmpl_out) {
     std::memcpy(cmpl_out, s->host->ptr_void(), REFP(state_bytes)(h));
 }
 
+static void up(RefState* s, GPUArray* a, const void* src, size_t bytes) {
+    std::memcpy(s->host->ptr_void(), src, bytes);
+    (*s->host) >> (*a);
+}
+static void down(RefState* s, GPUArray* a, void* dst, size_t bytes) {
+    (*a) >> (*s->host);
+    std::memcpy(dst, s->host->ptr_void(), bytes);
+}
+
+/* The polynomial-kernel update (eom.hpp:143-180) on host half spectra; kpsi in/out. */
+void REFP(update_eom_py)(void* h, void* kpsi, const void* knl, const void* knoise, double namp, double dt,
+                         double eps, double lx, double ly, double lz) {
+    RefState* s = (RefState*)h;
+    const size_t b = REFP(state_bytes)(h);
+    up(s, s->kpsi, kpsi, b);
+    up(s, s->knl, knl, b);
+    up(s, s->knoise, knoise, b);
+    call_kernel_update_eom_py(*s->kpsi, *s->knl, *s->knoise, Float(namp), Float(dt), Float(eps), mk3(lx, ly, lz));
+    down(s, s->kpsi, kpsi, b);
+}
+
+/* The 2D anisotropic-noise update (eom.hpp:16-58) on host half spectra; kpsi in/out. */
+void REFP(update_eom_hpfcnoise)(void* h, void* kpsi, const void* knl, const void* n1, const void* n2,
+                                const void* n3, double namp, double dt, double eps, double lx, double ly, double lz) {
+    RefState* s = (RefState*)h;
+    const size_t b = REFP(state_bytes)(h);
+    up(s, s->kpsi, kpsi, b);
+    up(s, s->knl, knl, b);
+    up(s, s->knoise, n1, b);
+    up(s, s->ktmp, n2, b);
+    up(s, s->lpsi, n3, b);
+    call_kernel_update_eom_hpfcnoise(*s->kpsi, *s->knl, *s->knoise, *s->ktmp, *s->lpsi, Float(namp), Float(dt),
+                                     Float(eps), mk3(lx, ly, lz));
+    down(s, s->kpsi, kpsi, b);
+}
+
 }  // extern "C"

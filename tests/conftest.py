@@ -30,15 +30,16 @@ SHIM_DRIVER = os.path.join(ROOT, "tests", "shim", "driver_step.cu")
 LIB_DIR = os.path.join(ROOT, "mcstar-libs_b200", "mcstar_b200", "lib")
 
 
-def build_shim_driver(flt, out):
-    """Compiles tests/shim/driver_step.cu against the mcstar-libs-named headers
-    (include/mcstar) and libpfc_b200 with FLOAT=flt; returns (returncode, output)."""
+def build_shim_driver(flt, out, source=SHIM_DRIVER):
+    """Compiles a driver of tests/shim/ (default driver_step.cu) against the
+    mcstar-libs-named headers (include/mcstar) and libpfc_b200 with FLOAT=flt;
+    returns (returncode, output)."""
     import shutil
     import subprocess
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
     cmd = [nvcc, "-std=c++17", "-O2", f"-DFLOAT={flt}", "-gencode", "arch=compute_100a,code=sm_100a",
            "-Xcompiler", "-Wall", "-I", os.path.join(ROOT, "include", "mcstar"), "-I", os.path.join(ROOT, "include"),
-           SHIM_DRIVER, "-L", LIB_DIR, "-lpfc_b200", f"-Xlinker", f"-rpath={LIB_DIR}", "-o", str(out)]
+           source, "-L", LIB_DIR, "-lpfc_b200", f"-Xlinker", f"-rpath={LIB_DIR}", "-o", str(out)]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
     return r.returncode, r.stdout + r.stderr
 

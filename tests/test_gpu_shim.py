@@ -18,13 +18,15 @@ pytestmark = pytest.mark.gpu
 _BUILT = {}
 
 
-def _driver(flt, tmp_path_factory):
-    if flt not in _BUILT:
+def _driver(flt, tmp_path_factory, name="driver_step.cu"):
+    key = (flt, name)
+    if key not in _BUILT:
+        from conftest import ROOT
         d = tmp_path_factory.mktemp("drv_" + flt)
-        rc, out = build_shim_driver(flt, d / "driver")
+        rc, out = build_shim_driver(flt, d / "driver", os.path.join(ROOT, "tests", "shim", name))
         assert rc == 0, out[-3000:]
-        _BUILT[flt] = str(d / "driver")
-    return _BUILT[flt]
+        _BUILT[key] = str(d / "driver")
+    return _BUILT[key]
 
 
 def _run(drv, shape, dx, steps, dt, eps, namp, seed, psi, outdir):
@@ -125,3 +127,36 @@ def test_reference_style_driver_matches_oracle(name, shape, flt, namp, steps, tm
             assert np.allclose(v, np.asarray(ref[col], dtype=np.float64), atol=2e-6), col
         if name.startswith("bcc"):
             assert np.all(table["nb"] == 8) and np.allclose(table["q6"], 0.628539, atol=1e-4)
+
+
+@pytest.mark.parametrize("flt", ["double", "float"])
+def test_relaxation_driver_matches_oracle(flt, tmp_path, tmp_path_factory):
+    """tests/shim/driver_relax.cu: exponential conserved steps (eom-exp.hpp) then the
+    non-conserved relaxation (el.hpp) until the largest mode change drops below 1e-3."""
+    dtype = np.float32 if flt == "float" else np.float64
+    drv = _driver(flt, tmp_path_factory, "driver_relax.cu")
+    shape, dx, steps, dt, eps = (32, 32, 16), math.pi / 4, 5, 0.5, 0.3
+    nx, ny, nz = shape
+    psi = (-0.2 + 0.05 * np.random.default_rng(21).uniform(-1, 1, (nz, ny, nx))).astype(dtype)
+    inp = os.path.join(tmp_path, "in.npy")
+    np.save(inp, psi)
+    r = subprocess.run([drv, str(nx), str(ny), str(nz), repr(dx), str(steps), repr(dt), repr(eps), inp, str(tmp_path)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    iters = int(next(ln.split()[1] for ln in r.stdout.splitlines() if ln.startswith("iters ")))
+    lens = _lens(shape, dx)
+    kop = O.init_eom_op(shape, lens, dt, eps)
+    k = O.r2c(psi.astype(np.float64))
+
+    def knl_of(k):
+        return O.r2c(O.psi3_split(O.c2r(k, shape), None, 0.0, norm=True))
+
+    for _ in range(steps):
+        k = O.update_eom_exp(kop, k, knl_of(k), None, 0.0, eps, lens, shape)
+    got = np.load(os.path.join(tmp_path, "kpsi_exp.npy")).reshape(O.cmpl_shape(shape))
+    tol = 1e-4 if dtype == np.float32 else 1e-12  # FP32: (e - 1)/L of the operator at small k
+    assert np.linalg.norm(got - k) / np.linalg.norm(k) < tol
+    for _ in range(min(iters + 1, 200)):
+        k, _change = O.update_el(k, knl_of(k), dt, eps, lens, shape)
+    got = np.load(os.path.join(tmp_path, "kpsi_el.npy")).reshape(O.cmpl_shape(shape))
+    assert np.linalg.norm(got - k) / np.linalg.norm(k) < tol

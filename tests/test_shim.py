@@ -11,7 +11,8 @@ from conftest import ROOT, build_shim_driver
 HEADERS = [
     "cuda/array_abstraction.hpp", "cuda/cufft_wrapper.hpp", "cuda/noise.hpp", "cuda/cutiming.hpp",
     "cuda/potentials.hpp", "cuda/kernels/common.hpp", "cuda/kernels/eom.hpp", "cuda/kernels/psi3_split.hpp",
-    "cuda/kernels/norm.hpp", "cuda/kernels/findpeaks.hpp", "cuda/kernels/findpeaks_2d.hpp", "common/pfc.hpp",
+    "cuda/kernels/norm.hpp", "cuda/kernels/findpeaks.hpp", "cuda/kernels/findpeaks_2d.hpp",
+    "cuda/kernels/eom-exp.hpp", "cuda/kernels/el.hpp", "cuda/kernels/el-exp.hpp", "common/pfc.hpp",
     "common/maximum_struct.hpp", "common/technicalities.hpp", "common/cu_error.hpp",
     "bond-order-analysis/bond-order.hpp",
 ]
@@ -29,9 +30,10 @@ def _lib_built():
 @pytest.mark.skipif(shutil.which("nvcc") is None and not os.path.exists("/usr/local/cuda/bin/nvcc"),
                     reason="nvcc not available")
 @pytest.mark.parametrize("flt", ["float", "double"])
-def test_reference_style_driver_compiles_and_links(flt, tmp_path):
+@pytest.mark.parametrize("driver", ["driver_step.cu", "driver_relax.cu"])
+def test_reference_style_driver_compiles_and_links(flt, driver, tmp_path):
     if not _lib_built():
         pytest.skip("libpfc_b200.so not built")
-    rc, out = build_shim_driver(flt, tmp_path / f"driver_{flt}")
+    rc, out = build_shim_driver(flt, tmp_path / f"drv_{flt}", os.path.join(ROOT, "tests", "shim", driver))
     assert rc == 0, out[-3000:]
     assert "warning" not in out.lower(), out[-3000:]
