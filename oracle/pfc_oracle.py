@@ -255,14 +255,18 @@ def update_eom_py(kpsi, knl, knoise, namp, dt, eps, lens, shape_xyz):
     return num / denom
 
 
-def update_eom_hpfcnoise(kpsi, knl, n1, n2, n3, namp, dt, eps, lens, shape_xyz):
+def update_eom_hpfcnoise(kpsi, knl, n1, n2, n3, namp, dt, eps, lens, shape_xyz, dtype=np.float64):
     """kernel_update_eom_hpfcnoise (eom.hpp:16-44), 2D: the noise
     (c1 kx^2 + c2 ky^2) xi1 + (c2 kx^2 + c1 ky^2) xi2 + 2 kx ky xi3 for |k| <= 0.25, kappa = 4/3,
-    c2 = sqrt(1 + kappa/2 + sqrt(1 + kappa)), c1 = kappa / (2 c2)."""
+    c2 = sqrt(1 + kappa/2 + sqrt(1 + kappa)), c1 = kappa / (2 c2): kappa and the sums in the
+    field's precision (dtype), both square roots in single precision (sqrtf)."""
     nx, ny, nz = shape_xyz
-    kappa = np.float32(4.0) / np.float32(3.0)
-    c2 = float(np.sqrt(np.float32(1.0) + kappa / np.float32(2.0) + np.sqrt(np.float32(1.0) + kappa)))
-    c1 = float(kappa) / c2 / 2.0
+    t = np.dtype(dtype).type
+    kappa = t(4.0) / t(3.0)
+    inner = t(np.sqrt(np.float32(t(1.0) + kappa)))
+    c2 = t(np.sqrt(np.float32(t(1.0) + kappa / t(2.0) + inner)))
+    c1 = float(kappa / c2 / t(2.0))
+    c2 = float(c2)
     k0 = wavenumbers(nx, lens[0], half=True)[None, None, :]
     k1 = wavenumbers(ny, lens[1])[None, :, None]
     dx, dy = _dops(shape_xyz, lens)

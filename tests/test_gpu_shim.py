@@ -154,7 +154,9 @@ def test_relaxation_driver_matches_oracle(flt, tmp_path, tmp_path_factory):
     for _ in range(steps):
         k = O.update_eom_exp(kop, k, knl_of(k), None, 0.0, eps, lens, shape)
     got = np.load(os.path.join(tmp_path, "kpsi_exp.npy")).reshape(O.cmpl_shape(shape))
-    tol = 1e-4 if dtype == np.float32 else 1e-12  # FP32: (e - 1)/L of the operator at small k
+    # the operator is exp(-L dt) in single precision (the reference's expf) in both
+    # precisions; CUDA's expf and numpy's float32 exp differ by up to a float ulp
+    tol = 1e-4 if dtype == np.float32 else 1e-7
     assert np.linalg.norm(got - k) / np.linalg.norm(k) < tol
     for _ in range(min(iters + 1, 200)):
         k, _change = O.update_el(k, knl_of(k), dt, eps, lens, shape)

@@ -17,6 +17,10 @@ pytestmark = pytest.mark.gpu
 
 # FP32 results against an FP64 restatement: a few ulps of the largest mode
 TOL = {F32: 4e-6, F64: 1e-12}
+# The operators of the exponential forms are exp(-L dt) evaluated by the reference with
+# expf, in single precision even for double fields; CUDA's expf and numpy's float32 exp
+# may differ by one float ulp, so operator-vs-oracle checks allow 2 float ulps.
+EXPF = 2.5e-7
 SHAPES = [(16, 12, 10), (32, 32, 32), (64, 48, 1), (15, 9, 7)]
 
 
@@ -78,9 +82,10 @@ def test_exponential_conserved_update(shape, dtype):
     ctx.init_eom_op(kop, dt, eps, lens)
     kop_w = O.init_eom_op(shape, lens, dt, eps)
     got_kop = down_c(ctx, kop)
-    assert rel_max(got_kop.real, kop_w.real) < TOL[dtype]
-    # the second factor loses digits to e - 1 at small k in single precision
-    assert rel_max(got_kop.imag, kop_w.imag) < (2e-4 if dtype == F32 else 1e-12)
+    assert rel_max(got_kop.real, kop_w.real) < max(TOL[dtype], EXPF)
+    # the second factor (e - 1)/L inherits the float ulp of e, amplified where L dt is
+    # small; in single precision it also loses digits to the subtraction
+    assert rel_max(got_kop.imag, kop_w.imag) < (2e-4 if dtype == F32 else 1e-5)
     kp, kn, kz = rand_c(shape, dtype, 1), rand_c(shape, dtype, 2), rand_c(shape, dtype, 3)
     for noise, fen in [(False, False), (True, False), (True, True)]:
         b, q, z = up_c(ctx, kp), up_c(ctx, kn), up_c(ctx, kz)
@@ -125,7 +130,7 @@ def test_relaxation_updates_and_largest_change(shape, dtype):
     ctx.init_el_op(kop, dt, eps, lens)
     got_kop = down_c(ctx, kop)
     kop_w = O.init_el_op(shape, lens, dt, eps)
-    assert rel_max(got_kop, kop_w) < TOL[dtype]
+    assert rel_max(got_kop, kop_w) < max(TOL[dtype], EXPF * 4)  # expf, see EXPF
     b, q = up_c(ctx, kp), up_c(ctx, kn)
     m = ctx.update_el_exp(kop, b, q)
     want, mw = O.update_el_exp(got_kop.astype(np.complex128), kp, kn)
@@ -161,7 +166,9 @@ def test_polynomial_kernel_update(shape, dtype):
     b = up_c(ctx, kp)
     ctx.update_eom_py(b, up_c(ctx, kn), up_c(ctx, kz), namp, dt, eps, lens)
     want = O.update_eom_py(kp, kn, kz, namp, dt, eps, lens, shape)
-    assert rel_max(down_c(ctx, b), want) < (2e-5 if dtype == F32 else 1e-11)  # P(k^2) cancels at large k
+    # P(k^2) (coefficients up to ~180) cancels strongly, so FP32 arithmetic -- the
+    # reference's own, checked tightly below -- is ~1e-4 from the FP64 restatement
+    assert rel_max(down_c(ctx, b), want) < (5e-4 if dtype == F32 else 1e-11)
     ref, L = ref_lib(dtype), ref_extra(dtype)
     if ref is not None and L is not None:
         nx, ny, nz = shape
@@ -181,7 +188,7 @@ def test_anisotropic_noise_update_2d(shape, dtype):
     n1, n2, n3 = (rand_c(shape, dtype, s) for s in (11, 12, 13))
     b = up_c(ctx, kp)
     ctx.update_eom_hpfcnoise(b, up_c(ctx, kn), up_c(ctx, n1), up_c(ctx, n2), up_c(ctx, n3), namp, dt, eps, lens)
-    want = O.update_eom_hpfcnoise(kp, kn, n1, n2, n3, namp, dt, eps, lens, shape)
+    want = O.update_eom_hpfcnoise(kp, kn, n1, n2, n3, namp, dt, eps, lens, shape, dtype=dtype)
     assert rel_max(down_c(ctx, b), want) < TOL[dtype]
     ref, L = ref_lib(dtype), ref_extra(dtype)
     if ref is not None and L is not None:
