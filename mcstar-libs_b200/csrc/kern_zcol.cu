@@ -39,9 +39,12 @@ struct ZCfg {
     // t-groups (kz = t U + ...) fall in different banks
     static constexpr int NHS = NZ * TX + (NZ / U) * 8;
     static constexpr int STG = NZ * TX;  // staging of one field tile, [z][c]
-    static constexpr size_t SMEM = (size_t)(2 * REG + NZ) * sizeof(float2);
-    static constexpr size_t SMEM_PIPE = (size_t)(2 * STG + 2 * REG + NHS + NZ) * sizeof(float2);
-    static constexpr size_t SMEM_CARRY = (size_t)(REG + STG + NZ) * sizeof(float2);  // TH threads, one field
+    // every kernel ends its shared memory with the twiddles W_NZ^m (NZ float2) and the
+    // wavenumbers k_z of the NZ modes (NZ floats)
+    static constexpr int TAIL = NZ + NZ / 2;
+    static constexpr size_t SMEM = (size_t)(2 * REG + TAIL) * sizeof(float2);
+    static constexpr size_t SMEM_PIPE = (size_t)(2 * STG + 2 * REG + NHS + TAIL) * sizeof(float2);
+    static constexpr size_t SMEM_CARRY = (size_t)(REG + STG + TAIL) * sizeof(float2);  // TH threads, one field
     // resident CTAs of k_zcarry the shared memory allows (228 KB per SM): its register cap
     static constexpr int CMINB = 4 * (SMEM_CARRY + 1024) <= 228 * 1024 ? 4 : 3;
     static_assert(TH % 32 == 0 && U * P == E && TX % U == 0 && 32 % TX == 0, "shape");
@@ -59,15 +62,44 @@ template <class Z> __device__ __forceinline__ int stg_row(int kz) {
     else return kz;
 }
 
+// Twiddles W_NZ^m and wavenumbers K(kz) = kz' 2 pi / L_z (common.hpp:27-28) of the
+// NZ modes into the shared tail of a z kernel (tw, then NZ floats).
+template <class Z>
+__device__ __forceinline__ float* load_tail(float2* tw, const float2* __restrict__ twg, const ZArgsF& a, int tid,
+                                           int nthreads) {
+    constexpr int NZ = Z::NZ;
+    float* kz_tab = reinterpret_cast<float*>(tw + NZ);
+    for (int i = tid; i < NZ; i += nthreads) {
+        tw[i] = twg[i];
+        kz_tab[i] = (float)(i < NZ / 2 + 1 ? i : i - NZ) * a.ckz;
+    }
+    return kz_tab;
+}
+
+// Non-finite watchdog of a column: every output of the inverse z transform depends on
+// every mode of its column, so one element per thread (all of them on the last step,
+// which has no inverse transform) shows a NaN or Inf anywhere in the column.
+template <class Z>
+__device__ __forceinline__ void watch(const float2 (&v)[Z::E], bool all, bool valid, int* flag) {
+    bool bad = !isfinite(v[0].x) || !isfinite(v[0].y);
+    if (all) {
+#pragma unroll
+        for (int j = 1; j < Z::E; ++j) bad |= !isfinite(v[j].x) || !isfinite(v[j].y);
+    }
+    if (bad && valid) atomicOr(flag, 1);
+}
+
 // The update of the thread's modes kz = (t U + u) + E k2 of column kx at ky; the result
 // replaces v.  kPsiInV: v holds psi^ and other(kz) returns N^; otherwise v holds N^ and
-// other(kz) returns psi^.  The noise pass is staged through the thread's own slots
-// scratch[slot(kz)]; kSync puts a barrier of the transforming threads (bar) first, for
-// a scratch that is an exchange buffer other threads may still be reading.
+// other(kz) returns psi^.  kz_tab: K(kz) of the NZ modes (load_tail).  The noise pass
+// is staged through the thread's own slots scratch[slot(kz)]; kSync puts a barrier of
+// the transforming threads (bar) first, for a scratch that is an exchange buffer other
+// threads may still be reading.  The k = 0 mode (register 0 of thread t = 0 in column
+// kx = 0 at ky = 0, where D = 1 and the noise vanishes) is set to the FP64 value k0.
 template <class Z, bool kPsiInV, bool kSync, class Bar, class OTHER, class SLOT>
 __device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2* scratch, SLOT slot, const Bar& bar,
-                                          int kx, int ky, int t, int nx, int ny, bool valid, const ZArgsF& a,
-                                          const double2* k0, int* flag) {
+                                          const float* kz_tab, int kx, int ky, int t, int nx, int ny,
+                                          const ZArgsF& a, const double2* k0) {
     constexpr int NZ = Z::NZ, E = Z::E, P = Z::P, U = Z::U;
     // wavenumbers K(i) = i' * 2 pi / L (common.hpp:27-28) with 2 pi / L precomputed
     const float k0x = (float)kx * a.ckx;
@@ -79,13 +111,12 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2
 #pragma unroll
         for (int k2 = 0; k2 < P; ++k2) {
             const int kz = (t * U + u) + E * k2;
-            float2 psi = kPsiInV ? v[u * P + k2] : other(kz);
+            const float2 psi = kPsiInV ? v[u * P + k2] : other(kz);
             const float2 n = kPsiInV ? other(kz) : v[u * P + k2];
-            const float k2z = (float)(kz < NZ / 2 + 1 ? kz : kz - NZ) * a.ckz;
+            const float k2z = kz_tab[kz];
             const float dopx = -kxy - k2z * k2z;
             const float dopy = dopx * dopx;
             const float inv = __frcp_rn(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
-            if (kx == 0 && ky == 0 && kz == 0) psi = make_float2((float)k0->x, (float)k0->y);
             const float f = a.dt * dopx;
             v[u * P + k2] = make_float2((psi.x + f * n.x) * inv, (psi.y + f * n.y) * inv);
         }
@@ -101,7 +132,7 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2
 #pragma unroll 1
         for (int m = 0; m < E; ++m) {
             const int kz = (t * U + m / P) + E * (m % P);
-            const float k2z = (float)(kz < NZ / 2 + 1 ? kz : kz - NZ) * a.ckz;
+            const float k2z = kz_tab[kz];
             const float dopx = -kxy - k2z * k2z;
             const float dopy = dopx * dopx;
             const float inv = __frcp_rn(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
@@ -117,10 +148,7 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2
 #pragma unroll
             for (int k2 = 0; k2 < P; ++k2) v[u * P + k2] = scratch[slot((t * U + u) + E * k2)];
     }
-    bool bad = false;
-#pragma unroll
-    for (int j = 0; j < E; ++j) bad |= !isfinite(v[j].x) || !isfinite(v[j].y);
-    if (bad && valid) atomicOr(flag, 1);
+    if (kx == 0 && ky == 0 && t == 0) v[0] = make_float2((float)k0->x, (float)k0->y);
 }
 
 // A' (D1 after the inverse FFT, scaled) or psi^' (D2, last step) for the thread's column
@@ -169,7 +197,7 @@ __global__ void __launch_bounds__(Z::T, Z::MINB) k_zcol(float2* A, const float2*
     float2* regB = sm + Z::REG;
     float2* tw = sm + 2 * Z::REG;
     const int tid = threadIdx.x;
-    for (int i = tid; i < NZ; i += Z::T) tw[i] = twg[i];
+    const float* kz_tab = load_tail<Z>(tw, twg, a, tid, Z::T);
     const int half = tid / TH;
     const int lt = tid - half * TH;
     const int c = lt % TX, t = lt / TX;
@@ -198,9 +226,10 @@ __global__ void __launch_bounds__(Z::T, Z::MINB) k_zcol(float2* A, const float2*
     }
     __syncthreads();
     if (half != 0) return;
-    propagate<Z, true, true>(v, [&](int kz) { return regB[own(kz)]; }, regB, own, bar, kx, ky, t, nx, ny, valid, a,
-                             k0, flag);
+    propagate<Z, true, true>(v, [&](int kz) { return regB[own(kz)]; }, regB, own, bar, kz_tab, kx, ky, t, nx, ny, a,
+                             k0);
     if (!a.final_step) fft_d2_to_d1<NZ, E, TX, 1, BarDyn, Z::PADG>(v, t, c, regA, tw, bar);
+    watch<Z>(v, a.final_step, valid, flag);
     store_state<Z>(v, A, base, zs, t, valid, a.final_step);
 }
 
@@ -246,7 +275,7 @@ __global__ void __launch_bounds__(Z::TH, Z::CMINB) k_zcarry(float2* kpsi, float2
         }
     }
     cp_commit();
-    for (int i = tid; i < NZ; i += TH) tw[i] = twg[i];
+    const float* kz_tab = load_tail<Z>(tw, twg, a, tid, TH);
     float2 v[E];
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = valid ? B[base + (int64_t)(t + P * j) * zs] : make_float2(0.f, 0.f);
@@ -257,11 +286,13 @@ __global__ void __launch_bounds__(Z::TH, Z::CMINB) k_zcarry(float2* kpsi, float2
     __syncthreads();  // psi^ staged by the other threads of the column is visible
     // the noise pass stages through the thread's own psi^ slots, read only by itself
     auto own = [&](int kz) { return stg_row<Z>(kz) * TX + c; };
-    propagate<Z, false, false>(v, [&](int kz) { return stg[own(kz)]; }, stg, own, BarCta{}, kx, ky, t, nx, ny, valid,
-                               a, k0, flag);
+    propagate<Z, false, false>(v, [&](int kz) { return stg[own(kz)]; }, stg, own, BarCta{}, kz_tab, kx, ky, t, nx, ny,
+                               a, k0);
+    if (a.final_step) watch<Z>(v, true, valid, flag);
     store_state<Z>(v, kpsi, base, zs, t, valid, true);
     if (a.final_step) return;
     fft_d2_to_d1<NZ, E, TX, 1, BarCta, Z::PADG>(v, t, c, xb, tw);
+    watch<Z>(v, false, valid, flag);
     store_state<Z>(v, A, base, zs, t, valid, false);
 }
 
@@ -285,7 +316,7 @@ __global__ void __launch_bounds__(Z::T, 1) k_zpipe(float2* A, const float2* __re
     float2* nh = regB + Z::REG;
     float2* tw = nh + Z::NHS;
     const int tid = threadIdx.x;
-    for (int i = tid; i < NZ; i += T) tw[i] = twg[i];
+    const float* kz_tab = load_tail<Z>(tw, twg, a, tid, T);
     __syncthreads();
     const int half = tid / TH;
     const int lt = tid - half * TH;
@@ -336,9 +367,10 @@ __global__ void __launch_bounds__(Z::T, 1) k_zpipe(float2* A, const float2* __re
             bar_sync(3, T);
             auto own = [&](int kz) { return kz * TX + c; };
             propagate<Z, true, true>(v, [&](int kz) { return nh[nh_slot<Z>(kz, c)]; }, regA, own, BarNamed<1, TH>{},
-                                     kx, ky, t, nx, ny, valid, a, k0, flag);
+                                     kz_tab, kx, ky, t, nx, ny, a, k0);
             if (has_next) bar_arrive(4, T);  // N^ slots free for the next tile
             if (!a.final_step) fft_d2_to_d1<NZ, E, TX, 1, BarNamed<1, TH>, Z::PADG>(v, t, c, regA, tw);
+            watch<Z>(v, a.final_step, valid, flag);
             store_state<Z>(v, A, base, zs, t, valid, a.final_step);
         }
         first = false;
