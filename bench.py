@@ -150,7 +150,8 @@ def kernel_table(prof, S, steps):
         # psi^ and B read, psi^' and A' written; the last step of a run writes psi^' only
         add("k_zcarry", 2, (4.0 * (steps - 1) + 3.0) / steps * S)
     else:
-        add("k_zcol" if prof["z_mode"] == 1 else "k_zprop", 2, 3.0 * S)
+        name = "k_zprop" if prof["z_mode"] == 0 else ("k_zcol3" if prof.get("z_variant") == 6 else "k_zcol")
+        add(name, 2, 3.0 * S)
     return t
 
 

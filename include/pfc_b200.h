@@ -243,7 +243,13 @@ typedef struct pfc_profile {
                                                     kernel, 2 register y/x/y passes  */
     int z_mode;                                  /* 0 general z pass, 1 register z pass
                                                     carrying A = IFFT_z(psi^)/nz, 2
-                                                    register z pass carrying psi^    */
+                                                    register z pass carrying psi^, 3
+                                                    register z pass carrying A in the
+                                                    kx-tiled layout                  */
+    int z_variant;                               /* register z kernel (0: none): 1-4
+                                                    square split for nz 512, 256, 128,
+                                                    64; 5: 16-column tiles; 6: 16
+                                                    values per thread (nz 512)       */
 } pfc_profile;
 pfc_status pfc_profile_enable(pfc_ctx* ctx, int on);
 pfc_status pfc_profile_read(pfc_ctx* ctx, pfc_profile* out);

@@ -173,15 +173,16 @@ ZPropArgs zargs(const pfc_ctx* c, const pfc_step_params* p) {
     return za;
 }
 
-// Where the stepper's mixed-grid field A = IFFT_z(psi^)/nz lives: beside the carried
-// psi^ (z_carry), or in place of it.
-void* carried_A(pfc_ctx* ctx, void* kpsi) { return ctx->z_carry ? ctx->work2 : kpsi; }
+// Where the stepper's mixed-grid field A = IFFT_z(psi^)/nz lives: in work2 beside the
+// carried psi^ (z_carry) or kx-tiled (tiled), else in place of psi^.
+void* carried_A(pfc_ctx* ctx, void* kpsi) { return ctx->z_carry || ctx->tiled ? ctx->work2 : kpsi; }
 
 // psi^ -> A = IFFT_z(psi^)/nz; the k = 0 mode is kept in FP64
 // complex FFT along z of a half-spectrum field: the register column kernel where the
 // length has one, else the general column pass
-cudaError_t zcols(const pfc_ctx* ctx, int dir, const void* in, void* out, double scale) {
-    if (ctx->fused_zfft) return launch_zfft(ctx, dir, in, out, scale);
+cudaError_t zcols(const pfc_ctx* ctx, int dir, const void* in, void* out, double scale, int lay = 0) {
+    if (ctx->fused_zfft) return launch_zfft(ctx, dir, in, out, scale, lay);
+    if (lay) return cudaErrorNotSupported;
     return launch_cols(ctx, 2, dir, in, out, scale);
 }
 // the same along y (register kernel only together with the register x rows)
@@ -194,7 +195,7 @@ cudaError_t step_entry(pfc_ctx* ctx, void* kpsi) {
     return traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
         cudaError_t e = launch_k0_save(ctx, kpsi);
         if (e || ctx->nz == 1) return e;
-        return zcols(ctx, 1, kpsi, carried_A(ctx, kpsi), 1.0 / ctx->nz);
+        return zcols(ctx, 1, kpsi, carried_A(ctx, kpsi), 1.0 / ctx->nz, ctx->tiled ? 2 : 0);
     });
 }
 
@@ -203,17 +204,24 @@ cudaError_t step_entry(pfc_ctx* ctx, void* kpsi) {
 cudaError_t step_exit(pfc_ctx* ctx, void* kpsi) {
     if (ctx->z_carry) return cudaSuccess;
     return traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
-        cudaError_t e = ctx->nz > 1 ? zcols(ctx, -1, kpsi, kpsi, 1.0) : cudaSuccess;
+        cudaError_t e = ctx->nz > 1 ? zcols(ctx, -1, carried_A(ctx, kpsi), kpsi, 1.0, ctx->tiled) : cudaSuccess;
         if (e) return e;
         return launch_k0_restore(ctx, kpsi);
     });
 }
 
-// B = FFT_xy(cubic term of IFFT_xy(A)) on the mixed grid
-cudaError_t step_xy(pfc_ctx* ctx, void* kpsi, const pfc_step_params* p) {
+// B = FFT_xy(cubic term of IFFT_xy(A)) on the mixed grid.  Tiled: A (work2) and, except
+// on the last step, the result B (the psi^ buffer, free while A carries the state) are
+// kx-tiled; the y-inverse writes work in the standard layout for the x pass.
+cudaError_t step_xy(pfc_ctx* ctx, void* kpsi, const pfc_step_params* p, bool last) {
     const void* A = carried_A(ctx, kpsi);
     void* B = ctx->work;
     const double mul = 1.0 / ((double)ctx->nx * (double)ctx->ny);
+    if (ctx->tiled)
+        return traced_xy3(
+            ctx, [&] { return launch_ypass(ctx, 1, A, B, 1.0, ctx->nz, 1); },
+            [&] { return launch_xpass(ctx, B, nullptr, mul, p->C, p->mu, ctx->nz); },
+            [&] { return last ? launch_ypass(ctx, -1, B, B, 1.0, ctx->nz) : launch_ypass(ctx, -1, B, kpsi, 1.0, ctx->nz, 2); });
     if (ctx->xy_mode == 1)
         return traced(ctx, 1, 1, [&] { return launch_fused_xy(ctx, A, B, nullptr, mul, p->C, p->mu); });
     if (ctx->xy_mode == 2) {
@@ -251,11 +259,17 @@ cudaError_t step_xy(pfc_ctx* ctx, void* kpsi, const pfc_step_params* p) {
     });
 }
 
-// the z pass with the semi-implicit update
+// the z pass with the semi-implicit update.  Tiled: A' stays kx-tiled in work2; the last
+// step reads B from work (standard) and writes psi^' to the caller's buffer.
 cudaError_t step_z(pfc_ctx* ctx, void* kpsi, const ZPropArgs& za) {
     void* B = ctx->work;
+    if (ctx->tiled) {
+        void* A = ctx->work2;
+        if (za.final_step) return traced(ctx, 2, 1, [&] { return launch_zcol(ctx, A, B, kpsi, za, 1); });
+        return traced(ctx, 2, 1, [&] { return launch_zcol(ctx, A, kpsi, A, za, 7); });
+    }
     if (ctx->z_carry) return traced(ctx, 2, 1, [&] { return launch_zcarry(ctx, kpsi, ctx->work2, B, za); });
-    if (ctx->fused_z) return traced(ctx, 2, 1, [&] { return launch_zcol(ctx, kpsi, B, za); });
+    if (ctx->fused_z) return traced(ctx, 2, 1, [&] { return launch_zcol(ctx, kpsi, B, kpsi, za); });
     return traced(ctx, 2, 1, [&] { return launch_zprop(ctx, kpsi, B, za); });
 }
 
@@ -390,8 +404,15 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
     // sweeps).  The slabbed xy passes and the pipelined z kernel need work2 / carry A.
     c->z_carry = 0;
     if (const char* s = getenv("PFC_Z_CARRY")) c->z_carry = c->fused_z && atoi(s) != 0;
-    if (c->fused_z == 5) c->z_pipe = 0;  // the 16-column z variant exists as k_zcol only
-    if (c->slab > 0 || c->z_pipe || c->fused_z == 5) c->z_carry = 0;
+    if (c->slab > 0 || c->z_pipe) c->z_carry = 0;
+    // the pipelined and the psi^-carrying z kernels exist for the square split only
+    if ((c->z_pipe || c->z_carry) && c->fused_z >= 5) c->fused_z = 1;
+    // kx-tiled A and B (measured faster: whole-block z columns); PFC_TILED=0 keeps the
+    // standard layout.  Needs the register y, x, z passes, whole fields, and the register
+    // column kernel for the entry / exit z transforms.
+    c->tiled = c->fused_z && c->fused_zfft && c->xy_mode == 2 && c->fused_y && c->fused_y < 6 && c->slab == 0 &&
+               !c->z_pipe && !c->z_carry;
+    if (const char* s = getenv("PFC_TILED")) c->tiled = c->tiled && atoi(s) != 0;
     // L2 prefetch of the register passes, in waves of CTAs ahead (PFC_PREFETCH)
     c->pf_waves = 0.f;
     if (const char* s = getenv("PFC_PREFETCH")) c->pf_waves = std::max(0.f, (float)atof(s));
@@ -601,7 +622,7 @@ pfc_status pfc_step(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params*
     PFC_CUDA(cudaMemsetAsync(ctx->flag, 0, sizeof(int), ctx->stream), "pfc_step flag");
     PFC_CUDA(step_entry(ctx, kpsi), "pfc_step entry");
     for (int t = 0; t < nsteps; ++t) {
-        PFC_CUDA(step_xy(ctx, kpsi, p), "pfc_step xy");
+        PFC_CUDA(step_xy(ctx, kpsi, p, t == nsteps - 1), "pfc_step xy");
         za.counter = p->counter + (uint64_t)t;
         za.final_step = (t == nsteps - 1);  // the last step writes psi^ itself
         PFC_CUDA(step_z(ctx, kpsi, za), "pfc_step z");
@@ -789,7 +810,7 @@ pfc_status pfc_ensemble_create(int n, pfc_ctx* const* ctxs, void* const* kpsis, 
             ZPropArgs za = zargs(c, &e->p[i]);
             za.dev_counter = e->ctr + i;
             for (int s = 0; s < steps_per_graph && !ie; ++s) {
-                ie = step_xy(c, e->kpsi[i], &e->p[i]);
+                ie = step_xy(c, e->kpsi[i], &e->p[i], false);
                 if (!ie) ie = step_z(c, e->kpsi[i], za);
                 if (!ie) ie = launch_counter(e->st[i], e->ctr + i, 0, 0);
             }
@@ -882,7 +903,8 @@ pfc_status pfc_profile_read(pfc_ctx* ctx, pfc_profile* out) {
     out->launches = ctx->launches;
     out->xy_variant = ctx->xy_mode == 1 ? ctx->fused_xy : 0;
     out->xy_mode = ctx->xy_mode;
-    out->z_mode = ctx->z_carry ? 2 : (ctx->fused_z ? 1 : 0);
+    out->z_mode = ctx->z_carry ? 2 : (ctx->tiled ? 3 : (ctx->fused_z ? 1 : 0));
+    out->z_variant = ctx->fused_z;
     for (int f = 0; f < PFC_PROFILE_FAMILIES; ++f) { out->calls[f] = ctx->prof_calls[f]; out->ms[f] = ctx->prof_ms[f]; }
     return PFC_OK;
 }

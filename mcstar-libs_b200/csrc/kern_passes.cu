@@ -32,14 +32,14 @@ struct YCfg {
 
 template <class Y, int DIR, bool kZ>
 __global__ void __launch_bounds__(Y::T, Y::MINB)
-    k_ycol(const float2* in, float2* out, int nxh, int64_t ps_z, int ls_z, const float2* __restrict__ twg,
+    k_ycol(const float2* in, float2* out, int nxh, int ny, int nz, int lay, const float2* __restrict__ twg,
            float scale, int pf) {
-    // columns of NY elements ls apart, starting at kx + blockIdx.y * ps: y columns of one
-    // z-plane (kZ false: ps = ny nxh, ls = nxh) or z columns at one ky (kZ: the strides
-    // passed, ps = nxh, ls = ny nxh)
+    // the columns of NY elements of kx tile blockIdx.x at plane blockIdx.y: y columns of
+    // z-plane blockIdx.y (kZ false) or z columns at ky = blockIdx.y (kZ); lay bit 0: the
+    // input is kx-tiled, bit 1: the output (standard layout otherwise; col_addr).  With the
+    // standard layout on both sides, in may equal out.  pf (standard input only): L2
+    // prefetch distance in tiles.
     constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P, U = Y::U;
-    const int64_t ps = kZ ? ps_z : (int64_t)NY * nxh;
-    const int ls = kZ ? ls_z : nxh;
     extern __shared__ __align__(16) float2 sm[];
     float2* xb = sm;
     float2* tw = sm + Y::XB;
@@ -48,31 +48,70 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
     const int c = tid % TX, t = tid / TX;
     const int kx = blockIdx.x * TX + c;
     const bool valid = kx < nxh;
-    const int64_t base = (int64_t)blockIdx.y * ps + kx;
+    const ColAddr ai = col_addr(lay & 1, kZ, kx, blockIdx.y, nxh, ny, nz);
     float2 v[E];
 #pragma unroll
-    for (int j = 0; j < E; ++j) v[j] = valid ? in[base + (int64_t)(t + P * j) * ls] : make_float2(0.f, 0.f);
+    for (int j = 0; j < E; ++j) v[j] = valid ? in[ai.base + (int64_t)(t + P * j) * ai.stride] : make_float2(0.f, 0.f);
     if (pf) {
         // L2 prefetch of the tile pf tiles ahead in launch order: its segment of every line
         const int ntx = (int)gridDim.x;
         const int tgt = (int)(blockIdx.y * gridDim.x + blockIdx.x) + pf;
         if (tgt < ntx * (int)gridDim.y) {
             const int kx0 = (tgt % ntx) * TX;
-            const float2* f = in + (int64_t)(tgt / ntx) * ps + kx0;
+            const ColAddr ap = col_addr(false, kZ, kx0, tgt / ntx, nxh, ny, nz);
             const unsigned bytes = (unsigned)(min(TX, nxh - kx0) * sizeof(float2));
-            for (int y = tid; y < NY; y += Y::T) l2_prefetch(f + (int64_t)y * ls, bytes);
+            for (int y = tid; y < NY; y += Y::T) l2_prefetch(in + ap.base + (int64_t)y * ap.stride, bytes);
         }
     }
     __syncthreads();
     fft_d1_to_d2<NY, E, TX, DIR, BarCta, Y::PADG>(v, t, c, xb, tw);
     if (valid) {
+        const ColAddr ao = col_addr(lay & 2, kZ, kx, blockIdx.y, nxh, ny, nz);
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
             for (int k2 = 0; k2 < P; ++k2) {
                 const float2 w = v[u * P + k2];
-                out[base + (int64_t)((t * U + u) + E * k2) * ls] = make_float2(w.x * scale, w.y * scale);
+                out[ao.base + (int64_t)((t * U + u) + E * k2) * ao.stride] = make_float2(w.x * scale, w.y * scale);
             }
+    }
+}
+
+// y columns of N = 2 E^2 points with E values per thread and 2E threads per column
+// (fft_d1_to_d3): half the registers of YCfg's square split, so more resident warps.
+template <int NY_, int E_, int TX_, int MINB_>
+struct YCfg3 {
+    static constexpr int NY = NY_, E = E_, TX = TX_, P = 2 * E, T = TX * P, MINB = MINB_;
+    static constexpr int XB = E * (P + 1) * TX;
+    static constexpr size_t SMEM = (size_t)(XB + NY) * sizeof(float2);
+    static_assert(P * E == NY && 32 % TX == 0, "shape");
+};
+
+template <class Y, int DIR>
+__global__ void __launch_bounds__(Y::T, Y::MINB)
+    k_ycol3(const float2* in, float2* out, int nxh, const float2* __restrict__ twg, float scale) {
+    constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* xb = sm;
+    float2* tw = sm + Y::XB;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < NY; i += Y::T) tw[i] = twg[i];
+    const int c = tid % TX, t = tid / TX;
+    const int kx = blockIdx.x * TX + c;
+    const bool valid = kx < nxh;
+    const int64_t base = (int64_t)blockIdx.y * NY * nxh + kx;
+    float2 v[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = valid ? in[base + (int64_t)(t + P * j) * nxh] : make_float2(0.f, 0.f);
+    __syncthreads();
+    fft_d1_to_d3<NY, E, TX, DIR>(v, t, c, xb, tw);
+    if (valid) {
+        const int p = t >> 1, h = t & 1;
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const int k = p + E * d3_k2<E>(r, h);
+            out[base + (int64_t)k * nxh] = make_float2(v[r].x * scale, v[r].y * scale);
+        }
     }
 }
 
@@ -191,6 +230,25 @@ __global__ void __launch_bounds__(X::T, X::MINB)
 
 using Y512 = YCfg<512, 32, 8>;
 using Y512w = YCfg<512, 32, 16>;  // 128-byte column segments, 256 threads
+using Y512h = YCfg3<512, 16, 8, 3>;  // 16 values per thread, 256 threads per 8 columns
+using Y512q = YCfg3<512, 16, 8, 4>;  // the same capped at 64 registers (4 CTAs per SM)
+
+template <class Y>
+cudaError_t y3attr() {
+    cudaError_t e = cudaFuncSetAttribute(k_ycol3<Y, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Y::SMEM);
+    if (e) return e;
+    return cudaFuncSetAttribute(k_ycol3<Y, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Y::SMEM);
+}
+template <class Y>
+cudaError_t y3launch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs) {
+    dim3 grid((c->nxh + Y::TX - 1) / Y::TX, nzs);
+    const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->ypass_tw_off;
+    if (dir > 0)
+        k_ycol3<Y, 1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, tw, (float)scale);
+    else
+        k_ycol3<Y, -1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, tw, (float)scale);
+    return cudaGetLastError();
+}
 using Y256 = YCfg<256, 16, 8>;
 using Y128 = YCfg<128, 16, 8>;
 using Y64 = YCfg<64, 8, 8>;
@@ -215,31 +273,31 @@ cudaError_t xattr() {
     return e;
 }
 
-// complex FFTs of the columns (lines of Y::NY elements ls apart) of the kx tiles of
-// `planes` planes ps apart (kZ; y columns of z-planes otherwise); twiddles W_NY^m at tw_off
+// complex FFTs of the columns of the kx tiles of `planes` planes: z columns at each ky
+// (kZ) or y columns of each z-plane; lay: the layouts of in / out (k_ycol); twiddles
+// W_NY^m at tw_off
 template <class Y, bool kZ>
-cudaError_t collaunch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int planes, int64_t ps,
-                      int ls, int tw_off) {
+cudaError_t collaunch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int planes, int lay,
+                      int tw_off) {
     dim3 grid((c->nxh + Y::TX - 1) / Y::TX, planes);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + tw_off;
     static const int per_sm = resident_ctas(k_ycol<Y, 1, kZ>, Y::T, Y::SMEM);
-    const int pf = prefetch_ahead(c, per_sm, in);
+    const int pf = (lay & 1) ? 0 : prefetch_ahead(c, per_sm, in);
     if (dir > 0)
-        k_ycol<Y, 1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, ps, ls, tw,
-                                                             (float)scale, pf);
+        k_ycol<Y, 1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->ny, c->nz,
+                                                             lay, tw, (float)scale, pf);
     else
-        k_ycol<Y, -1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, ps, ls, tw,
-                                                              (float)scale, pf);
+        k_ycol<Y, -1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->ny, c->nz,
+                                                              lay, tw, (float)scale, pf);
     return cudaGetLastError();
 }
 template <class Y>
-cudaError_t ylaunch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs) {
-    return collaunch<Y, false>(c, dir, in, out, scale, nzs, 0, 0, c->ypass_tw_off);
+cudaError_t ylaunch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs, int lay) {
+    return collaunch<Y, false>(c, dir, in, out, scale, nzs, lay, c->ypass_tw_off);
 }
 template <class Y>
-cudaError_t zlaunch_fft(const pfc_ctx* c, int dir, const void* in, void* out, double scale) {
-    // z line stride ny nxh: an int for every shape with fewer than 2^31 complex modes
-    return collaunch<Y, true>(c, dir, in, out, scale, c->ny, c->nxh, c->ny * c->nxh, c->zfft_tw_off);
+cudaError_t zlaunch_fft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay) {
+    return collaunch<Y, true>(c, dir, in, out, scale, c->ny, lay, c->zfft_tw_off);
 }
 template <class X, int MODE>
 cudaError_t xlaunch(const pfc_ctx* c, const void* in, void* out, const void* pot, double mul, double C, double mu,
@@ -266,7 +324,10 @@ static int env_choice(const char* name) {
 int fused_y_variant(int ny, int dtype) {
     if (dtype != PFC_F32) return 0;
     switch (ny) {
-        case 512: return env_choice("PFC_Y_VARIANT") == 5 ? 5 : 1;
+        case 512: {
+            const int v = env_choice("PFC_Y_VARIANT");  // 5: 128-byte segments; 6, 7: 16 values per thread
+            return (v == 5 || v == 6 || v == 7) ? v : 1;
+        }
         case 256: return 2;
         case 128: return 3;
         case 64: return 4;
@@ -292,6 +353,8 @@ cudaError_t set_pass_attributes(const pfc_ctx* c) {
         case 3: e = yattr<Y128, false>(); break;
         case 4: e = yattr<Y64, false>(); break;
         case 5: e = yattr<Y512w, false>(); break;
+        case 6: e = y3attr<Y512h>(); break;
+        case 7: e = y3attr<Y512q>(); break;
     }
     if (e) return e;
     switch (c->fused_x) {
@@ -304,13 +367,16 @@ cudaError_t set_pass_attributes(const pfc_ctx* c) {
     return e;
 }
 
-cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs) {
+cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs, int lay) {
+    if (lay && (nzs != c->nz || c->fused_y >= 6)) return cudaErrorNotSupported;  // whole fields, k_ycol only
     switch (c->fused_y) {
-        case 1: return ylaunch<Y512>(c, dir, in, out, scale, nzs);
-        case 2: return ylaunch<Y256>(c, dir, in, out, scale, nzs);
-        case 3: return ylaunch<Y128>(c, dir, in, out, scale, nzs);
-        case 4: return ylaunch<Y64>(c, dir, in, out, scale, nzs);
-        case 5: return ylaunch<Y512w>(c, dir, in, out, scale, nzs);
+        case 1: return ylaunch<Y512>(c, dir, in, out, scale, nzs, lay);
+        case 2: return ylaunch<Y256>(c, dir, in, out, scale, nzs, lay);
+        case 3: return ylaunch<Y128>(c, dir, in, out, scale, nzs, lay);
+        case 4: return ylaunch<Y64>(c, dir, in, out, scale, nzs, lay);
+        case 5: return ylaunch<Y512w>(c, dir, in, out, scale, nzs, lay);
+        case 6: return y3launch<Y512h>(c, dir, in, out, scale, nzs);
+        case 7: return y3launch<Y512q>(c, dir, in, out, scale, nzs);
     }
     return cudaErrorNotSupported;
 }
@@ -357,12 +423,12 @@ cudaError_t set_zfft_attributes(const pfc_ctx* c) {
     }
     return cudaSuccess;
 }
-cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, double scale) {
+cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay) {
     switch (c->fused_zfft) {
-        case 1: return zlaunch_fft<Y512>(c, dir, in, out, scale);
-        case 2: return zlaunch_fft<Y256>(c, dir, in, out, scale);
-        case 3: return zlaunch_fft<Y128>(c, dir, in, out, scale);
-        case 4: return zlaunch_fft<Y64>(c, dir, in, out, scale);
+        case 1: return zlaunch_fft<Y512>(c, dir, in, out, scale, lay);
+        case 2: return zlaunch_fft<Y256>(c, dir, in, out, scale, lay);
+        case 3: return zlaunch_fft<Y128>(c, dir, in, out, scale, lay);
+        case 4: return zlaunch_fft<Y64>(c, dir, in, out, scale, lay);
     }
     return cudaErrorNotSupported;
 }

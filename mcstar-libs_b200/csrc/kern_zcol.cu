@@ -187,8 +187,11 @@ __device__ __forceinline__ void prefetch_ztile(const float2* f0, const float2* f
     }
 }
 
+// lay bits 0, 1, 2: A, B, O kx-tiled (col_addr); O may be A when their layouts agree.
+// pf: L2 prefetch distance in tiles (standard layouts only).
 template <class Z>
-__global__ void __launch_bounds__(Z::T, Z::MINB) k_zcol(float2* A, const float2* __restrict__ B, int nx, int ny, ZArgsF a,
+__global__ void __launch_bounds__(Z::T, Z::MINB) k_zcol(const float2* A, const float2* __restrict__ B, float2* O,
+                                                   int nx, int ny, int lay, ZArgsF a,
                                                    const double2* __restrict__ k0, int* flag,
                                                    const float2* __restrict__ twg, int pf) {
     constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, U = Z::U, TH = Z::TH;
@@ -205,13 +208,12 @@ __global__ void __launch_bounds__(Z::T, Z::MINB) k_zcol(float2* A, const float2*
     const int ky = blockIdx.y;
     const int nxh = nx / 2 + 1;
     const bool valid = kx < nxh;  // the last tile holds only the kx = nx/2 column
-    const int64_t zs = (int64_t)ny * nxh;
-    const int64_t base = (int64_t)ky * nxh + kx;
     const float2* src = half ? B : A;
+    const ColAddr ca = col_addr(lay & (half ? 2 : 1), true, kx, ky, nxh, ny, NZ);
     float2 v[E];
 #pragma unroll
-    for (int j = 0; j < E; ++j) v[j] = valid ? src[base + (int64_t)(t + P * j) * zs] : make_float2(0.f, 0.f);
-    if (pf) prefetch_ztile<NZ, TX>(A, B, pf, nxh, zs, tid, Z::T);
+    for (int j = 0; j < E; ++j) v[j] = valid ? src[ca.base + (int64_t)(t + P * j) * ca.stride] : make_float2(0.f, 0.f);
+    if (pf) prefetch_ztile<NZ, TX>(A, B, pf, nxh, (int64_t)ny * nxh, tid, Z::T);
     __syncthreads();
     // both halves run one copy of the forward transform, each on its own named barrier
     const BarDyn bar{1 + half, TH};
@@ -230,7 +232,121 @@ __global__ void __launch_bounds__(Z::T, Z::MINB) k_zcol(float2* A, const float2*
                              k0);
     if (!a.final_step) fft_d2_to_d1<NZ, E, TX, 1, BarDyn, Z::PADG>(v, t, c, regA, tw, bar);
     watch<Z>(v, a.final_step, valid, flag);
-    store_state<Z>(v, A, base, zs, t, valid, a.final_step);
+    const ColAddr co = col_addr(lay & 4, true, kx, ky, nxh, ny, NZ);
+    store_state<Z>(v, O, co.base, co.stride, t, valid, a.final_step);
+}
+
+// ---- the z pass with E values per thread over 2E threads per column (NZ = 2 E^2,
+// fft_d1_to_d3): half the registers of k_zcol's square split, so twice the resident warps.
+template <int NZ_, int E_, int TX_>
+struct Z3Cfg {
+    static constexpr int NZ = NZ_, E = E_, TX = TX_, P = 2 * E, TH = TX * P, T = 2 * TH;
+    static constexpr int REG = E * (P + 1) * TX;  // exchange buffer of one half
+    static constexpr int TAIL = NZ + NZ / 2;
+    static constexpr size_t SMEM = (size_t)(2 * REG + TAIL) * sizeof(float2);
+    static_assert(P * E == NZ && TH % 32 == 0 && REG >= NZ * TX, "shape");
+};
+
+// propagate for distribution D3: register r of thread t = 2p + h holds mode
+// kz = p + E d3_k2(r, h); nl(kz) returns N^ (v holds psi^)
+template <class Z, class Bar, class NL, class SLOT>
+__device__ __forceinline__ void propagate3(float2 (&v)[Z::E], NL nl, float2* scratch, SLOT slot, const Bar& bar,
+                                           const float* kz_tab, int kx, int ky, int t, int nx, int ny,
+                                           const ZArgsF& a, const double2* k0) {
+    constexpr int NZ = Z::NZ, E = Z::E;
+    const int p = t >> 1, h = t & 1;
+    const float k0x = (float)kx * a.ckx;
+    const float k1y = (float)(ky < ny / 2 + 1 ? ky : ky - ny) * a.cky;
+    const float kxy = k0x * k0x + k1y * k1y;
+    const float deps = 1.0f + a.C - a.eps;
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const int kz = p + E * d3_k2<E>(r, h);
+        const float2 psi = v[r];
+        const float2 n = nl(kz);
+        const float k2z = kz_tab[kz];
+        const float dopx = -kxy - k2z * k2z;
+        const float dopy = dopx * dopx;
+        const float inv = __frcp_rn(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
+        const float f = a.dt * dopx;
+        v[r] = make_float2((psi.x + f * n.x) * inv, (psi.y + f * n.y) * inv);
+    }
+    if (a.use_noise) {
+        bar.sync();  // the scratch is the exchange buffer of the transform
+        const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
+#pragma unroll
+        for (int r = 0; r < E; ++r) scratch[slot(p + E * d3_k2<E>(r, h))] = v[r];
+#pragma unroll 1
+        for (int r = 0; r < E; ++r) {
+            const int kz = p + E * d3_k2<E>(r, h);
+            const float k2z = kz_tab[kz];
+            const float dopx = -kxy - k2z * k2z;
+            const float dopy = dopx * dopx;
+            const float inv = __frcp_rn(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
+            const float2 xi = kspace_noise<float>(kx, ky, kz, nx, ny, NZ, a.seed, ctr);
+            const float g = a.dt * a.namp_eff * sqrtf(-dopx) * inv;
+            float2 w = scratch[slot(kz)];
+            w.x += g * xi.x;
+            w.y += g * xi.y;
+            scratch[slot(kz)] = w;
+        }
+#pragma unroll
+        for (int r = 0; r < E; ++r) v[r] = scratch[slot(p + E * d3_k2<E>(r, h))];
+    }
+    if (kx == 0 && ky == 0 && t == 0) v[0] = make_float2((float)k0->x, (float)k0->y);  // kz = 0 at r = 0
+}
+
+// LAY: the layouts of A, B, O as k_zcol's lay, fixed at compile time (0, 1 or 7)
+template <class Z, int LAY>
+__global__ void __launch_bounds__(Z::T, 2) k_zcol3(const float2* A, const float2* __restrict__ B, float2* O, int nx,
+                                                    int ny, ZArgsF a, const double2* __restrict__ k0, int* flag,
+                                                    const float2* __restrict__ twg) {
+    constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, TH = Z::TH;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* regA = sm;
+    float2* regB = sm + Z::REG;
+    float2* tw = sm + 2 * Z::REG;
+    const int tid = threadIdx.x;
+    const float* kz_tab = load_tail<Z>(tw, twg, a, tid, Z::T);
+    const int half = tid / TH;
+    const int lt = tid - half * TH;
+    const int c = lt % TX, t = lt / TX;
+    const int kx = blockIdx.x * TX + c;
+    const int ky = blockIdx.y;
+    const int nxh = nx / 2 + 1;
+    const bool valid = kx < nxh;
+    const float2* src = half ? B : A;
+    static_assert(TX == kTileW, "the tiles of the kx-tiled layout");
+    const ColAddr ca = half ? zcol_addr<(LAY & 2) != 0>(blockIdx.x, c, ky, nxh, ny, NZ)
+                            : zcol_addr<(LAY & 1) != 0>(blockIdx.x, c, ky, nxh, ny, NZ);
+    float2 v[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = valid ? src[ca.base + (int64_t)(t + P * j) * ca.stride] : make_float2(0.f, 0.f);
+    __syncthreads();
+    const BarDyn bar{1 + half, TH};
+    fft_d1_to_d3<NZ, E, TX, -1, BarDyn>(v, t, c, half ? regB : regA, tw, bar);
+    const int p = t >> 1, h = t & 1;
+    auto own = [&](int kz) { return kz * TX + c; };  // N^ hand-over slots (two wavefronts per access)
+    if (half != 0) {
+        bar.sync();
+#pragma unroll
+        for (int r = 0; r < E; ++r) regB[own(p + E * d3_k2<E>(r, h))] = v[r];
+    }
+    __syncthreads();
+    if (half != 0) return;
+    propagate3<Z>(v, [&](int kz) { return regB[own(kz)]; }, regB, own, bar, kz_tab, kx, ky, t, nx, ny, a, k0);
+    if (!a.final_step) fft_d3_to_d1<NZ, E, TX, 1, BarDyn>(v, t, c, regA, tw, bar);
+    watch<Z>(v, a.final_step, valid, flag);
+    if (!valid) return;
+    const ColAddr co = zcol_addr<(LAY & 4) != 0>(blockIdx.x, c, ky, nxh, ny, NZ);
+    if (a.final_step) {
+#pragma unroll
+        for (int r = 0; r < E; ++r) O[co.base + (int64_t)(p + E * d3_k2<E>(r, h)) * co.stride] = v[r];
+    } else {
+        const float s = 1.0f / (float)NZ;
+#pragma unroll
+        for (int j = 0; j < E; ++j) O[co.base + (int64_t)(t + P * j) * co.stride] = make_float2(v[j].x * s, v[j].y * s);
+    }
 }
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
@@ -380,6 +496,7 @@ __global__ void __launch_bounds__(Z::T, 1) k_zpipe(float2* A, const float2* __re
 
 using Z512 = ZCfg<512, 32, 8>;
 using Z512w = ZCfg<512, 32, 16>;  // 128-byte column segments, one 512-thread CTA per SM (k_zcol only)
+using Z3_512 = Z3Cfg<512, 16, 8>;  // 16 values per thread (k_zcol3)
 using Z256 = ZCfg<256, 16, 8>;
 using Z128 = ZCfg<128, 16, 8>;
 using Z64 = ZCfg<64, 8, 8>;
@@ -411,20 +528,22 @@ cudaError_t zlaunch_carry(const pfc_ctx* c, void* kpsi, void* A, const void* B, 
 }
 
 template <class Z>
-cudaError_t zlaunch(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& p) {
+cudaError_t zlaunch(const pfc_ctx* c, const void* A, const void* B, void* O, const ZPropArgs& p, int lay) {
     const ZArgsF a = zargs_f(p);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
     const int ntx = (c->nxh + Z::TX - 1) / Z::TX;
     if (c->z_pipe) {
+        if (lay || O != A) return cudaErrorNotSupported;  // standard layout, in place
         const int ntiles = ntx * c->ny;
         const int grid = ntiles < c->num_sms ? ntiles : c->num_sms;
-        k_zpipe<Z><<<grid, Z::T, Z::SMEM_PIPE, c->stream>>>((float2*)A, (const float2*)B, c->nx, c->ny, a, c->k0,
+        k_zpipe<Z><<<grid, Z::T, Z::SMEM_PIPE, c->stream>>>((float2*)O, (const float2*)B, c->nx, c->ny, a, c->k0,
                                                              c->flag, tw);
     } else {
         static const int per_sm = resident_ctas(k_zcol<Z>, Z::T, Z::SMEM);
         dim3 grid(ntx, c->ny);
-        k_zcol<Z><<<grid, Z::T, Z::SMEM, c->stream>>>((float2*)A, (const float2*)B, c->nx, c->ny, a, c->k0, c->flag,
-                                                       tw, prefetch_ahead(c, per_sm, A, B));
+        const int pf = lay ? 0 : prefetch_ahead(c, per_sm, A, B);
+        k_zcol<Z><<<grid, Z::T, Z::SMEM, c->stream>>>((const float2*)A, (const float2*)B, (float2*)O, c->nx, c->ny,
+                                                       lay, a, c->k0, c->flag, tw, pf);
     }
     return cudaGetLastError();
 }
@@ -435,8 +554,10 @@ int fused_z_variant(int nx, int nz, int dtype) {
     if (dtype != PFC_F32 || nx < 16 || (nx / 2) % 8 != 0 || nx % 2 != 0) return 0;
     switch (nz) {
         case 512: {
-            const char* s = getenv("PFC_Z_VARIANT");  // 5: 16-column tiles (measurement variant)
-            return s && atoi(s) == 5 ? 5 : 1;
+            // 6 (default): 16 values per thread; 1: the square split; 5: 16-column tiles
+            const char* s = getenv("PFC_Z_VARIANT");
+            const int v = s ? atoi(s) : 6;
+            return (v == 1 || v == 5) ? v : 6;
         }
         case 256: return 2;
         case 128: return 3;
@@ -454,6 +575,17 @@ cudaError_t set_zcol_attributes(const pfc_ctx* c) {
         case 5:
             return cudaFuncSetAttribute(k_zcol<Z512w>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)Z512w::SMEM);
+        case 6: {
+            cudaError_t e = cudaFuncSetAttribute(k_zcol3<Z3_512, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)Z3_512::SMEM);
+            if (!e)
+                e = cudaFuncSetAttribute(k_zcol3<Z3_512, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)Z3_512::SMEM);
+            if (!e)
+                e = cudaFuncSetAttribute(k_zcol3<Z3_512, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)Z3_512::SMEM);
+            return e;
+        }
     }
     return cudaSuccess;
 }
@@ -468,21 +600,32 @@ cudaError_t launch_zcarry(const pfc_ctx* c, void* kpsi, void* A, const void* B, 
     return cudaErrorNotSupported;
 }
 
-cudaError_t launch_zcol(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a) {
+cudaError_t launch_zcol(const pfc_ctx* c, const void* A, const void* B, void* O, const ZPropArgs& a, int lay) {
     switch (c->fused_z) {
         case 5: {
             using Z = Z512w;
             static const int per_sm = resident_ctas(k_zcol<Z>, Z::T, Z::SMEM);
             const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
             dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny);
-            k_zcol<Z><<<grid, Z::T, Z::SMEM, c->stream>>>((float2*)A, (const float2*)B, c->nx, c->ny, zargs_f(a), c->k0,
-                                                           c->flag, tw, prefetch_ahead(c, per_sm, A, B));
+            const int pf = lay ? 0 : prefetch_ahead(c, per_sm, A, B);
+            k_zcol<Z><<<grid, Z::T, Z::SMEM, c->stream>>>((const float2*)A, (const float2*)B, (float2*)O, c->nx, c->ny,
+                                                           lay, zargs_f(a), c->k0, c->flag, tw, pf);
             return cudaGetLastError();
         }
-        case 1: return zlaunch<Z512>(c, A, B, a);
-        case 2: return zlaunch<Z256>(c, A, B, a);
-        case 3: return zlaunch<Z128>(c, A, B, a);
-        case 4: return zlaunch<Z64>(c, A, B, a);
+        case 6: {
+            using Z = Z3_512;
+            const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
+            dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny);
+            auto k = lay == 7 ? k_zcol3<Z, 7> : lay == 1 ? k_zcol3<Z, 1> : k_zcol3<Z, 0>;
+            if (lay != 0 && lay != 1 && lay != 7) return cudaErrorNotSupported;
+            k<<<grid, Z::T, Z::SMEM, c->stream>>>((const float2*)A, (const float2*)B, (float2*)O, c->nx, c->ny,
+                                                  zargs_f(a), c->k0, c->flag, tw);
+            return cudaGetLastError();
+        }
+        case 1: return zlaunch<Z512>(c, A, B, O, a, lay);
+        case 2: return zlaunch<Z256>(c, A, B, O, a, lay);
+        case 3: return zlaunch<Z128>(c, A, B, O, a, lay);
+        case 4: return zlaunch<Z64>(c, A, B, O, a, lay);
     }
     return cudaErrorNotSupported;
 }

@@ -144,6 +144,37 @@ __device__ __forceinline__ void l2_prefetch(const void* p, unsigned n) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
 }
 
+// Layouts of a half-spectrum field of nxh x ny x nz complex modes (nxh = nx/2 + 1):
+//  standard  [z][ky][kx], cuFFT's R2C output;
+//  kx-tiled  tiles of kTileW consecutive kx; tile kt stores [ky][z][c], c < wt =
+//            min(kTileW, nxh - kTileW kt), and the tiles follow each other in kx order.
+//            The same nxh ny nz elements.  A z column segment of a tile (all z at one ky)
+//            is one contiguous block of nz wt elements: the stepper's z pass reads and
+//            writes whole blocks instead of 64-byte pieces one plane (about 1 MB) apart.
+// col_addr: element s of the column of mode kx at q (q = ky for z columns, q = z for y
+// columns) sits at base + s * stride.
+constexpr int kTileW = 8;
+struct ColAddr {
+    int64_t base, stride;
+};
+__device__ __forceinline__ ColAddr col_addr(bool tiled, bool zaxis, int kx, int q, int nxh, int ny, int nz) {
+    if (!tiled)
+        return zaxis ? ColAddr{(int64_t)q * nxh + kx, (int64_t)ny * nxh}
+                     : ColAddr{(int64_t)q * ny * nxh + kx, (int64_t)nxh};
+    const int kt = kx / kTileW, c = kx - kt * kTileW;
+    const int wt = min(kTileW, nxh - kt * kTileW);
+    const int64_t tb = (int64_t)kt * kTileW * ny * nz + c;
+    return zaxis ? ColAddr{tb + (int64_t)q * nz * wt, (int64_t)wt} : ColAddr{tb + (int64_t)q * wt, (int64_t)nz * wt};
+}
+// The z column of column c of kx tile kt at ky, for kernels whose tiles are the layout's
+// (kt uniform over the CTA): the same address as col_addr with fewer live values.
+template <bool kTiled>
+__device__ __forceinline__ ColAddr zcol_addr(int kt, int c, int ky, int nxh, int ny, int nz) {
+    if (!kTiled) return ColAddr{(int64_t)ky * nxh + kt * kTileW + c, (int64_t)ny * nxh};
+    const int wt = min(kTileW, nxh - kt * kTileW);
+    return ColAddr{((int64_t)kt * kTileW * ny + ky * wt) * nz + c, (int64_t)wt};
+}
+
 // Exchange slots: group g of NG interleaved groups, logical index (a, b) of an
 // E x P matrix -> (a P + b) NG + a PADG + g.  Warps run over consecutive g (and, when
 // NG < 32, over 32/NG consecutive t); PADG shifts successive blocks of P rows so that
@@ -203,6 +234,103 @@ __device__ __forceinline__ void fft_d2_to_d1(float2 (&v)[E], int t, int g, float
 #pragma unroll
     for (int n1 = 0; n1 < E; ++n1) v[n1] = xb[xslot<N, E, NG, PADG>(n1, t, g)];
     RF<E, DIR>::run(v);
+}
+
+// ---- N = E x 2E over P = 2E threads holding E values each (half the registers of the
+// square four-step above, for N = 2 E^2: 512 = 16 x 32, 128 = 8 x 16).
+// Stage 1: E-point DFTs in registers, twiddles W_N^{t k1}, a transpose through shared
+// memory.  Stage 2: the 2E-point DFTs over t (one per k1) split across thread pairs
+// s = 2p + h (p = k1): thread h takes the E-point DFT of the t = 2m + h inputs, h = 1
+// scales by W_2E^{k2}, and the radix-2 combination exchanges half of the values with the
+// partner through one round of warp shuffles (the partner is NG lanes away).
+// D1: thread t holds x[t + P j].  D3: thread (p, h) holds X[p + E k2] with
+// k2 = h E/2 + i at register i and k2 = E + h E/2 + i at register E/2 + i (i < E/2).
+// Exchange slots (k1, t, g) -> (k1 P + t) NG + k1 NG + g: the pad of NG per k1 row puts
+// the four (p, h) of a warp in alternate halves of the banks.  Buffer: E (P + 1) NG.
+template <int N, int E, int NG>
+__device__ __forceinline__ int xslot3(int k1, int t, int g) {
+    return (k1 * (2 * E) + t) * NG + k1 * NG + g;
+}
+
+template <int N, int E, int NG, int DIR, class Bar = BarCta>
+__device__ __forceinline__ void fft_d1_to_d3(float2 (&v)[E], int t, int g, float2* xb, const float2* twN,
+                                             const Bar& bar = Bar{}) {
+    constexpr int P = 2 * E, H = E / 2;
+    static_assert(P * E == N && (E & (E - 1)) == 0 && NG <= 16 && 32 % NG == 0, "shape");
+    RF<E, DIR>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < E; ++k1) {
+        float2 w = twN[(t * k1) & (N - 1)];
+        if (DIR > 0) w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+    }
+    bar.sync();
+#pragma unroll
+    for (int k1 = 0; k1 < E; ++k1) xb[xslot3<N, E, NG>(k1, t, g)] = v[k1];
+    bar.sync();
+    const int p = t >> 1, h = t & 1;
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = xb[xslot3<N, E, NG>(p, 2 * m + h, g)];
+    RF<E, DIR>::run(v);
+    if (h) {
+#pragma unroll
+        for (int k = 1; k < E; ++k) {
+            float2 w = twN[(k * E) & (N - 1)];  // W_2E^k = W_N^{k E}
+            if (DIR > 0) w.y = -w.y;
+            v[k] = cmul(v[k], w);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+        const float2 send = h ? v[i] : v[H + i];
+        const float2 recv = make_float2(__shfl_xor_sync(0xffffffffu, send.x, NG),
+                                        __shfl_xor_sync(0xffffffffu, send.y, NG));
+        const float2 a = h ? recv : v[i];
+        const float2 b = h ? v[H + i] : recv;
+        v[i] = a + b;
+        v[H + i] = a - b;
+    }
+}
+
+template <int N, int E, int NG, int DIR, class Bar = BarCta>
+__device__ __forceinline__ void fft_d3_to_d1(float2 (&v)[E], int t, int g, float2* xb, const float2* twN,
+                                             const Bar& bar = Bar{}) {
+    constexpr int P = 2 * E, H = E / 2;
+    static_assert(P * E == N && (E & (E - 1)) == 0 && NG <= 16 && 32 % NG == 0, "shape");
+    const int p = t >> 1, h = t & 1;
+    // radix-2 split of the 2E-point transforms: A_k = X_k + X_{k+E}, B_k = (X_k - X_{k+E}) W_2E^k
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+        const int k = h * H + i;
+        const float2 a = v[i] + v[H + i];
+        float2 w = twN[(k * E) & (N - 1)];
+        if (DIR > 0) w.y = -w.y;
+        const float2 b = cmul(v[i] - v[H + i], w);
+        const float2 send = h ? a : b;
+        const float2 recv = make_float2(__shfl_xor_sync(0xffffffffu, send.x, NG),
+                                        __shfl_xor_sync(0xffffffffu, send.y, NG));
+        v[i] = h ? recv : a;       // h = 0 collects A_0..A_{E-1}, h = 1 collects B_0..B_{E-1}
+        v[H + i] = h ? b : recv;
+    }
+    RF<E, DIR>::run(v);  // outputs t = 2m + h
+    bar.sync();
+#pragma unroll
+    for (int m = 0; m < E; ++m) xb[xslot3<N, E, NG>(p, 2 * m + h, g)] = v[m];
+    bar.sync();
+#pragma unroll
+    for (int k1 = 0; k1 < E; ++k1) v[k1] = xb[xslot3<N, E, NG>(k1, t, g)];
+#pragma unroll
+    for (int k1 = 1; k1 < E; ++k1) {
+        float2 w = twN[(t * k1) & (N - 1)];
+        if (DIR > 0) w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+    }
+    RF<E, DIR>::run(v);
+}
+
+// k2 of register r of thread half h in distribution D3
+template <int E> __device__ __forceinline__ int d3_k2(int r, int h) {
+    return r < E / 2 ? h * (E / 2) + r : E + h * (E / 2) + (r - E / 2);
 }
 
 // Split / merge of a real FFT of length 2M done as an M-point complex FFT

@@ -35,6 +35,8 @@ CASES = [
     # including a partial last tile of kx columns (nx/2 + 1 = 17)
     ((16, 16, 512), F32, 0.03), ((16, 8, 512), F32, 0.0), ((32, 32, 256), F32, 0.02), ((32, 16, 128), F32, 0.05),
     ((64, 64, 64), F32, 0.02),
+    # the kx-tiled carry (register y, x and z passes; partial last tile of one column)
+    ((64, 64, 512), F32, 0.02), ((128, 64, 256), F32, 0.0), ((64, 128, 128), F32, 0.03),
 ]
 
 
@@ -60,7 +62,7 @@ import pfc_oracle as O
 from mcstar_b200 import Stepper
 out = {{}}
 for shape, namp in [((64, 64, 64), 0.02), ((128, 128, 16), 0.0), ((32, 16, 128), 0.05), ((256, 256, 8), 0.0),
-                    ((512, 512, 4), 0.0)]:
+                    ((512, 512, 4), 0.0), ((16, 16, 512), 0.03), ((16, 8, 512), 0.0), ((64, 64, 512), 0.02)]:
     nx, ny, nz = shape
     st = Stepper(shape, math.pi / 4, 0.5, 0.3, dtype=np.float32, namp=namp, seed=5)
     rng = np.random.default_rng(3)
@@ -76,6 +78,8 @@ print(json.dumps(out))
 
 @pytest.mark.parametrize("env", [{"PFC_Z_PIPE": "1"}, {"PFC_Z_CARRY": "1"}, {"PFC_PREFETCH": "1"},
                                  {"PFC_Z_CARRY": "1", "PFC_PREFETCH": "1"}, {"PFC_Z_VARIANT": "5"},
+                                 {"PFC_Z_VARIANT": "1"}, {"PFC_TILED": "0"}, {"PFC_TILED": "0", "PFC_Z_VARIANT": "1"},
+                                 {"PFC_Y_VARIANT": "6"}, {"PFC_Y_VARIANT": "7"},
                                  {"PFC_XY_MODE": "1"}, {"PFC_XY_MODE": "0"},
                                  {"PFC_XY_MODE": "2", "PFC_SLAB": "3"}, {"PFC_X_VARIANT": "1", "PFC_Y_VARIANT": "5"}],
                          ids=lambda e: ",".join(f"{k}={v}" for k, v in e.items()))
@@ -94,6 +98,18 @@ def test_step_kernel_variants_match_oracle(env):
     errs = json.loads(res.stdout.strip().splitlines()[-1])
     for shape, e in errs.items():
         assert e < 2e-6, (shape, e)
+
+
+@pytest.mark.parametrize("shape,dtype,z_mode", [((64, 64, 64), F32, 3), ((64, 64, 512), F32, 3),
+                                                 ((512, 512, 4), F32, 0), ((16, 16, 512), F32, 1),
+                                                 ((16, 12, 10), F64, 0)])
+def test_stepper_layout_mode(shape, dtype, z_mode):
+    """FP32 grids with register y, x and z passes carry A and the z pass input kx-tiled
+    (z_mode 3); the register z pass alone keeps the standard layout (1); other shapes use
+    the general z pass (0)."""
+    if "PFC_TILED" in __import__("os").environ:
+        pytest.skip("layout chosen by the environment")
+    assert stepper(shape, dtype).ctx.profile_read()["z_mode"] == z_mode
 
 
 @pytest.mark.parametrize("shape,dtype", [((64, 64, 64), F32), ((32, 32, 32), F32), ((16, 12, 10), F64)],
@@ -129,11 +145,11 @@ def test_step_stabilisation_constant_and_mu():
     assert rel_l2(st.kspace(), want) < 1e-12
 
 
-def test_k0_mode_bit_invariant_with_noise():
-    shape = (32, 32, 32)
+@pytest.mark.parametrize("shape", [(32, 32, 32), (64, 64, 64)])
+def test_k0_mode_bit_invariant_with_noise(shape):
     st = stepper(shape, F32, namp=0.05, seed=3)
     rng = np.random.default_rng(2)
-    st.set_real(-0.18 + 0.05 * rng.uniform(-1, 1, (32, 32, 32)))
+    st.set_real(-0.18 + 0.05 * rng.uniform(-1, 1, shape[::-1]))
     k0 = st.kspace()[0, 0, 0]
     for _ in range(4):
         st.step(25)
@@ -149,12 +165,12 @@ def test_uniform_state_fixed_point():
     np.testing.assert_allclose(st.kspace(), k, atol=1e-9)
 
 
-def test_resume_is_bit_exact():
-    shape = (32, 32, 32)
+@pytest.mark.parametrize("shape", [(32, 32, 32), (64, 64, 64)])
+def test_resume_is_bit_exact(shape):
     a = stepper(shape, F32, namp=0.05, seed=9)
     b = stepper(shape, F32, namp=0.05, seed=9)
     rng = np.random.default_rng(5)
-    psi = -0.2 + 0.05 * rng.uniform(-1, 1, (32, 32, 32))
+    psi = -0.2 + 0.05 * rng.uniform(-1, 1, shape[::-1])
     a.set_real(psi)
     b.set_real(psi)
     a.step(10)
