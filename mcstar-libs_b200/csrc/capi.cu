@@ -173,6 +173,9 @@ ZPropArgs zargs(const pfc_ctx* c, const pfc_step_params* p) {
     return za;
 }
 
+// Layout codes of col_addr (kx-tiled fields of the tiled stepper)
+constexpr int kLayZ = 1, kLayRow = 2;
+
 // Where the stepper's mixed-grid field A = IFFT_z(psi^)/nz lives: in work2 beside the
 // carried psi^ (z_carry) or kx-tiled (tiled), else in place of psi^.
 void* carried_A(pfc_ctx* ctx, void* kpsi) { return ctx->z_carry || ctx->tiled ? ctx->work2 : kpsi; }
@@ -195,7 +198,7 @@ cudaError_t step_entry(pfc_ctx* ctx, void* kpsi) {
     return traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
         cudaError_t e = launch_k0_save(ctx, kpsi);
         if (e || ctx->nz == 1) return e;
-        return zcols(ctx, 1, kpsi, carried_A(ctx, kpsi), 1.0 / ctx->nz, ctx->tiled ? 2 : 0);
+        return zcols(ctx, 1, kpsi, carried_A(ctx, kpsi), 1.0 / ctx->nz, ctx->tiled ? kLayZ << 2 : 0);
     });
 }
 
@@ -204,24 +207,26 @@ cudaError_t step_entry(pfc_ctx* ctx, void* kpsi) {
 cudaError_t step_exit(pfc_ctx* ctx, void* kpsi) {
     if (ctx->z_carry) return cudaSuccess;
     return traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
-        cudaError_t e = ctx->nz > 1 ? zcols(ctx, -1, carried_A(ctx, kpsi), kpsi, 1.0, ctx->tiled) : cudaSuccess;
+        cudaError_t e = ctx->nz > 1 ? zcols(ctx, -1, carried_A(ctx, kpsi), kpsi, 1.0, ctx->tiled ? kLayZ : 0)
+                                    : cudaSuccess;
         if (e) return e;
         return launch_k0_restore(ctx, kpsi);
     });
 }
 
-// B = FFT_xy(cubic term of IFFT_xy(A)) on the mixed grid.  Tiled: A (work2) and, except
-// on the last step, the result B (the psi^ buffer, free while A carries the state) are
-// kx-tiled; the y-inverse writes work in the standard layout for the x pass.
+// B = FFT_xy(cubic term of IFFT_xy(A)) on the mixed grid.  Tiled: A (work2, z-tiled) ->
+// work (row-tiled), the x pass in place, then B into the psi^ buffer (free while A
+// carries the state): z-tiled, or on the last step in the standard layout, where the z
+// pass then writes psi^' in place.
 cudaError_t step_xy(pfc_ctx* ctx, void* kpsi, const pfc_step_params* p, bool last) {
     const void* A = carried_A(ctx, kpsi);
     void* B = ctx->work;
     const double mul = 1.0 / ((double)ctx->nx * (double)ctx->ny);
     if (ctx->tiled)
         return traced_xy3(
-            ctx, [&] { return launch_ypass(ctx, 1, A, B, 1.0, ctx->nz, 1); },
-            [&] { return launch_xpass(ctx, B, nullptr, mul, p->C, p->mu, ctx->nz); },
-            [&] { return last ? launch_ypass(ctx, -1, B, B, 1.0, ctx->nz) : launch_ypass(ctx, -1, B, kpsi, 1.0, ctx->nz, 2); });
+            ctx, [&] { return launch_ypass(ctx, 1, A, B, 1.0, ctx->nz, kLayZ | kLayRow << 2); },
+            [&] { return launch_xpass(ctx, B, nullptr, mul, p->C, p->mu, ctx->nz, kLayRow); },
+            [&] { return launch_ypass(ctx, -1, B, kpsi, 1.0, ctx->nz, kLayRow | (last ? 0 : kLayZ << 2)); });
     if (ctx->xy_mode == 1)
         return traced(ctx, 1, 1, [&] { return launch_fused_xy(ctx, A, B, nullptr, mul, p->C, p->mu); });
     if (ctx->xy_mode == 2) {
@@ -259,13 +264,13 @@ cudaError_t step_xy(pfc_ctx* ctx, void* kpsi, const pfc_step_params* p, bool las
     });
 }
 
-// the z pass with the semi-implicit update.  Tiled: A' stays kx-tiled in work2; the last
-// step reads B from work (standard) and writes psi^' to the caller's buffer.
+// the z pass with the semi-implicit update.  Tiled: B is in the psi^ buffer; A' stays
+// z-tiled in work2, and the last step writes psi^' over B (standard layout, in place).
 cudaError_t step_z(pfc_ctx* ctx, void* kpsi, const ZPropArgs& za) {
     void* B = ctx->work;
     if (ctx->tiled) {
         void* A = ctx->work2;
-        if (za.final_step) return traced(ctx, 2, 1, [&] { return launch_zcol(ctx, A, B, kpsi, za, 1); });
+        if (za.final_step) return traced(ctx, 2, 1, [&] { return launch_zcol(ctx, A, kpsi, kpsi, za, 1); });
         return traced(ctx, 2, 1, [&] { return launch_zcol(ctx, A, kpsi, A, za, 7); });
     }
     if (ctx->z_carry) return traced(ctx, 2, 1, [&] { return launch_zcarry(ctx, kpsi, ctx->work2, B, za); });

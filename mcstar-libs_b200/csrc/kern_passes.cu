@@ -35,10 +35,10 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
     k_ycol(const float2* in, float2* out, int nxh, int ny, int nz, int lay, const float2* __restrict__ twg,
            float scale, int pf) {
     // the columns of NY elements of kx tile blockIdx.x at plane blockIdx.y: y columns of
-    // z-plane blockIdx.y (kZ false) or z columns at ky = blockIdx.y (kZ); lay bit 0: the
-    // input is kx-tiled, bit 1: the output (standard layout otherwise; col_addr).  With the
-    // standard layout on both sides, in may equal out.  pf (standard input only): L2
-    // prefetch distance in tiles.
+    // z-plane blockIdx.y (kZ false) or z columns at ky = blockIdx.y (kZ); lay & 3: the
+    // layout of the input, lay >> 2: of the output (col_addr).  With the standard layout on
+    // both sides, in may equal out.  pf (standard input only): L2 prefetch distance in
+    // tiles.
     constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P, U = Y::U;
     extern __shared__ __align__(16) float2 sm[];
     float2* xb = sm;
@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
     const int c = tid % TX, t = tid / TX;
     const int kx = blockIdx.x * TX + c;
     const bool valid = kx < nxh;
-    const ColAddr ai = col_addr(lay & 1, kZ, kx, blockIdx.y, nxh, ny, nz);
+    const ColAddr ai = col_addr(lay & 3, kZ, kx, blockIdx.y, nxh, ny, nz);
     float2 v[E];
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = valid ? in[ai.base + (int64_t)(t + P * j) * ai.stride] : make_float2(0.f, 0.f);
@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
         const int tgt = (int)(blockIdx.y * gridDim.x + blockIdx.x) + pf;
         if (tgt < ntx * (int)gridDim.y) {
             const int kx0 = (tgt % ntx) * TX;
-            const ColAddr ap = col_addr(false, kZ, kx0, tgt / ntx, nxh, ny, nz);
+            const ColAddr ap = col_addr(0, kZ, kx0, tgt / ntx, nxh, ny, nz);
             const unsigned bytes = (unsigned)(min(TX, nxh - kx0) * sizeof(float2));
             for (int y = tid; y < NY; y += Y::T) l2_prefetch(in + ap.base + (int64_t)y * ap.stride, bytes);
         }
@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
     __syncthreads();
     fft_d1_to_d2<NY, E, TX, DIR, BarCta, Y::PADG>(v, t, c, xb, tw);
     if (valid) {
-        const ColAddr ao = col_addr(lay & 2, kZ, kx, blockIdx.y, nxh, ny, nz);
+        const ColAddr ao = col_addr(lay >> 2, kZ, kx, blockIdx.y, nxh, ny, nz);
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
@@ -126,10 +126,50 @@ struct XCfg {
     static_assert(P * E == M && U * P == E && (R % 32 == 0 || R == 16) && R * P == T, "shape");
 };
 
+// The R rows from row0 of a row-tiled field (k_xrow MODE 3) between global memory and the
+// shared row buffer (row pitch LDR): kStore false loads, true stores.  Each tile holds the
+// R rows as one contiguous block of R kTileW elements.  Eight lanes move one row's 64-byte
+// piece (four whole pieces per warp access); the two rows of a half-warp are 8 apart, so
+// with the odd pitch they fall in opposite halves of the shared-memory banks.
+template <class X, bool kStore>
+__device__ __forceinline__ void row_tiles(float2* rb, float2* g, int row0, int nrows, int tid) {
+    constexpr int M = X::M, R = X::R, T = X::T, LDR = X::LDR, FT = M / kTileW;  // full tiles; the last: kx = M
+    constexpr int CH = R * kTileW;  // elements of one tile's block of R rows
+    static_assert(M % kTileW == 0 && kTileW == 8 && R % 16 == 0 && LDR % 2 == 1, "shape");
+    static_assert(CH % T == 0 ? true : (T % CH == 0 && FT % (T / CH) == 0), "threads per tile block");
+    constexpr int NPOS = CH >= T ? CH / T : 1;        // positions of a block per thread
+    constexpr int TSTEP = CH >= T ? 1 : T / CH;       // tiles apart of a thread's blocks
+    const int64_t ts = (int64_t)kTileW * nrows;       // elements between tiles
+    const int kt0 = CH >= T ? 0 : tid / CH;
+#pragma unroll
+    for (int m = 0; m < NPOS; ++m) {
+        const int pos = CH >= T ? tid + m * T : tid % CH;
+        const int c = pos % kTileW, q = pos / kTileW, p = q >> 1;
+        const int rr = (p & 7) + ((p >> 3) << 4) + ((q & 1) << 3);  // a bijection of [0, R)
+        float2* gp = g + kt0 * ts + (int64_t)(row0 + rr) * kTileW + c;
+        float2* sp = rb + rr * LDR + kt0 * kTileW + c;
+#pragma unroll
+        for (int k = 0; k < FT / TSTEP; ++k) {
+            if (kStore) *gp = sp[k * TSTEP * kTileW];
+            else sp[k * TSTEP * kTileW] = *gp;
+            gp += TSTEP * ts;
+        }
+    }
+    if (tid < R) {
+        float2* gp = g + FT * ts + row0 + tid;
+        float2* sp = rb + tid * LDR + M;
+        if (kStore) *gp = *sp;
+        else *sp = *gp;
+    }
+}
+
 // MODE 0: the step's x pass, in place (in == out).  MODE 1: R2C of real rows (in: rows
 // of M float2 pairs x[2m] + i x[2m+1]) into half-spectrum rows (out: rows of NXH).
-// MODE 2: C2R of half-spectrum rows (in) into real rows (out, M pairs per row).  The
-// transforms are unnormalised, as cufft_wrapper.hpp:61-86.
+// MODE 2: C2R of half-spectrum rows (in) into real rows (out, M pairs per row).  MODE 3:
+// MODE 0 on the row-tiled layout (col_addr layout 2: element kx of row n = z ny + y at
+// tile_base(kx / kTileW) + n wt + kx % kTileW, tile_base(kt) = kt kTileW nrows; nrows
+// the field's rows, a multiple of R).  The transforms are unnormalised, as
+// cufft_wrapper.hpp:61-86.
 template <class X, int MODE>
 __global__ void __launch_bounds__(X::T, X::MINB)
     k_xrow(const float2* in, float2* out, const float* __restrict__ pot, int nrows, const float2* __restrict__ twg,
@@ -146,7 +186,9 @@ __global__ void __launch_bounds__(X::T, X::MINB)
     const int row0 = blockIdx.x * R;
     const int nr = min(R, nrows - row0);
     const int64_t g0 = (int64_t)row0 * LIN;
-    if constexpr (LIN == LDR) {
+    if constexpr (MODE == 3) {
+        row_tiles<X, false>(rb, const_cast<float2*>(in), row0, nrows, tid);
+    } else if constexpr (LIN == LDR) {
         for (int i = tid; i < nr * LIN; i += X::T) rb[i] = in[g0 + i];
     } else {
         for (int i = tid; i < nr * LIN; i += X::T) rb[(i / LIN) * LDR + i % LIN] = in[g0 + i];
@@ -224,8 +266,12 @@ __global__ void __launch_bounds__(X::T, X::MINB)
     for (int j = 0; j < E; ++j) rb[r * LDR + t + P * j] = v[j];
     if (t == 0) rb[r * LDR + M] = xm_last;
     __syncthreads();
-    const int64_t o0 = (int64_t)row0 * NXH;
-    for (int i = tid; i < nr * NXH; i += X::T) out[o0 + i] = rb[i];
+    if constexpr (MODE == 3) {
+        row_tiles<X, true>(rb, out, row0, nrows, tid);
+    } else {
+        const int64_t o0 = (int64_t)row0 * NXH;
+        for (int i = tid; i < nr * NXH; i += X::T) out[o0 + i] = rb[i];
+    }
 }
 
 using Y512 = YCfg<512, 32, 8>;
@@ -270,6 +316,7 @@ cudaError_t xattr() {
     cudaError_t e = cudaFuncSetAttribute(k_xrow<X, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)X::SMEM);
     if (!e) e = cudaFuncSetAttribute(k_xrow<X, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)X::SMEM);
     if (!e) e = cudaFuncSetAttribute(k_xrow<X, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)X::SMEM);
+    if (!e) e = cudaFuncSetAttribute(k_xrow<X, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)X::SMEM);
     return e;
 }
 
@@ -282,7 +329,7 @@ cudaError_t collaunch(const pfc_ctx* c, int dir, const void* in, void* out, doub
     dim3 grid((c->nxh + Y::TX - 1) / Y::TX, planes);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + tw_off;
     static const int per_sm = resident_ctas(k_ycol<Y, 1, kZ>, Y::T, Y::SMEM);
-    const int pf = (lay & 1) ? 0 : prefetch_ahead(c, per_sm, in);
+    const int pf = (lay & 3) ? 0 : prefetch_ahead(c, per_sm, in);
     if (dir > 0)
         k_ycol<Y, 1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->ny, c->nz,
                                                              lay, tw, (float)scale, pf);
@@ -305,9 +352,10 @@ cudaError_t xlaunch(const pfc_ctx* c, const void* in, void* out, const void* pot
     dim3 grid((nrows + X::R - 1) / X::R);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->xpass_tw_off;
     static const int per_sm = resident_ctas(k_xrow<X, MODE>, X::T, X::SMEM);
+    if (MODE == 3 && nrows % X::R) return cudaErrorNotSupported;  // whole tiles of rows
     k_xrow<X, MODE><<<grid, X::T, X::SMEM, c->stream>>>((const float2*)in, (float2*)out, (const float*)pot, nrows, tw,
                                                         (float)mul, (float)C, (float)mu,
-                                                        prefetch_ahead(c, per_sm, in));
+                                                        MODE == 3 ? 0 : prefetch_ahead(c, per_sm, in));
     return cudaGetLastError();
 }
 
@@ -394,7 +442,10 @@ cudaError_t xdispatch(const pfc_ctx* c, const void* in, void* out, const void* p
     return cudaErrorNotSupported;
 }
 
-cudaError_t launch_xpass(const pfc_ctx* c, void* b, const void* pot, double mul, double C, double mu, int nzs) {
+cudaError_t launch_xpass(const pfc_ctx* c, void* b, const void* pot, double mul, double C, double mu, int nzs,
+                         int lay) {
+    if (lay == 2) return nzs == c->nz ? xdispatch<3>(c, b, b, pot, mul, C, mu, nzs * c->ny) : cudaErrorNotSupported;
+    if (lay != 0) return cudaErrorNotSupported;
     return xdispatch<0>(c, b, b, pot, mul, C, mu, nzs * c->ny);
 }
 cudaError_t launch_xrows_r2c(const pfc_ctx* c, const void* in_real, void* out_cmpl) {

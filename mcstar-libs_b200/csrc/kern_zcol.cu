@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(Z::T, Z::MINB) k_zcol(const float2* A, const f
     const int nxh = nx / 2 + 1;
     const bool valid = kx < nxh;  // the last tile holds only the kx = nx/2 column
     const float2* src = half ? B : A;
-    const ColAddr ca = col_addr(lay & (half ? 2 : 1), true, kx, ky, nxh, ny, NZ);
+    const ColAddr ca = col_addr((lay & (half ? 2 : 1)) ? 1 : 0, true, kx, ky, nxh, ny, NZ);
     float2 v[E];
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = valid ? src[ca.base + (int64_t)(t + P * j) * ca.stride] : make_float2(0.f, 0.f);
@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(Z::T, Z::MINB) k_zcol(const float2* A, const f
                              k0);
     if (!a.final_step) fft_d2_to_d1<NZ, E, TX, 1, BarDyn, Z::PADG>(v, t, c, regA, tw, bar);
     watch<Z>(v, a.final_step, valid, flag);
-    const ColAddr co = col_addr(lay & 4, true, kx, ky, nxh, ny, NZ);
+    const ColAddr co = col_addr((lay & 4) ? 1 : 0, true, kx, ky, nxh, ny, NZ);
     store_state<Z>(v, O, co.base, co.stride, t, valid, a.final_step);
 }
 

@@ -57,8 +57,9 @@ struct pfc_ctx {
     int fused_z;                  // 0: general z pass; otherwise the register z kernel variant id
     int z_pipe;                   // register z pass as the persistent pipelined kernel (1) or one tile per CTA (0)
     int z_carry;                  // carry psi^ itself (A = IFFT_z(psi^)/nz lives in work2) instead of A
-    int tiled;                    // register passes with A and the z pass input B kx-tiled (col_addr):
-                                  // A lives in work2, B in the caller's psi^ buffer between steps
+    int tiled;                    // register passes on kx-tiled fields (col_addr): A z-tiled in work2,
+                                  // the x pass field row-tiled in work, the z pass input B z-tiled
+                                  // in the caller's psi^ buffer
     int num_sms;                  // multiprocessors of the device the context was made on
     int zcol_tw_off;              // twiddles of the register z kernel: W_nz^m
     int fused_y, fused_x;         // register y / x pass variants (0: none)
@@ -126,25 +127,29 @@ cudaError_t launch_zprop_cols(const pfc_ctx* c, void* A, const void* B, const ZP
 int fused_y_variant(int ny, int dtype);
 int fused_x_variant(int nx, int dtype);
 cudaError_t set_pass_attributes(const pfc_ctx* c);
-// y FFT of nzs consecutive planes starting at in / out (in may equal out); lay bit 0 / 1:
-// in / out kx-tiled (col_addr; whole fields only, not in place)
+// y FFT of nzs consecutive planes starting at in / out (in may equal out); lay & 3 / lay
+// >> 2: the layouts of in / out (col_addr; tiled: whole fields only, not in place)
 cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs, int lay = 0);
 // C2R, cubic term, R2C on the rows of nzs consecutive planes starting at b, in place;
-// pot (real field, or null) starts at the same first plane
-cudaError_t launch_xpass(const pfc_ctx* c, void* b, const void* pot, double mul, double C, double mu, int nzs);
+// pot (real field, or null) starts at the same first plane; lay: 0 standard, 2 row-tiled
+// (col_addr; whole fields only)
+cudaError_t launch_xpass(const pfc_ctx* c, void* b, const void* pot, double mul, double C, double mu, int nzs,
+                         int lay = 0);
 // unnormalised real transforms of every x row (register kernels; out of place)
 cudaError_t launch_xrows_r2c(const pfc_ctx* c, const void* in_real, void* out_cmpl);
 cudaError_t launch_xrows_c2r(const pfc_ctx* c, const void* in_cmpl, void* out_real);
 // complex FFT along z of a half-spectrum-shaped field with the register column kernel
 int fused_zfft_variant(int nz, int dtype);
 cudaError_t set_zfft_attributes(const pfc_ctx* c);
+// (lay as launch_ypass)
 cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay = 0);
 
 // ---- register-resident z pass (kern_zcol.cu) ----
 int fused_z_variant(int nx, int nz, int dtype);
 cudaError_t set_zcol_attributes(const pfc_ctx* c);
 // reads A and B, writes A' (or psi^' on the last step) to O; lay bits 0, 1, 2: A, B, O
-// kx-tiled (col_addr).  O may be A when both have the same layout.
+// z-tiled (col_addr layout 1; standard otherwise).  O may be A or B when it has the same
+// layout.
 cudaError_t launch_zcol(const pfc_ctx* c, const void* A, const void* B, void* O, const ZPropArgs& a, int lay = 0);
 // the z pass that carries psi^: reads psi^ (kpsi) and B, writes psi^' and (unless last) A'
 cudaError_t launch_zcarry(const pfc_ctx* c, void* kpsi, void* A, const void* B, const ZPropArgs& a);

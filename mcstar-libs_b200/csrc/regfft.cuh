@@ -145,26 +145,32 @@ __device__ __forceinline__ void l2_prefetch(const void* p, unsigned n) {
 }
 
 // Layouts of a half-spectrum field of nxh x ny x nz complex modes (nxh = nx/2 + 1):
-//  standard  [z][ky][kx], cuFFT's R2C output;
-//  kx-tiled  tiles of kTileW consecutive kx; tile kt stores [ky][z][c], c < wt =
-//            min(kTileW, nxh - kTileW kt), and the tiles follow each other in kx order.
-//            The same nxh ny nz elements.  A z column segment of a tile (all z at one ky)
-//            is one contiguous block of nz wt elements: the stepper's z pass reads and
-//            writes whole blocks instead of 64-byte pieces one plane (about 1 MB) apart.
-// col_addr: element s of the column of mode kx at q (q = ky for z columns, q = z for y
-// columns) sits at base + s * stride.
+//  0 standard    [z][ky][kx], cuFFT's R2C output;
+//  1 z-tiled     tiles of kTileW consecutive kx; tile kt stores [ky][z][c], c < wt =
+//                min(kTileW, nxh - kTileW kt), the tiles in kx order.  A z column segment of
+//                a tile (all z at one ky) is one contiguous block of nz wt elements: the
+//                stepper's z pass reads and writes whole blocks instead of 64-byte pieces
+//                one plane (about 1 MB) apart;
+//  2 row-tiled   the same tiles storing [z][y][c]: the y column segment of a tile (all y
+//                at one z) is one contiguous block, and R consecutive x rows are one block
+//                of R wt elements per tile.
+// All three hold the same nxh ny nz elements.  col_addr: element s of the column of mode
+// kx at q (q = ky for z columns, q = z for y columns) sits at base + s * stride.
 constexpr int kTileW = 8;
 struct ColAddr {
     int64_t base, stride;
 };
-__device__ __forceinline__ ColAddr col_addr(bool tiled, bool zaxis, int kx, int q, int nxh, int ny, int nz) {
-    if (!tiled)
+__device__ __forceinline__ ColAddr col_addr(int layout, bool zaxis, int kx, int q, int nxh, int ny, int nz) {
+    if (layout == 0)
         return zaxis ? ColAddr{(int64_t)q * nxh + kx, (int64_t)ny * nxh}
                      : ColAddr{(int64_t)q * ny * nxh + kx, (int64_t)nxh};
     const int kt = kx / kTileW, c = kx - kt * kTileW;
     const int wt = min(kTileW, nxh - kt * kTileW);
     const int64_t tb = (int64_t)kt * kTileW * ny * nz + c;
-    return zaxis ? ColAddr{tb + (int64_t)q * nz * wt, (int64_t)wt} : ColAddr{tb + (int64_t)q * wt, (int64_t)nz * wt};
+    if (layout == 1)
+        return zaxis ? ColAddr{tb + (int64_t)q * nz * wt, (int64_t)wt}
+                     : ColAddr{tb + (int64_t)q * wt, (int64_t)nz * wt};
+    return zaxis ? ColAddr{tb + (int64_t)q * wt, (int64_t)ny * wt} : ColAddr{tb + (int64_t)q * ny * wt, (int64_t)wt};
 }
 // The z column of column c of kx tile kt at ky, for kernels whose tiles are the layout's
 // (kt uniform over the CTA): the same address as col_addr with fewer live values.
