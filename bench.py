@@ -138,7 +138,8 @@ def kernel_table(prof, S, steps):
                        "bytes_per_launch": bytes_per_launch}
 
     if prof["xy_mode"] == 2 and prof["calls"][3]:
-        add("k_ycol", 3, 2.0 * S)  # y-inverse A -> B, y-forward B -> B
+        # y-inverse A -> B, y-forward B -> B
+        add("k_ycol3" if prof.get("y_variant") in (6, 7) else "k_ycol", 3, 2.0 * S)
         add("k_xrow", 4, 2.0 * S)  # C2R, cubic term, R2C of every row, in place
     elif prof["xy_mode"] == 2:
         add("k_ycol+k_xrow+k_ycol (z slabs)", 1, 6.0 * S)
@@ -146,9 +147,9 @@ def kernel_table(prof, S, steps):
         add("k_plane_xy", 1, 2.0 * S)
     else:
         add("k_cols+k_rows_nonlin+k_cols", 1, 6.0 * S)
-    if prof["z_mode"] == 2:
+    if prof["z_mode"] in (2, 4):
         # psi^ and B read, psi^' and A' written; the last step of a run writes psi^' only
-        add("k_zcarry", 2, (4.0 * (steps - 1) + 3.0) / steps * S)
+        add("k_zcarry3" if prof["z_mode"] == 4 else "k_zcarry", 2, (4.0 * (steps - 1) + 3.0) / steps * S)
     else:
         name = "k_zprop" if prof["z_mode"] == 0 else ("k_zcol3" if prof.get("z_variant") == 6 else "k_zcol")
         add(name, 2, 3.0 * S)

@@ -245,11 +245,17 @@ typedef struct pfc_profile {
                                                     carrying A = IFFT_z(psi^)/nz, 2
                                                     register z pass carrying psi^, 3
                                                     register z pass carrying A in the
-                                                    kx-tiled layout                  */
+                                                    kx-tiled layout, 4 carrying psi^
+                                                    in the kx-tiled layout           */
     int z_variant;                               /* register z kernel (0: none): 1-4
                                                     square split for nz 512, 256, 128,
                                                     64; 5: 16-column tiles; 6: 16
                                                     values per thread (nz 512)       */
+    int y_variant;                               /* register y kernel (0: none): 1-4
+                                                    32 / 16 / 16 / 8 values per thread
+                                                    for ny 512, 256, 128, 64; 5: 16
+                                                    columns; 6, 7: 16 values per
+                                                    thread over 32 threads (ny 512)  */
 } pfc_profile;
 pfc_status pfc_profile_enable(pfc_ctx* ctx, int on);
 pfc_status pfc_profile_read(pfc_ctx* ctx, pfc_profile* out);

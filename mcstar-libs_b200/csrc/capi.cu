@@ -177,8 +177,12 @@ ZPropArgs zargs(const pfc_ctx* c, const pfc_step_params* p) {
 constexpr int kLayZ = 1, kLayRow = 2;
 
 // Where the stepper's mixed-grid field A = IFFT_z(psi^)/nz lives: in work2 beside the
-// carried psi^ (z_carry) or kx-tiled (tiled), else in place of psi^.
-void* carried_A(pfc_ctx* ctx, void* kpsi) { return ctx->z_carry || ctx->tiled ? ctx->work2 : kpsi; }
+// carried psi^ (z_carry) or z-tiled (tiled), in the psi^ buffer when tiled with psi^
+// carried z-tiled in work2, else in place of psi^.
+void* carried_A(pfc_ctx* ctx, void* kpsi) {
+    if (ctx->tiled) return ctx->z_carry ? kpsi : ctx->work2;
+    return ctx->z_carry ? ctx->work2 : kpsi;
+}
 
 // psi^ -> A = IFFT_z(psi^)/nz; the k = 0 mode is kept in FP64
 // complex FFT along z of a half-spectrum field: the register column kernel where the
@@ -195,6 +199,13 @@ cudaError_t ycols(const pfc_ctx* ctx, int dir, const void* in, void* out) {
 }
 
 cudaError_t step_entry(pfc_ctx* ctx, void* kpsi) {
+    if (ctx->tiled && ctx->z_carry)
+        return traced(ctx, 0, 3, [&] {
+            cudaError_t e = launch_k0_save(ctx, kpsi);
+            if (!e) e = launch_relayout(ctx, kpsi, ctx->work2, 1);
+            if (!e) e = zcols(ctx, 1, ctx->work2, kpsi, 1.0 / ctx->nz, kLayZ | kLayZ << 2);
+            return e;
+        });
     return traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
         cudaError_t e = launch_k0_save(ctx, kpsi);
         if (e || ctx->nz == 1) return e;
@@ -205,6 +216,7 @@ cudaError_t step_entry(pfc_ctx* ctx, void* kpsi) {
 // back to psi^ after non-final steps: FFT_z(A) with the k = 0 mode restored from FP64
 // (nothing to do when psi^ is carried)
 cudaError_t step_exit(pfc_ctx* ctx, void* kpsi) {
+    if (ctx->tiled && ctx->z_carry) return traced(ctx, 0, 1, [&] { return launch_relayout(ctx, ctx->work2, kpsi, 0); });
     if (ctx->z_carry) return cudaSuccess;
     return traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
         cudaError_t e = ctx->nz > 1 ? zcols(ctx, -1, carried_A(ctx, kpsi), kpsi, 1.0, ctx->tiled ? kLayZ : 0)
@@ -268,6 +280,11 @@ cudaError_t step_xy(pfc_ctx* ctx, void* kpsi, const pfc_step_params* p, bool las
 // z-tiled in work2, and the last step writes psi^' over B (standard layout, in place).
 cudaError_t step_z(pfc_ctx* ctx, void* kpsi, const ZPropArgs& za) {
     void* B = ctx->work;
+    if (ctx->tiled && ctx->z_carry)
+        return traced(ctx, 2, 1, [&] {
+            return launch_zcarry_tiled(ctx, ctx->work2, kpsi, za.final_step ? kpsi : ctx->work2,
+                                       za.final_step ? nullptr : kpsi, za);
+        });
     if (ctx->tiled) {
         void* A = ctx->work2;
         if (za.final_step) return traced(ctx, 2, 1, [&] { return launch_zcol(ctx, A, kpsi, kpsi, za, 1); });
@@ -407,17 +424,17 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
     // the register z pass carries A = IFFT_z(psi^)/nz (three z transforms, three field
     // sweeps; measured faster); PFC_Z_CARRY=1 carries psi^ itself (two transforms, four
     // sweeps).  The slabbed xy passes and the pipelined z kernel need work2 / carry A.
-    c->z_carry = 0;
-    if (const char* s = getenv("PFC_Z_CARRY")) c->z_carry = c->fused_z && atoi(s) != 0;
-    if (c->slab > 0 || c->z_pipe) c->z_carry = 0;
-    // the pipelined and the psi^-carrying z kernels exist for the square split only
-    if ((c->z_pipe || c->z_carry) && c->fused_z >= 5) c->fused_z = 1;
-    // kx-tiled A and B (measured faster: whole-block z columns); PFC_TILED=0 keeps the
+    bool carry = false;
+    if (const char* s = getenv("PFC_Z_CARRY")) carry = c->fused_z && atoi(s) != 0 && c->slab == 0 && !c->z_pipe;
+    // kx-tiled fields (measured faster: whole-block z and y columns); PFC_TILED=0 keeps the
     // standard layout.  Needs the register y, x, z passes, whole fields, and the register
     // column kernel for the entry / exit z transforms.
-    c->tiled = c->fused_z && c->fused_zfft && c->xy_mode == 2 && c->fused_y && c->fused_y < 6 && c->slab == 0 &&
-               !c->z_pipe && !c->z_carry;
+    c->tiled = c->fused_z && c->fused_zfft && c->xy_mode == 2 && c->fused_y && c->slab == 0 && !c->z_pipe;
     if (const char* s = getenv("PFC_TILED")) c->tiled = c->tiled && atoi(s) != 0;
+    // psi^ carried: tiled, with the 16-values-per-thread kernel (nz 512); standard layout,
+    // with the square split
+    c->z_carry = carry && (!c->tiled || c->fused_z == 6);
+    if (!c->tiled && (c->z_pipe || c->z_carry) && c->fused_z >= 5) c->fused_z = 1;
     // L2 prefetch of the register passes, in waves of CTAs ahead (PFC_PREFETCH)
     c->pf_waves = 0.f;
     if (const char* s = getenv("PFC_PREFETCH")) c->pf_waves = std::max(0.f, (float)atof(s));
@@ -908,8 +925,9 @@ pfc_status pfc_profile_read(pfc_ctx* ctx, pfc_profile* out) {
     out->launches = ctx->launches;
     out->xy_variant = ctx->xy_mode == 1 ? ctx->fused_xy : 0;
     out->xy_mode = ctx->xy_mode;
-    out->z_mode = ctx->z_carry ? 2 : (ctx->tiled ? 3 : (ctx->fused_z ? 1 : 0));
+    out->z_mode = ctx->z_carry ? (ctx->tiled ? 4 : 2) : (ctx->tiled ? 3 : (ctx->fused_z ? 1 : 0));
     out->z_variant = ctx->fused_z;
+    out->y_variant = ctx->xy_mode == 2 ? ctx->fused_y : 0;
     for (int f = 0; f < PFC_PROFILE_FAMILIES; ++f) { out->calls[f] = ctx->prof_calls[f]; out->ms[f] = ctx->prof_ms[f]; }
     return PFC_OK;
 }

@@ -87,9 +87,10 @@ struct YCfg3 {
     static_assert(P * E == NY && 32 % TX == 0, "shape");
 };
 
+// (lay as k_ycol: the layouts of in and out, y columns of z-plane blockIdx.y)
 template <class Y, int DIR>
 __global__ void __launch_bounds__(Y::T, Y::MINB)
-    k_ycol3(const float2* in, float2* out, int nxh, const float2* __restrict__ twg, float scale) {
+    k_ycol3(const float2* in, float2* out, int nxh, int nz, int lay, const float2* __restrict__ twg, float scale) {
     constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P;
     extern __shared__ __align__(16) float2 sm[];
     float2* xb = sm;
@@ -99,18 +100,19 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
     const int c = tid % TX, t = tid / TX;
     const int kx = blockIdx.x * TX + c;
     const bool valid = kx < nxh;
-    const int64_t base = (int64_t)blockIdx.y * NY * nxh + kx;
+    const ColAddr ai = col_addr(lay & 3, false, kx, blockIdx.y, nxh, NY, nz);
     float2 v[E];
 #pragma unroll
-    for (int j = 0; j < E; ++j) v[j] = valid ? in[base + (int64_t)(t + P * j) * nxh] : make_float2(0.f, 0.f);
+    for (int j = 0; j < E; ++j) v[j] = valid ? in[ai.base + (int64_t)(t + P * j) * ai.stride] : make_float2(0.f, 0.f);
     __syncthreads();
     fft_d1_to_d3<NY, E, TX, DIR>(v, t, c, xb, tw);
     if (valid) {
+        const ColAddr ao = col_addr(lay >> 2, false, kx, blockIdx.y, nxh, NY, nz);
         const int p = t >> 1, h = t & 1;
 #pragma unroll
         for (int r = 0; r < E; ++r) {
             const int k = p + E * d3_k2<E>(r, h);
-            out[base + (int64_t)k * nxh] = make_float2(v[r].x * scale, v[r].y * scale);
+            out[ao.base + (int64_t)k * ao.stride] = make_float2(v[r].x * scale, v[r].y * scale);
         }
     }
 }
@@ -286,13 +288,15 @@ cudaError_t y3attr() {
     return cudaFuncSetAttribute(k_ycol3<Y, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Y::SMEM);
 }
 template <class Y>
-cudaError_t y3launch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs) {
+cudaError_t y3launch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs, int lay) {
     dim3 grid((c->nxh + Y::TX - 1) / Y::TX, nzs);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->ypass_tw_off;
     if (dir > 0)
-        k_ycol3<Y, 1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, tw, (float)scale);
+        k_ycol3<Y, 1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->nz, lay, tw,
+                                                          (float)scale);
     else
-        k_ycol3<Y, -1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, tw, (float)scale);
+        k_ycol3<Y, -1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->nz, lay, tw,
+                                                           (float)scale);
     return cudaGetLastError();
 }
 using Y256 = YCfg<256, 16, 8>;
@@ -362,8 +366,9 @@ cudaError_t xlaunch(const pfc_ctx* c, const void* in, void* out, const void* pot
 }  // namespace
 
 // 512-point variants, measured against each other: the x pass defaults to 16 values per
-// thread (three CTAs per SM; PFC_X_VARIANT=1 selects 32), the y pass to 64-byte column
-// segments (PFC_Y_VARIANT=5 selects 128-byte segments).
+// thread (three CTAs per SM; PFC_X_VARIANT=1 selects 32), the y pass to 16 values per
+// thread capped at 64 registers (k_ycol3, 32 warps per SM; PFC_Y_VARIANT=1 selects
+// k_ycol's 32 values per thread, 5 its 128-byte segments, 6 k_ycol3 uncapped).
 static int env_choice(const char* name) {
     const char* s = getenv(name);
     return s ? atoi(s) : 0;
@@ -373,8 +378,8 @@ int fused_y_variant(int ny, int dtype) {
     if (dtype != PFC_F32) return 0;
     switch (ny) {
         case 512: {
-            const int v = env_choice("PFC_Y_VARIANT");  // 5: 128-byte segments; 6, 7: 16 values per thread
-            return (v == 5 || v == 6 || v == 7) ? v : 1;
+            const int v = env_choice("PFC_Y_VARIANT");
+            return (v == 1 || v == 5 || v == 6) ? v : 7;
         }
         case 256: return 2;
         case 128: return 3;
@@ -416,15 +421,15 @@ cudaError_t set_pass_attributes(const pfc_ctx* c) {
 }
 
 cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs, int lay) {
-    if (lay && (nzs != c->nz || c->fused_y >= 6)) return cudaErrorNotSupported;  // whole fields, k_ycol only
+    if (lay && nzs != c->nz) return cudaErrorNotSupported;  // tiled: whole fields
     switch (c->fused_y) {
         case 1: return ylaunch<Y512>(c, dir, in, out, scale, nzs, lay);
         case 2: return ylaunch<Y256>(c, dir, in, out, scale, nzs, lay);
         case 3: return ylaunch<Y128>(c, dir, in, out, scale, nzs, lay);
         case 4: return ylaunch<Y64>(c, dir, in, out, scale, nzs, lay);
         case 5: return ylaunch<Y512w>(c, dir, in, out, scale, nzs, lay);
-        case 6: return y3launch<Y512h>(c, dir, in, out, scale, nzs);
-        case 7: return y3launch<Y512q>(c, dir, in, out, scale, nzs);
+        case 6: return y3launch<Y512h>(c, dir, in, out, scale, nzs, lay);
+        case 7: return y3launch<Y512q>(c, dir, in, out, scale, nzs, lay);
     }
     return cudaErrorNotSupported;
 }

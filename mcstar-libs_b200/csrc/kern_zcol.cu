@@ -41,7 +41,7 @@ struct ZCfg {
     static constexpr int STG = NZ * TX;  // staging of one field tile, [z][c]
     // every kernel ends its shared memory with the twiddles W_NZ^m (NZ float2) and the
     // wavenumbers k_z of the NZ modes (NZ floats)
-    static constexpr int TAIL = NZ + NZ / 2;
+    static constexpr int TAIL = NZ + NZ / 2 + 4;
     static constexpr size_t SMEM = (size_t)(2 * REG + TAIL) * sizeof(float2);
     static constexpr size_t SMEM_PIPE = (size_t)(2 * STG + 2 * REG + NHS + TAIL) * sizeof(float2);
     static constexpr size_t SMEM_CARRY = (size_t)(REG + STG + TAIL) * sizeof(float2);  // TH threads, one field
@@ -62,8 +62,12 @@ template <class Z> __device__ __forceinline__ int stg_row(int kz) {
     else return kz;
 }
 
+// Slot of mode kz in the shared table of wavenumbers: one float of padding per 128 modes,
+// so that modes 128 apart (the two threads of a D3 pair) read different banks.
+__device__ __forceinline__ int kz_slot(int kz) { return kz + (kz >> 7); }
+
 // Twiddles W_NZ^m and wavenumbers K(kz) = kz' 2 pi / L_z (common.hpp:27-28) of the
-// NZ modes into the shared tail of a z kernel (tw, then NZ floats).
+// NZ modes into the shared tail of a z kernel (tw, then NZ + NZ / 128 floats).
 template <class Z>
 __device__ __forceinline__ float* load_tail(float2* tw, const float2* __restrict__ twg, const ZArgsF& a, int tid,
                                            int nthreads) {
@@ -71,7 +75,7 @@ __device__ __forceinline__ float* load_tail(float2* tw, const float2* __restrict
     float* kz_tab = reinterpret_cast<float*>(tw + NZ);
     for (int i = tid; i < NZ; i += nthreads) {
         tw[i] = twg[i];
-        kz_tab[i] = (float)(i < NZ / 2 + 1 ? i : i - NZ) * a.ckz;
+        kz_tab[kz_slot(i)] = (float)(i < NZ / 2 + 1 ? i : i - NZ) * a.ckz;
     }
     return kz_tab;
 }
@@ -113,7 +117,7 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2
             const int kz = (t * U + u) + E * k2;
             const float2 psi = kPsiInV ? v[u * P + k2] : other(kz);
             const float2 n = kPsiInV ? other(kz) : v[u * P + k2];
-            const float k2z = kz_tab[kz];
+            const float k2z = kz_tab[kz_slot(kz)];
             const float dopx = -kxy - k2z * k2z;
             const float dopy = dopx * dopx;
             const float inv = __frcp_rn(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
@@ -132,7 +136,7 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2
 #pragma unroll 1
         for (int m = 0; m < E; ++m) {
             const int kz = (t * U + m / P) + E * (m % P);
-            const float k2z = kz_tab[kz];
+            const float k2z = kz_tab[kz_slot(kz)];
             const float dopx = -kxy - k2z * k2z;
             const float dopy = dopx * dopx;
             const float inv = __frcp_rn(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
@@ -242,29 +246,36 @@ template <int NZ_, int E_, int TX_>
 struct Z3Cfg {
     static constexpr int NZ = NZ_, E = E_, TX = TX_, P = 2 * E, TH = TX * P, T = 2 * TH;
     static constexpr int REG = E * (P + 1) * TX;  // exchange buffer of one half
-    static constexpr int TAIL = NZ + NZ / 2;
+    static constexpr int TAIL = NZ + NZ / 2 + 4;
     static constexpr size_t SMEM = (size_t)(2 * REG + TAIL) * sizeof(float2);
+    static constexpr size_t SMEM_CARRY = (size_t)(REG + NZ * TX + TAIL) * sizeof(float2);  // k_zcarry3
     static_assert(P * E == NZ && TH % 32 == 0 && REG >= NZ * TX, "shape");
 };
 
 // propagate for distribution D3: register r of thread t = 2p + h holds mode
-// kz = p + E d3_k2(r, h); nl(kz) returns N^ (v holds psi^)
-template <class Z, class Bar, class NL, class SLOT>
-__device__ __forceinline__ void propagate3(float2 (&v)[Z::E], NL nl, float2* scratch, SLOT slot, const Bar& bar,
+// kz = p + h E^2/2 + d3_off(r).  kPsiInV: v holds psi^ and the tile N^, else the converse;
+// the tile ([row][TX], rows as d3_off's comment, column c) is also the noise pass's scratch
+// (the thread's own slots).  kSync: a barrier before that use.
+template <class Z, bool kPsiInV, bool kSync, class Bar>
+__device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int c, const Bar& bar,
                                            const float* kz_tab, int kx, int ky, int t, int nx, int ny,
                                            const ZArgsF& a, const double2* k0) {
-    constexpr int NZ = Z::NZ, E = Z::E;
+    constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, B = E * E / 2;
+    static_assert(B == 128, "kz_slot pads one float per 128 modes");
     const int p = t >> 1, h = t & 1;
+    const int kzb = p + h * B;                   // kz = kzb + d3_off(r)
+    float2* trow = tile + ((p ^ h) + h * B) * TX + c;  // + d3_off(r) TX
+    const float* tab = kz_tab + kzb + h;         // kz_slot(kz) = kzb + h + d3_off(r) + 2 [r >= E/2]
     const float k0x = (float)kx * a.ckx;
     const float k1y = (float)(ky < ny / 2 + 1 ? ky : ky - ny) * a.cky;
     const float kxy = k0x * k0x + k1y * k1y;
     const float deps = 1.0f + a.C - a.eps;
 #pragma unroll
     for (int r = 0; r < E; ++r) {
-        const int kz = p + E * d3_k2<E>(r, h);
-        const float2 psi = v[r];
-        const float2 n = nl(kz);
-        const float k2z = kz_tab[kz];
+        const float2 o = trow[d3_off<E>(r) * TX];
+        const float2 psi = kPsiInV ? v[r] : o;
+        const float2 n = kPsiInV ? o : v[r];
+        const float k2z = tab[d3_off<E>(r) + (r >= E / 2 ? 2 : 0)];
         const float dopx = -kxy - k2z * k2z;
         const float dopy = dopx * dopx;
         const float inv = __frcp_rn(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
@@ -272,26 +283,27 @@ __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], NL nl, float2* scr
         v[r] = make_float2((psi.x + f * n.x) * inv, (psi.y + f * n.y) * inv);
     }
     if (a.use_noise) {
-        bar.sync();  // the scratch is the exchange buffer of the transform
+        if (kSync) bar.sync();
         const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
 #pragma unroll
-        for (int r = 0; r < E; ++r) scratch[slot(p + E * d3_k2<E>(r, h))] = v[r];
+        for (int r = 0; r < E; ++r) trow[d3_off<E>(r) * TX] = v[r];
 #pragma unroll 1
         for (int r = 0; r < E; ++r) {
-            const int kz = p + E * d3_k2<E>(r, h);
-            const float k2z = kz_tab[kz];
+            const int off = r < E / 2 ? E * r : E * E + E * (r - E / 2);
+            const int kz = kzb + off;
+            const float k2z = tab[off + (r >= E / 2 ? 2 : 0)];
             const float dopx = -kxy - k2z * k2z;
             const float dopy = dopx * dopx;
             const float inv = __frcp_rn(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
             const float2 xi = kspace_noise<float>(kx, ky, kz, nx, ny, NZ, a.seed, ctr);
             const float g = a.dt * a.namp_eff * sqrtf(-dopx) * inv;
-            float2 w = scratch[slot(kz)];
+            float2 w = trow[off * TX];
             w.x += g * xi.x;
             w.y += g * xi.y;
-            scratch[slot(kz)] = w;
+            trow[off * TX] = w;
         }
 #pragma unroll
-        for (int r = 0; r < E; ++r) v[r] = scratch[slot(p + E * d3_k2<E>(r, h))];
+        for (int r = 0; r < E; ++r) v[r] = trow[d3_off<E>(r) * TX];
     }
     if (kx == 0 && ky == 0 && t == 0) v[0] = make_float2((float)k0->x, (float)k0->y);  // kz = 0 at r = 0
 }
@@ -326,15 +338,16 @@ __global__ void __launch_bounds__(Z::T, 2) k_zcol3(const float2* A, const float2
     const BarDyn bar{1 + half, TH};
     fft_d1_to_d3<NZ, E, TX, -1, BarDyn>(v, t, c, half ? regB : regA, tw, bar);
     const int p = t >> 1, h = t & 1;
-    auto own = [&](int kz) { return kz * TX + c; };  // N^ hand-over slots (two wavefronts per access)
     if (half != 0) {
+        // N^ hand-over in the rows of propagate3's tile
+        float2* trow = regB + ((p ^ h) + h * (E * E / 2)) * TX + c;
         bar.sync();
 #pragma unroll
-        for (int r = 0; r < E; ++r) regB[own(p + E * d3_k2<E>(r, h))] = v[r];
+        for (int r = 0; r < E; ++r) trow[d3_off<E>(r) * TX] = v[r];
     }
     __syncthreads();
     if (half != 0) return;
-    propagate3<Z>(v, [&](int kz) { return regB[own(kz)]; }, regB, own, bar, kz_tab, kx, ky, t, nx, ny, a, k0);
+    propagate3<Z, true, false>(v, regB, c, bar, kz_tab, kx, ky, t, nx, ny, a, k0);
     if (!a.final_step) fft_d3_to_d1<NZ, E, TX, 1, BarDyn>(v, t, c, regA, tw, bar);
     watch<Z>(v, a.final_step, valid, flag);
     if (!valid) return;
@@ -410,6 +423,78 @@ __global__ void __launch_bounds__(Z::TH, Z::CMINB) k_zcarry(float2* kpsi, float2
     fft_d2_to_d1<NZ, E, TX, 1, BarCta, Z::PADG>(v, t, c, xb, tw);
     watch<Z>(v, false, valid, flag);
     store_state<Z>(v, A, base, zs, t, valid, false);
+}
+
+// The psi^-carrying z pass with 16 values per thread (fft_d1_to_d3) on the z-tiled layout,
+// one field per CTA of TH threads: the psi^ block of the tile (contiguous) is staged in
+// shared memory with cp.async while B is loaded and transformed; the update reads psi^
+// from the stage and writes psi^' (in place), then A' = IFFT_z(psi^')/nz over B's block.
+// kLast: B and psi^' in the standard layout (psi^' over B, in place), no A'.  Shared
+// memory: the exchange buffer, the stage [kz][c] (a warp's four modes per register have
+// two even and two odd kz: no bank conflicts), the tail.
+template <class Z, bool kLast>
+__global__ void __launch_bounds__(Z::TH, 3) k_zcarry3(const float2* psi_in, const float2* B, float2* psi_out,
+                                                       float2* A, int nx, int ny, ZArgsF a,
+                                                       const double2* __restrict__ k0, int* flag,
+                                                       const float2* __restrict__ twg) {
+    constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, TH = Z::TH;
+    static_assert(TX == kTileW, "the tiles of the z-tiled layout");
+    extern __shared__ __align__(16) float2 sm[];
+    float2* xb = sm;
+    float2* stg = sm + Z::REG;
+    float2* tw = stg + NZ * TX;
+    const int tid = threadIdx.x;
+    const int c = tid % TX, t = tid / TX;
+    const int kx = blockIdx.x * TX + c;
+    const int ky = blockIdx.y;
+    const int nxh = nx / 2 + 1;
+    const bool valid = kx < nxh;
+    const ColAddr cp = zcol_addr<true>(blockIdx.x, c, ky, nxh, ny, NZ);
+    const ColAddr cb = zcol_addr<!kLast>(blockIdx.x, c, ky, nxh, ny, NZ);
+    if (valid) {
+#pragma unroll
+        for (int j = 0; j < E; ++j) {
+            const int z = t + P * j;
+            cp_async8(&stg[((t ^ d1_flip<E>(j)) + P * j) * TX + c], psi_in + cp.base + (int64_t)z * cp.stride);
+        }
+    }
+    cp_commit();
+    const float* kz_tab = load_tail<Z>(tw, twg, a, tid, TH);
+    float2 v[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = valid ? B[cb.base + (int64_t)(t + P * j) * cb.stride] : make_float2(0.f, 0.f);
+    __syncthreads();
+    fft_d1_to_d3<NZ, E, TX, -1>(v, t, c, xb, tw);
+    cp_wait_all();
+    __syncthreads();  // psi^ staged by the other threads of the column is visible
+    propagate3<Z, false, false>(v, stg, c, BarCta{}, kz_tab, kx, ky, t, nx, ny, a, k0);
+    const int p = t >> 1, h = t & 1;
+    if (kLast) watch<Z>(v, true, valid, flag);
+    if (valid) {
+        const ColAddr co = kLast ? cb : cp;
+#pragma unroll
+        for (int r = 0; r < E; ++r) psi_out[co.base + (int64_t)(p + E * d3_k2<E>(r, h)) * co.stride] = v[r];
+    }
+    if (kLast) return;
+    fft_d3_to_d1<NZ, E, TX, 1>(v, t, c, xb, tw);
+    watch<Z>(v, false, valid, flag);
+    if (valid) {
+        const float s = 1.0f / (float)NZ;
+#pragma unroll
+        for (int j = 0; j < E; ++j) A[cb.base + (int64_t)(t + P * j) * cb.stride] = make_float2(v[j].x * s, v[j].y * s);
+    }
+}
+
+// Copy between the standard and the z-tiled layouts (col_addr layouts 0, 1): one kx tile
+// of the z columns at one ky per CTA of TX * 32 threads.
+__global__ void __launch_bounds__(256) k_relayout(const float2* __restrict__ in, float2* __restrict__ out, int nxh,
+                                                  int ny, int nz, int to_tiled) {
+    const int c = threadIdx.x % kTileW, t = threadIdx.x / kTileW;
+    const int kt = blockIdx.x, ky = blockIdx.y;
+    if (kt * kTileW + c >= nxh) return;
+    const ColAddr s = to_tiled ? zcol_addr<false>(kt, c, ky, nxh, ny, nz) : zcol_addr<true>(kt, c, ky, nxh, ny, nz);
+    const ColAddr d = to_tiled ? zcol_addr<true>(kt, c, ky, nxh, ny, nz) : zcol_addr<false>(kt, c, ky, nxh, ny, nz);
+    for (int z = t; z < nz; z += 32) out[d.base + (int64_t)z * d.stride] = in[s.base + (int64_t)z * s.stride];
 }
 
 __device__ __forceinline__ void bar_arrive(int id, int count) {
@@ -584,6 +669,12 @@ cudaError_t set_zcol_attributes(const pfc_ctx* c) {
             if (!e)
                 e = cudaFuncSetAttribute(k_zcol3<Z3_512, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)Z3_512::SMEM);
+            if (!e)
+                e = cudaFuncSetAttribute(k_zcarry3<Z3_512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)Z3_512::SMEM_CARRY);
+            if (!e)
+                e = cudaFuncSetAttribute(k_zcarry3<Z3_512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)Z3_512::SMEM_CARRY);
             return e;
         }
     }
@@ -598,6 +689,25 @@ cudaError_t launch_zcarry(const pfc_ctx* c, void* kpsi, void* A, const void* B, 
         case 4: return zlaunch_carry<Z64>(c, kpsi, A, B, a);
     }
     return cudaErrorNotSupported;
+}
+
+cudaError_t launch_zcarry_tiled(const pfc_ctx* c, const void* psi_in, const void* B, void* psi_out, void* A,
+                                const ZPropArgs& a) {
+    if (c->fused_z != 6) return cudaErrorNotSupported;
+    using Z = Z3_512;
+    const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
+    dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny);
+    auto k = a.final_step ? k_zcarry3<Z, true> : k_zcarry3<Z, false>;
+    k<<<grid, Z::TH, Z::SMEM_CARRY, c->stream>>>((const float2*)psi_in, (const float2*)B, (float2*)psi_out, (float2*)A,
+                                                  c->nx, c->ny, zargs_f(a), c->k0, c->flag, tw);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_relayout(const pfc_ctx* c, const void* in, void* out, int to_tiled) {
+    if (c->dtype != PFC_F32 || in == out) return cudaErrorNotSupported;
+    dim3 grid((c->nxh + kTileW - 1) / kTileW, c->ny);
+    k_relayout<<<grid, 256, 0, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->ny, c->nz, to_tiled);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_zcol(const pfc_ctx* c, const void* A, const void* B, void* O, const ZPropArgs& a, int lay) {

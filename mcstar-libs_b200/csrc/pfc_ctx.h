@@ -56,7 +56,8 @@ struct pfc_ctx {
     int plane_tw_off;             // twiddles of the plane kernel: W_ny^m, W_{nx/2}^m, W_nx^k (k <= nx/2)
     int fused_z;                  // 0: general z pass; otherwise the register z kernel variant id
     int z_pipe;                   // register z pass as the persistent pipelined kernel (1) or one tile per CTA (0)
-    int z_carry;                  // carry psi^ itself (A = IFFT_z(psi^)/nz lives in work2) instead of A
+    int z_carry;                  // carry psi^ itself instead of A: standard layout, A = IFFT_z(psi^)/nz
+                                  // in work2; tiled, psi^ z-tiled in work2 and A in the psi^ buffer
     int tiled;                    // register passes on kx-tiled fields (col_addr): A z-tiled in work2,
                                   // the x pass field row-tiled in work, the z pass input B z-tiled
                                   // in the caller's psi^ buffer
@@ -153,6 +154,12 @@ cudaError_t set_zcol_attributes(const pfc_ctx* c);
 cudaError_t launch_zcol(const pfc_ctx* c, const void* A, const void* B, void* O, const ZPropArgs& a, int lay = 0);
 // the z pass that carries psi^: reads psi^ (kpsi) and B, writes psi^' and (unless last) A'
 cudaError_t launch_zcarry(const pfc_ctx* c, void* kpsi, void* A, const void* B, const ZPropArgs& a);
+// the same on the z-tiled layout (nz = 512): psi^ z-tiled (psi_out may be psi_in); B and A
+// z-tiled (A may be B), or on the last step B and psi_out standard (psi_out may be B), no A
+cudaError_t launch_zcarry_tiled(const pfc_ctx* c, const void* psi_in, const void* B, void* psi_out, void* A,
+                                const ZPropArgs& a);
+// FP32 field copy between the standard and the z-tiled layout (out of place)
+cudaError_t launch_relayout(const pfc_ctx* c, const void* in, void* out, int to_tiled);
 
 // ---- pointwise kernels, noise and reductions (kern_point.cu) ----
 cudaError_t launch_update_eom(const pfc_ctx* c, void* kpsi, const void* knl, const void* knoise,

@@ -338,6 +338,16 @@ __device__ __forceinline__ void fft_d3_to_d1(float2 (&v)[E], int t, int g, float
 template <int E> __device__ __forceinline__ int d3_k2(int r, int h) {
     return r < E / 2 ? h * (E / 2) + r : E + h * (E / 2) + (r - E / 2);
 }
+// Mode of register r of D3 thread (p, h) relative to p + h E^2/2: kz = p + h E^2/2 + d3_off(r).
+template <int E> __device__ __forceinline__ constexpr int d3_off(int r) {
+    return r < E / 2 ? E * r : E * E + E * (r - E / 2);
+}
+// Tiles of 8-byte values [row][g] (8 groups g per row) read in distribution D3 keep mode kz
+// in row kz ^ ((kz / (E^2/2)) & 1): the two threads of a pair (one half-warp) hold modes
+// E^2/2 apart, and the swapped parity puts them in opposite bank halves.  For the modes of
+// D3 thread (p, h) the swapped bit is h: row = (p ^ h) + h E^2/2 + d3_off(r).  For D1
+// (thread t, kz = t + 2E j) it is bit 0 of j / (E/4): row = (t ^ d1_flip(j)) + 2E j.
+template <int E> __device__ __forceinline__ constexpr int d1_flip(int j) { return (j / (E / 4)) & 1; }
 
 // Split / merge of a real FFT of length 2M done as an M-point complex FFT
 // (z[m] = x[2m] + i x[2m+1]); w = W_2M^k = exp(-2 pi i k / 2M).

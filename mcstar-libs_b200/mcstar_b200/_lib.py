@@ -55,7 +55,7 @@ PROFILE_FAMILIES = 5  # PFC_PROFILE_FAMILIES
 class PfcProfile(ctypes.Structure):
     _fields_ = [("launches", ctypes.c_longlong), ("calls", ctypes.c_longlong * PROFILE_FAMILIES),
                 ("ms", ctypes.c_double * PROFILE_FAMILIES), ("xy_variant", ctypes.c_int), ("xy_mode", ctypes.c_int),
-                ("z_mode", ctypes.c_int), ("z_variant", ctypes.c_int)]
+                ("z_mode", ctypes.c_int), ("z_variant", ctypes.c_int), ("y_variant", ctypes.c_int)]
 
 
 _lib = None

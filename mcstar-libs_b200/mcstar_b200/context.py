@@ -206,7 +206,7 @@ class Context:
         check(lib().pfc_profile_read(self._h, ctypes.byref(p)), self._h, "pfc_profile_read")
         return {"launches": int(p.launches), "calls": [int(v) for v in p.calls], "ms": [float(v) for v in p.ms],
                 "xy_variant": int(p.xy_variant), "xy_mode": int(p.xy_mode), "z_mode": int(p.z_mode),
-                "z_variant": int(p.z_variant)}
+                "z_variant": int(p.z_variant), "y_variant": int(p.y_variant)}
 
     def free_energy(self, kpsi, eps, lens, hh):
         out = ctypes.c_double()
