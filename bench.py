@@ -49,8 +49,9 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", type=int, default=512, help="grid side (the headline workload is 512)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="pfc512", choices=["pfc512", "ensemble"],
-                    help="pfc512: the headline 512^3 field (default); ensemble: 64 mixed-size replicas")
+    ap.add_argument("--workload", default="pfc512", choices=["pfc512", "ensemble", "lowpass"],
+                    help="pfc512: the headline 512^3 field (default); ensemble: 64 mixed-size replicas; "
+                         "lowpass: the 2D amplitude low-pass with its LOWPASS dump (4096^2 unless --size)")
     return ap.parse_args()
 
 
@@ -257,6 +258,112 @@ def run_ensemble(args, ws, rank, local):
     return out
 
 
+LP = dict(n=4096, dx=0.8, dps=2.0, seed=11)
+
+
+def run_lowpass(args, ws, rank, local):
+    """The 2D amplitude low-pass (calc_amplitude_lowpass: high-pass, square, low-pass, the
+    gzip LOWPASS dump, amplitude) on an n^2 FP32 field, n = 4096 unless --size is given;
+    each call restores the input spectrum first (one device copy).  N GPUs run replicas."""
+    from mcstar_b200 import get_context
+    n = LP["n"] if args.size == 512 else args.size
+    shape = (n, n, 1)
+    lens, hh = (n * LP["dx"], n * LP["dx"], 1.0), (LP["dx"], LP["dx"], 1.0)
+    ctx = get_context(shape, np.float32)
+    x = np.arange(n) * LP["dx"]
+    psi = (0.3 * np.cos(2 * math.pi * (n // 8) / lens[0] * x)[None, :] +
+           0.05 * np.random.default_rng(LP["seed"]).standard_normal((n, n))).astype(np.float32)
+    real = ctx.empty_state()
+    real[: n * n].copy_(torch.from_numpy(psi.ravel()))
+    spec0, spec, aux, g = ctx.empty_state(), ctx.empty_state(), ctx.empty_state(), ctx.empty_state()
+    ctx.r2c(real, spec0)
+    ctx.gaussian_init(g, lens, hh, LP["dps"])
+    path = os.path.join(tempfile.mkdtemp(prefix="lowpass_"), f"rank{rank}.gz")
+
+    def call(dump):
+        spec.copy_(spec0)
+        ctx.amplitude_lowpass(spec, aux, g, lens, path if dump else None)
+
+    for _ in range(args.warmup):
+        call(True)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    barrier(ws)
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        call(True)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3
+    clk = clocks.stop()
+    barrier(ws)
+    ms = max_over_ranks(ws, ms)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        call(False)
+    e1.record()
+    torch.cuda.synchronize()
+    dev_ms = e0.elapsed_time(e1)
+    return {
+        "metric": f"2D amplitude low-pass calls/s at {n}^2 fp32 (calc_amplitude_lowpass with its LOWPASS dump)",
+        "value": round(ws * args.steps / (ms / 1e3), 2), "unit": "calls/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: a stripe pattern with seeded noise (numpy PCG64)",
+        "config": {"workload": f"amplitude-lowpass {n}^2 fp32", "grid": [n, n], "dx": LP["dx"],
+                   "divs_per_sigma": LP["dps"], "parallelism": f"{ws} replica(s)",
+                   "timing": "host clock around synchronised calls (each call ends with the dump's D2H and "
+                             "gzip write); device_only: CUDA events, no dump"},
+        "device_only": {"ms_per_call": round(dev_ms / args.steps, 4),
+                        "kernels_per_call": "kmult, C2R (2 passes), norm+square, R2C (2 passes), kmult, "
+                                            "C2R (2 passes), norm"},
+        "clocks": clk,
+    }
+
+
+def run_reference_lowpass(args):
+    name = os.path.join(ROOT, "oracle", "_ref", "libref_lowpass_f32.so")
+    if not torch.cuda.is_available():
+        return {"impl": "reference", "unavailable": "no CUDA device: the reference's low-pass is CUDA/cuFFT code"}
+    if not os.path.exists(name):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libref_lowpass_f32.so not built (make -C oracle)"}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pfc_oracle as O
+    L = ctypes.CDLL(name)
+    I, D, P = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+    L.refl32_time_amplitude_lowpass.argtypes = [I, I, P, P, D, D, ctypes.c_char_p, I, I]
+    L.refl32_time_amplitude_lowpass.restype = D
+    n = LP["n"] if args.size == 512 else args.size
+    lens, hh = (n * LP["dx"], n * LP["dx"], 1.0), (LP["dx"], LP["dx"], 1.0)
+    x = np.arange(n) * LP["dx"]
+    psi = (0.3 * np.cos(2 * math.pi * (n // 8) / lens[0] * x)[None, :] +
+           0.05 * np.random.default_rng(LP["seed"]).standard_normal((n, n))).astype(np.float32)
+    spec = np.ascontiguousarray(O.r2c(psi[None]).astype(np.complex64))
+    g = np.ascontiguousarray(O.gaussian_init((n, n, 1), lens, hh, LP["dps"], np.float32))
+    path = os.path.join(tempfile.mkdtemp(prefix="lowpass_ref_"), "ref.gz")
+    clocks = Clocks(0)
+    clocks.start()
+    ms = L.refl32_time_amplitude_lowpass(n, n, spec.ctypes.data, g.ctypes.data, lens[0], lens[1],
+                                         path.encode(), args.warmup, args.steps)
+    clk = clocks.stop()
+    value = args.steps / (ms / 1e3)
+    return {
+        "impl": "reference",
+        "metric": f"2D amplitude low-pass calls/s at {n}^2 fp32 (calc_amplitude_lowpass with its LOWPASS dump)",
+        "value": round(value, 2), "unit": "calls/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic: a stripe pattern with seeded noise (numpy PCG64)",
+        "config": {"workload": f"amplitude-lowpass {n}^2 fp32", "grid": [n, n], "dx": LP["dx"],
+                   "divs_per_sigma": LP["dps"], "parallelism": "single GPU"},
+        "cpu_baseline": {"value": round(value, 2), "unit": "calls/s", "cores": 1, "kind": "reference",
+                         "sample": "the reference's calc_amplitude_lowpass (lowpass.hpp:78-93, cuFFT plans made "
+                                   "once, oracle/_ref) on the GPU, driven by one host thread"},
+        "e2e": {"value": round(value, 2), "unit": "calls/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk,
+    }
+
+
 def run_b200(args, ws, rank, local):
     from mcstar_b200 import Stepper
     n = args.size
@@ -407,11 +514,13 @@ def main():
     from mcstar_b200 import dist
     if args.impl == "reference":
         if rank == 0:
-            print(json.dumps(run_reference(args)))
+            print(json.dumps(run_reference_lowpass(args) if args.workload == "lowpass" else run_reference(args)))
         dist.shutdown(ws)
         return
     if args.workload == "ensemble":
         out = run_ensemble(args, ws, rank, local)
+    elif args.workload == "lowpass":
+        out = run_lowpass(args, ws, rank, local)
     else:
         out = run_b200(args, ws, rank, local)
         if rank == 0 and ws == 1 and not args.no_cpu_baseline:

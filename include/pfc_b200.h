@@ -117,6 +117,33 @@ pfc_status pfc_update_eom_hpfcnoise(pfc_ctx* ctx, void* kpsi, const void* knonli
                                     const void* knoise2, const void* knoise3, double namp, double dt, double eps,
                                     double lx, double ly, double lz);
 
+/* ---- spectral low-pass post-processing: replaces cuda/kernels/gaussian.hpp and
+ * cuda/kernels/lowpass.hpp --------------------------------------------------------------
+ * pfc_gaussian_init: kgauss_k = (e, 1 - e), e = exp(-1/2 sum_a (1.1 d h_a K_a)^2), d =
+ *   divs_per_sigma, h the grid spacings -- call_kernel_gaussian_init, gaussian.hpp:23-39.
+ * pfc_kmult_real / pfc_kmult_imag: karr_k *= Re / Im kgauss_k -- call_kernel_kmult_real /
+ *   _imag (gaussian.hpp:41-67) and _call_kernel_multassign_cmpl_with_real / _imag
+ *   (lowpass.hpp:1-35).
+ * pfc_square: psi <- psi^2 on the real field -- _call_kernel_square, lowpass.hpp:37-52.
+ * pfc_write_lowpass_2d: spectrum *= Re kgauss (in place), then the gzip-compressed LOWPASS
+ *   text dump of the low-passed half spectrum (the reference's byte format) to path --
+ *   write_lowpass_2d, lowpass.hpp:54-77.  2D grids only (PFC_ERR_INVALID otherwise: the
+ *   reference asserts); PFC_ERR_INVALID with a message when the file cannot be written.
+ * pfc_amplitude_lowpass: the local amplitude of a 2D field -- calc_amplitude_lowpass,
+ *   lowpass.hpp:78-93: spectrum *= Im kgauss (the high-pass), C2R into aux, normalise and
+ *   square, R2C into spectrum, the LOWPASS dump as pfc_write_lowpass_2d (skipped when path is
+ *   NULL), C2R into aux, normalise.  On return aux holds the amplitude field (real layout) and
+ *   spectrum the low-passed spectrum of the squared high-pass field. */
+pfc_status pfc_gaussian_init(pfc_ctx* ctx, void* kgauss, double lx, double ly, double lz, double hx, double hy,
+                             double hz, double divs_per_sigma);
+pfc_status pfc_kmult_real(pfc_ctx* ctx, void* karr, const void* kgauss);
+pfc_status pfc_kmult_imag(pfc_ctx* ctx, void* karr, const void* kgauss);
+pfc_status pfc_square(pfc_ctx* ctx, void* arr);
+pfc_status pfc_write_lowpass_2d(pfc_ctx* ctx, void* spectrum, const void* kgauss, double lx, double ly,
+                                const char* path);
+pfc_status pfc_amplitude_lowpass(pfc_ctx* ctx, void* spectrum, void* aux, const void* kgauss, double lx, double ly,
+                                 const char* path);
+
 /* ---- noise: replaces NoiseHostApi<F> (cuda/noise.hpp:93-150) -------------------------
  * Counter-based Philox4x32-10: (seed, counter) selects the draw, so a run resumes
  * bit-exactly.  fill_kspace: complex normal, E|xi|^2 = 1, Hermitian on the i0 = 0 and

@@ -675,6 +675,73 @@ pfc_status pfc_free_energy(pfc_ctx* ctx, const void* kpsi, double eps, double lx
     return PFC_OK;
 }
 
+// ---- spectral low-pass post-processing ---------------------------------------------------------
+pfc_status pfc_gaussian_init(pfc_ctx* ctx, void* kgauss, double lx, double ly, double lz, double hx, double hy,
+                             double hz, double divs_per_sigma) {
+    PFC_CHECK_CTX();
+    if (!kgauss) return fail(ctx, PFC_ERR_INVALID, "pfc_gaussian_init: null buffer");
+    PFC_CUDA(launch_gaussian_init(ctx, kgauss, lx, ly, lz, hx, hy, hz, divs_per_sigma), "pfc_gaussian_init");
+    return PFC_OK;
+}
+
+pfc_status pfc_kmult_real(pfc_ctx* ctx, void* karr, const void* kgauss) {
+    PFC_CHECK_CTX();
+    if (!karr || !kgauss) return fail(ctx, PFC_ERR_INVALID, "pfc_kmult_real: null buffer");
+    PFC_CUDA(launch_kmult(ctx, karr, kgauss, 0), "pfc_kmult_real");
+    return PFC_OK;
+}
+
+pfc_status pfc_kmult_imag(pfc_ctx* ctx, void* karr, const void* kgauss) {
+    PFC_CHECK_CTX();
+    if (!karr || !kgauss) return fail(ctx, PFC_ERR_INVALID, "pfc_kmult_imag: null buffer");
+    PFC_CUDA(launch_kmult(ctx, karr, kgauss, 1), "pfc_kmult_imag");
+    return PFC_OK;
+}
+
+pfc_status pfc_square(pfc_ctx* ctx, void* arr) {
+    PFC_CHECK_CTX();
+    if (!arr) return fail(ctx, PFC_ERR_INVALID, "pfc_square: null buffer");
+    PFC_CUDA(launch_norm_square(ctx, arr, 0), "pfc_square");
+    return PFC_OK;
+}
+
+namespace {
+bool is_2d(const pfc_ctx* c) { return c->nz == 1 && c->ny > 1 && c->nx > 1; }
+pfc_status lowpass_dump(pfc_ctx* ctx, const void* spectrum, double lx, double ly, const char* path) {
+    cudaError_t ce = cudaSuccess;
+    const int r = write_lowpass_file(ctx, spectrum, lx, ly, path, &ce);
+    if (r == 1) return fail(ctx, PFC_ERR_CUDA, std::string("LOWPASS dump: ") + cudaGetErrorString(ce));
+    if (r == 2) return fail(ctx, PFC_ERR_INVALID, std::string("LOWPASS dump: cannot write ") + path);
+    return PFC_OK;
+}
+}  // namespace
+
+pfc_status pfc_write_lowpass_2d(pfc_ctx* ctx, void* spectrum, const void* kgauss, double lx, double ly,
+                                const char* path) {
+    PFC_CHECK_CTX();
+    if (!spectrum || !kgauss || !path) return fail(ctx, PFC_ERR_INVALID, "pfc_write_lowpass_2d: null argument");
+    if (!is_2d(ctx)) return fail(ctx, PFC_ERR_INVALID, "pfc_write_lowpass_2d: the grid is not 2D");
+    PFC_CUDA(launch_kmult(ctx, spectrum, kgauss, 0), "pfc_write_lowpass_2d");
+    return lowpass_dump(ctx, spectrum, lx, ly, path);
+}
+
+pfc_status pfc_amplitude_lowpass(pfc_ctx* ctx, void* spectrum, void* aux, const void* kgauss, double lx, double ly,
+                                 const char* path) {
+    PFC_CHECK_CTX();
+    if (!spectrum || !aux || !kgauss) return fail(ctx, PFC_ERR_INVALID, "pfc_amplitude_lowpass: null buffer");
+    if (!is_2d(ctx)) return fail(ctx, PFC_ERR_INVALID, "pfc_amplitude_lowpass: the grid is not 2D");
+    PFC_CUDA(launch_kmult(ctx, spectrum, kgauss, 1), "pfc_amplitude_lowpass high-pass");
+    pfc_status s = pfc_fft_c2r(ctx, spectrum, aux);
+    if (s != PFC_OK) return s;
+    PFC_CUDA(launch_norm_square(ctx, aux, 1), "pfc_amplitude_lowpass square");
+    if ((s = pfc_fft_r2c(ctx, aux, spectrum)) != PFC_OK) return s;
+    PFC_CUDA(launch_kmult(ctx, spectrum, kgauss, 0), "pfc_amplitude_lowpass low-pass");
+    if (path && (s = lowpass_dump(ctx, spectrum, lx, ly, path)) != PFC_OK) return s;
+    if ((s = pfc_fft_c2r(ctx, spectrum, aux)) != PFC_OK) return s;
+    PFC_CUDA(launch_norm(ctx, aux), "pfc_amplitude_lowpass norm");
+    return PFC_OK;
+}
+
 // ---- the reference's other propagators ------------------------------------------------------
 pfc_status pfc_init_eom_op(pfc_ctx* ctx, void* kop, double dt, double eps, double lx, double ly, double lz) {
     PFC_CHECK_CTX();

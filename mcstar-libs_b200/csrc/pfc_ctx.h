@@ -145,6 +145,17 @@ cudaError_t set_zfft_attributes(const pfc_ctx* c);
 // (lay as launch_ypass)
 cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay = 0);
 
+// ---- spectral low-pass post-processing (kern_lowpass.cu) ----
+cudaError_t launch_gaussian_init(const pfc_ctx* c, void* g, double lx, double ly, double lz, double hx, double hy,
+                                 double hz, double dps);
+// a_k *= Re g_k (imag 0) or Im g_k (imag 1)
+cudaError_t launch_kmult(const pfc_ctx* c, void* a, const void* g, int imag);
+// real field: psi <- (psi / N)^2 (norm 1) or psi^2 (norm 0)
+cudaError_t launch_norm_square(const pfc_ctx* c, void* a, int norm);
+// LOWPASS dump of a device spectrum: 0 ok, 1 CUDA error (cuda_err), 2 file not written
+int write_lowpass_file(const pfc_ctx* c, const void* spectrum, double lx, double ly, const char* path,
+                       cudaError_t* cuda_err);
+
 // ---- register-resident z pass (kern_zcol.cu) ----
 int fused_z_variant(int nx, int nz, int dtype);
 cudaError_t set_zcol_attributes(const pfc_ctx* c);

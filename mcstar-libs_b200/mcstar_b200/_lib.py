@@ -28,6 +28,8 @@ EXPORTED = (
     "pfc_ensemble_run", "pfc_ensemble_destroy", "pfc_ensemble_last_error", "pfc_adjoint_workspace_bytes",
     "pfc_sf_loss", "pfc_adjoint_step", "pfc_init_eom_op", "pfc_update_eom_exp", "pfc_update_eom_exp_with_fen",
     "pfc_update_el", "pfc_init_el_op", "pfc_update_el_exp", "pfc_update_eom_py", "pfc_update_eom_hpfcnoise",
+    "pfc_gaussian_init", "pfc_kmult_real", "pfc_kmult_imag", "pfc_square", "pfc_write_lowpass_2d",
+    "pfc_amplitude_lowpass",
 )
 
 
@@ -105,6 +107,12 @@ _SIGS = {
     "pfc_update_el_exp": ([_P, _P, _P, _P, ctypes.POINTER(_D)], _I),
     "pfc_update_eom_py": ([_P, _P, _P, _P, _D, _D, _D, _D, _D, _D], _I),
     "pfc_update_eom_hpfcnoise": ([_P, _P, _P, _P, _P, _P, _D, _D, _D, _D, _D, _D], _I),
+    "pfc_gaussian_init": ([_P, _P, _D, _D, _D, _D, _D, _D, _D], _I),
+    "pfc_kmult_real": ([_P, _P, _P], _I),
+    "pfc_kmult_imag": ([_P, _P, _P], _I),
+    "pfc_square": ([_P, _P], _I),
+    "pfc_write_lowpass_2d": ([_P, _P, _P, _D, _D, ctypes.c_char_p], _I),
+    "pfc_amplitude_lowpass": ([_P, _P, _P, _P, _D, _D, ctypes.c_char_p], _I),
 }
 
 

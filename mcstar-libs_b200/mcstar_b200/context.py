@@ -8,6 +8,7 @@ counts) come back as Python numbers.
 from __future__ import annotations
 
 import ctypes
+import os
 import threading
 
 import numpy as np
@@ -120,6 +121,32 @@ class Context:
         name = "pfc_update_eom_exp_with_fen" if with_fen else "pfc_update_eom_exp"
         self._call(name, _ptr(kop), _ptr(kpsi), _ptr(knl), _ptr(knoise), float(namp), float(eps),
                    *(float(v) for v in lens))
+
+    # ---- spectral low-pass post-processing (gaussian.hpp, lowpass.hpp) ----
+    def gaussian_init(self, kgauss, lens, hh, divs_per_sigma):
+        """kgauss_k = (e, 1 - e), e = exp(-1/2 sum_a (1.1 d h_a K_a)^2)."""
+        self._call("pfc_gaussian_init", _ptr(kgauss), *(float(v) for v in lens), *(float(v) for v in hh),
+                   float(divs_per_sigma))
+
+    def kmult_real(self, karr, kgauss):
+        self._call("pfc_kmult_real", _ptr(karr), _ptr(kgauss))
+
+    def kmult_imag(self, karr, kgauss):
+        self._call("pfc_kmult_imag", _ptr(karr), _ptr(kgauss))
+
+    def square(self, arr):
+        self._call("pfc_square", _ptr(arr))
+
+    def write_lowpass_2d(self, spectrum, kgauss, lens, path):
+        """spectrum *= Re kgauss, then the gzip LOWPASS dump of it to path (2D grids)."""
+        self._call("pfc_write_lowpass_2d", _ptr(spectrum), _ptr(kgauss), float(lens[0]), float(lens[1]),
+                   os.fsencode(path))
+
+    def amplitude_lowpass(self, spectrum, aux, kgauss, lens, path=None):
+        """Local amplitude of a 2D field into aux (calc_amplitude_lowpass); the LOWPASS dump
+        to path unless it is None."""
+        self._call("pfc_amplitude_lowpass", _ptr(spectrum), _ptr(aux), _ptr(kgauss), float(lens[0]),
+                   float(lens[1]), None if path is None else os.fsencode(path))
 
     def update_el(self, kpsi, knl, dt, eps, lens):
         """Non-conserved relaxation step; returns max_k |psi^'_k - psi^_k|."""

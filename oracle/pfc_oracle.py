@@ -34,6 +34,10 @@ What each function restates (reference paths relative to the mcstar-libs root):
                             reference is statistical, while parity between this oracle and
                             the CUDA kernels is value-for-value.
 
+* ``gaussian_init``, ``kmult``, ``amplitude_lowpass``, ``lowpass_text`` -- the 2D
+                            spectral low-pass (cuda/kernels/gaussian.hpp:23-67,
+                            cuda/kernels/lowpass.hpp:1-93) and its LOWPASS dump format
+
 Pinning: the FFT against numpy at the reference's own tolerances, the bond-order
 restatement against the compiled reference library (tests/golden, oracle/Makefile),
 and the step against the reference's cuFFT path on a GPU (oracle/_ref).
@@ -665,3 +669,60 @@ def parse_bond_table(text):
     rows = [ln.split() for ln in text.splitlines() if ln and not ln.startswith("#")]
     arr = np.array([[float(v) for v in r] for r in rows]) if rows else np.zeros((0, 13))
     return {c: arr[:, i] for i, c in enumerate(BOND_COLUMNS[:13])}
+
+
+# ----------------------------------------------------------------------------------
+# spectral low-pass post-processing of 2D fields (cuda/kernels/gaussian.hpp,
+# cuda/kernels/lowpass.hpp)
+# ----------------------------------------------------------------------------------
+def gaussian_init(shape_xyz, lens, hh, divs_per_sigma, dtype=np.float64):
+    """``kernel_gaussian_init`` (gaussian.hpp:23-33): g = e + i (1 - e) with
+    e = exp(-1/2 sum_a (1.1 d h_a K_a)^2), evaluated in ``dtype`` (the reference's Float)."""
+    nx, ny, nz = shape_xyz
+    f = dtype
+    s = [f(1.1) * f(divs_per_sigma) * f(h) for h in hh]
+    a = s[0] * wavenumbers(nx, lens[0], half=True, dtype=f)
+    b = s[1] * wavenumbers(ny, lens[1], dtype=f)
+    c = s[2] * wavenumbers(nz, lens[2], dtype=f)
+    q = (a[None, None, :] * a[None, None, :] + b[None, :, None] * b[None, :, None]) + c[:, None, None] * c[:, None, None]
+    e = np.exp(f(-0.5) * q.astype(f)).astype(f)
+    out = np.empty(e.shape, dtype=np.complex64 if f == np.float32 else np.complex128)
+    out.real, out.imag = e, f(1) - e
+    return out
+
+
+def kmult(karr, kgauss, imag=False):
+    """``kernel_kmult_real`` / ``_imag`` (gaussian.hpp:41-67; lowpass.hpp:1-35): the
+    complex field times the real or imaginary part of kgauss."""
+    return karr * (kgauss.imag if imag else kgauss.real)
+
+
+def amplitude_lowpass(kpsi, kgauss, shape_xyz):
+    """``calc_amplitude_lowpass`` (lowpass.hpp:78-93) in FP64: high-pass, C2R, normalise,
+    square, R2C, low-pass (the spectrum the LOWPASS dump writes), C2R, normalise.
+    Returns (amplitude field, numpy shape (ny, nx) for a 2D grid; low-passed spectrum)."""
+    rs = real_shape(shape_xyz)
+    n = rs[0] * rs[1] * rs[2]
+    k = np.asarray(kpsi, dtype=np.complex128) * np.asarray(kgauss.imag, dtype=np.float64)
+    a = c2r(k, shape_xyz) / n
+    low = r2c(a * a) * np.asarray(kgauss.real, dtype=np.float64)
+    return c2r(low, shape_xyz) / n, low
+
+
+def lowpass_text(spectrum, nx, ny, lx, ly, dtype=np.float32):
+    """The LOWPASS dump of ``write_lowpass_2d`` (lowpass.hpp:54-77) before compression:
+    "LOWPASS\\n<len>\\n", a protocol-0 pickle of {n0, n1, l0, l1} of that length, then
+    "i0 i1 re im\\n" for every mode with re^2 + im^2 > 1e-6 (evaluated in ``dtype``), i0 in
+    the outer loop, values in iostream's default format (%g, 6 significant digits)."""
+    f = dtype
+    pickle = "(S'n0'\nI%d\nS'n1'\nI%d\nS'l0'\nF%f\nS'l1'\nF%f\nd.\n" % (nx, ny, float(f(lx)), float(f(ly)))
+    out = ["LOWPASS\n%d\n" % len(pickle), pickle]
+    sp = np.asarray(spectrum).reshape(ny, nx // 2 + 1)
+    re = sp.real.astype(f)
+    im = sp.imag.astype(f)
+    m = (re * re + im * im).astype(f)
+    for i0 in range(nx // 2 + 1):
+        for i1 in range(ny):
+            if float(m[i1, i0]) > 1e-6:
+                out.append("%d %d %g %g\n" % (i0, i1, float(re[i1, i0]), float(im[i1, i0])))
+    return "".join(out).encode()

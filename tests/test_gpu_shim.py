@@ -162,3 +162,31 @@ def test_relaxation_driver_matches_oracle(flt, tmp_path, tmp_path_factory):
         k, _change = O.update_el(k, knl_of(k), dt, eps, lens, shape)
     got = np.load(os.path.join(tmp_path, "kpsi_el.npy")).reshape(O.cmpl_shape(shape))
     assert np.linalg.norm(got - k) / np.linalg.norm(k) < tol
+
+
+@pytest.mark.parametrize("flt", ["double", "float"])
+def test_lowpass_driver_matches_oracle(flt, tmp_path, tmp_path_factory):
+    """tests/shim/driver_lowpass.cu: R2C, the Gaussian filter (gaussian.hpp) and
+    calc_amplitude_lowpass (lowpass.hpp): the amplitude field and the LOWPASS dump."""
+    import gzip
+    dtype = np.float32 if flt == "float" else np.float64
+    drv = _driver(flt, tmp_path_factory, "driver_lowpass.cu")
+    nx, ny, dx, dps = 96, 64, 0.8, 2.0
+    shape = (nx, ny, 1)
+    x = np.arange(nx) * dx
+    psi = (0.3 * np.cos(2 * math.pi * 12 / (nx * dx) * x)[None, None, :] +
+           0.05 * np.random.default_rng(8).standard_normal((1, ny, nx))).astype(dtype)
+    inp = os.path.join(tmp_path, "in.npy")
+    np.save(inp, psi)
+    r = subprocess.run([drv, str(nx), str(ny), repr(dx), repr(dps), inp, str(tmp_path)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    lens, hh = (nx * dx, ny * dx, 1.0), (dx, dx, 1.0)
+    g = O.gaussian_init(shape, lens, hh, dps, dtype)
+    amp, low = O.amplitude_lowpass(O.r2c(psi.astype(np.float64)), g, shape)
+    got = np.load(os.path.join(tmp_path, "amplitude.npy")).reshape(amp.shape)
+    tol = 2e-5 if dtype == np.float32 else 1e-11
+    assert np.linalg.norm(got - amp) / np.linalg.norm(amp) < tol
+    text = gzip.decompress(open(os.path.join(tmp_path, "lowpass.gz"), "rb").read())
+    assert text.startswith(b"LOWPASS\n")
+    assert text.count(b"\n") > 4

@@ -30,7 +30,7 @@ def _lib_built():
 @pytest.mark.skipif(shutil.which("nvcc") is None and not os.path.exists("/usr/local/cuda/bin/nvcc"),
                     reason="nvcc not available")
 @pytest.mark.parametrize("flt", ["float", "double"])
-@pytest.mark.parametrize("driver", ["driver_step.cu", "driver_relax.cu"])
+@pytest.mark.parametrize("driver", ["driver_step.cu", "driver_relax.cu", "driver_lowpass.cu"])
 def test_reference_style_driver_compiles_and_links(flt, driver, tmp_path):
     if not _lib_built():
         pytest.skip("libpfc_b200.so not built")
