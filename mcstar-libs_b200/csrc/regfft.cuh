@@ -198,7 +198,7 @@ __device__ __forceinline__ void fft_d1_to_d2(float2 (&v)[E], int t, int g, float
     RF<E, DIR>::run(v);
 #pragma unroll
     for (int k1 = 1; k1 < E; ++k1) {
-        float2 w = twN[(t * k1) & (N - 1)];
+        float2 w = twN[t * k1];  // t k1 < N: no wrap, a running index
         if (DIR > 0) w.y = -w.y;
         v[k1] = cmul(v[k1], w);
     }
@@ -226,7 +226,7 @@ __device__ __forceinline__ void fft_d2_to_d1(float2 (&v)[E], int t, int g, float
         const int n1 = t * U + u;
 #pragma unroll
         for (int k2 = 1; k2 < P; ++k2) {
-            float2 w = twN[(n1 * k2) & (N - 1)];
+            float2 w = twN[n1 * k2];  // n1 k2 < E P = N
             if (DIR > 0) w.y = -w.y;
             v[u * P + k2] = cmul(v[u * P + k2], w);
         }
@@ -266,7 +266,7 @@ __device__ __forceinline__ void fft_d1_to_d3(float2 (&v)[E], int t, int g, float
     RF<E, DIR>::run(v);
 #pragma unroll
     for (int k1 = 1; k1 < E; ++k1) {
-        float2 w = twN[(t * k1) & (N - 1)];
+        float2 w = twN[t * k1];  // t k1 < N: no wrap, a running index
         if (DIR > 0) w.y = -w.y;
         v[k1] = cmul(v[k1], w);
     }
@@ -327,7 +327,7 @@ __device__ __forceinline__ void fft_d3_to_d1(float2 (&v)[E], int t, int g, float
     for (int k1 = 0; k1 < E; ++k1) v[k1] = xb[xslot3<N, E, NG>(k1, t, g)];
 #pragma unroll
     for (int k1 = 1; k1 < E; ++k1) {
-        float2 w = twN[(t * k1) & (N - 1)];
+        float2 w = twN[t * k1];  // t k1 < N: no wrap, a running index
         if (DIR > 0) w.y = -w.y;
         v[k1] = cmul(v[k1], w);
     }
