@@ -140,7 +140,7 @@ def kernel_table(prof, S, steps):
 
     if prof["xy_mode"] == 2 and prof["calls"][3]:
         # y-inverse A -> B, y-forward B -> B
-        add("k_ycol3" if prof.get("y_variant") in (6, 7) else "k_ycol", 3, 2.0 * S)
+        add("k_ycol3" if prof.get("y_variant") in (6, 7, 8) else "k_ycol", 3, 2.0 * S)
         add("k_xrow", 4, 2.0 * S)  # C2R, cubic term, R2C of every row, in place
     elif prof["xy_mode"] == 2:
         add("k_ycol+k_xrow+k_ycol (z slabs)", 1, 6.0 * S)

@@ -79,11 +79,13 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
 
 // y columns of N = 2 E^2 points with E values per thread and 2E threads per column
 // (fft_d1_to_d3): half the registers of YCfg's square split, so more resident warps.
-template <int NY_, int E_, int TX_, int MINB_>
+template <int NY_, int E_, int TX_, int MINB_, bool BAL_>
 struct YCfg3 {
     static constexpr int NY = NY_, E = E_, TX = TX_, P = 2 * E, T = TX * P, MINB = MINB_;
+    static constexpr bool BAL = BAL_;                  // the balanced radix-2 step of fft_d1_to_d3
+    static constexpr int TW = BAL ? 2 * NY : NY;       // its signed twiddle table, or W_NY^m alone
     static constexpr int XB = E * (P + 1) * TX;
-    static constexpr size_t SMEM = (size_t)(XB + NY) * sizeof(float2);
+    static constexpr size_t SMEM = (size_t)(XB + TW) * sizeof(float2);
     static_assert(P * E == NY && 32 % TX == 0, "shape");
 };
 
@@ -94,9 +96,13 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
     constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P;
     extern __shared__ __align__(16) float2 sm[];
     float2* xb = sm;
-    float2* tw = sm + Y::XB;
+    float2* tw = sm + Y::XB;  // W_NY^m, then -W_NY^m (fft_d1_to_d3)
     const int tid = threadIdx.x;
-    for (int i = tid; i < NY; i += Y::T) tw[i] = twg[i];
+    for (int i = tid; i < NY; i += Y::T) {
+        const float2 w = twg[i];
+        tw[i] = w;
+        if (Y::BAL) tw[NY + i] = make_float2(-w.x, -w.y);
+    }
     const int c = tid % TX, t = tid / TX;
     const int kx = blockIdx.x * TX + c;
     const bool valid = kx < nxh;
@@ -105,7 +111,7 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = valid ? in[ai.base + (int64_t)(t + P * j) * ai.stride] : make_float2(0.f, 0.f);
     __syncthreads();
-    fft_d1_to_d3<NY, E, TX, DIR>(v, t, c, xb, tw);
+    fft_d1_to_d3<NY, E, TX, DIR, BarCta, Y::BAL>(v, t, c, xb, tw);
     if (valid) {
         const ColAddr ao = col_addr(lay >> 2, false, kx, blockIdx.y, nxh, NY, nz);
         const int p = t >> 1, h = t & 1;
@@ -278,8 +284,9 @@ __global__ void __launch_bounds__(X::T, X::MINB)
 
 using Y512 = YCfg<512, 32, 8>;
 using Y512w = YCfg<512, 32, 16>;  // 128-byte column segments, 256 threads
-using Y512h = YCfg3<512, 16, 8, 3>;  // 16 values per thread, 256 threads per 8 columns
-using Y512q = YCfg3<512, 16, 8, 4>;  // the same capped at 64 registers (4 CTAs per SM)
+using Y512h = YCfg3<512, 16, 8, 3, false>;  // 16 values per thread, 256 threads per 8 columns
+using Y512q = YCfg3<512, 16, 8, 4, false>;  // the same capped at 64 registers (4 CTAs per SM)
+using Y512b = YCfg3<512, 16, 8, 4, true>;   // Y512q with the balanced radix-2 step
 
 template <class Y>
 cudaError_t y3attr() {
@@ -379,7 +386,7 @@ int fused_y_variant(int ny, int dtype) {
     switch (ny) {
         case 512: {
             const int v = env_choice("PFC_Y_VARIANT");
-            return (v == 1 || v == 5 || v == 6) ? v : 7;
+            return (v == 1 || v == 5 || v == 6 || v == 8) ? v : 7;
         }
         case 256: return 2;
         case 128: return 3;
@@ -408,6 +415,7 @@ cudaError_t set_pass_attributes(const pfc_ctx* c) {
         case 5: e = yattr<Y512w, false>(); break;
         case 6: e = y3attr<Y512h>(); break;
         case 7: e = y3attr<Y512q>(); break;
+        case 8: e = y3attr<Y512b>(); break;
     }
     if (e) return e;
     switch (c->fused_x) {
@@ -430,6 +438,7 @@ cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, d
         case 5: return ylaunch<Y512w>(c, dir, in, out, scale, nzs, lay);
         case 6: return y3launch<Y512h>(c, dir, in, out, scale, nzs, lay);
         case 7: return y3launch<Y512q>(c, dir, in, out, scale, nzs, lay);
+        case 8: return y3launch<Y512b>(c, dir, in, out, scale, nzs, lay);
     }
     return cudaErrorNotSupported;
 }

@@ -41,7 +41,8 @@ struct ZCfg {
     static constexpr int STG = NZ * TX;  // staging of one field tile, [z][c]
     // every kernel ends its shared memory with the twiddles W_NZ^m (NZ float2) and the
     // wavenumbers k_z of the NZ modes (NZ floats)
-    static constexpr int TAIL = NZ + NZ / 2 + 4;
+    static constexpr int TW = NZ;  // twiddles in the tail
+    static constexpr int TAIL = TW + NZ / 2 + 4;
     static constexpr size_t SMEM = (size_t)(2 * REG + TAIL) * sizeof(float2);
     static constexpr size_t SMEM_PIPE = (size_t)(2 * STG + 2 * REG + NHS + TAIL) * sizeof(float2);
     static constexpr size_t SMEM_CARRY = (size_t)(REG + STG + TAIL) * sizeof(float2);  // TH threads, one field
@@ -70,15 +71,18 @@ __device__ __forceinline__ float prop_inv(float d) { return __fdividef(1.0f, d);
 // so that modes 128 apart (the two threads of a D3 pair) read different banks.
 __device__ __forceinline__ int kz_slot(int kz) { return kz + (kz >> 7); }
 
-// Twiddles W_NZ^m and wavenumbers K(kz) = kz' 2 pi / L_z (common.hpp:27-28) of the
-// NZ modes into the shared tail of a z kernel (tw, then NZ + NZ / 128 floats).
+// Twiddles W_NZ^m (Z::TW = NZ of them, or 2 NZ: then -W_NZ^m follow, the signed table of
+// fft_d1_to_d3) and wavenumbers K(kz) = kz' 2 pi / L_z (common.hpp:27-28) of the NZ modes
+// into the shared tail of a z kernel (tw, then NZ + NZ / 128 floats).
 template <class Z>
 __device__ __forceinline__ float* load_tail(float2* tw, const float2* __restrict__ twg, const ZArgsF& a, int tid,
                                            int nthreads) {
     constexpr int NZ = Z::NZ;
-    float* kz_tab = reinterpret_cast<float*>(tw + NZ);
+    float* kz_tab = reinterpret_cast<float*>(tw + Z::TW);
     for (int i = tid; i < NZ; i += nthreads) {
-        tw[i] = twg[i];
+        const float2 w = twg[i];
+        tw[i] = w;
+        if (Z::TW == 2 * NZ) tw[NZ + i] = make_float2(-w.x, -w.y);
         kz_tab[kz_slot(i)] = (float)(i < NZ / 2 + 1 ? i : i - NZ) * a.ckz;
     }
     return kz_tab;
@@ -250,7 +254,8 @@ template <int NZ_, int E_, int TX_>
 struct Z3Cfg {
     static constexpr int NZ = NZ_, E = E_, TX = TX_, P = 2 * E, TH = TX * P, T = 2 * TH;
     static constexpr int REG = E * (P + 1) * TX;  // exchange buffer of one half
-    static constexpr int TAIL = NZ + NZ / 2 + 4;
+    static constexpr int TW = 2 * NZ;  // the signed twiddle table of fft_d1_to_d3
+    static constexpr int TAIL = TW + NZ / 2 + 4;
     static constexpr size_t SMEM = (size_t)(2 * REG + TAIL) * sizeof(float2);
     static constexpr size_t SMEM_CARRY = (size_t)(REG + NZ * TX + TAIL) * sizeof(float2);  // k_zcarry3
     static_assert(P * E == NZ && TH % 32 == 0 && REG >= NZ * TX, "shape");

@@ -246,11 +246,18 @@ __device__ __forceinline__ void fft_d2_to_d1(float2 (&v)[E], int t, int g, float
 // square four-step above, for N = 2 E^2: 512 = 16 x 32, 128 = 8 x 16).
 // Stage 1: E-point DFTs in registers, twiddles W_N^{t k1}, a transpose through shared
 // memory.  Stage 2: the 2E-point DFTs over t (one per k1) split across thread pairs
-// s = 2p + h (p = k1): thread h takes the E-point DFT of the t = 2m + h inputs, h = 1
-// scales by W_2E^{k2}, and the radix-2 combination exchanges half of the values with the
-// partner through one round of warp shuffles (the partner is NG lanes away).
+// s = 2p + h (p = k1): thread h takes the E-point DFT of the t = 2m + h inputs, and the
+// radix-2 combination with W_2E^{k2} exchanges half of the values with the partner through
+// one round of warp shuffles (the partner is NG lanes away).
 // D1: thread t holds x[t + P j].  D3: thread (p, h) holds X[p + E k2] with
 // k2 = h E/2 + i at register i and k2 = E + h E/2 + i at register E/2 + i (i < E/2).
+// Balance of the radix-2 step: the t = 2m + 1 values reach thread h = 1 multiplied by
+// (-1)^m, which rotates its E-point DFT by E/2 (F[(k + E/2) mod E] at register k, since
+// (-1)^m = W_E^{m E/2}).  Both threads of a pair then send register E/2 + i, and each
+// applies E/2 of the W_2E twiddles.  The inverse keeps thread h = 1's B values rotated the
+// same way, so its outputs carry (-1)^m, removed by their readers.  Each sign rides on the
+// stage-1 twiddles: twN holds W_N^m for m < N, then -W_N^m, and a thread of odd t with odd
+// t/2 takes its twiddles from the second half (k1 = 0 included: twN[N] = -1).
 // Exchange slots (k1, t, g) -> (k1 P + t) NG + k1 NG + g: the pad of NG per k1 row puts
 // the four (p, h) of a warp in alternate halves of the banks.  Buffer: E (P + 1) NG.
 template <int N, int E, int NG>
@@ -258,15 +265,27 @@ __device__ __forceinline__ int xslot3(int k1, int t, int g) {
     return (k1 * (2 * E) + t) * NG + k1 * NG + g;
 }
 
-template <int N, int E, int NG, int DIR, class Bar = BarCta>
+// the stage-1 twiddles of D1 thread t (signed as above)
+template <int N> __device__ __forceinline__ const float2* d3_tw1(const float2* twN, int t) {
+    return twN + ((t & 1) & ((t >> 1) & 1)) * N;
+}
+
+// kBal false: the same transform without the balance (twN of N entries; thread h = 1 applies
+// all E - 1 W_2E twiddles and the pair selects what it sends).
+template <int N, int E, int NG, int DIR, class Bar = BarCta, bool kBal = true>
 __device__ __forceinline__ void fft_d1_to_d3(float2 (&v)[E], int t, int g, float2* xb, const float2* twN,
                                              const Bar& bar = Bar{}) {
     constexpr int P = 2 * E, H = E / 2;
     static_assert(P * E == N && (E & (E - 1)) == 0 && NG <= 16 && 32 % NG == 0, "shape");
     RF<E, DIR>::run(v);
+    const float2* tw1 = kBal ? d3_tw1<N>(twN, t) : twN;
+    if (kBal) {
+        const float s0 = tw1[0].x;  // +-1
+        v[0] = make_float2(v[0].x * s0, v[0].y * s0);
+    }
 #pragma unroll
     for (int k1 = 1; k1 < E; ++k1) {
-        float2 w = twN[t * k1];  // t k1 < N: no wrap, a running index
+        float2 w = tw1[t * k1];  // t k1 < N: no wrap, a running index
         if (DIR > 0) w.y = -w.y;
         v[k1] = cmul(v[k1], w);
     }
@@ -277,24 +296,41 @@ __device__ __forceinline__ void fft_d1_to_d3(float2 (&v)[E], int t, int g, float
     const int p = t >> 1, h = t & 1;
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = xb[xslot3<N, E, NG>(p, 2 * m + h, g)];
-    RF<E, DIR>::run(v);
-    if (h) {
+    RF<E, DIR>::run(v);  // h = 0: F0[k] at k; h = 1: F1[(k + H) mod E] at k (kBal)
+    if constexpr (!kBal) {
+        if (h) {
 #pragma unroll
-        for (int k = 1; k < E; ++k) {
-            float2 w = twN[(k * E) & (N - 1)];  // W_2E^k = W_N^{k E}
-            if (DIR > 0) w.y = -w.y;
-            v[k] = cmul(v[k], w);
+            for (int k = 1; k < E; ++k) {
+                float2 w = twN[k * E];  // W_2E^k = W_N^{k E}
+                if (DIR > 0) w.y = -w.y;
+                v[k] = cmul(v[k], w);
+            }
         }
+#pragma unroll
+        for (int i = 0; i < H; ++i) {
+            const float2 send = h ? v[i] : v[H + i];
+            const float2 recv = make_float2(__shfl_xor_sync(0xffffffffu, send.x, NG),
+                                            __shfl_xor_sync(0xffffffffu, send.y, NG));
+            const float2 a = h ? recv : v[i];
+            const float2 b = h ? v[H + i] : recv;
+            v[i] = a + b;
+            v[H + i] = a - b;
+        }
+        return;
     }
+    const float2* tw2 = twN + h * H * E;  // W_2E^{h H + i} = tw2[i E]
 #pragma unroll
     for (int i = 0; i < H; ++i) {
-        const float2 send = h ? v[i] : v[H + i];
+        const float2 send = v[H + i];  // h = 0: F0[H + i]; h = 1: F1[i]
         const float2 recv = make_float2(__shfl_xor_sync(0xffffffffu, send.x, NG),
                                         __shfl_xor_sync(0xffffffffu, send.y, NG));
-        const float2 a = h ? recv : v[i];
-        const float2 b = h ? v[H + i] : recv;
-        v[i] = a + b;
-        v[H + i] = a - b;
+        const float2 u = h ? v[i] : recv;  // F1[h H + i]
+        const float2 o = h ? recv : v[i];  // F0[h H + i]
+        float2 w = tw2[i * E];
+        if (DIR > 0) w.y = -w.y;
+        const float2 gk = cmul(u, w);
+        v[i] = o + gk;      // X[h H + i]
+        v[H + i] = o - gk;  // X[E + h H + i]
     }
 }
 
@@ -305,29 +341,32 @@ __device__ __forceinline__ void fft_d3_to_d1(float2 (&v)[E], int t, int g, float
     static_assert(P * E == N && (E & (E - 1)) == 0 && NG <= 16 && 32 % NG == 0, "shape");
     const int p = t >> 1, h = t & 1;
     // radix-2 split of the 2E-point transforms: A_k = X_k + X_{k+E}, B_k = (X_k - X_{k+E}) W_2E^k
+    const float2* tw2 = twN + h * H * E;
 #pragma unroll
     for (int i = 0; i < H; ++i) {
-        const int k = h * H + i;
-        const float2 a = v[i] + v[H + i];
-        float2 w = twN[(k * E) & (N - 1)];
+        const float2 a = v[i] + v[H + i];  // A_{h H + i}
+        float2 w = tw2[i * E];
         if (DIR > 0) w.y = -w.y;
-        const float2 b = cmul(v[i] - v[H + i], w);
+        const float2 b = cmul(v[i] - v[H + i], w);  // B_{h H + i}
         const float2 send = h ? a : b;
         const float2 recv = make_float2(__shfl_xor_sync(0xffffffffu, send.x, NG),
                                         __shfl_xor_sync(0xffffffffu, send.y, NG));
-        v[i] = h ? recv : a;       // h = 0 collects A_0..A_{E-1}, h = 1 collects B_0..B_{E-1}
-        v[H + i] = h ? b : recv;
+        v[i] = h ? b : a;  // h = 0: A_i, A_{H+i}; h = 1: B_{H+i}, B_i (rotated)
+        v[H + i] = recv;
     }
-    RF<E, DIR>::run(v);  // outputs t = 2m + h
+    RF<E, DIR>::run(v);  // outputs t = 2m + h, times (-1)^m for h = 1
     bar.sync();
 #pragma unroll
     for (int m = 0; m < E; ++m) xb[xslot3<N, E, NG>(p, 2 * m + h, g)] = v[m];
     bar.sync();
 #pragma unroll
     for (int k1 = 0; k1 < E; ++k1) v[k1] = xb[xslot3<N, E, NG>(k1, t, g)];
+    const float2* tw1 = d3_tw1<N>(twN, t);
+    const float s0 = tw1[0].x;  // +-1
+    v[0] = make_float2(v[0].x * s0, v[0].y * s0);
 #pragma unroll
     for (int k1 = 1; k1 < E; ++k1) {
-        float2 w = twN[t * k1];  // t k1 < N: no wrap, a running index
+        float2 w = tw1[t * k1];  // t k1 < N: no wrap, a running index
         if (DIR > 0) w.y = -w.y;
         v[k1] = cmul(v[k1], w);
     }

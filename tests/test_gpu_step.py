@@ -79,7 +79,7 @@ print(json.dumps(out))
 @pytest.mark.parametrize("env", [{"PFC_Z_PIPE": "1"}, {"PFC_Z_CARRY": "1"}, {"PFC_PREFETCH": "1"},
                                  {"PFC_Z_CARRY": "1", "PFC_PREFETCH": "1"}, {"PFC_Z_VARIANT": "5"},
                                  {"PFC_Z_VARIANT": "1"}, {"PFC_TILED": "0"}, {"PFC_TILED": "0", "PFC_Z_VARIANT": "1"},
-                                 {"PFC_Y_VARIANT": "6"}, {"PFC_Y_VARIANT": "1"}, {"PFC_Y_VARIANT": "1", "PFC_TILED": "0"},
+                                 {"PFC_Y_VARIANT": "6"}, {"PFC_Y_VARIANT": "8"}, {"PFC_Y_VARIANT": "1"}, {"PFC_Y_VARIANT": "1", "PFC_TILED": "0"},
                                  {"PFC_XY_MODE": "1"}, {"PFC_XY_MODE": "0"},
                                  {"PFC_XY_MODE": "2", "PFC_SLAB": "3"}, {"PFC_X_VARIANT": "1", "PFC_Y_VARIANT": "5"}],
                          ids=lambda e: ",".join(f"{k}={v}" for k, v in e.items()))
