@@ -171,6 +171,40 @@ __device__ __forceinline__ void row_tiles(float2* rb, float2* g, int row0, int n
     }
 }
 
+// The R2C merge of the x pass fused into the store of the R rows from row0 to a row-tiled
+// field: rb holds y (the inverse transform's output, M per row); out[kx] =
+// r2c_post_f(y[kx], y[(M - kx) mod M], W_NX^kx) for kx < M and out[M] = (Re y0 - Im y0, 0),
+// in row_tiles's order (one shared-memory round trip fewer than merging in registers).
+template <class X>
+__device__ __forceinline__ void row_tiles_r2c(const float2* rb, const float2* twP, float2* g, int row0, int nrows,
+                                              int tid) {
+    constexpr int M = X::M, R = X::R, T = X::T, LDR = X::LDR, FT = M / kTileW;
+    constexpr int CH = R * kTileW;
+    static_assert(M % kTileW == 0 && kTileW == 8 && R % 16 == 0 && LDR % 2 == 1, "shape");
+    constexpr int NPOS = CH >= T ? CH / T : 1;
+    constexpr int TSTEP = CH >= T ? 1 : T / CH;
+    const int64_t ts = (int64_t)kTileW * nrows;
+    const int kt0 = CH >= T ? 0 : tid / CH;
+#pragma unroll
+    for (int m = 0; m < NPOS; ++m) {
+        const int pos = CH >= T ? tid + m * T : tid % CH;
+        const int c = pos % kTileW, q = pos / kTileW, p = q >> 1;
+        const int rr = (p & 7) + ((p >> 3) << 4) + ((q & 1) << 3);
+        float2* gp = g + kt0 * ts + (int64_t)(row0 + rr) * kTileW + c;
+        const float2* row = rb + rr * LDR;
+#pragma unroll
+        for (int k = 0; k < FT / TSTEP; ++k) {
+            const int kx = (kt0 + k * TSTEP) * kTileW + c;
+            *gp = r2c_post_f(row[kx], row[(M - kx) & (M - 1)], twP[kx]);
+            gp += TSTEP * ts;
+        }
+    }
+    if (tid < R) {
+        const float2 y0 = rb[tid * LDR];
+        g[FT * ts + row0 + tid] = make_float2(y0.x - y0.y, 0.f);
+    }
+}
+
 // MODE 0: the step's x pass, in place (in == out).  MODE 1: R2C of real rows (in: rows
 // of M float2 pairs x[2m] + i x[2m+1]) into half-spectrum rows (out: rows of NXH).
 // MODE 2: C2R of half-spectrum rows (in) into real rows (out, M pairs per row).  MODE 3:
@@ -261,6 +295,10 @@ __global__ void __launch_bounds__(X::T, X::MINB)
 #pragma unroll
     for (int j = 0; j < E; ++j) rb[r * LDR + t + P * j] = v[j];
     __syncthreads();
+    if constexpr (MODE == 3) {
+        row_tiles_r2c<X>(rb, twP, out, row0, nrows, tid);
+        return;
+    }
     float2 xm_last = make_float2(0.f, 0.f);
 #pragma unroll
     for (int j = 0; j < E; ++j) {
@@ -274,12 +312,8 @@ __global__ void __launch_bounds__(X::T, X::MINB)
     for (int j = 0; j < E; ++j) rb[r * LDR + t + P * j] = v[j];
     if (t == 0) rb[r * LDR + M] = xm_last;
     __syncthreads();
-    if constexpr (MODE == 3) {
-        row_tiles<X, true>(rb, out, row0, nrows, tid);
-    } else {
-        const int64_t o0 = (int64_t)row0 * NXH;
-        for (int i = tid; i < nr * NXH; i += X::T) out[o0 + i] = rb[i];
-    }
+    const int64_t o0 = (int64_t)row0 * NXH;
+    for (int i = tid; i < nr * NXH; i += X::T) out[o0 + i] = rb[i];
 }
 
 using Y512 = YCfg<512, 32, 8>;
