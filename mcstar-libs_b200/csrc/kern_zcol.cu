@@ -264,11 +264,12 @@ struct Z3Cfg {
 // propagate for distribution D3: register r of thread t = 2p + h holds mode
 // kz = p + h E^2/2 + d3_off(r).  kPsiInV: v holds psi^ and the tile N^, else the converse;
 // the tile ([row][TX], rows as d3_off's comment, column c) is also the noise pass's scratch
-// (the thread's own slots).  kSync: a barrier before that use.
+// (the thread's own slots).  kSync: a barrier before that use.  sc scales the result (a
+// power of two: exact), the 1/nz of a following inverse transform folded into 1/D(k).
 template <class Z, bool kPsiInV, bool kSync, class Bar>
 __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int c, const Bar& bar,
                                            const float* kz_tab, int kx, int ky, int t, int nx, int ny,
-                                           const ZArgsF& a, const double2* k0) {
+                                           const ZArgsF& a, const double2* k0, float sc) {
     constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, B = E * E / 2;
     static_assert(B == 128, "kz_slot pads one float per 128 modes");
     const int p = t >> 1, h = t & 1;
@@ -287,7 +288,7 @@ __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int 
         const float k2z = tab[d3_off<E>(r) + (r >= E / 2 ? 2 : 0)];
         const float dopx = -kxy - k2z * k2z;
         const float dopy = dopx * dopx;
-        const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
+        const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy)) * sc;
         const float f = a.dt * dopx;
         v[r] = make_float2((psi.x + f * n.x) * inv, (psi.y + f * n.y) * inv);
     }
@@ -303,7 +304,7 @@ __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int 
             const float k2z = tab[off + (r >= E / 2 ? 2 : 0)];
             const float dopx = -kxy - k2z * k2z;
             const float dopy = dopx * dopx;
-            const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
+            const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy)) * sc;
             const float2 xi = kspace_noise<float>(kx, ky, kz, nx, ny, NZ, a.seed, ctr);
             const float g = a.dt * a.namp_eff * sqrtf(-dopx) * inv;
             float2 w = trow[off * TX];
@@ -314,7 +315,7 @@ __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int 
 #pragma unroll
         for (int r = 0; r < E; ++r) v[r] = trow[d3_off<E>(r) * TX];
     }
-    if (kx == 0 && ky == 0 && t == 0) v[0] = make_float2((float)k0->x, (float)k0->y);  // kz = 0 at r = 0
+    if (kx == 0 && ky == 0 && t == 0) v[0] = make_float2((float)k0->x * sc, (float)k0->y * sc);  // kz = 0 at r = 0
 }
 
 // LAY: the layouts of A, B, O as k_zcol's lay, fixed at compile time (0, 1 or 7)
@@ -356,7 +357,8 @@ __global__ void __launch_bounds__(Z::T, 2) k_zcol3(const float2* A, const float2
     }
     __syncthreads();
     if (half != 0) return;
-    propagate3<Z, true, false>(v, regB, c, bar, kz_tab, kx, ky, t, nx, ny, a, k0);
+    propagate3<Z, true, false>(v, regB, c, bar, kz_tab, kx, ky, t, nx, ny, a, k0,
+                               a.final_step ? 1.0f : 1.0f / (float)NZ);
     if (!a.final_step) fft_d3_to_d1<NZ, E, TX, 1, BarDyn>(v, t, c, regA, tw, bar);
     watch<Z>(v, a.final_step, valid, flag);
     if (!valid) return;
@@ -364,10 +366,9 @@ __global__ void __launch_bounds__(Z::T, 2) k_zcol3(const float2* A, const float2
     if (a.final_step) {
 #pragma unroll
         for (int r = 0; r < E; ++r) O[co.base + (int64_t)(p + E * d3_k2<E>(r, h)) * co.stride] = v[r];
-    } else {
-        const float s = 1.0f / (float)NZ;
+    } else {  // A' = IFFT_z(psi^')/nz, the 1/nz applied in propagate3
 #pragma unroll
-        for (int j = 0; j < E; ++j) O[co.base + (int64_t)(t + P * j) * co.stride] = make_float2(v[j].x * s, v[j].y * s);
+        for (int j = 0; j < E; ++j) O[co.base + (int64_t)(t + P * j) * co.stride] = v[j];
     }
 }
 
@@ -476,7 +477,7 @@ __global__ void __launch_bounds__(Z::TH, 3) k_zcarry3(const float2* psi_in, cons
     fft_d1_to_d3<NZ, E, TX, -1>(v, t, c, xb, tw);
     cp_wait_all();
     __syncthreads();  // psi^ staged by the other threads of the column is visible
-    propagate3<Z, false, false>(v, stg, c, BarCta{}, kz_tab, kx, ky, t, nx, ny, a, k0);
+    propagate3<Z, false, false>(v, stg, c, BarCta{}, kz_tab, kx, ky, t, nx, ny, a, k0, 1.0f);
     const int p = t >> 1, h = t & 1;
     if (kLast) watch<Z>(v, true, valid, flag);
     if (valid) {
