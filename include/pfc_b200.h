@@ -3,7 +3,7 @@
  *
  * Every entry point replaces one host interface of mcstar-libs' header API (paths
  * relative to the mcstar-libs root are cited beside each declaration).  The
- * reference-name C++ headers shipped with this library (mcstar-libs_b200/shim/)
+ * reference-name C++ headers shipped with this library (include/mcstar/)
  * forward to these functions, so a driver written against mcstar-libs compiles
  * unchanged against this library; other languages bind the functions directly
  * (plain pointers, sizes and scalars; no C++ or torch types).
@@ -12,7 +12,8 @@
  *  - A context (pfc_ctx) is made for one grid shape (nx, ny, nz) and one precision.
  *    It owns every workspace (FFT twiddles and scratch, reduction and peak scratch,
  *    the FP64 k=0 slot of the fused stepper); no entry point allocates device
- *    memory after pfc_create.  Field buffers belong to the caller.
+ *    memory after pfc_create, except that pfc_bond_order and pfc_bond_reserve grow
+ *    the bond-order scratch.  Field buffers belong to the caller.
  *  - Layouts are the reference's (cuda/array_abstraction.hpp:37-70): x fastest,
  *    real field F[nz][ny][nx], half spectrum {F re, F im}[nz][ny][nx/2+1].  All
  *    field pointers are DEVICE pointers.  F = float (PFC_F32) or double (PFC_F64).
@@ -37,7 +38,7 @@ typedef enum pfc_status {
     PFC_ERR_INVALID = 1,      /* bad argument or shape                                */
     PFC_ERR_UNSUPPORTED = 2,  /* valid but not implemented (e.g. a prime FFT length)  */
     PFC_ERR_CUDA = 3,         /* a CUDA runtime error; see pfc_last_error            */
-    PFC_ERR_NOMEM = 4,        /* device allocation failed in pfc_create              */
+    PFC_ERR_NOMEM = 4,        /* a device allocation failed (pfc_create, bond order)  */
     PFC_ERR_CAPACITY = 5,     /* an output buffer was too small (count still set)    */
     PFC_ERR_NONFINITE = 6     /* the stepper's watchdog saw NaN/Inf in the state     */
 } pfc_status;
@@ -57,6 +58,40 @@ typedef struct pfc_ctx pfc_ctx;
  * drivers keep to 2, 3, 5 (cufft_unittest/main.cu:32-36, cuda/math.hpp:125-149). */
 pfc_status  pfc_create(const pfc_desc* desc, pfc_ctx** out);
 pfc_status  pfc_destroy(pfc_ctx* ctx);
+
+/* ---- kernel schedules and their autotuner (no counterpart in mcstar-libs, which leaves
+ * every choice to cuFFT's planner: cuda/cufft_wrapper.hpp:68-77; its only related code
+ * is the 2-3-5 size rounding of cuda/math.hpp:125-149).
+ * pfc_options selects, per context, among schedules that compute the same step:
+ *   z_carry      the state the stepper's z pass carries between steps: 0 A = IFFT_z(psi^)/nz
+ *                (three z transforms, three field sweeps), 1 psi^ itself (two transforms,
+ *                four sweeps); -1 the library's choice
+ *   x_pair       the register x pass: 0 one row per transform, 1 row pairs packed into one
+ *                complex transform (nx = 128, 512); -1 the library's choice
+ *   tiled        the register passes' field layout: 0 the reference layout, 1 kx tiles of
+ *                8 columns (contiguous z and y column blocks); -1 the library's choice
+ *   radix_order  the general (mixed-radix Stockham) passes: 0 radix 8 first, 1 radices 4
+ *                and 2 only, 2 the odd radices first
+ *   tile_shift   the general passes' lines per CTA halved this many times (0..4), for the
+ *                x rows, the y columns, the z columns and the stepper's z pass
+ * A choice the shape has no kernel for is PFC_ERR_UNSUPPORTED at creation.
+ * pfc_tune times the step (pfc_step, FP32 or FP64 per desc) under candidate options on
+ * the current device -- a coordinate search, one option at a time from the library's
+ * choice -- and returns the fastest in *best (and its time per step in *ms_per_step, may
+ * be NULL).  With a cache_path, results are kept in that JSON file keyed by shape,
+ * precision and device, and a cached entry is returned without timing.  Tuning creates
+ * and destroys contexts and allocates device memory (setup time, not the step). */
+typedef struct pfc_options {
+    int z_carry;
+    int x_pair;
+    int tiled;
+    int radix_order;
+    int tile_shift[4];
+} pfc_options;
+pfc_status  pfc_default_options(pfc_options* opts);
+pfc_status  pfc_create_with(const pfc_desc* desc, const pfc_options* opts, pfc_ctx** out);
+pfc_status  pfc_get_options(const pfc_ctx* ctx, pfc_options* opts);
+pfc_status  pfc_tune(const pfc_desc* desc, const char* cache_path, pfc_options* best, double* ms_per_step);
 pfc_status  pfc_set_stream(pfc_ctx* ctx, void* cuda_stream);
 const char* pfc_last_error(const pfc_ctx* ctx);
 const char* pfc_status_string(pfc_status s);
@@ -172,8 +207,11 @@ pfc_status pfc_findpeaks(pfc_ctx* ctx, const void* psi, double ths,
  * array of 4 MiB that every GPU loading the library holds until exit; grids of more
  * than 2^27 cells (512^3) are refused with PFC_ERR_CAPACITY and a message on stderr.
  * The first call on a device looks up the array's address (make that first call
- * before any stream capture).  All calls share the array: calls whose work overlaps
- * on the GPU race.  Output, ordering, counts and errors as pfc_findpeaks. */
+ * before any stream capture); after a cudaDeviceReset the next call looks it up
+ * again.  All calls share the array: calls whose work overlaps on the GPU race.  A
+ * CUDA error already pending when the call starts is returned as PFC_ERR_CUDA (with
+ * a message on stderr) and left pending.  Output, ordering, counts and errors
+ * otherwise as pfc_findpeaks. */
 pfc_status pfc_findpeaks_static(const void* psi, int nx, int ny, int nz, int dtype, double ths,
                                 void* out_maxima, int capacity, int* n_found, void* cuda_stream);
 
@@ -185,11 +223,18 @@ pfc_status pfc_findpeaks_static(const void* psi, int nx, int ny, int nz, int dty
  * out_rows (device), in input order, with the columns
  *   x y z nb xi q4 q6 q8 w4 q4b q6b q8b w4b w6
  * (the reference's table, bond-order.cpp:333-338, plus w6).  *n_rows receives the
- * row count; PFC_ERR_CAPACITY if it exceeds row_capacity. */
+ * row count; PFC_ERR_CAPACITY if it exceeds row_capacity.  Like the reference there is
+ * no limit on the atom count or on the neighbours of an atom: the context's bond-order
+ * scratch (about 700 bytes per atom plus 4 bytes per neighbour entry) grows inside this
+ * call when an input needs more -- the one entry point that may allocate device memory
+ * after pfc_create (PFC_ERR_NOMEM when that fails).  pfc_bond_reserve makes that
+ * allocation up front (for max_atoms input records and max_pairs neighbour entries in
+ * total); a context starts with room for 4096 atoms and 262144 entries. */
 #define PFC_BOND_NCOL 14
 pfc_status pfc_bond_order(pfc_ctx* ctx, const void* maxima, int n,
                           double h0, double h1, double h2, double ths, double boxsize, double rlim,
                           double* out_rows, int row_capacity, int* n_rows);
+pfc_status pfc_bond_reserve(pfc_ctx* ctx, int max_atoms, long long max_pairs);
 
 /* ---- fused stepper (no reference counterpart as one call: it is the driver loop of
  * copy, C2R, psi3_split(norm), R2C, [fill_kspace], update_eom that every mcstar-libs

@@ -12,27 +12,42 @@ using namespace pfc;
 
 namespace {
 
-bool factor_radices(int n, std::vector<int>& rs) {
+// The radices of an n-point Stockham plan, in stage order.  order 0: radix 8 first, then
+// 4, 2, 3, 5 and the other primes up to kMaxOddRadix; 1: radices 4 and 2 only for the
+// power of two; 2: the odd radices first, then 8, 4, 2.
+bool factor_radices(int n, std::vector<int>& rs, int order = 0) {
     rs.clear();
     if (n < 1) return false;
-    while (n % 8 == 0) { rs.push_back(8); n /= 8; }
-    while (n % 4 == 0) { rs.push_back(4); n /= 4; }
-    while (n % 2 == 0) { rs.push_back(2); n /= 2; }
-    while (n % 3 == 0) { rs.push_back(3); n /= 3; }
-    while (n % 5 == 0) { rs.push_back(5); n /= 5; }
+    std::vector<int> pow2, odd;
+    if (order == 1) {
+        while (n % 4 == 0) { pow2.push_back(4); n /= 4; }
+    } else {
+        while (n % 8 == 0) { pow2.push_back(8); n /= 8; }
+        while (n % 4 == 0) { pow2.push_back(4); n /= 4; }
+    }
+    while (n % 2 == 0) { pow2.push_back(2); n /= 2; }
+    while (n % 3 == 0) { odd.push_back(3); n /= 3; }
+    while (n % 5 == 0) { odd.push_back(5); n /= 5; }
     for (int p = 7; p <= kMaxOddRadix; p += 2) {
         bool prime = true;
         for (int d = 3; d * d <= p; d += 2) prime = prime && (p % d != 0);
         if (!prime) continue;
-        while (n % p == 0) { rs.push_back(p); n /= p; }
+        while (n % p == 0) { odd.push_back(p); n /= p; }
+    }
+    if (order == 2) {
+        rs = odd;
+        rs.insert(rs.end(), pow2.begin(), pow2.end());
+    } else {
+        rs = pow2;
+        rs.insert(rs.end(), odd.begin(), odd.end());
     }
     return n == 1 && (int)rs.size() <= kMaxStages;
 }
 
 // Appends the Stockham twiddles of an n-point plan to tab (forward sign, FP64).
-bool make_plan(int n, LinePlan& p, std::vector<std::complex<double>>& tab) {
+bool make_plan(int n, LinePlan& p, std::vector<std::complex<double>>& tab, int order) {
     std::vector<int> rs;
-    if (!factor_radices(n, rs)) return false;
+    if (!factor_radices(n, rs, order)) return false;
     std::memset(&p, 0, sizeof(p));
     p.n = n;
     p.nst = (int)rs.size();
@@ -58,6 +73,9 @@ bool make_plan(int n, LinePlan& p, std::vector<std::complex<double>>& tab) {
     }
     return true;
 }
+
+// The z pass carries psi^ itself unless the options say otherwise.
+constexpr bool kCarryPsiDefault = false;
 
 int pow2_floor(size_t v, int cap) {
     int t = 1;
@@ -88,7 +106,8 @@ pfc_status cuda_fail(pfc_ctx* c, cudaError_t e, const char* where) {
 void free_ctx(pfc_ctx* c) {
     if (!c) return;
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
-    void* ptrs[] = {c->tw, c->work, c->work2, c->red, c->k0, c->flag, c->peak_counts, c->peak_offsets, c->bond_scratch};
+    void* ptrs[] = {c->tw,          c->work,         c->work2,        c->red,       c->k0,
+                    c->flag,        c->peak_counts,  c->peak_offsets, c->bond_scratch, c->bond_pairs};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete c;
@@ -239,33 +258,11 @@ cudaError_t step_xy(pfc_ctx* ctx, void* kpsi, const pfc_step_params* p, bool las
             ctx, [&] { return launch_ypass(ctx, 1, A, B, 1.0, ctx->nz, kLayZ | kLayRow << 2); },
             [&] { return launch_xpass(ctx, B, nullptr, mul, p->C, p->mu, ctx->nz, kLayRow); },
             [&] { return launch_ypass(ctx, -1, B, kpsi, 1.0, ctx->nz, kLayRow | (last ? 0 : kLayZ << 2)); });
-    if (ctx->xy_mode == 1)
-        return traced(ctx, 1, 1, [&] { return launch_fused_xy(ctx, A, B, nullptr, mul, p->C, p->mu); });
-    if (ctx->xy_mode == 2) {
-        // y-inverse, x (C2R, cubic, R2C), y-forward; with slabs the intermediate of each
-        // slab of z-planes lives in one reused slab-sized buffer (L2-resident)
-        const int slab = (ctx->slab > 0 && ctx->slab < ctx->nz) ? ctx->slab : ctx->nz;
-        const int nslab = (ctx->nz + slab - 1) / slab;
-        const int64_t pe = (int64_t)ctx->ny * ctx->nxh;  // complex elements per plane
-        if (nslab == 1)
-            return traced_xy3(
-                ctx, [&] { return launch_ypass(ctx, 1, A, B, 1.0, ctx->nz); },
-                [&] { return launch_xpass(ctx, B, nullptr, mul, p->C, p->mu, ctx->nz); },
-                [&] { return launch_ypass(ctx, -1, B, B, 1.0, ctx->nz); });
-        return traced(ctx, 1, 3 * nslab, [&] {
-            cudaError_t e = cudaSuccess;
-            for (int z0 = 0; z0 < ctx->nz && !e; z0 += slab) {
-                const int nzs = std::min(slab, ctx->nz - z0);
-                const float2* a = (const float2*)A + z0 * pe;
-                float2* b = (float2*)B + z0 * pe;
-                float2* s = slab < ctx->nz ? (float2*)ctx->work2 : b;
-                if ((e = launch_ypass(ctx, 1, a, s, 1.0, nzs))) break;
-                if ((e = launch_xpass(ctx, s, nullptr, mul, p->C, p->mu, nzs))) break;
-                e = launch_ypass(ctx, -1, s, b, 1.0, nzs);
-            }
-            return e;
-        });
-    }
+    if (ctx->xy_mode == 2)
+        return traced_xy3(
+            ctx, [&] { return launch_ypass(ctx, 1, A, B, 1.0, ctx->nz); },
+            [&] { return launch_xpass(ctx, B, nullptr, mul, p->C, p->mu, ctx->nz); },
+            [&] { return launch_ypass(ctx, -1, B, B, 1.0, ctx->nz); });
     return traced(ctx, 1, ctx->ny > 1 ? 3 : 1, [&] {
         cudaError_t e;
         if (ctx->ny > 1) e = launch_cols(ctx, 1, 1, A, B, 1.0);
@@ -344,9 +341,35 @@ const char* pfc_status_string(pfc_status s) {
 
 const char* pfc_last_error(const pfc_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
-pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
+pfc_status pfc_default_options(pfc_options* o) {
+    if (!o) return PFC_ERR_INVALID;
+    o->z_carry = -1;
+    o->x_pair = -1;
+    o->tiled = -1;
+    o->radix_order = 0;
+    for (int i = 0; i < 4; ++i) o->tile_shift[i] = 0;
+    return PFC_OK;
+}
+
+pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) { return pfc_create_with(d, nullptr, out); }
+
+pfc_status pfc_get_options(const pfc_ctx* ctx, pfc_options* o) {
+    if (!ctx || !o) return PFC_ERR_INVALID;
+    *o = ctx->opt;
+    return PFC_OK;
+}
+
+pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx** out) {
     if (!d || !out) return PFC_ERR_INVALID;
     *out = nullptr;
+    pfc_options o;
+    pfc_default_options(&o);
+    if (opts) o = *opts;
+    if (o.z_carry < -1 || o.z_carry > 1 || o.x_pair < -1 || o.x_pair > 1 || o.tiled < -1 || o.tiled > 1 ||
+        o.radix_order < 0 || o.radix_order > 2)
+        return PFC_ERR_INVALID;
+    for (int i = 0; i < 4; ++i)
+        if (o.tile_shift[i] < 0 || o.tile_shift[i] > 4) return PFC_ERR_INVALID;
     if (d->nx < 1 || d->ny < 1 || d->nz < 1) return PFC_ERR_INVALID;
     // the reference plans a 1D transform of the first row for (nx, 1, nz > 1)
     // (technicalities.hpp:16-32 with cufft_wrapper.hpp:72-75); such shapes are refused.
@@ -367,7 +390,8 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
     std::vector<std::complex<double>> tab;
     const bool even = (c->nx % 2) == 0;
     const int lx = even ? c->nx / 2 : c->nx;
-    if (!make_plan(lx, c->px.plan, tab) || !make_plan(c->ny, c->py.plan, tab) || !make_plan(c->nz, c->pz.plan, tab)) {
+    if (!make_plan(lx, c->px.plan, tab, o.radix_order) || !make_plan(c->ny, c->py.plan, tab, o.radix_order) ||
+        !make_plan(c->nz, c->pz.plan, tab, o.radix_order)) {
         free_ctx(c);
         return PFC_ERR_UNSUPPORTED;
     }
@@ -375,17 +399,6 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
     for (int k = 0; k <= c->nx / 2; ++k) {
         const double ang = -2.0 * M_PI * (double)k / (double)c->nx;
         tab.emplace_back(std::cos(ang), std::sin(ang));
-    }
-    c->fused_xy = fused_xy_variant(c->nx, c->ny, c->dtype);
-    c->plane_tw_off = (int)tab.size();
-    if (c->fused_xy) {
-        const int lens[3] = {c->ny, c->nx / 2, c->nx};
-        const int cnt[3] = {c->ny, c->nx / 2, c->nx / 2 + 1};
-        for (int a = 0; a < 3; ++a)
-            for (int m = 0; m < cnt[a]; ++m) {
-                const double ang = -2.0 * M_PI * (double)m / (double)lens[a];
-                tab.emplace_back(std::cos(ang), std::sin(ang));
-            }
     }
     auto roots = [&](int n, int count) {
         for (int m = 0; m < count; ++m) {
@@ -406,38 +419,50 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
         roots(c->nx / 2, c->nx / 2);
         roots(c->nx, c->nx / 2 + 1);
     }
+    // the row-pair x pass where it exists, unless the options ask for single rows
+    c->xpair = c->fused_x ? xpair_variant(c->nx, c->dtype) : 0;
+    if (o.x_pair == 1 && !c->xpair) {
+        free_ctx(c);
+        return PFC_ERR_UNSUPPORTED;
+    }
+    if (o.x_pair == 0) c->xpair = 0;
+    c->xpair_tw_off = (int)tab.size();
+    if (c->xpair) roots(c->nx, c->nx);
     // (its line stride ny (nx/2+1) is a 32-bit int)
     c->fused_zfft = c->nz > 1 && c->n_cmpl < (1ull << 31) ? fused_zfft_variant(c->nz, c->dtype) : 0;
     c->zfft_tw_off = (int)tab.size();
     if (c->fused_zfft) roots(c->nz, c->nz);
-    // xy part of a step: register passes where available, else the cluster plane kernel,
-    // else the general passes; PFC_XY_MODE=0|1|2 overrides (for measurements).
-    c->xy_mode = c->fused_y ? 2 : (c->fused_xy ? 1 : 0);
-    if (const char* m = getenv("PFC_XY_MODE")) {
-        const int w = atoi(m);
-        if ((w == 1 && c->fused_xy) || (w == 2 && c->fused_y) || w == 0) c->xy_mode = w;
-    }
-    c->slab = 0;
-    if (const char* s = getenv("PFC_SLAB")) c->slab = std::max(0, atoi(s));
-    c->z_pipe = 0;
-    if (const char* s = getenv("PFC_Z_PIPE")) c->z_pipe = atoi(s) != 0;
+    // xy part of a step: the register y/x/y passes where the y and x lengths have them,
+    // else the general passes
+    c->xy_mode = c->fused_y ? 2 : 0;
     // the register z pass carries A = IFFT_z(psi^)/nz (three z transforms, three field
-    // sweeps; measured faster); PFC_Z_CARRY=1 carries psi^ itself (two transforms, four
-    // sweeps).  The slabbed xy passes and the pipelined z kernel need work2 / carry A.
-    bool carry = false;
-    if (const char* s = getenv("PFC_Z_CARRY")) carry = c->fused_z && atoi(s) != 0 && c->slab == 0 && !c->z_pipe;
+    // sweeps) or psi^ itself (two transforms, four sweeps)
+    if (o.z_carry == 1 && !c->fused_z) {
+        free_ctx(c);
+        return PFC_ERR_UNSUPPORTED;
+    }
+    const bool carry = c->fused_z && (o.z_carry == 1 || (o.z_carry == -1 && kCarryPsiDefault));
     // kx-tiled fields (measured faster: whole-block z and y columns); PFC_TILED=0 keeps the
     // standard layout.  Needs the register y, x, z passes, whole fields, and the register
     // column kernel for the entry / exit z transforms.
-    c->tiled = c->fused_z && c->fused_zfft && c->xy_mode == 2 && c->fused_y && c->slab == 0 && !c->z_pipe;
-    if (const char* s = getenv("PFC_TILED")) c->tiled = c->tiled && atoi(s) != 0;
+    c->tiled = c->fused_z && c->fused_zfft && c->xy_mode == 2 && c->fused_y;
+    if (o.tiled == 1 && !c->tiled) {
+        free_ctx(c);
+        return PFC_ERR_UNSUPPORTED;
+    }
+    if (o.tiled == 0) c->tiled = 0;
     // psi^ carried: tiled, with the 16-values-per-thread kernel (nz 512); standard layout,
-    // with the square split
+    // with the square split.  A tiled context whose z length has no tiled psi^-carrying
+    // kernel carries A unless the options ask for psi^ (then the layout is standard).
+    if (carry && c->tiled && c->fused_z != 6) {
+        if (o.z_carry == 1 && o.tiled == 1) {
+            free_ctx(c);
+            return PFC_ERR_UNSUPPORTED;
+        }
+        if (o.z_carry == 1) c->tiled = 0;
+    }
     c->z_carry = carry && (!c->tiled || c->fused_z == 6);
-    if (!c->tiled && (c->z_pipe || c->z_carry) && c->fused_z >= 5) c->fused_z = 1;
-    // L2 prefetch of the register passes, in waves of CTAs ahead (PFC_PREFETCH)
-    c->pf_waves = 0.f;
-    if (const char* s = getenv("PFC_PREFETCH")) c->pf_waves = std::max(0.f, (float)atof(s));
+    if (!c->tiled && c->z_carry && c->fused_z == 6) c->fused_z = 1;
     {
         int dev = 0;
         c->num_sms = 148;
@@ -445,14 +470,15 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
             cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
         cudaGetLastError();
     }
-    // tiles: two ping-pong buffers of `tile` lines per CTA
-    c->px.tile = pow2_floor((64 * 1024) / (2 * (size_t)lx * csz), 16);
+    // tiles: two ping-pong buffers of `tile` lines per CTA, halved tile_shift times
+    auto shifted = [](int t, int sh) { return std::max(1, t >> sh); };
+    c->px.tile = shifted(pow2_floor((64 * 1024) / (2 * (size_t)lx * csz), 16), o.tile_shift[0]);
     c->px.smem = 2 * (size_t)c->px.tile * lx * csz;
-    c->py.tile = pow2_floor((64 * 1024) / (2 * (size_t)c->ny * csz), 16);
+    c->py.tile = shifted(pow2_floor((64 * 1024) / (2 * (size_t)c->ny * csz), 16), o.tile_shift[1]);
     c->py.smem = 2 * (size_t)c->py.tile * c->ny * csz;
-    c->pz.tile = pow2_floor((64 * 1024) / (2 * (size_t)c->nz * csz), 16);
+    c->pz.tile = shifted(pow2_floor((64 * 1024) / (2 * (size_t)c->nz * csz), 16), o.tile_shift[2]);
     c->pz.smem = 2 * (size_t)c->pz.tile * c->nz * csz;
-    c->pzprop.tile = pow2_floor((96 * 1024) / (4 * (size_t)c->nz * csz), 8);
+    c->pzprop.tile = shifted(pow2_floor((96 * 1024) / (4 * (size_t)c->nz * csz), 8), o.tile_shift[3]);
     c->pzprop.smem = 4 * (size_t)c->pzprop.tile * c->nz * csz;
     if (c->px.smem > kMaxDynSmem || c->py.smem > kMaxDynSmem || c->pz.smem > kMaxDynSmem ||
         c->pzprop.smem > kMaxDynSmem) {
@@ -460,8 +486,11 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
         return PFC_ERR_UNSUPPORTED;
     }
     c->n_peak_blocks = (int)((c->n_real + kPeakBlock - 1) / kPeakBlock);
-    c->max_atoms = (int)std::max<size_t>(4096, c->n_real / 512);
+    // bond order starts with room for 4096 atoms and 64 neighbours each; pfc_bond_order
+    // grows both when a call needs more (pfc_bond_reserve does it up front)
+    c->max_atoms = 4096;
     c->bond_scratch_bytes = bond_scratch_bytes(c->max_atoms);
+    c->max_pairs = 64 * 4096;
 
     cudaError_t e = cudaSuccess;
     auto alloc = [&](void** p, size_t bytes) {
@@ -476,6 +505,7 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
     alloc((void**)&c->peak_counts, sizeof(int) * c->n_peak_blocks);
     alloc((void**)&c->peak_offsets, sizeof(int) * (c->n_peak_blocks + 1));
     alloc(&c->bond_scratch, c->bond_scratch_bytes);
+    alloc((void**)&c->bond_pairs, sizeof(int) * (size_t)c->max_pairs);
     if (e != cudaSuccess) {
         cudaGetLastError();
         free_ctx(c);
@@ -490,7 +520,6 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
     }
     if (e == cudaSuccess) e = cudaMemset(c->flag, 0, sizeof(int) * 4);
     if (e == cudaSuccess) e = set_fft_attributes(c);
-    if (e == cudaSuccess && c->fused_xy) e = set_fused_attributes(c);
     if (e == cudaSuccess && c->fused_z) e = set_zcol_attributes(c);
     if (e == cudaSuccess && c->fused_y) e = set_pass_attributes(c);
     if (e == cudaSuccess && c->fused_zfft) e = set_zfft_attributes(c);
@@ -498,6 +527,11 @@ pfc_status pfc_create(const pfc_desc* d, pfc_ctx** out) {
         free_ctx(c);
         return PFC_ERR_CUDA;
     }
+    // the options in effect (the library's choices filled in)
+    c->opt = o;
+    c->opt.z_carry = c->z_carry ? 1 : 0;
+    c->opt.x_pair = c->xpair ? 1 : 0;
+    c->opt.tiled = c->tiled ? 1 : 0;
     *out = c;
     return PFC_OK;
 }
@@ -518,8 +552,8 @@ size_t pfc_state_bytes(const pfc_ctx* ctx) { return ctx ? ctx->state_bytes : 0; 
 
 size_t pfc_workspace_bytes(const pfc_ctx* ctx) {
     if (!ctx) return 0;
-    return 2 * ctx->state_bytes + ctx->bond_scratch_bytes + sizeof(double) * (kRedBlocks + 8) +
-           sizeof(int) * (2 * ctx->n_peak_blocks + 1);
+    return 2 * ctx->state_bytes + ctx->bond_scratch_bytes + sizeof(int) * (size_t)ctx->max_pairs +
+           sizeof(double) * (kRedBlocks + 8) + sizeof(int) * (2 * ctx->n_peak_blocks + 1);
 }
 
 // ---- FFT ------------------------------------------------------------------------------
@@ -625,13 +659,29 @@ pfc_status pfc_bond_order(pfc_ctx* ctx, const void* maxima, int n, double h0, do
     if (!n_rows || n < 0 || (n > 0 && !maxima) || row_capacity < 0 || (row_capacity > 0 && !out_rows) ||
         !(boxsize > 0.0))
         return fail(ctx, PFC_ERR_INVALID, "pfc_bond_order: bad arguments");
-    if (n > ctx->max_atoms) return fail(ctx, PFC_ERR_CAPACITY, "pfc_bond_order: more atoms than the context holds");
-    int rows = 0, overflow = 0;
-    PFC_CUDA(launch_bond_order(ctx, maxima, n, h0, h1, h2, ths, boxsize, rlim, out_rows, row_capacity, &rows,
-                               &overflow), "pfc_bond_order");
+    int rows = 0;
+    cudaError_t e = launch_bond_order(ctx, maxima, n, h0, h1, h2, ths, boxsize, rlim, out_rows, row_capacity, &rows);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return fail(ctx, PFC_ERR_NOMEM, "pfc_bond_order: cannot grow the bond-order scratch");
+    }
+    PFC_CUDA(e, "pfc_bond_order");
     *n_rows = rows;
-    if (overflow) return fail(ctx, PFC_ERR_CAPACITY, "pfc_bond_order: an atom has more than 64 neighbours");
     if (rows > row_capacity) return fail(ctx, PFC_ERR_CAPACITY, "pfc_bond_order: more rows than capacity");
+    return PFC_OK;
+}
+
+pfc_status pfc_bond_reserve(pfc_ctx* ctx, int max_atoms, long long max_pairs) {
+    PFC_CHECK_CTX();
+    if (max_atoms < 0 || max_pairs < 0) return fail(ctx, PFC_ERR_INVALID, "pfc_bond_reserve: negative size");
+    if (max_pairs > INT32_MAX)
+        return fail(ctx, PFC_ERR_UNSUPPORTED, "pfc_bond_reserve: more than 2^31 - 1 neighbour entries");
+    cudaError_t e = bond_reserve(ctx, max_atoms, max_pairs);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return fail(ctx, PFC_ERR_NOMEM, "pfc_bond_reserve: out of device memory");
+    }
+    PFC_CUDA(e, "pfc_bond_reserve");
     return PFC_OK;
 }
 
@@ -990,7 +1040,7 @@ pfc_status pfc_profile_read(pfc_ctx* ctx, pfc_profile* out) {
     if (!out) return fail(ctx, PFC_ERR_INVALID, "pfc_profile_read: null output");
     PFC_CUDA(prof_resolve(ctx), "pfc_profile_read");
     out->launches = ctx->launches;
-    out->xy_variant = ctx->xy_mode == 1 ? ctx->fused_xy : 0;
+    out->xy_variant = 0;
     out->xy_mode = ctx->xy_mode;
     out->z_mode = ctx->z_carry ? (ctx->tiled ? 4 : 2) : (ctx->tiled ? 3 : (ctx->fused_z ? 1 : 0));
     out->z_variant = ctx->fused_z;

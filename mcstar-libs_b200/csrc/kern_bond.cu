@@ -11,6 +11,7 @@
 // powers of (dx + i dy)/rho; the reference's pole band (prefF, bond-order.cpp:123-133:
 // Y_lm = 0 for m > 0 when |1 - cos theta| < 1e-3 and for m < 0 when |1 + cos theta| <
 // 1e-3) is kept.  Wigner 3j symbols come from the Racah formula, evaluated on the host.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 #include "pfc_ctx.h"
@@ -31,9 +32,9 @@ struct BondScratch {
     double* pos;      // 3 * P
     int* keep_cnt;    // blocks
     int* keep_off;    // blocks + 1
-    int* nb;          // P
+    int* nb;          // P: neighbours of each atom
+    int* nb_off;      // P + 1: exclusive scan of nb, the start of each atom's list in the pair buffer
     int* maxj;        // P
-    int* nbr;         // P * kBondMaxNbr
     double2* q;       // P * kNQ
     int* row_cnt;     // blocks
     int* row_off;     // blocks + 1
@@ -41,13 +42,15 @@ struct BondScratch {
     int* cell_off;    // cells + 1
     int* cell_fill;   // cells
     int* cell_atoms;  // P
-    int* flags;       // [0] overflow of the neighbour cap, [1] position outside the box, [2] kept count
+    int* flags;       // [1] position outside the box, [2] kept count
 };
 constexpr int kMaxCellsDim = 64;
 constexpr int kBlk = 256;
 
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// The per-atom scratch of P atoms (the neighbour lists live in a separate pair buffer,
+// sized by the neighbour count the search finds).
 size_t scratch_layout(int P, BondScratch* s, char* base) {
     const size_t blocks = (size_t)(P + kBlk - 1) / kBlk + 1;
     const size_t cells = (size_t)kMaxCellsDim * kMaxCellsDim * kMaxCellsDim;
@@ -58,8 +61,8 @@ size_t scratch_layout(int P, BondScratch* s, char* base) {
     t.keep_cnt = (int*)take(sizeof(int) * blocks);
     t.keep_off = (int*)take(sizeof(int) * (blocks + 1));
     t.nb = (int*)take(sizeof(int) * P);
+    t.nb_off = (int*)take(sizeof(int) * ((size_t)P + 1));
     t.maxj = (int*)take(sizeof(int) * P);
-    t.nbr = (int*)take(sizeof(int) * (size_t)P * kBondMaxNbr);
     t.q = (double2*)take(sizeof(double2) * (size_t)P * kNQ);
     t.row_cnt = (int*)take(sizeof(int) * blocks);
     t.row_off = (int*)take(sizeof(int) * (blocks + 1));
@@ -162,36 +165,40 @@ __device__ __forceinline__ double get_diff(double x1, double x2, double w) {
     return fabs(d2) < fabs(d3) ? d2 : d3;
 }
 
+// kFill false: count the neighbours of atom i; true: also write them to list (whose
+// length the counting pass found).
+template <bool kFill>
 __device__ __forceinline__ void try_pair(const double* __restrict__ pos, int i, int j, double xi, double yi,
-                                         double zi, double box, double rlim, int* list, int& cnt, int& maxj,
-                                         int* flags) {
+                                         double zi, double box, double rlim, int* list, int& cnt, int& maxj) {
     if (j == i) return;
     const double dx = get_diff(pos[3 * j], xi, box);
     const double dy = get_diff(pos[3 * j + 1], yi, box);
     const double dz = get_diff(pos[3 * j + 2], zi, box);
     const double r = sqrt(dx * dx + dy * dy + dz * dz);
     if (r <= rlim) {
-        if (cnt < kBondMaxNbr) list[cnt] = j;
-        else atomicOr(&flags[0], 1);
+        if (kFill) list[cnt] = j;
         ++cnt;
         maxj = max(maxj, j);
     }
 }
 
-// one thread per atom; cells == 0 selects all-pairs (positions outside the box or a
-// box too small for three cells per side)
+// One thread per atom; nc == 0 selects all pairs (positions outside the box or a box too
+// small for three cells per side).  Counting pass (kFill false): nbc, maxjs.  Filling
+// pass: the list of atom i at nbr + nb_off[i], sorted by index (the reference sums over
+// neighbours in index order, bond-order.cpp:289-349).
+template <bool kFill>
 __global__ void k_neighbours(const double* __restrict__ pos, const int* __restrict__ np, double box, double rlim,
                              int nc, const int* __restrict__ cell_off, const int* __restrict__ cell_atoms,
-                             int* __restrict__ nbr, int* __restrict__ nbc, int* __restrict__ maxjs,
-                             int* __restrict__ flags) {
+                             const int* __restrict__ nb_off, int* __restrict__ nbr, int* __restrict__ nbc,
+                             int* __restrict__ maxjs) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int P = *np;
     if (i >= P) return;
     const double xi = pos[3 * i], yi = pos[3 * i + 1], zi = pos[3 * i + 2];
-    int* list = nbr + (size_t)i * kBondMaxNbr;
+    int* list = kFill ? nbr + nb_off[i] : nullptr;
     int cnt = 0, maxj = -1;
     if (nc == 0) {
-        for (int j = 0; j < P; ++j) try_pair(pos, i, j, xi, yi, zi, box, rlim, list, cnt, maxj, flags);
+        for (int j = 0; j < P; ++j) try_pair<kFill>(pos, i, j, xi, yi, zi, box, rlim, list, cnt, maxj);
     } else {
         const int cx = cell_of(xi, box, nc), cy = cell_of(yi, box, nc), cz = cell_of(zi, box, nc);
         for (int dz = -1; dz <= 1; ++dz)
@@ -199,18 +206,20 @@ __global__ void k_neighbours(const double* __restrict__ pos, const int* __restri
                 for (int dx = -1; dx <= 1; ++dx) {
                     const int c = (((cz + dz + nc) % nc) * nc + (cy + dy + nc) % nc) * nc + (cx + dx + nc) % nc;
                     for (int k = cell_off[c]; k < cell_off[c + 1]; ++k)
-                        try_pair(pos, i, cell_atoms[k], xi, yi, zi, box, rlim, list, cnt, maxj, flags);
+                        try_pair<kFill>(pos, i, cell_atoms[k], xi, yi, zi, box, rlim, list, cnt, maxj);
                 }
     }
-    const int m = min(cnt, kBondMaxNbr);
-    for (int a = 1; a < m; ++a) {  // insertion sort: the reference sums in index order
+    if (!kFill) {
+        nbc[i] = cnt;
+        maxjs[i] = maxj;
+        return;
+    }
+    for (int a = 1; a < cnt; ++a) {  // insertion sort into index order
         const int v = list[a];
         int b = a - 1;
         while (b >= 0 && list[b] > v) { list[b + 1] = list[b]; --b; }
         list[b + 1] = v;
     }
-    nbc[i] = cnt;
-    maxjs[i] = maxj;
 }
 
 // q_lm for one (atom, l): thread t handles atom t/3, l = 4, 6, 8
@@ -270,13 +279,14 @@ __device__ void qlm_atom(const double* __restrict__ pos, int i, const int* __res
 }
 
 __global__ void k_qlm(const double* __restrict__ pos, const int* __restrict__ np, const int* __restrict__ nbr,
-                      const int* __restrict__ nbc, double box, double2* __restrict__ q) {
+                      const int* __restrict__ nb_off, const int* __restrict__ nbc, double box,
+                      double2* __restrict__ q) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = t / 3, which = t - 3 * (t / 3);
     if (i >= *np) return;
-    const int cnt = min(nbc[i], kBondMaxNbr);
+    const int cnt = nbc[i];
     if (cnt == 0) return;
-    const int* list = nbr + (size_t)i * kBondMaxNbr;
+    const int* list = nbr + nb_off[i];
     double2* qi = q + (size_t)i * kNQ;
     if (which == 0) qlm_atom<4>(pos, i, list, cnt, box, qi, 0);
     else if (which == 1) qlm_atom<6>(pos, i, list, cnt, box, qi + 9, 1);
@@ -315,7 +325,8 @@ constexpr double kPi = 3.14159265358979323846;
 
 // per-atom invariants; rows of PFC_BOND_NCOL doubles for atoms with neighbours
 __global__ void __launch_bounds__(kBlk) k_bond_rows(const double* __restrict__ pos, const int* __restrict__ np,
-                                                    const int* __restrict__ nbr, const int* __restrict__ nbc,
+                                                    const int* __restrict__ nbr, const int* __restrict__ nb_off,
+                                                    const int* __restrict__ nbc,
                                                     const int* __restrict__ maxjs, const double2* __restrict__ q,
                                                     const int* __restrict__ row_off, double* __restrict__ rows,
                                                     int row_capacity, int count_only, int* __restrict__ row_cnt) {
@@ -332,8 +343,8 @@ __global__ void __launch_bounds__(kBlk) k_bond_rows(const double* __restrict__ p
     if (!has) return;
     const int row = row_off[blockIdx.x] + rank;
     if (row >= row_capacity) return;
-    const int cnt = min(nbc[i], kBondMaxNbr);
-    const int* list = nbr + (size_t)i * kBondMaxNbr;
+    const int cnt = nbc[i];
+    const int* list = nbr + nb_off[i];
     const double2* qi = q + (size_t)i * kNQ;
     double out[PFC_BOND_NCOL];
     out[0] = pos[3 * i]; out[1] = pos[3 * i + 1]; out[2] = pos[3 * i + 2];
@@ -436,11 +447,35 @@ cudaError_t upload_tables() {
 
 size_t bond_scratch_bytes(int max_atoms) { return scratch_layout(max_atoms, nullptr, nullptr); }
 
+// Grows the context's bond-order scratch to hold `atoms` atoms and `pairs` neighbour
+// entries (allocation sizes only grow; nothing is kept across calls, so no copy).
+cudaError_t bond_reserve(pfc_ctx* c, int atoms, int64_t pairs) {
+    cudaError_t e = cudaSuccess;
+    if (atoms > c->max_atoms) {
+        const int want = std::max(atoms, c->max_atoms + c->max_atoms / 2);
+        void* p = nullptr;
+        if ((e = cudaMalloc(&p, bond_scratch_bytes(want)))) return e;
+        if (c->bond_scratch) cudaFree(c->bond_scratch);
+        c->bond_scratch = p;
+        c->max_atoms = want;
+        c->bond_scratch_bytes = bond_scratch_bytes(want);
+    }
+    if (pairs > c->max_pairs) {
+        const int64_t want = std::max<int64_t>(pairs, c->max_pairs + c->max_pairs / 2);
+        void* p = nullptr;
+        if ((e = cudaMalloc(&p, sizeof(int) * (size_t)want))) return e;
+        if (c->bond_pairs) cudaFree(c->bond_pairs);
+        c->bond_pairs = (int*)p;
+        c->max_pairs = want;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t launch_bond_order(pfc_ctx* c, const void* maxima, int n, double h0, double h1, double h2, double ths,
-                              double boxsize, double rlim, double* out_rows, int row_capacity, int* n_rows_host,
-                              int* overflow_host) {
+                              double boxsize, double rlim, double* out_rows, int row_capacity, int* n_rows_host) {
     cudaError_t e = upload_tables();
     if (e) return e;
+    if ((e = bond_reserve(c, n, 0))) return e;
     BondScratch s;
     scratch_layout(c->max_atoms, &s, (char*)c->bond_scratch);
     cudaStream_t st = c->stream;
@@ -464,7 +499,7 @@ cudaError_t launch_bond_order(pfc_ctx* c, const void* maxima, int n, double h0, 
     if ((e = cudaStreamSynchronize(st))) return e;
     const int P = hflags[2];
     const int* np = s.flags + 2;
-    if (P == 0) { *n_rows_host = 0; *overflow_host = 0; return cudaSuccess; }
+    if (P == 0) { *n_rows_host = 0; return cudaSuccess; }
     // 2. cells of side >= rlim (all pairs when fewer than 3 per side or atoms outside the box)
     int nc = (int)std::floor(boxsize / rlim);
     if (nc > kMaxCellsDim) nc = kMaxCellsDim;
@@ -478,21 +513,29 @@ cudaError_t launch_bond_order(pfc_ctx* c, const void* maxima, int n, double h0, 
         k_scan_b<<<1, 1024, 0, st>>>(s.cell_cnt, cells, s.cell_off);
         k_cell_fill<<<pb, 256, 0, st>>>(s.pos, np, boxsize, nc, s.cell_off, s.cell_fill, s.cell_atoms);
     }
-    k_neighbours<<<pb, 256, 0, st>>>(s.pos, np, boxsize, rlim, nc, s.cell_off, s.cell_atoms, s.nbr, s.nb, s.maxj,
-                                     s.flags);
-    k_qlm<<<(3 * P + 127) / 128, 128, 0, st>>>(s.pos, np, s.nbr, s.nb, boxsize, s.q);
+    // 3. neighbour lists: count, scan into list offsets, grow the pair buffer, fill
+    k_neighbours<false><<<pb, 256, 0, st>>>(s.pos, np, boxsize, rlim, nc, s.cell_off, s.cell_atoms, nullptr, nullptr,
+                                            s.nb, s.maxj);
+    k_scan_b<<<1, 1024, 0, st>>>(s.nb, P, s.nb_off);
+    if ((e = cudaGetLastError())) return e;
+    int pairs = 0;
+    if ((e = cudaMemcpyAsync(&pairs, s.nb_off + P, sizeof(int), cudaMemcpyDeviceToHost, st))) return e;
+    if ((e = cudaStreamSynchronize(st))) return e;
+    if ((e = bond_reserve(c, 0, pairs))) return e;
+    k_neighbours<true><<<pb, 256, 0, st>>>(s.pos, np, boxsize, rlim, nc, s.cell_off, s.cell_atoms, s.nb_off,
+                                           c->bond_pairs, nullptr, nullptr);
+    k_qlm<<<(3 * P + 127) / 128, 128, 0, st>>>(s.pos, np, c->bond_pairs, s.nb_off, s.nb, boxsize, s.q);
     const int rb = (P + kBlk - 1) / kBlk;
-    k_bond_rows<<<rb, kBlk, 0, st>>>(s.pos, np, s.nbr, s.nb, s.maxj, s.q, nullptr, nullptr, 0, 1, s.row_cnt);
-    k_scan_b<<<1, 1024, 0, st>>>(s.row_cnt, rb, s.row_off);
-    k_bond_rows<<<rb, kBlk, 0, st>>>(s.pos, np, s.nbr, s.nb, s.maxj, s.q, s.row_off, out_rows, row_capacity, 0,
+    k_bond_rows<<<rb, kBlk, 0, st>>>(s.pos, np, c->bond_pairs, s.nb_off, s.nb, s.maxj, s.q, nullptr, nullptr, 0, 1,
                                      s.row_cnt);
+    k_scan_b<<<1, 1024, 0, st>>>(s.row_cnt, rb, s.row_off);
+    k_bond_rows<<<rb, kBlk, 0, st>>>(s.pos, np, c->bond_pairs, s.nb_off, s.nb, s.maxj, s.q, s.row_off, out_rows,
+                                     row_capacity, 0, s.row_cnt);
     if ((e = cudaGetLastError())) return e;
     int rows = 0;
     if ((e = cudaMemcpyAsync(&rows, s.row_off + rb, sizeof(int), cudaMemcpyDeviceToHost, st))) return e;
-    if ((e = cudaMemcpyAsync(hflags, s.flags, sizeof(int), cudaMemcpyDeviceToHost, st))) return e;
     if ((e = cudaStreamSynchronize(st))) return e;
     *n_rows_host = rows;
-    *overflow_host = hflags[0];
     return cudaSuccess;
 }
 

@@ -10,7 +10,6 @@
 // A y pass, the x pass and a y pass replace the general y/x/y passes of the step;
 // they stream whole tiles (contiguous rows for x, 64-byte column segments for y)
 // and keep every FFT in registers with one shared-memory transpose per transform.
-#include <cstdlib>
 #include "pfc_ctx.h"
 #include "regfft.cuh"
 
@@ -33,12 +32,11 @@ struct YCfg {
 template <class Y, int DIR, bool kZ>
 __global__ void __launch_bounds__(Y::T, Y::MINB)
     k_ycol(const float2* in, float2* out, int nxh, int ny, int nz, int lay, const float2* __restrict__ twg,
-           float scale, int pf) {
+           float scale) {
     // the columns of NY elements of kx tile blockIdx.x at plane blockIdx.y: y columns of
     // z-plane blockIdx.y (kZ false) or z columns at ky = blockIdx.y (kZ); lay & 3: the
     // layout of the input, lay >> 2: of the output (col_addr).  With the standard layout on
-    // both sides, in may equal out.  pf (standard input only): L2 prefetch distance in
-    // tiles.
+    // both sides, in may equal out.
     constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P, U = Y::U;
     extern __shared__ __align__(16) float2 sm[];
     float2* xb = sm;
@@ -52,17 +50,6 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
     float2 v[E];
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = valid ? in[ai.base + (int64_t)(t + P * j) * ai.stride] : make_float2(0.f, 0.f);
-    if (pf) {
-        // L2 prefetch of the tile pf tiles ahead in launch order: its segment of every line
-        const int ntx = (int)gridDim.x;
-        const int tgt = (int)(blockIdx.y * gridDim.x + blockIdx.x) + pf;
-        if (tgt < ntx * (int)gridDim.y) {
-            const int kx0 = (tgt % ntx) * TX;
-            const ColAddr ap = col_addr(0, kZ, kx0, tgt / ntx, nxh, ny, nz);
-            const unsigned bytes = (unsigned)(min(TX, nxh - kx0) * sizeof(float2));
-            for (int y = tid; y < NY; y += Y::T) l2_prefetch(in + ap.base + (int64_t)y * ap.stride, bytes);
-        }
-    }
     __syncthreads();
     fft_d1_to_d2<NY, E, TX, DIR, BarCta, Y::PADG>(v, t, c, xb, tw);
     if (valid) {
@@ -215,7 +202,7 @@ __device__ __forceinline__ void row_tiles_r2c(const float2* rb, const float2* tw
 template <class X, int MODE>
 __global__ void __launch_bounds__(X::T, X::MINB)
     k_xrow(const float2* in, float2* out, const float* __restrict__ pot, int nrows, const float2* __restrict__ twg,
-           float mul, float Cc, float mu, int pf) {
+           float mul, float Cc, float mu) {
     constexpr int NX = X::NX, M = X::M, NXH = X::NXH, E = X::E, P = X::P, U = X::U, R = X::R, LDR = X::LDR;
     constexpr int LIN = MODE == 1 ? M : NXH;  // input row length (float2)
     extern __shared__ __align__(16) float2 sm[];
@@ -234,17 +221,6 @@ __global__ void __launch_bounds__(X::T, X::MINB)
         for (int i = tid; i < nr * LIN; i += X::T) rb[i] = in[g0 + i];
     } else {
         for (int i = tid; i < nr * LIN; i += X::T) rb[(i / LIN) * LDR + i % LIN] = in[g0 + i];
-    }
-    if (pf) {
-        // L2 prefetch of the rows of the CTA pf CTAs ahead, in 4 KB pieces
-        const int row1 = (blockIdx.x + pf) * R;
-        if (row1 < nrows) {
-            const int64_t e0 = (int64_t)row1 * LIN;
-            const int64_t n = (int64_t)min(R, nrows - row1) * LIN;
-            constexpr int kPiece = 512;  // float2
-            for (int64_t i = (int64_t)tid * kPiece; i < n; i += (int64_t)X::T * kPiece)
-                l2_prefetch(in + e0 + i, (unsigned)(min((int64_t)kPiece, n - i) * sizeof(float2)));
-        }
     }
     __syncthreads();
     float2 v[E];
@@ -316,11 +292,118 @@ __global__ void __launch_bounds__(X::T, X::MINB)
     for (int i = tid; i < nr * NXH; i += X::T) out[o0 + i] = rb[i];
 }
 
-using Y512 = YCfg<512, 32, 8>;
-using Y512w = YCfg<512, 32, 16>;  // 128-byte column segments, 256 threads
-using Y512h = YCfg3<512, 16, 8, 3, false>;  // 16 values per thread, 256 threads per 8 columns
-using Y512q = YCfg3<512, 16, 8, 4, false>;  // the same capped at 64 registers (4 CTAs per SM)
-using Y512b = YCfg3<512, 16, 8, 4, true>;   // Y512q with the balanced radix-2 step
+// The x pass on row pairs (row-tiled layout, nx = 2 E^2 real points, e.g. 512 = 2 16^2):
+// the two half-spectrum rows a, b of a pair make one full complex spectrum
+// Z[k] = X_a[k] + i X_b[k] (X[nx - k] = conj X[k] for real rows), whose inverse FFT is
+// x_a + i x_b; the cubic term of psi3_split.hpp:8-13 acts on real and imaginary parts;
+// the forward FFT Z' of n_a + i n_b gives N_a[k] = (Z'[k] + conj Z'[nx - k]) / 2 and
+// N_b[k] = (Z'[k] - conj Z'[nx - k]) / (2 i).  One nx-point complex FFT per pair and
+// direction (fft_d1_to_d3 / fft_d3_to_d1: E values per thread, 2E threads per pair), no
+// split or merge twiddles.  A CTA of 8 pairs (16 consecutive rows) holds its rows in
+// shared memory interleaved by pair, [pair][kx][row of the pair], so that one 16-byte
+// load gives both rows' mode kx.  Global traffic: the 16 rows of a tile are one
+// contiguous 1 KB block of the row-tiled field; a warp moves 4 rows x 8 columns (256
+// contiguous bytes) per access.
+template <int NX_, int E_>
+struct XPCfg {
+    static constexpr int NX = NX_, E = E_, P = 2 * E, NG = 8, T = P * NG, R = 2 * NG;
+    static constexpr int NXH = NX / 2 + 1;
+    static constexpr int LDP = NXH;          // kx stride of a pair in the row stage (float4 units)
+    static constexpr int LDZ = NX + 2;       // pair stride of the Z' stage (float2 units)
+    static constexpr int XB = E * P * NG;    // exchange buffer (unpadded)
+    static constexpr int BUF = cmaxi(cmaxi(NG * LDP * 2, XB), NG * LDZ);
+    static constexpr int TW = 2 * NX;        // signed twiddles of fft_d1_to_d3
+    static constexpr size_t SMEM = (size_t)(BUF + TW) * sizeof(float2);
+    static_assert(P * E == NX && NX % (2 * kTileW) == 0, "shape");
+};
+
+template <class X>
+__global__ void __launch_bounds__(X::T, 4) k_xpair(float2* g, int nrows, const float2* __restrict__ twg, float mul,
+                                                   float Cc, float mu) {
+    constexpr int NX = X::NX, E = X::E, P = X::P, NG = X::NG, T = X::T, R = X::R, NXH = X::NXH;
+    constexpr int FT = (NX / 2) / kTileW;  // whole tiles; the last tile holds kx = NX/2 alone
+    extern __shared__ __align__(16) float2 sm[];
+    float2* buf = sm;
+    float2* tw = sm + X::BUF;
+    float4* rows4 = reinterpret_cast<float4*>(buf);  // [pair][kx]: {row a, row b}
+    const int tid = threadIdx.x;
+    for (int i = tid; i < NX; i += T) {
+        const float2 w = twg[i];
+        tw[i] = w;
+        tw[NX + i] = make_float2(-w.x, -w.y);
+    }
+    const int row0 = blockIdx.x * R;
+    const int64_t ts = (int64_t)kTileW * nrows;  // elements between tiles
+    const int lane = tid & 31, warp = tid >> 5, riw = lane >> 3, c = lane & 7;
+    // load: unit u = (tile, group of 4 rows); a warp takes one unit per iteration
+#pragma unroll 4
+    for (int u = warp; u < FT * (R / 4); u += T / 32) {
+        const int kt = u / (R / 4), rg = u % (R / 4);
+        const int r = rg * 4 + riw;
+        const float2 x = g[kt * ts + (int64_t)(row0 + r) * kTileW + c];
+        buf[((r >> 1) * X::LDP + kt * kTileW + c) * 2 + (r & 1)] = x;
+    }
+    if (tid < R) buf[((tid >> 1) * X::LDP + NX / 2) * 2 + (tid & 1)] = g[FT * ts + row0 + tid];
+    __syncthreads();
+    // the pair's full spectrum Z in distribution D1 (thread t holds Z[t + P j])
+    const int pg = tid % NG, t = tid / NG;
+    float2 v[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+        const int k = t + P * j;
+        const bool lo = k <= NX / 2;
+        float4 ab = rows4[pg * X::LDP + (lo ? k : NX - k)];
+        if (k == 0 || k == NX / 2) ab.y = ab.w = 0.f;  // real modes of real rows (as a C2R takes them)
+        v[j] = lo ? make_float2(ab.x - ab.w, ab.y + ab.z) : make_float2(ab.x + ab.w, ab.z - ab.y);
+    }
+    // (fft_d1_to_d3 synchronises before it first writes the buffer)
+    fft_d1_to_d3<NX, E, NG, 1, BarCta, true, 0>(v, t, pg, buf, tw);
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const float a = v[r].x * mul, b = v[r].y * mul;
+        v[r] = make_float2(a * a * a - Cc * a - mu, b * b * b - Cc * b - mu);
+    }
+    fft_d3_to_d1<NX, E, NG, -1, BarCta, 0>(v, t, pg, buf, tw);
+    __syncthreads();  // the last exchange reads are done
+#pragma unroll
+    for (int j = 0; j < E; ++j) buf[pg * X::LDZ + t + P * j] = v[j];
+    __syncthreads();
+    // store: lanes (pair of the warp's two, 16 consecutive kx); each writes both rows
+    const int hp = lane >> 4, kk = lane & 15;
+#pragma unroll 2
+    for (int u = warp; u < (NG / 2) * (FT / 2); u += T / 32) {
+        const int pp = 2 * (u % (NG / 2)) + hp, k = (u / (NG / 2)) * 16 + kk;
+        const float2 z = buf[pp * X::LDZ + k], zm = buf[pp * X::LDZ + ((NX - k) & (NX - 1))];
+        const float2 na = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+        const float2 nb = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+        float2* gp = g + (k / kTileW) * ts + (int64_t)(row0 + 2 * pp) * kTileW + (k % kTileW);
+        gp[0] = na;
+        gp[kTileW] = nb;
+    }
+    if (tid < NG) {  // kx = NX/2 of both rows
+        const float2 z = buf[tid * X::LDZ + NX / 2];
+        g[FT * ts + row0 + 2 * tid] = make_float2(z.x, 0.f);
+        g[FT * ts + row0 + 2 * tid + 1] = make_float2(z.y, 0.f);
+    }
+}
+
+using XP512 = XPCfg<512, 16>;
+using XP128 = XPCfg<128, 8>;
+
+template <class X>
+cudaError_t xpattr() {
+    return cudaFuncSetAttribute(k_xpair<X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)X::SMEM);
+}
+template <class X>
+cudaError_t xplaunch(const pfc_ctx* c, void* b, double mul, double C, double mu, int nrows) {
+    if (nrows % X::R) return cudaErrorNotSupported;
+    const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->xpair_tw_off;
+    k_xpair<X><<<nrows / X::R, X::T, X::SMEM, c->stream>>>((float2*)b, nrows, tw, (float)mul, (float)C, (float)mu);
+    return cudaGetLastError();
+}
+
+using Y512 = YCfg<512, 32, 8>;              // z columns of the plain transforms (nz = 512)
+using Y512q = YCfg3<512, 16, 8, 4, false>;  // the y pass: 16 values per thread, 64 registers
 
 template <class Y>
 cudaError_t y3attr() {
@@ -343,7 +426,6 @@ cudaError_t y3launch(const pfc_ctx* c, int dir, const void* in, void* out, doubl
 using Y256 = YCfg<256, 16, 8>;
 using Y128 = YCfg<128, 16, 8>;
 using Y64 = YCfg<64, 8, 8>;
-using X512 = XCfg<512, 32, 256>;
 using X512h = XCfg<512, 16, 256>;  // 16 rows per CTA, 16 values per thread: three CTAs per SM
 using X256 = XCfg<256, 16, 256>;
 using X128 = XCfg<128, 16, 128>;
@@ -373,14 +455,12 @@ cudaError_t collaunch(const pfc_ctx* c, int dir, const void* in, void* out, doub
                       int tw_off) {
     dim3 grid((c->nxh + Y::TX - 1) / Y::TX, planes);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + tw_off;
-    static const int per_sm = resident_ctas(k_ycol<Y, 1, kZ>, Y::T, Y::SMEM);
-    const int pf = (lay & 3) ? 0 : prefetch_ahead(c, per_sm, in);
     if (dir > 0)
         k_ycol<Y, 1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->ny, c->nz,
-                                                             lay, tw, (float)scale, pf);
+                                                             lay, tw, (float)scale);
     else
         k_ycol<Y, -1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->ny, c->nz,
-                                                              lay, tw, (float)scale, pf);
+                                                              lay, tw, (float)scale);
     return cudaGetLastError();
 }
 template <class Y>
@@ -396,32 +476,21 @@ cudaError_t xlaunch(const pfc_ctx* c, const void* in, void* out, const void* pot
                     int nrows) {
     dim3 grid((nrows + X::R - 1) / X::R);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->xpass_tw_off;
-    static const int per_sm = resident_ctas(k_xrow<X, MODE>, X::T, X::SMEM);
     if (MODE == 3 && nrows % X::R) return cudaErrorNotSupported;  // whole tiles of rows
     k_xrow<X, MODE><<<grid, X::T, X::SMEM, c->stream>>>((const float2*)in, (float2*)out, (const float*)pot, nrows, tw,
-                                                        (float)mul, (float)C, (float)mu,
-                                                        MODE == 3 ? 0 : prefetch_ahead(c, per_sm, in));
+                                                        (float)mul, (float)C, (float)mu);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-// 512-point variants, measured against each other: the x pass defaults to 16 values per
-// thread (three CTAs per SM; PFC_X_VARIANT=1 selects 32), the y pass to 16 values per
-// thread capped at 64 registers (k_ycol3, 32 warps per SM; PFC_Y_VARIANT=1 selects
-// k_ycol's 32 values per thread, 5 its 128-byte segments, 6 k_ycol3 uncapped).
-static int env_choice(const char* name) {
-    const char* s = getenv(name);
-    return s ? atoi(s) : 0;
-}
-
+// Register y and x passes by length (0: none, the general passes run).  512 points: the y
+// pass with 16 values per thread over 32 threads per column, capped at 64 registers
+// (k_ycol3); the x pass with 16 values per thread, three CTAs per SM.
 int fused_y_variant(int ny, int dtype) {
     if (dtype != PFC_F32) return 0;
     switch (ny) {
-        case 512: {
-            const int v = env_choice("PFC_Y_VARIANT");
-            return (v == 1 || v == 5 || v == 6 || v == 8) ? v : 7;
-        }
+        case 512: return 7;
         case 256: return 2;
         case 128: return 3;
         case 64: return 4;
@@ -431,7 +500,7 @@ int fused_y_variant(int ny, int dtype) {
 int fused_x_variant(int nx, int dtype) {
     if (dtype != PFC_F32) return 0;
     switch (nx) {
-        case 512: return env_choice("PFC_X_VARIANT") == 1 ? 1 : 5;
+        case 512: return 5;
         case 256: return 2;
         case 128: return 3;
         case 64: return 4;
@@ -442,37 +511,29 @@ int fused_x_variant(int nx, int dtype) {
 cudaError_t set_pass_attributes(const pfc_ctx* c) {
     cudaError_t e = cudaSuccess;
     switch (c->fused_y) {
-        case 1: e = yattr<Y512, false>(); break;
         case 2: e = yattr<Y256, false>(); break;
         case 3: e = yattr<Y128, false>(); break;
         case 4: e = yattr<Y64, false>(); break;
-        case 5: e = yattr<Y512w, false>(); break;
-        case 6: e = y3attr<Y512h>(); break;
         case 7: e = y3attr<Y512q>(); break;
-        case 8: e = y3attr<Y512b>(); break;
     }
     if (e) return e;
     switch (c->fused_x) {
-        case 1: e = xattr<X512>(); break;
         case 2: e = xattr<X256>(); break;
         case 3: e = xattr<X128>(); break;
         case 4: e = xattr<X64>(); break;
         case 5: e = xattr<X512h>(); break;
     }
+    if (!e && c->xpair) e = c->nx == 512 ? xpattr<XP512>() : xpattr<XP128>();
     return e;
 }
 
 cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs, int lay) {
     if (lay && nzs != c->nz) return cudaErrorNotSupported;  // tiled: whole fields
     switch (c->fused_y) {
-        case 1: return ylaunch<Y512>(c, dir, in, out, scale, nzs, lay);
         case 2: return ylaunch<Y256>(c, dir, in, out, scale, nzs, lay);
         case 3: return ylaunch<Y128>(c, dir, in, out, scale, nzs, lay);
         case 4: return ylaunch<Y64>(c, dir, in, out, scale, nzs, lay);
-        case 5: return ylaunch<Y512w>(c, dir, in, out, scale, nzs, lay);
-        case 6: return y3launch<Y512h>(c, dir, in, out, scale, nzs, lay);
         case 7: return y3launch<Y512q>(c, dir, in, out, scale, nzs, lay);
-        case 8: return y3launch<Y512b>(c, dir, in, out, scale, nzs, lay);
     }
     return cudaErrorNotSupported;
 }
@@ -481,7 +542,6 @@ template <int MODE>
 cudaError_t xdispatch(const pfc_ctx* c, const void* in, void* out, const void* pot, double mul, double C, double mu,
                       int nrows) {
     switch (c->fused_x) {
-        case 1: return xlaunch<X512, MODE>(c, in, out, pot, mul, C, mu, nrows);
         case 2: return xlaunch<X256, MODE>(c, in, out, pot, mul, C, mu, nrows);
         case 3: return xlaunch<X128, MODE>(c, in, out, pot, mul, C, mu, nrows);
         case 4: return xlaunch<X64, MODE>(c, in, out, pot, mul, C, mu, nrows);
@@ -492,7 +552,14 @@ cudaError_t xdispatch(const pfc_ctx* c, const void* in, void* out, const void* p
 
 cudaError_t launch_xpass(const pfc_ctx* c, void* b, const void* pot, double mul, double C, double mu, int nzs,
                          int lay) {
-    if (lay == 2) return nzs == c->nz ? xdispatch<3>(c, b, b, pot, mul, C, mu, nzs * c->ny) : cudaErrorNotSupported;
+    if (lay == 2 && nzs != c->nz) return cudaErrorNotSupported;
+    if (lay == 2 && !pot && c->xpair) {
+        switch (c->nx) {
+            case 512: return xplaunch<XP512>(c, b, mul, C, mu, nzs * c->ny);
+            case 128: return xplaunch<XP128>(c, b, mul, C, mu, nzs * c->ny);
+        }
+    }
+    if (lay == 2) return xdispatch<3>(c, b, b, pot, mul, C, mu, nzs * c->ny);
     if (lay != 0) return cudaErrorNotSupported;
     return xdispatch<0>(c, b, b, pot, mul, C, mu, nzs * c->ny);
 }
@@ -522,6 +589,9 @@ cudaError_t set_zfft_attributes(const pfc_ctx* c) {
     }
     return cudaSuccess;
 }
+// the packed row-pair x pass exists for nx = 2 E^2 (128 and 512)
+int xpair_variant(int nx, int dtype) { return dtype == PFC_F32 && (nx == 512 || nx == 128) ? 1 : 0; }
+
 cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay) {
     switch (c->fused_zfft) {
         case 1: return zlaunch_fft<Y512>(c, dir, in, out, scale, lay);

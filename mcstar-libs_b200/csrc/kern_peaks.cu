@@ -4,6 +4,7 @@
 // kPeakBlock consecutive cells (__syncthreads_count), one block scans the counts,
 // pass 2 writes each peak at block offset + warp-ballot rank.  Blocks cover linear
 // index ranges in order, so the output is sorted by linear index.
+#include <cuda.h>
 #include <cstdio>
 #include <mutex>
 #include "pfc_ctx.h"
@@ -136,16 +137,39 @@ cudaError_t launch_findpeaks(const pfc_ctx* c, const void* psi, double ths, void
 // at most kStaticPeakCells cells (512^3); every GPU that loads the library holds it
 // (4 MiB) until the process exits.  Host code must not pass the array's name to a
 // kernel: on the host it is only a stand-in for the symbol.  The device address is
-// looked up once per device, by the first call on that device, with that device
-// current (cudaGetSymbolAddress) and cached.
+// looked up by the first call on a device, with that device current
+// (cudaGetSymbolAddress), and cached per device and primary context: a call after
+// cudaDeviceReset (a new context, in which the module and its array are loaded afresh)
+// looks it up again.
 // ---------------------------------------------------------------------------------------
 namespace {
 constexpr int64_t kStaticPeakCells = (int64_t)1 << 27;
 constexpr int kStaticPeakBlocks = (int)(kStaticPeakCells / pfc::kPeakBlock);
 static __device__ __align__(256) int g_peak_scratch[2 * kStaticPeakBlocks + 1];
 constexpr int kMaxDevices = 64;
-int* g_peak_scratch_dev[kMaxDevices];
+struct StaticScratch {
+    CUcontext ctx;  // the context the address belongs to
+    int* ptr;
+};
+StaticScratch g_peak_scratch_dev[kMaxDevices];
 std::mutex g_peak_scratch_mutex;
+
+// The current context of the calling thread, through the driver entry point that the
+// runtime hands out (no link-time dependency on the driver library).
+CUcontext current_context() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    static GetCurrent fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return (GetCurrent)p;
+    }();
+    CUcontext c = nullptr;
+    if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+    return c;
+}
 }  // namespace
 
 extern "C" pfc_status pfc_findpeaks_static(const void* psi, int nx, int ny, int nz, int dtype, double ths,
@@ -159,17 +183,32 @@ extern "C" pfc_status pfc_findpeaks_static(const void* psi, int nx, int ny, int 
                 (long long)cells, (long long)kStaticPeakCells);
         return PFC_ERR_CAPACITY;
     }
+    // an error left pending by earlier work of the caller is reported as such, not
+    // taken for (and cleared as) a failure of this call's launches
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        fprintf(stderr, "pfc_findpeaks_static: a CUDA error was pending before the call: %s\n",
+                cudaGetErrorString(pending));
+        return PFC_ERR_CUDA;
+    }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PFC_ERR_CUDA;
     int* scratch;
     {
         std::lock_guard<std::mutex> lock(g_peak_scratch_mutex);
-        if (!g_peak_scratch_dev[dev]) {
+        // cudaFree(0) makes the device's primary context current (the runtime API's
+        // initialisation of the device); the driver's current context then names it
+        if (cudaFree(0) != cudaSuccess) return PFC_ERR_CUDA;
+        const CUcontext cur = current_context();
+        if (!cur) return PFC_ERR_CUDA;
+        StaticScratch& slot = g_peak_scratch_dev[dev];
+        if (!slot.ptr || slot.ctx != cur) {
             void* p = nullptr;
             if (cudaGetSymbolAddress(&p, g_peak_scratch) != cudaSuccess || !p) return PFC_ERR_CUDA;
-            g_peak_scratch_dev[dev] = (int*)p;
+            slot.ptr = (int*)p;
+            slot.ctx = cur;
         }
-        scratch = g_peak_scratch_dev[dev];
+        scratch = slot.ptr;
     }
     // counts and offsets are rewritten in full by every call: nothing needs clearing
     int* counts = scratch;

@@ -8,11 +8,7 @@
 //
 //  k_zcol   one tile per CTA; both halves load and transform concurrently, N^ is
 //           handed over through shared memory, then the A half finishes alone.
-//  k_zpipe  persistent, one CTA per SM: each half prefetches its next tile with
-//           cp.async into a shared staging buffer while it computes the current one,
-//           and the B half's forward FFT of tile i+1 overlaps the A half's update and
-//           inverse FFT of tile i.  The hand-over of N^ is a producer/consumer pair of
-//           named barriers (3: N^ written, 4: slots free again).
+#include "bulk.cuh"
 #include "pfc_ctx.h"
 #include "regfft.cuh"
 
@@ -35,23 +31,17 @@ struct ZCfg {
     static constexpr int MINB = T <= 256 ? 2 : 1;  // k_zcol CTAs per SM its register cap allows
     static constexpr int PADG = TX / U;  // exchange padding: the 32/TX t-groups of a warp hit distinct banks
     static constexpr int REG = E * (P * TX + PADG);
-    // N^ slots of the pipelined kernel, skewed by 8 per U modes so that a warp's four
-    // t-groups (kz = t U + ...) fall in different banks
-    static constexpr int NHS = NZ * TX + (NZ / U) * 8;
     static constexpr int STG = NZ * TX;  // staging of one field tile, [z][c]
     // every kernel ends its shared memory with the twiddles W_NZ^m (NZ float2) and the
     // wavenumbers k_z of the NZ modes (NZ floats)
     static constexpr int TW = NZ;  // twiddles in the tail
     static constexpr int TAIL = TW + NZ / 2 + 4;
     static constexpr size_t SMEM = (size_t)(2 * REG + TAIL) * sizeof(float2);
-    static constexpr size_t SMEM_PIPE = (size_t)(2 * STG + 2 * REG + NHS + TAIL) * sizeof(float2);
     static constexpr size_t SMEM_CARRY = (size_t)(REG + STG + TAIL) * sizeof(float2);  // TH threads, one field
     // resident CTAs of k_zcarry the shared memory allows (228 KB per SM): its register cap
     static constexpr int CMINB = 4 * (SMEM_CARRY + 1024) <= 228 * 1024 ? 4 : 3;
     static_assert(TH % 32 == 0 && U * P == E && TX % U == 0 && 32 % TX == 0, "shape");
 };
-
-template <class Z> __device__ __forceinline__ int nh_slot(int kz, int c) { return kz * Z::TX + c + (kz / Z::U) * 8; }
 
 // Row of mode kz in a [row][c] tile of modes (TX = 8 float2 per row: the N^ hand-over
 // and the psi^ staging).  A warp touches the modes kz = t U + u + E k2 of four
@@ -181,31 +171,12 @@ __device__ __forceinline__ void store_state(float2 (&v)[Z::E], float2* A, int64_
     }
 }
 
-// L2 prefetch of the tile `ahead` tiles after this CTA's in launch order (grid x: kx
-// tiles of TX columns, grid y: ky): the column segment of every z row of the fields
-// f0 and f1, spread over the CTA's threads.
-template <int NZ, int TX>
-__device__ __forceinline__ void prefetch_ztile(const float2* f0, const float2* f1, int ahead, int nxh, int64_t zs,
-                                               int tid, int nthreads) {
-    const int ntx = (int)gridDim.x;
-    const int tgt = (int)(blockIdx.y * gridDim.x + blockIdx.x) + ahead;
-    if (tgt >= ntx * (int)gridDim.y) return;
-    const int kx0 = (tgt % ntx) * TX;
-    const int64_t off = (int64_t)(tgt / ntx) * nxh + kx0;
-    const unsigned bytes = (unsigned)(min(TX, nxh - kx0) * sizeof(float2));
-    for (int i = tid; i < 2 * NZ; i += nthreads) {
-        const int z = i < NZ ? i : i - NZ;
-        l2_prefetch((i < NZ ? f0 : f1) + off + (int64_t)z * zs, bytes);
-    }
-}
-
 // lay bits 0, 1, 2: A, B, O kx-tiled (col_addr); O may be A when their layouts agree.
-// pf: L2 prefetch distance in tiles (standard layouts only).
 template <class Z>
 __global__ void __launch_bounds__(Z::T, Z::MINB) k_zcol(const float2* A, const float2* __restrict__ B, float2* O,
                                                    int nx, int ny, int lay, ZArgsF a,
                                                    const double2* __restrict__ k0, int* flag,
-                                                   const float2* __restrict__ twg, int pf) {
+                                                   const float2* __restrict__ twg) {
     constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, U = Z::U, TH = Z::TH;
     extern __shared__ __align__(16) float2 sm[];
     float2* regA = sm;
@@ -225,7 +196,6 @@ __global__ void __launch_bounds__(Z::T, Z::MINB) k_zcol(const float2* A, const f
     float2 v[E];
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = valid ? src[ca.base + (int64_t)(t + P * j) * ca.stride] : make_float2(0.f, 0.f);
-    if (pf) prefetch_ztile<NZ, TX>(A, B, pf, nxh, (int64_t)ny * nxh, tid, Z::T);
     __syncthreads();
     // both halves run one copy of the forward transform, each on its own named barrier
     const BarDyn bar{1 + half, TH};
@@ -266,7 +236,13 @@ struct Z3Cfg {
 // the tile ([row][TX], rows as d3_off's comment, column c) is also the noise pass's scratch
 // (the thread's own slots).  kSync: a barrier before that use.  sc scales the result (a
 // power of two: exact), the 1/nz of a following inverse transform folded into 1/D(k).
-template <class Z, bool kPsiInV, bool kSync, class Bar>
+// kPadRows: the tile holds mode kz in row kz + kz / 128 (blocks of 128 rows, each followed
+// by one row of padding: the two threads of a pair, 128 modes apart, meet opposite bank
+// halves) instead of the swizzled rows.
+template <int E, bool kPadRows> __device__ __forceinline__ constexpr int d3_row(int r) {
+    return kPadRows ? d3_off<E>(r) + (d3_off<E>(r) >> 7) : d3_off<E>(r);
+}
+template <class Z, bool kPsiInV, bool kSync, class Bar, bool kPadRows = false>
 __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int c, const Bar& bar,
                                            const float* kz_tab, int kx, int ky, int t, int nx, int ny,
                                            const ZArgsF& a, const double2* k0, float sc) {
@@ -274,7 +250,7 @@ __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int 
     static_assert(B == 128, "kz_slot pads one float per 128 modes");
     const int p = t >> 1, h = t & 1;
     const int kzb = p + h * B;                   // kz = kzb + d3_off(r)
-    float2* trow = tile + ((p ^ h) + h * B) * TX + c;  // + d3_off(r) TX
+    float2* trow = tile + (kPadRows ? p + h * (B + 1) : (p ^ h) + h * B) * TX + c;  // + d3_row(r) TX
     const float* tab = kz_tab + kzb + h;         // kz_slot(kz) = kzb + h + d3_off(r) + 2 [r >= E/2]
     const float k0x = (float)kx * a.ckx;
     const float k1y = (float)(ky < ny / 2 + 1 ? ky : ky - ny) * a.cky;
@@ -282,7 +258,7 @@ __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int 
     const float deps = 1.0f + a.C - a.eps;
 #pragma unroll
     for (int r = 0; r < E; ++r) {
-        const float2 o = trow[d3_off<E>(r) * TX];
+        const float2 o = trow[d3_row<E, kPadRows>(r) * TX];
         const float2 psi = kPsiInV ? v[r] : o;
         const float2 n = kPsiInV ? o : v[r];
         const float k2z = tab[d3_off<E>(r) + (r >= E / 2 ? 2 : 0)];
@@ -296,10 +272,11 @@ __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int 
         if (kSync) bar.sync();
         const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
 #pragma unroll
-        for (int r = 0; r < E; ++r) trow[d3_off<E>(r) * TX] = v[r];
+        for (int r = 0; r < E; ++r) trow[d3_row<E, kPadRows>(r) * TX] = v[r];
 #pragma unroll 1
         for (int r = 0; r < E; ++r) {
             const int off = r < E / 2 ? E * r : E * E + E * (r - E / 2);
+            const int row = kPadRows ? off + (off >> 7) : off;
             const int kz = kzb + off;
             const float k2z = tab[off + (r >= E / 2 ? 2 : 0)];
             const float dopx = -kxy - k2z * k2z;
@@ -307,13 +284,13 @@ __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int 
             const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy)) * sc;
             const float2 xi = kspace_noise<float>(kx, ky, kz, nx, ny, NZ, a.seed, ctr);
             const float g = a.dt * a.namp_eff * sqrtf(-dopx) * inv;
-            float2 w = trow[off * TX];
+            float2 w = trow[row * TX];
             w.x += g * xi.x;
             w.y += g * xi.y;
-            trow[off * TX] = w;
+            trow[row * TX] = w;
         }
 #pragma unroll
-        for (int r = 0; r < E; ++r) v[r] = trow[d3_off<E>(r) * TX];
+        for (int r = 0; r < E; ++r) v[r] = trow[d3_row<E, kPadRows>(r) * TX];
     }
     if (kx == 0 && ky == 0 && t == 0) v[0] = make_float2((float)k0->x * sc, (float)k0->y * sc);  // kz = 0 at r = 0
 }
@@ -391,7 +368,7 @@ __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_grou
 template <class Z>
 __global__ void __launch_bounds__(Z::TH, Z::CMINB) k_zcarry(float2* kpsi, float2* A, const float2* __restrict__ B, int nx,
                                                       int ny, ZArgsF a, const double2* __restrict__ k0, int* flag,
-                                                      const float2* __restrict__ twg, int pf) {
+                                                      const float2* __restrict__ twg) {
     constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, TH = Z::TH;
     static_assert(TX == 8 && (Z::U == 1 || Z::U == 2), "staging swizzle assumes 8 columns per tile");
     extern __shared__ __align__(16) float2 sm[];
@@ -418,7 +395,6 @@ __global__ void __launch_bounds__(Z::TH, Z::CMINB) k_zcarry(float2* kpsi, float2
     float2 v[E];
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = valid ? B[base + (int64_t)(t + P * j) * zs] : make_float2(0.f, 0.f);
-    if (pf) prefetch_ztile<NZ, TX>(kpsi, B, pf, nxh, zs, tid, TH);
     __syncthreads();
     fft_d1_to_d2<NZ, E, TX, -1, BarCta, Z::PADG>(v, t, c, xb, tw);
     cp_wait_all();
@@ -442,11 +418,12 @@ __global__ void __launch_bounds__(Z::TH, Z::CMINB) k_zcarry(float2* kpsi, float2
 // kLast: B and psi^' in the standard layout (psi^' over B, in place), no A'.  Shared
 // memory: the exchange buffer, the stage [kz][c] (a warp's four modes per register have
 // two even and two odd kz: no bank conflicts), the tail.
+// kt0: the kx tile of blockIdx.x = 0 (a launch may cover only some tiles).
 template <class Z, bool kLast>
 __global__ void __launch_bounds__(Z::TH, 3) k_zcarry3(const float2* psi_in, const float2* B, float2* psi_out,
                                                        float2* A, int nx, int ny, ZArgsF a,
                                                        const double2* __restrict__ k0, int* flag,
-                                                       const float2* __restrict__ twg) {
+                                                       const float2* __restrict__ twg, int kt0) {
     constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, TH = Z::TH;
     static_assert(TX == kTileW, "the tiles of the z-tiled layout");
     extern __shared__ __align__(16) float2 sm[];
@@ -455,12 +432,13 @@ __global__ void __launch_bounds__(Z::TH, 3) k_zcarry3(const float2* psi_in, cons
     float2* tw = stg + NZ * TX;
     const int tid = threadIdx.x;
     const int c = tid % TX, t = tid / TX;
-    const int kx = blockIdx.x * TX + c;
+    const int kt = blockIdx.x + kt0;
+    const int kx = kt * TX + c;
     const int ky = blockIdx.y;
     const int nxh = nx / 2 + 1;
     const bool valid = kx < nxh;
-    const ColAddr cp = zcol_addr<true>(blockIdx.x, c, ky, nxh, ny, NZ);
-    const ColAddr cb = zcol_addr<!kLast>(blockIdx.x, c, ky, nxh, ny, NZ);
+    const ColAddr cp = zcol_addr<true>(kt, c, ky, nxh, ny, NZ);
+    const ColAddr cb = zcol_addr<!kLast>(kt, c, ky, nxh, ny, NZ);
     if (valid) {
 #pragma unroll
         for (int j = 0; j < E; ++j) {
@@ -495,6 +473,94 @@ __global__ void __launch_bounds__(Z::TH, 3) k_zcarry3(const float2* psi_in, cons
     }
 }
 
+// The psi^-carrying z pass on whole kx tiles of the z-tiled layout with bulk asynchronous
+// copies (the TMA unit) for every byte it moves: per CTA (one tile of TX = 8 columns at one
+// ky, 32 threads per column, 16 values per thread) the psi^ block and the B block, each
+// one contiguous 32 KB block, arrive in shared memory on one mbarrier while the CTA loads
+// its twiddles; N^ = FFT_z(B) in registers; the update reads psi^ from shared memory and
+// writes psi^' back in place, which one bulk copy per 128 modes stores; A' = IFFT_z(psi^')
+// / nz goes through shared memory into one bulk store over B's block.  No thread issues a
+// global load or store of field data.  Shared memory (float2 units): psi^ in four pieces
+// of 128 kz rows of TX, each followed by a row of padding (kz at row kz + kz / 128); the B
+// stage, reused as the unpadded exchange buffer and as the A' stage; the signed twiddles;
+// the wavenumbers; the mbarrier.  About 75 KB: three CTAs per SM.
+template <class Z>
+struct ZBulkCfg {
+    static constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, TH = Z::TH;
+    static constexpr int PIECE = 128;                        // kz rows per bulk piece of psi^
+    static constexpr int NPIECE = NZ / PIECE;
+    static constexpr int STP = NPIECE * (PIECE + 1) * TX;    // psi^ stage
+    static constexpr int XB = E * P * TX;                    // B stage / exchange (PADX = 0)
+    static constexpr int TAIL = Z::TW + NZ / 2 + 2;          // twiddles, NZ + NZ/128 floats
+    static constexpr size_t SMEM = (size_t)(STP + XB + TAIL) * sizeof(float2) + 16;
+    static_assert(XB == NZ * TX && NZ % PIECE == 0 && TX == kTileW, "shape");
+};
+
+template <class Z>
+__global__ void __launch_bounds__(Z::TH, 3) k_zbulk(float2* psi, float2* BA, int nx, int ny, ZArgsF a,
+                                                     const double2* __restrict__ k0, int* flag,
+                                                     const float2* __restrict__ twg) {
+    using C = ZBulkCfg<Z>;
+    constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, TH = Z::TH;
+    extern __shared__ __align__(128) float2 sm[];
+    float2* stp = sm;
+    float2* xb = sm + C::STP;
+    float2* tw = xb + C::XB;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tw + C::TAIL);
+    const int tid = threadIdx.x;
+    const int c = tid % TX, t = tid / TX;
+    const int kt = blockIdx.x, ky = blockIdx.y;
+    const int kx = kt * TX + c;
+    const int nxh = nx / 2 + 1;
+    // the tile's blocks: [z][c] rows of TX (a whole tile: wt = TX)
+    const int64_t blk = ((int64_t)kt * TX * ny + (int64_t)ky * TX) * NZ;
+    constexpr unsigned kBlockBytes = NZ * TX * sizeof(float2);
+    constexpr unsigned kPieceBytes = C::PIECE * TX * sizeof(float2);
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_init_fence();
+        mbar_arrive_expect_tx(bar, 2 * kBlockBytes);
+#pragma unroll
+        for (int q = 0; q < C::NPIECE; ++q)
+            bulk_load(stp + q * (C::PIECE + 1) * TX, psi + blk + q * C::PIECE * TX, kPieceBytes, bar);
+        bulk_load(xb, BA + blk, kBlockBytes, bar);
+    }
+    const float* kz_tab = load_tail<Z>(tw, twg, a, tid, TH);
+    __syncthreads();  // the tail, and the barrier's initialisation
+    if (!mbar_wait(bar, 0, kWaitPolls)) {
+        if (tid == 0) atomicOr(flag, kFlagWaitTimeout);
+        return;
+    }
+    float2 v[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = xb[(t + P * j) * TX + c];
+    // (fft_d1_to_d3 synchronises before its first write to xb)
+    fft_d1_to_d3<NZ, E, TX, -1, BarCta, true, 0>(v, t, c, xb, tw);
+    propagate3<Z, false, false, BarCta, true>(v, stp, c, BarCta{}, kz_tab, kx, ky, t, nx, ny, a, k0, 1.0f);
+    // psi^' replaced psi^ in each thread's own slots: hand them to the async proxy
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < C::NPIECE; ++q)
+            bulk_store(psi + blk + q * C::PIECE * TX, stp + q * (C::PIECE + 1) * TX, kPieceBytes);
+        bulk_commit();
+    }
+    fft_d3_to_d1<NZ, E, TX, 1, BarCta, 0>(v, t, c, xb, tw);
+    watch<Z>(v, false, kx < nxh, flag);
+    const float s = 1.0f / (float)NZ;
+    __syncthreads();  // every thread's last exchange reads are done
+#pragma unroll
+    for (int j = 0; j < E; ++j) xb[(t + P * j) * TX + c] = make_float2(v[j].x * s, v[j].y * s);
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+        bulk_store(BA + blk, xb, kBlockBytes);
+        bulk_commit();
+        bulk_wait_read();  // shared memory stays valid until both stores have read it
+    }
+}
+
 // Copy between the standard and the z-tiled layouts (col_addr layouts 0, 1): one kx tile
 // of the z columns at one ky per CTA of TX * 32 threads.
 __global__ void __launch_bounds__(256) k_relayout(const float2* __restrict__ in, float2* __restrict__ out, int nxh,
@@ -507,90 +573,7 @@ __global__ void __launch_bounds__(256) k_relayout(const float2* __restrict__ in,
     for (int z = t; z < nz; z += 32) out[d.base + (int64_t)z * d.stride] = in[s.base + (int64_t)z * s.stride];
 }
 
-__device__ __forceinline__ void bar_arrive(int id, int count) {
-    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
-}
-__device__ __forceinline__ void bar_sync(int id, int count) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
-}
-
-template <class Z>
-__global__ void __launch_bounds__(Z::T, 1) k_zpipe(float2* A, const float2* __restrict__ B, int nx, int ny, ZArgsF a,
-                                                    const double2* __restrict__ k0, int* flag,
-                                                    const float2* __restrict__ twg) {
-    constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, U = Z::U, TH = Z::TH, T = Z::T;
-    extern __shared__ __align__(16) float2 sm[];
-    float2* stgA = sm;
-    float2* stgB = stgA + Z::STG;
-    float2* regA = stgB + Z::STG;
-    float2* regB = regA + Z::REG;
-    float2* nh = regB + Z::REG;
-    float2* tw = nh + Z::NHS;
-    const int tid = threadIdx.x;
-    const float* kz_tab = load_tail<Z>(tw, twg, a, tid, T);
-    __syncthreads();
-    const int half = tid / TH;
-    const int lt = tid - half * TH;
-    const int c = lt % TX, t = lt / TX;
-    const int nxh = nx / 2 + 1;
-    const int ntx = (nxh + TX - 1) / TX;
-    const int ntiles = ntx * ny;
-    const int64_t zs = (int64_t)ny * nxh;
-    const float2* src = half ? B : A;
-    float2* stg = half ? stgB : stgA;
-
-    // each thread stages exactly the elements it later reads: no barrier around staging
-    auto issue = [&](int tile) {
-        const int kxq = (tile % ntx) * TX + c;
-        if (kxq < nxh) {
-            const float2* g = src + (int64_t)(tile / ntx) * nxh + kxq + (int64_t)t * zs;
-            float2* s = stg + t * TX + c;
-#pragma unroll 1
-            for (int j = 0; j < E; ++j, g += P * zs, s += P * TX) cp_async8(s, g);
-        }
-        cp_commit();
-    };
-
-    int tile = blockIdx.x;
-    if (tile < ntiles) issue(tile);
-    bool first = true;
-    for (; tile < ntiles; tile += gridDim.x) {
-        const int kx = (tile % ntx) * TX + c;
-        const int ky = tile / ntx;
-        const bool valid = kx < nxh;
-        const int64_t base = (int64_t)ky * nxh + kx;
-        const bool has_next = tile + (int)gridDim.x < ntiles;
-        cp_wait_all();
-        float2 v[E];
-#pragma unroll
-        for (int j = 0; j < E; ++j) v[j] = valid ? stg[(t + P * j) * TX + c] : make_float2(0.f, 0.f);
-        if (has_next) issue(tile + gridDim.x);  // the staging buffer is free once read
-        if (half == 1) {
-            fft_d1_to_d2<NZ, E, TX, -1, BarNamed<2, TH>, Z::PADG>(v, t, c, regB, tw);
-            if (!first) bar_sync(4, T);  // the A half is done with the previous N^
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-#pragma unroll
-                for (int k2 = 0; k2 < P; ++k2) nh[nh_slot<Z>((t * U + u) + E * k2, c)] = v[u * P + k2];
-            bar_arrive(3, T);  // N^ of this tile written
-        } else {
-            fft_d1_to_d2<NZ, E, TX, -1, BarNamed<1, TH>, Z::PADG>(v, t, c, regA, tw);
-            bar_sync(3, T);
-            auto own = [&](int kz) { return kz * TX + c; };
-            propagate<Z, true, true>(v, [&](int kz) { return nh[nh_slot<Z>(kz, c)]; }, regA, own, BarNamed<1, TH>{},
-                                     kz_tab, kx, ky, t, nx, ny, a, k0);
-            if (has_next) bar_arrive(4, T);  // N^ slots free for the next tile
-            if (!a.final_step) fft_d2_to_d1<NZ, E, TX, 1, BarNamed<1, TH>, Z::PADG>(v, t, c, regA, tw);
-            watch<Z>(v, a.final_step, valid, flag);
-            store_state<Z>(v, A, base, zs, t, valid, a.final_step);
-        }
-        first = false;
-    }
-    cp_wait_all();
-}
-
 using Z512 = ZCfg<512, 32, 8>;
-using Z512w = ZCfg<512, 32, 16>;  // 128-byte column segments, one 512-thread CTA per SM (k_zcol only)
 using Z3_512 = Z3Cfg<512, 16, 8>;  // 16 values per thread (k_zcol3)
 using Z256 = ZCfg<256, 16, 8>;
 using Z128 = ZCfg<128, 16, 8>;
@@ -600,9 +583,7 @@ template <class Z>
 cudaError_t zattr() {
     cudaError_t e = cudaFuncSetAttribute(k_zcol<Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Z::SMEM);
     if (e) return e;
-    if ((e = cudaFuncSetAttribute(k_zcarry<Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Z::SMEM_CARRY)))
-        return e;
-    return cudaFuncSetAttribute(k_zpipe<Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Z::SMEM_PIPE);
+    return cudaFuncSetAttribute(k_zcarry<Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Z::SMEM_CARRY);
 }
 
 ZArgsF zargs_f(const ZPropArgs& p) {
@@ -614,46 +595,30 @@ ZArgsF zargs_f(const ZPropArgs& p) {
 template <class Z>
 cudaError_t zlaunch_carry(const pfc_ctx* c, void* kpsi, void* A, const void* B, const ZPropArgs& p) {
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
-    static const int per_sm = resident_ctas(k_zcarry<Z>, Z::TH, Z::SMEM_CARRY);
     dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny);
     k_zcarry<Z><<<grid, Z::TH, Z::SMEM_CARRY, c->stream>>>((float2*)kpsi, (float2*)A, (const float2*)B, c->nx, c->ny,
-                                                           zargs_f(p), c->k0, c->flag, tw,
-                                                           prefetch_ahead(c, per_sm, kpsi, B));
+                                                           zargs_f(p), c->k0, c->flag, tw);
     return cudaGetLastError();
 }
 
 template <class Z>
 cudaError_t zlaunch(const pfc_ctx* c, const void* A, const void* B, void* O, const ZPropArgs& p, int lay) {
-    const ZArgsF a = zargs_f(p);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
-    const int ntx = (c->nxh + Z::TX - 1) / Z::TX;
-    if (c->z_pipe) {
-        if (lay || O != A) return cudaErrorNotSupported;  // standard layout, in place
-        const int ntiles = ntx * c->ny;
-        const int grid = ntiles < c->num_sms ? ntiles : c->num_sms;
-        k_zpipe<Z><<<grid, Z::T, Z::SMEM_PIPE, c->stream>>>((float2*)O, (const float2*)B, c->nx, c->ny, a, c->k0,
-                                                             c->flag, tw);
-    } else {
-        static const int per_sm = resident_ctas(k_zcol<Z>, Z::T, Z::SMEM);
-        dim3 grid(ntx, c->ny);
-        const int pf = lay ? 0 : prefetch_ahead(c, per_sm, A, B);
-        k_zcol<Z><<<grid, Z::T, Z::SMEM, c->stream>>>((const float2*)A, (const float2*)B, (float2*)O, c->nx, c->ny,
-                                                       lay, a, c->k0, c->flag, tw, pf);
-    }
+    dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny);
+    k_zcol<Z><<<grid, Z::T, Z::SMEM, c->stream>>>((const float2*)A, (const float2*)B, (float2*)O, c->nx, c->ny, lay,
+                                                   zargs_f(p), c->k0, c->flag, tw);
     return cudaGetLastError();
 }
 
 }  // namespace
 
+// Register z kernels by length: 6 (nz = 512) 16 values per thread over 32 threads per
+// column (fft_d1_to_d3); 1-4 the square split for 512 (psi^-carrying, standard layout
+// only), 256, 128, 64.
 int fused_z_variant(int nx, int nz, int dtype) {
     if (dtype != PFC_F32 || nx < 16 || (nx / 2) % 8 != 0 || nx % 2 != 0) return 0;
     switch (nz) {
-        case 512: {
-            // 6 (default): 16 values per thread; 1: the square split; 5: 16-column tiles
-            const char* s = getenv("PFC_Z_VARIANT");
-            const int v = s ? atoi(s) : 6;
-            return (v == 1 || v == 5) ? v : 6;
-        }
+        case 512: return 6;
         case 256: return 2;
         case 128: return 3;
         case 64: return 4;
@@ -667,9 +632,6 @@ cudaError_t set_zcol_attributes(const pfc_ctx* c) {
         case 2: return zattr<Z256>();
         case 3: return zattr<Z128>();
         case 4: return zattr<Z64>();
-        case 5:
-            return cudaFuncSetAttribute(k_zcol<Z512w>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)Z512w::SMEM);
         case 6: {
             cudaError_t e = cudaFuncSetAttribute(k_zcol3<Z3_512, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)Z3_512::SMEM);
@@ -685,6 +647,9 @@ cudaError_t set_zcol_attributes(const pfc_ctx* c) {
             if (!e)
                 e = cudaFuncSetAttribute(k_zcarry3<Z3_512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)Z3_512::SMEM_CARRY);
+            if (!e)
+                e = cudaFuncSetAttribute(k_zbulk<Z3_512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)ZBulkCfg<Z3_512>::SMEM);
             return e;
         }
     }
@@ -706,10 +671,25 @@ cudaError_t launch_zcarry_tiled(const pfc_ctx* c, const void* psi_in, const void
     if (c->fused_z != 6) return cudaErrorNotSupported;
     using Z = Z3_512;
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
-    dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny);
-    auto k = a.final_step ? k_zcarry3<Z, true> : k_zcarry3<Z, false>;
-    k<<<grid, Z::TH, Z::SMEM_CARRY, c->stream>>>((const float2*)psi_in, (const float2*)B, (float2*)psi_out, (float2*)A,
-                                                  c->nx, c->ny, zargs_f(a), c->k0, c->flag, tw);
+    const ZArgsF za = zargs_f(a);
+    const int ntx = (c->nxh + Z::TX - 1) / Z::TX;
+    if (a.final_step) {
+        k_zcarry3<Z, true><<<dim3(ntx, c->ny), Z::TH, Z::SMEM_CARRY, c->stream>>>(
+            (const float2*)psi_in, (const float2*)B, (float2*)psi_out, (float2*)A, c->nx, c->ny, za, c->k0, c->flag,
+            tw, 0);
+        return cudaGetLastError();
+    }
+    // whole tiles with bulk copies (psi^ in place, A' over B); the partial last tile with
+    // per-thread accesses
+    const int full = c->nxh / Z::TX;
+    if (psi_in != psi_out || B != A) return cudaErrorNotSupported;
+    if (full > 0)
+        k_zbulk<Z><<<dim3(full, c->ny), Z::TH, ZBulkCfg<Z>::SMEM, c->stream>>>((float2*)psi_out, (float2*)A, c->nx,
+                                                                                 c->ny, za, c->k0, c->flag, tw);
+    if (full < ntx)
+        k_zcarry3<Z, false><<<dim3(ntx - full, c->ny), Z::TH, Z::SMEM_CARRY, c->stream>>>(
+            (const float2*)psi_in, (const float2*)B, (float2*)psi_out, (float2*)A, c->nx, c->ny, za, c->k0, c->flag,
+            tw, full);
     return cudaGetLastError();
 }
 
@@ -722,16 +702,6 @@ cudaError_t launch_relayout(const pfc_ctx* c, const void* in, void* out, int to_
 
 cudaError_t launch_zcol(const pfc_ctx* c, const void* A, const void* B, void* O, const ZPropArgs& a, int lay) {
     switch (c->fused_z) {
-        case 5: {
-            using Z = Z512w;
-            static const int per_sm = resident_ctas(k_zcol<Z>, Z::T, Z::SMEM);
-            const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
-            dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny);
-            const int pf = lay ? 0 : prefetch_ahead(c, per_sm, A, B);
-            k_zcol<Z><<<grid, Z::T, Z::SMEM, c->stream>>>((const float2*)A, (const float2*)B, (float2*)O, c->nx, c->ny,
-                                                           lay, zargs_f(a), c->k0, c->flag, tw, pf);
-            return cudaGetLastError();
-        }
         case 6: {
             using Z = Z3_512;
             const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;

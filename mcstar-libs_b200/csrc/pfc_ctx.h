@@ -14,7 +14,6 @@ namespace pfc {
 constexpr size_t kMaxDynSmem = 200 * 1024;
 constexpr int kRedBlocks = 1184;        // 8 x 148 SMs: fixed grid of the FP64 reductions
 constexpr int kPeakBlock = 256;         // cells per block of the peak finder
-constexpr int kBondMaxNbr = 64;         // neighbour cap per atom of the bond-order kernels
 
 struct AxisPlan {
     LinePlan plan;
@@ -32,6 +31,7 @@ struct pfc_ctx {
     size_t state_bytes;           // n_cmpl * 2 * fsize
     cudaStream_t stream;
     std::string err;
+    pfc_options opt;              // the options in effect (pfc_get_options)
 
     pfc::AxisPlan px;             // x: complex length nx/2 (even nx) or nx (odd nx)
     pfc::AxisPlan py, pz;         // y, z: complex length ny, nz
@@ -47,15 +47,14 @@ struct pfc_ctx {
     int* peak_counts;             // per-block peak counts (kPeakBlock cells per block)
     int* peak_offsets;            // exclusive scan of peak_counts (+ total)
     int n_peak_blocks;
-    // bond order
+    // bond order: per-atom scratch for max_atoms atoms and the neighbour lists (max_pairs
+    // entries), both grown by pfc_bond_order / pfc_bond_reserve when a call needs more
     int max_atoms;
     void* bond_scratch;
     size_t bond_scratch_bytes;
-    // fused plane kernels available for this shape
-    int fused_xy;                 // 0: general passes; otherwise the plane kernel variant id
-    int plane_tw_off;             // twiddles of the plane kernel: W_ny^m, W_{nx/2}^m, W_nx^k (k <= nx/2)
+    int64_t max_pairs;
+    int* bond_pairs;
     int fused_z;                  // 0: general z pass; otherwise the register z kernel variant id
-    int z_pipe;                   // register z pass as the persistent pipelined kernel (1) or one tile per CTA (0)
     int z_carry;                  // carry psi^ itself instead of A: standard layout, A = IFFT_z(psi^)/nz
                                   // in work2; tiled, psi^ z-tiled in work2 and A in the psi^ buffer
     int tiled;                    // register passes on kx-tiled fields (col_addr): A z-tiled in work2,
@@ -68,9 +67,9 @@ struct pfc_ctx {
     int zfft_tw_off;              // W_nz^m of the plain z transforms
     int ypass_tw_off;             // W_ny^m
     int xpass_tw_off;             // W_{nx/2}^m, then W_nx^k (k <= nx/2)
-    int xy_mode;                  // 0 general passes, 1 cluster plane kernel, 2 register y/x/y passes
-    int slab;                     // z-planes per slab of the register xy passes (0: whole field)
-    float pf_waves;               // L2 prefetch distance of the register passes, in waves of CTAs (0: off)
+    int xpair;                    // the row-tiled x pass on row pairs (k_xpair) for this nx
+    int xpair_tw_off;             // W_nx^m, m < nx
+    int xy_mode;                  // 0 general passes, 2 register y/x/y passes
     // tracing (pfc_profile_enable / pfc_profile_read)
     bool prof_on = false;
     long long launches = 0;
@@ -93,15 +92,6 @@ int resident_ctas(K kernel, int threads, size_t smem) {
         n = 1;
     }
     return n > 0 ? n : 1;
-}
-
-// Tiles ahead of the L2 prefetch of a register pass whose CTAs run `per_sm` to an SM:
-// pf_waves full waves; 0 (off) unless every prefetched field starts on a 16-byte boundary
-// (field sizes are multiples of 16 bytes for every shape the register passes take).
-inline int prefetch_ahead(const pfc_ctx* c, int per_sm, const void* f0, const void* f1 = nullptr) {
-    if (c->pf_waves <= 0.f) return 0;
-    if (((uintptr_t)f0 & 15) || ((uintptr_t)f1 & 15)) return 0;
-    return (int)(c->pf_waves * (float)(c->num_sms * per_sm) + 0.5f);
 }
 
 // ---- general FFT passes (kern_fft.cu) ----
@@ -127,6 +117,7 @@ cudaError_t launch_zprop_cols(const pfc_ctx* c, void* A, const void* B, const ZP
 // ---- register-resident y and x passes (kern_passes.cu) ----
 int fused_y_variant(int ny, int dtype);
 int fused_x_variant(int nx, int dtype);
+int xpair_variant(int nx, int dtype);
 cudaError_t set_pass_attributes(const pfc_ctx* c);
 // y FFT of nzs consecutive planes starting at in / out (in may equal out); lay & 3 / lay
 // >> 2: the layouts of in / out (col_addr; tiled: whole fields only, not in place)
@@ -195,9 +186,11 @@ cudaError_t launch_findpeaks(const pfc_ctx* c, const void* psi, double ths, void
 
 // ---- bond order (kern_bond.cu) ----
 size_t bond_scratch_bytes(int max_atoms);
+// grows the bond-order scratch to `atoms` atoms and `pairs` neighbour entries
+cudaError_t bond_reserve(pfc_ctx* c, int atoms, int64_t pairs);
 cudaError_t launch_bond_order(pfc_ctx* c, const void* maxima, int n, double h0, double h1, double h2,
                               double ths, double boxsize, double rlim, double* out_rows, int row_capacity,
-                              int* n_rows_host, int* overflow_host);
+                              int* n_rows_host);
 
 // ---- the reference's other propagators (kern_variants.cu) ----
 cudaError_t launch_init_eom_op(const pfc_ctx* c, void* kop, double dt, double eps, double lx, double ly, double lz);
@@ -217,11 +210,5 @@ cudaError_t launch_adj_mul(const pfc_ctx* c, const void* in, void* out, const pf
 cudaError_t launch_adj_eps(const pfc_ctx* c, const void* lam_hat, const void* kpsi_np1, const pfc_step_params* p);
 cudaError_t launch_adj_combine(const pfc_ctx* c, void* lam, const void* psi_u, const void* b, double C);
 cudaError_t launch_sf_loss(const pfc_ctx* c, const void* kpsi, const void* s_target, void* out);
-
-// ---- fused plane kernels (kern_fused.cu) ----
-int fused_xy_variant(int nx, int ny, int dtype);
-cudaError_t set_fused_attributes(const pfc_ctx* c);
-cudaError_t launch_fused_xy(const pfc_ctx* c, const void* A, void* B, const void* pot, double mul, double C,
-                            double mu);
 
 }  // namespace pfc

@@ -258,11 +258,12 @@ __device__ __forceinline__ void fft_d2_to_d1(float2 (&v)[E], int t, int g, float
 // same way, so its outputs carry (-1)^m, removed by their readers.  Each sign rides on the
 // stage-1 twiddles: twN holds W_N^m for m < N, then -W_N^m, and a thread of odd t with odd
 // t/2 takes its twiddles from the second half (k1 = 0 included: twN[N] = -1).
-// Exchange slots (k1, t, g) -> (k1 P + t) NG + k1 NG + g: the pad of NG per k1 row puts
-// the four (p, h) of a warp in alternate halves of the banks.  Buffer: E (P + 1) NG.
-template <int N, int E, int NG>
+// Exchange slots (k1, t, g) -> (k1 P + t) NG + k1 NG PADX + g: with PADX = 1 a pad of NG
+// per k1 row puts the four (p, h) of a warp in alternate halves of the banks.  Buffer:
+// E (P + PADX) NG.
+template <int N, int E, int NG, int PADX = 1>
 __device__ __forceinline__ int xslot3(int k1, int t, int g) {
-    return (k1 * (2 * E) + t) * NG + k1 * NG + g;
+    return (k1 * (2 * E) + t) * NG + k1 * NG * PADX + g;
 }
 
 // the stage-1 twiddles of D1 thread t (signed as above)
@@ -272,7 +273,7 @@ template <int N> __device__ __forceinline__ const float2* d3_tw1(const float2* t
 
 // kBal false: the same transform without the balance (twN of N entries; thread h = 1 applies
 // all E - 1 W_2E twiddles and the pair selects what it sends).
-template <int N, int E, int NG, int DIR, class Bar = BarCta, bool kBal = true>
+template <int N, int E, int NG, int DIR, class Bar = BarCta, bool kBal = true, int PADX = 1>
 __device__ __forceinline__ void fft_d1_to_d3(float2 (&v)[E], int t, int g, float2* xb, const float2* twN,
                                              const Bar& bar = Bar{}) {
     constexpr int P = 2 * E, H = E / 2;
@@ -291,11 +292,11 @@ __device__ __forceinline__ void fft_d1_to_d3(float2 (&v)[E], int t, int g, float
     }
     bar.sync();
 #pragma unroll
-    for (int k1 = 0; k1 < E; ++k1) xb[xslot3<N, E, NG>(k1, t, g)] = v[k1];
+    for (int k1 = 0; k1 < E; ++k1) xb[xslot3<N, E, NG, PADX>(k1, t, g)] = v[k1];
     bar.sync();
     const int p = t >> 1, h = t & 1;
 #pragma unroll
-    for (int m = 0; m < E; ++m) v[m] = xb[xslot3<N, E, NG>(p, 2 * m + h, g)];
+    for (int m = 0; m < E; ++m) v[m] = xb[xslot3<N, E, NG, PADX>(p, 2 * m + h, g)];
     RF<E, DIR>::run(v);  // h = 0: F0[k] at k; h = 1: F1[(k + H) mod E] at k (kBal)
     if constexpr (!kBal) {
         if (h) {
@@ -334,7 +335,7 @@ __device__ __forceinline__ void fft_d1_to_d3(float2 (&v)[E], int t, int g, float
     }
 }
 
-template <int N, int E, int NG, int DIR, class Bar = BarCta>
+template <int N, int E, int NG, int DIR, class Bar = BarCta, int PADX = 1>
 __device__ __forceinline__ void fft_d3_to_d1(float2 (&v)[E], int t, int g, float2* xb, const float2* twN,
                                              const Bar& bar = Bar{}) {
     constexpr int P = 2 * E, H = E / 2;
@@ -357,10 +358,10 @@ __device__ __forceinline__ void fft_d3_to_d1(float2 (&v)[E], int t, int g, float
     RF<E, DIR>::run(v);  // outputs t = 2m + h, times (-1)^m for h = 1
     bar.sync();
 #pragma unroll
-    for (int m = 0; m < E; ++m) xb[xslot3<N, E, NG>(p, 2 * m + h, g)] = v[m];
+    for (int m = 0; m < E; ++m) xb[xslot3<N, E, NG, PADX>(p, 2 * m + h, g)] = v[m];
     bar.sync();
 #pragma unroll
-    for (int k1 = 0; k1 < E; ++k1) v[k1] = xb[xslot3<N, E, NG>(k1, t, g)];
+    for (int k1 = 0; k1 < E; ++k1) v[k1] = xb[xslot3<N, E, NG, PADX>(k1, t, g)];
     const float2* tw1 = d3_tw1<N>(twN, t);
     const float s0 = tw1[0].x;  // +-1
     v[0] = make_float2(v[0].x * s0, v[0].y * s0);

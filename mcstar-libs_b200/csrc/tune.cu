@@ -1,0 +1,237 @@
+// The autotuner of the kernel schedules (pfc_tune): times pfc_step under candidate
+// pfc_options on the current device and keeps the fastest, optionally caching results in
+// a JSON file keyed by shape, precision and device.
+//
+// Search: coordinate descent from the library's choice -- each option in turn takes each
+// of its values with the others fixed, and a value replaces the current one when it is at
+// least 2% faster.  Only options that change a kernel of this shape are tried (the general
+// passes' radix order and tiles when a general pass runs, the z and x schedules when the
+// register passes run).  Each candidate is a fresh context stepping a synthetic liquid
+// (psi0 = -0.18 with real noise of standard deviation 0.05, eps = 0.3, dt = 0.25).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+#include "pfc_ctx.h"
+
+namespace {
+
+struct Knob {
+    const char* name;
+    int* field;
+    std::vector<int> values;
+};
+
+std::string device_key(const pfc_desc* d) {
+    int dev = 0;
+    cudaDeviceProp prop;
+    std::string name = "unknown";
+    int sms = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaGetDeviceProperties(&prop, dev) == cudaSuccess) {
+        name = prop.name;
+        sms = prop.multiProcessorCount;
+    }
+    for (char& ch : name)
+        if (ch == '"' || ch == '\\') ch = '_';
+    std::ostringstream k;
+    k << d->nx << "x" << d->ny << "x" << d->nz << ":" << (d->dtype == PFC_F64 ? "f64" : "f32") << ":" << name << ":"
+      << sms << "sm";
+    return k.str();
+}
+
+std::string options_json(const pfc_options& o, double ms) {
+    std::ostringstream s;
+    s << "{\"z_carry\": " << o.z_carry << ", \"x_pair\": " << o.x_pair << ", \"tiled\": " << o.tiled
+      << ", \"radix_order\": " << o.radix_order << ", \"tile_shift\": [" << o.tile_shift[0] << ", " << o.tile_shift[1]
+      << ", " << o.tile_shift[2] << ", " << o.tile_shift[3] << "], \"ms_per_step\": " << ms << "}";
+    return s.str();
+}
+
+// The cache file: {"pfc_tune": 1, "entries": {"<key>": {...}, ...}} with one entry per
+// line, as options_json writes them.  Returns the entries as key -> object text.
+std::map<std::string, std::string> read_cache(const char* path) {
+    std::map<std::string, std::string> out;
+    std::ifstream f(path);
+    if (!f) return out;
+    std::string line;
+    while (std::getline(f, line)) {
+        const size_t q0 = line.find('"');
+        const size_t q1 = q0 == std::string::npos ? q0 : line.find('"', q0 + 1);
+        const size_t b0 = q1 == std::string::npos ? q1 : line.find('{', q1);
+        const size_t b1 = line.rfind('}');
+        if (b0 == std::string::npos || b1 == std::string::npos || b1 < b0) continue;
+        const std::string key = line.substr(q0 + 1, q1 - q0 - 1);
+        if (key == "pfc_tune" || key == "entries") continue;
+        out[key] = line.substr(b0, b1 - b0 + 1);
+    }
+    return out;
+}
+
+bool write_cache(const char* path, const std::map<std::string, std::string>& entries) {
+    const std::string tmp = std::string(path) + ".tmp";
+    {
+        std::ofstream f(tmp);
+        if (!f) return false;
+        f << "{\"pfc_tune\": 1, \"entries\": {\n";
+        size_t i = 0;
+        for (const auto& kv : entries)
+            f << "  \"" << kv.first << "\": " << kv.second << (++i < entries.size() ? ",\n" : "\n");
+        f << "}}\n";
+        if (!f) return false;
+    }
+    return std::rename(tmp.c_str(), path) == 0;
+}
+
+bool field_int(const std::string& obj, const char* name, int* v) {
+    const std::string pat = std::string("\"") + name + "\":";
+    const size_t p = obj.find(pat);
+    if (p == std::string::npos) return false;
+    return std::sscanf(obj.c_str() + p + pat.size(), " %d", v) == 1;
+}
+
+bool parse_entry(const std::string& obj, pfc_options* o, double* ms) {
+    pfc_default_options(o);
+    if (!field_int(obj, "z_carry", &o->z_carry) || !field_int(obj, "x_pair", &o->x_pair) ||
+        !field_int(obj, "tiled", &o->tiled) || !field_int(obj, "radix_order", &o->radix_order))
+        return false;
+    const size_t p = obj.find("\"tile_shift\":");
+    if (p == std::string::npos ||
+        std::sscanf(obj.c_str() + p + 13, " [%d, %d, %d, %d]", &o->tile_shift[0], &o->tile_shift[1], &o->tile_shift[2],
+                    &o->tile_shift[3]) != 4)
+        return false;
+    const size_t m = obj.find("\"ms_per_step\":");
+    double t = 0.0;
+    if (m != std::string::npos) std::sscanf(obj.c_str() + m + 14, " %lf", &t);
+    if (ms) *ms = t;
+    return true;
+}
+
+// Device time per step of one candidate (< 0: the options are not available for the shape
+// or a call failed; *avail false in the first case).
+double time_candidate(const pfc_desc* d, const pfc_options& o, cudaStream_t st, bool* avail, pfc_options* eff) {
+    *avail = false;
+    pfc_ctx* c = nullptr;
+    if (pfc_create_with(d, &o, &c) != PFC_OK) return -1.0;
+    *avail = true;
+    if (eff) pfc_get_options(c, eff);
+    pfc_set_stream(c, st);
+    void *kpsi = nullptr, *real = nullptr;
+    double best = -1.0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const double dx = 0.7853981633974483;
+    pfc_step_params p{0.25, 0.3, 0.0, 1.0, 0.0, d->nx * dx, d->ny * dx, d->nz > 1 ? d->nz * dx : 1.0, 0, 0};
+    do {
+        if (cudaMalloc(&kpsi, c->state_bytes) || cudaMalloc(&real, c->state_bytes)) break;
+        if (pfc_noise_fill(c, real, 0.05, 12345, 0) != PFC_OK) break;
+        if (pfc_fft_r2c(c, real, kpsi) != PFC_OK) break;
+        // mean density psi0 = -0.18: the k = 0 mode is N psi0 (unnormalised transform)
+        if (c->dtype == PFC_F64) {
+            double v = -0.18 * (double)c->n_real;
+            if (cudaMemcpyAsync(kpsi, &v, sizeof(double), cudaMemcpyHostToDevice, st)) break;
+        } else {
+            float v = (float)(-0.18 * (double)c->n_real);
+            if (cudaMemcpyAsync(kpsi, &v, sizeof(float), cudaMemcpyHostToDevice, st)) break;
+        }
+        if (cudaEventCreate(&e0) || cudaEventCreate(&e1)) break;
+        if (pfc_step(c, kpsi, 2, &p) != PFC_OK) break;  // warm-up
+        auto timed = [&](int n) -> double {
+            if (cudaEventRecord(e0, st) || pfc_step(c, kpsi, n, &p) != PFC_OK || cudaEventRecord(e1, st) ||
+                cudaEventSynchronize(e1))
+                return -1.0;
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, e0, e1)) return -1.0;
+            return (double)ms / n;
+        };
+        const double t1 = timed(2);
+        if (t1 <= 0.0) break;
+        const int reps = std::max(3, std::min(100, (int)std::ceil(30.0 / t1)));
+        const double a = timed(reps), b = timed(reps);
+        if (a <= 0.0 || b <= 0.0) break;
+        best = std::min(a, b);
+    } while (false);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (kpsi) cudaFree(kpsi);
+    if (real) cudaFree(real);
+    pfc_destroy(c);
+    cudaGetLastError();
+    return best;
+}
+
+}  // namespace
+
+extern "C" pfc_status pfc_tune(const pfc_desc* d, const char* cache_path, pfc_options* best, double* ms_per_step) {
+    if (!d || !best) return PFC_ERR_INVALID;
+    const std::string key = device_key(d);
+    std::map<std::string, std::string> cache;
+    if (cache_path) {
+        cache = read_cache(cache_path);
+        auto it = cache.find(key);
+        double ms = 0.0;
+        if (it != cache.end() && parse_entry(it->second, best, &ms)) {
+            if (ms_per_step) *ms_per_step = ms;
+            return PFC_OK;
+        }
+    }
+    // which options touch a kernel of this shape: ask a context with the library's choice
+    pfc_options cur;
+    pfc_default_options(&cur);
+    bool general = false, zreg = false, xpair = false, tiled_ok = false;
+    {
+        pfc_ctx* c = nullptr;
+        pfc_status s = pfc_create_with(d, &cur, &c);
+        if (s != PFC_OK) return s;
+        general = c->xy_mode != 2 || (c->nz > 1 && !c->fused_z);
+        zreg = c->fused_z != 0;
+        xpair = c->fused_x && pfc::xpair_variant(c->nx, c->dtype);
+        tiled_ok = c->fused_z && c->fused_zfft && c->xy_mode == 2 && c->fused_y;
+        pfc_get_options(c, &cur);  // the library's choices, explicit
+        pfc_destroy(c);
+    }
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) return PFC_ERR_CUDA;
+    bool avail = false;
+    double t_cur = time_candidate(d, cur, st, &avail, nullptr);
+    if (t_cur <= 0.0) {
+        cudaStreamDestroy(st);
+        return PFC_ERR_CUDA;
+    }
+    std::vector<Knob> knobs;
+    if (zreg) knobs.push_back({"z_carry", &cur.z_carry, {0, 1}});
+    if (xpair) knobs.push_back({"x_pair", &cur.x_pair, {0, 1}});
+    if (tiled_ok) knobs.push_back({"tiled", &cur.tiled, {0, 1}});
+    if (general) {
+        knobs.push_back({"radix_order", &cur.radix_order, {0, 1, 2}});
+        for (int i = 0; i < 4; ++i) knobs.push_back({"tile_shift", &cur.tile_shift[i], {0, 1, 2}});
+    }
+    for (Knob& k : knobs) {
+        const int keep = *k.field;
+        int best_v = keep;
+        double best_t = t_cur;
+        for (int v : k.values) {
+            if (v == keep) continue;
+            *k.field = v;
+            pfc_options eff;
+            const double t = time_candidate(d, cur, st, &avail, &eff);
+            if (t > 0.0 && t < 0.98 * best_t) {
+                best_t = t;
+                best_v = v;
+            }
+        }
+        *k.field = best_v;
+        t_cur = best_t;
+    }
+    cudaStreamDestroy(st);
+    *best = cur;
+    if (ms_per_step) *ms_per_step = t_cur;
+    if (cache_path) {
+        cache[key] = options_json(cur, t_cur);
+        if (!write_cache(cache_path, cache)) fprintf(stderr, "pfc_tune: cannot write %s\n", cache_path);
+    }
+    return PFC_OK;
+}

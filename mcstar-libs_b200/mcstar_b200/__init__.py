@@ -6,7 +6,7 @@ for device memory and streams only.
 """
 from ._lib import PfcError, LIB_PATH, lib
 from .array import GPUArray, CPUArray, AsReal, AsCmpl, shape_tr
-from .context import Context, get_context
+from .context import Context, get_context, tune
 from .kernels import (CufftPlan, R2C, C2R, NoiseHostApi, call_kernel_update_eom, call_kernel_update_eom_with_fen,
                       call_kernel_calc_fen, call_kernel_psi3_split, call_kernel_norm, call_kernel_findpeaks,
                       call_kernel_findpeaks_2d, bond_order_analysis, write_bond_table, maximum_dtype, Maximum,

@@ -29,7 +29,8 @@ EXPORTED = (
     "pfc_sf_loss", "pfc_adjoint_step", "pfc_init_eom_op", "pfc_update_eom_exp", "pfc_update_eom_exp_with_fen",
     "pfc_update_el", "pfc_init_el_op", "pfc_update_el_exp", "pfc_update_eom_py", "pfc_update_eom_hpfcnoise",
     "pfc_gaussian_init", "pfc_kmult_real", "pfc_kmult_imag", "pfc_square", "pfc_write_lowpass_2d",
-    "pfc_amplitude_lowpass",
+    "pfc_amplitude_lowpass", "pfc_bond_reserve", "pfc_default_options", "pfc_create_with", "pfc_get_options",
+    "pfc_tune",
 )
 
 
@@ -51,6 +52,27 @@ class PfcStepParams(ctypes.Structure):
                 ("lz", ctypes.c_double), ("seed", ctypes.c_uint64), ("counter", ctypes.c_uint64)]
 
 
+class PfcOptions(ctypes.Structure):
+    _fields_ = [("z_carry", ctypes.c_int), ("x_pair", ctypes.c_int), ("tiled", ctypes.c_int),
+                ("radix_order", ctypes.c_int), ("tile_shift", ctypes.c_int * 4)]
+
+    def to_dict(self):
+        return {"z_carry": self.z_carry, "x_pair": self.x_pair, "tiled": self.tiled,
+                "radix_order": self.radix_order, "tile_shift": list(self.tile_shift)}
+
+    @classmethod
+    def from_dict(cls, d):
+        o = cls()
+        lib().pfc_default_options(ctypes.byref(o))
+        for k in ("z_carry", "x_pair", "tiled", "radix_order"):
+            if k in d:
+                setattr(o, k, int(d[k]))
+        if "tile_shift" in d:
+            for i, v in enumerate(d["tile_shift"]):
+                o.tile_shift[i] = int(v)
+        return o
+
+
 PROFILE_FAMILIES = 5  # PFC_PROFILE_FAMILIES
 
 
@@ -69,6 +91,10 @@ _I = ctypes.c_int
 _U64 = ctypes.c_uint64
 _SIGS = {
     "pfc_create": ([ctypes.POINTER(PfcDesc), ctypes.POINTER(_P)], _I),
+    "pfc_default_options": ([ctypes.POINTER(PfcOptions)], _I),
+    "pfc_create_with": ([ctypes.POINTER(PfcDesc), ctypes.POINTER(PfcOptions), ctypes.POINTER(_P)], _I),
+    "pfc_get_options": ([_P, ctypes.POINTER(PfcOptions)], _I),
+    "pfc_tune": ([ctypes.POINTER(PfcDesc), ctypes.c_char_p, ctypes.POINTER(PfcOptions), ctypes.POINTER(_D)], _I),
     "pfc_destroy": ([_P], _I),
     "pfc_set_stream": ([_P, _P], _I),
     "pfc_last_error": ([_P], ctypes.c_char_p),
@@ -86,6 +112,7 @@ _SIGS = {
     "pfc_noise_fill": ([_P, _P, _D, _U64, _U64], _I),
     "pfc_findpeaks": ([_P, _P, _D, _P, _I, ctypes.POINTER(_I)], _I),
     "pfc_bond_order": ([_P, _P, _I, _D, _D, _D, _D, _D, _D, _P, _I, ctypes.POINTER(_I)], _I),
+    "pfc_bond_reserve": ([_P, _I, ctypes.c_longlong], _I),
     "pfc_step": ([_P, _P, _I, ctypes.POINTER(PfcStepParams)], _I),
     "pfc_free_energy": ([_P, _P, _D, _D, _D, _D, _D, _D, _D, ctypes.POINTER(_D)], _I),
     "pfc_profile_enable": ([_P, _I], _I),

@@ -32,7 +32,10 @@ def _ptr(t):
 class Context:
     """One context per (shape, precision); owns the library's workspaces."""
 
-    def __init__(self, shape, dtype=np.float32):
+    def __init__(self, shape, dtype=np.float32, options=None):
+        """options: None (the library's choices) or a dict of pfc_options fields (the
+        kernel schedules: z_carry, x_pair, tiled, radix_order, tile_shift), e.g. the
+        result of ``tune``."""
         nx, ny, nz = (int(v) for v in shape)
         self.shape = (nx, ny, nz)
         self.np_dtype = np.dtype(dtype)
@@ -44,13 +47,21 @@ class Context:
             raise RuntimeError("the pfc_b200 kernels need a CUDA device (B200, sm_100a)")
         torch.cuda.init()
         h = ctypes.c_void_p()
-        check(lib().pfc_create(ctypes.byref(PfcDesc(nx, ny, nz, self.code)), ctypes.byref(h)), None,
+        opts = None if options is None else ctypes.byref(_lib.PfcOptions.from_dict(options))
+        check(lib().pfc_create_with(ctypes.byref(PfcDesc(nx, ny, nz, self.code)), opts, ctypes.byref(h)), None,
               f"pfc_create{self.shape}")
         self._h = h
         self.nxh = nx // 2 + 1
         self.n_real = nx * ny * nz
         self.n_cmpl = self.nxh * ny * nz
         self.state_bytes = int(lib().pfc_state_bytes(h))
+
+    @property
+    def options(self):
+        """The kernel schedules in effect (pfc_get_options), as a dict."""
+        o = _lib.PfcOptions()
+        check(lib().pfc_get_options(self._h, ctypes.byref(o)), self._h, "pfc_get_options")
+        return o.to_dict()
 
     # -- plumbing ---------------------------------------------------------------------
     @property
@@ -193,6 +204,10 @@ class Context:
                    float(rlim), _ptr(rows), int(capacity), ctypes.byref(nr))
         return rows[: nr.value * _lib.PFC_BOND_NCOL].view(nr.value, _lib.PFC_BOND_NCOL)
 
+    def bond_reserve(self, max_atoms, max_pairs):
+        """Grows the bond-order scratch up front (pfc_bond_order grows it on demand)."""
+        check(lib().pfc_bond_reserve(self._h, int(max_atoms), int(max_pairs)), self._h, "pfc_bond_reserve")
+
     # -- stepper ------------------------------------------------------------------------
     def step(self, kpsi, nsteps, dt, eps, lens, mu=0.0, C=1.0, namp=0.0, seed=0, counter=0):
         p = PfcStepParams(float(dt), float(eps), float(mu), float(C), float(namp), float(lens[0]),
@@ -255,3 +270,19 @@ def get_context(shape, dtype):
     if ctx is None:
         ctx = d[key] = Context(shape, dtype)
     return ctx
+
+
+def tune(shape, dtype=np.float32, cache_path=None):
+    """pfc_tune: the fastest kernel schedules for this shape and precision on the current
+    device, as (options dict, ms per step).  With a cache_path, results are read from and
+    written to that JSON file."""
+    nx, ny, nz = (int(v) for v in shape)
+    if not torch.cuda.is_available():
+        raise RuntimeError("the pfc_b200 kernels need a CUDA device (B200, sm_100a)")
+    torch.cuda.init()
+    o = _lib.PfcOptions()
+    ms = ctypes.c_double(0.0)
+    path = None if cache_path is None else os.fsencode(cache_path)
+    check(lib().pfc_tune(ctypes.byref(PfcDesc(nx, ny, nz, _NP[np.dtype(dtype)])), path, ctypes.byref(o),
+                         ctypes.byref(ms)), None, f"pfc_tune{(nx, ny, nz)}")
+    return o.to_dict(), ms.value

@@ -207,9 +207,8 @@ def bond_order_analysis(maxima, input_len, h0, h1, h2, ths, boxsize, rlim, fp=No
         dev = torch.from_numpy(np.ascontiguousarray(maxima).view(np.uint8).ravel()).cuda()
     else:
         dev = maxima
-    # a context of any shape carries the bond-order workspace; size it by the input
-    side = max(8, int(math.ceil((512.0 * max(1, input_len)) ** (1.0 / 3.0))))
-    ctx = get_context((side, side, side), dtype)
+    # a context of any shape carries the bond-order workspace, which grows with the input
+    ctx = get_context((8, 8, 8), dtype)
     rows = ctx.bond_order(dev, input_len, (h0, h1, h2), ths, boxsize, rlim).cpu().numpy()
     if fp is not None:
         write_bond_table(fp, rows)

@@ -12,7 +12,7 @@ import math
 import numpy as np
 import torch
 
-from .context import get_context
+from .context import Context, get_context
 
 # The six <110>/sqrt(2) wave vectors of the one-mode bcc ansatz (|q| = 1).
 BCC_Q = np.array([[1, 1, 0], [1, -1, 0], [1, 0, 1], [1, 0, -1], [0, 1, 1], [0, 1, -1]], dtype=np.float64) / math.sqrt(2.0)
@@ -52,10 +52,12 @@ def bcc_sphere(shape, dx, psi0, amp, radius):
 class Stepper:
     """Device state psi^ of one field and the fused step."""
 
-    def __init__(self, shape, dx, dt, eps, dtype=np.float32, mu=0.0, C=1.0, namp=0.0, seed=0, counter=0):
+    def __init__(self, shape, dx, dt, eps, dtype=np.float32, mu=0.0, C=1.0, namp=0.0, seed=0, counter=0,
+                 options=None):
         self.shape = tuple(int(v) for v in shape)
         self.dtype = np.dtype(dtype)
-        self.ctx = get_context(self.shape, self.dtype)
+        # the shared per-shape context, or a context of its own with the given kernel schedules
+        self.ctx = get_context(self.shape, self.dtype) if options is None else Context(self.shape, self.dtype, options)
         self.dx = float(dx)
         self.lens = tuple(n * self.dx for n in self.shape)
         self.hh = (self.dx, self.dx, self.dx)

@@ -63,3 +63,32 @@ def test_bond_order_from_stepper_peaks():
     assert rows.shape[0] == len(res["x"]) > 10
     for i, c in enumerate(O.BOND_COLUMNS):
         np.testing.assert_allclose(rows[:, i], res[c], atol=1e-9, err_msg=c)
+
+
+def test_bond_order_beyond_initial_scratch_many_atoms_and_neighbours():
+    """A perfect bcc crystal of 8192 sites with rlim past the eighth shell (112 neighbours
+    per atom): more atoms and neighbour entries than a context's bond-order
+    scratch starts with; the call grows it and matches the oracle.  A second call with
+    fewer atoms reuses the grown scratch."""
+    from mcstar_b200 import get_context, maximum_dtype
+    n_cells, a = 16, 4  # lattice constant 4 grid cells
+    g = np.arange(n_cells) * a
+    corners = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    idx = np.concatenate([corners, corners + a // 2])
+    idx = idx[np.lexsort((idx[:, 0], idx[:, 1], idx[:, 2]))]
+    field = 0.1 + 1e-3 * np.random.default_rng(3).uniform(size=len(idx))
+    h, box = 0.9, n_cells * a * 0.9
+    rlim = 2.25 * a * h  # the bcc shells up to sqrt(5) a: 8 + 6 + 12 + 24 + 8 + 6 + 24 + 24 = 112 neighbours
+    ctx = get_context((64, 64, 64), np.float32)
+    for take in (len(idx), 3000):
+        M = np.zeros(take, dtype=maximum_dtype(np.float32))
+        M["i0"], M["i1"], M["i2"] = idx[:take, 0], idx[:take, 1], idx[:take, 2]
+        M["field"] = field[:take]
+        dev = torch.from_numpy(M.view(np.uint8).ravel().copy()).cuda()
+        rows = ctx.bond_order(dev, take, (h, h, h), 0.0, box, rlim).cpu().numpy()
+        res, nbrs = O.bond_order(idx[:take], M["field"], (h, h, h), 0.0, box, rlim)
+        if take == len(idx):
+            assert min(len(v) for v in nbrs) > 64
+        assert rows.shape[0] == len(res["x"]) == take
+        for i, c in enumerate(O.BOND_COLUMNS):
+            np.testing.assert_allclose(rows[:, i], res[c], atol=1e-9, err_msg=c)

@@ -54,50 +54,37 @@ def test_step_matches_oracle(shape, dtype, namp):
     assert rel_l2(got, want) < tol
 
 
-_VARIANT_SCRIPT = r"""
-import sys, json, math
-import numpy as np
-sys.path[:0] = [{pkg!r}, {orc!r}]
-import pfc_oracle as O
-from mcstar_b200 import Stepper
-out = {{}}
-for shape, namp in [((64, 64, 64), 0.02), ((128, 128, 16), 0.0), ((32, 16, 128), 0.05), ((256, 256, 8), 0.0),
-                    ((512, 512, 4), 0.0), ((16, 16, 512), 0.03), ((16, 8, 512), 0.0), ((64, 64, 512), 0.02)]:
-    nx, ny, nz = shape
-    st = Stepper(shape, math.pi / 4, 0.5, 0.3, dtype=np.float32, namp=namp, seed=5)
-    rng = np.random.default_rng(3)
-    k = O.r2c(-0.2 + 0.1 * rng.uniform(-1, 1, (nz, ny, nx)))
-    st.set_kspace(k.astype(np.complex64))
-    st.step(4)
-    want = O.step(k, 4, 0.5, 0.3, st.lens, shape, namp=namp, seed=5, noise_dtype=np.float32)
-    got = st.kspace()
-    out[str(shape)] = float(np.linalg.norm(got - want) / np.linalg.norm(want))
-print(json.dumps(out))
-"""
+VARIANT_SHAPES = [((64, 64, 64), 0.02), ((128, 128, 16), 0.0), ((32, 16, 128), 0.05), ((256, 256, 8), 0.0),
+                  ((512, 512, 4), 0.0), ((16, 16, 512), 0.03), ((16, 8, 512), 0.0), ((64, 64, 512), 0.02),
+                  ((128, 64, 512), 0.0), ((48, 40, 30), 0.02), ((96, 80, 1), 0.0)]
+OPTIONS = [dict(z_carry=1), dict(z_carry=0), dict(tiled=0), dict(x_pair=0), dict(z_carry=1, tiled=0),
+           dict(radix_order=1), dict(radix_order=2), dict(tile_shift=[1, 2, 1, 2]), dict(tile_shift=[3, 3, 4, 3])]
 
 
-@pytest.mark.parametrize("env", [{"PFC_Z_PIPE": "1"}, {"PFC_Z_CARRY": "1"}, {"PFC_PREFETCH": "1"},
-                                 {"PFC_Z_CARRY": "1", "PFC_PREFETCH": "1"}, {"PFC_Z_VARIANT": "5"},
-                                 {"PFC_Z_VARIANT": "1"}, {"PFC_TILED": "0"}, {"PFC_TILED": "0", "PFC_Z_VARIANT": "1"},
-                                 {"PFC_Y_VARIANT": "6"}, {"PFC_Y_VARIANT": "8"}, {"PFC_Y_VARIANT": "1"}, {"PFC_Y_VARIANT": "1", "PFC_TILED": "0"},
-                                 {"PFC_XY_MODE": "1"}, {"PFC_XY_MODE": "0"},
-                                 {"PFC_XY_MODE": "2", "PFC_SLAB": "3"}, {"PFC_X_VARIANT": "1", "PFC_Y_VARIANT": "5"}],
-                         ids=lambda e: ",".join(f"{k}={v}" for k, v in e.items()))
-def test_step_kernel_variants_match_oracle(env):
-    """The kernel variants chosen per context from the environment: the one-tile-per-CTA
-    z kernel, the cluster plane kernel, the general passes, slabbed register passes."""
-    import json
-    import os
-    import subprocess
-    import sys
-    from conftest import ROOT
-    code = _VARIANT_SCRIPT.format(pkg=os.path.join(ROOT, "mcstar-libs_b200"), orc=os.path.join(ROOT, "oracle"))
-    res = subprocess.run([sys.executable, "-c", code], env={**os.environ, **env}, capture_output=True, text=True,
-                         timeout=600)
-    assert res.returncode == 0, res.stderr[-2000:]
-    errs = json.loads(res.stdout.strip().splitlines()[-1])
-    for shape, e in errs.items():
-        assert e < 2e-6, (shape, e)
+@pytest.mark.parametrize("options", OPTIONS, ids=lambda o: ",".join(f"{k}={v}" for k, v in o.items()))
+def test_step_kernel_schedules_match_oracle(options):
+    """Every kernel schedule a context can be made with (pfc_options: the z pass carrying
+    psi^ or A, the standard or kx-tiled layout, single-row or row-pair x pass, the general
+    passes' radix order and tiles) computes the same step.  Options a shape has no kernel
+    for are refused at creation (PFC_ERR_UNSUPPORTED) and skipped."""
+    from mcstar_b200 import PfcError, Stepper
+    tried = 0
+    for shape, namp in VARIANT_SHAPES:
+        nx, ny, nz = shape
+        try:
+            st = Stepper(shape, math.pi / 4, 0.5, 0.3, dtype=F32, namp=namp, seed=5, options=options)
+        except PfcError as e:
+            assert e.status == 2, (shape, options, e)
+            continue
+        tried += 1
+        rng = np.random.default_rng(3)
+        k = O.r2c(-0.2 + 0.1 * rng.uniform(-1, 1, (nz, ny, nx)))
+        st.set_kspace(k.astype(np.complex64))
+        st.step(4)
+        want = O.step(k, 4, 0.5, 0.3, st.lens, shape, namp=namp, seed=5, noise_dtype=F32)
+        assert rel_l2(st.kspace(), want) < 2e-6, (shape, options, st.ctx.options)
+        st.ctx.close()
+    assert tried >= 3
 
 
 @pytest.mark.parametrize("shape,dtype,z_mode", [((64, 64, 64), F32, 3), ((64, 64, 512), F32, 3),
@@ -107,8 +94,6 @@ def test_stepper_layout_mode(shape, dtype, z_mode):
     """FP32 grids with register y, x and z passes carry A and the z pass input kx-tiled
     (z_mode 3); the register z pass alone keeps the standard layout (1); other shapes use
     the general z pass (0)."""
-    if "PFC_TILED" in __import__("os").environ:
-        pytest.skip("layout chosen by the environment")
     assert stepper(shape, dtype).ctx.profile_read()["z_mode"] == z_mode
 
 
