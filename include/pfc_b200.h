@@ -252,6 +252,31 @@ typedef struct pfc_step_params {
 } pfc_step_params;
 pfc_status pfc_step(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params* params);
 
+/* The same fused step with the reference's other update kernels in the propagator slot
+ * (the driver loops of eom-exp.hpp, el.hpp and el-exp.hpp run as one call):
+ *   PFC_PROP_CONSERVED      the semi-implicit conserved update above (= pfc_step)
+ *   PFC_PROP_CONSERVED_EXP  exponential time differencing of the same equation,
+ *                           psi^' = E psi^ + k^2 Q N^ - namp sqrt(N) |k| Q xi^ with
+ *                           L = k^2 ((1 - k^2)^2 + C - eps), E = exp(-L dt), Q = (E - 1)/L
+ *                           (-dt where L = 0) -- kernel_init_eom_op / kernel_update_eom,
+ *                           eom-exp.hpp:3-40
+ *   PFC_PROP_RELAX          non-conserved relaxation psi^' = (psi^ - dt N^) / (1 + dt
+ *                           ((1 - k^2)^2 + C - eps)) -- kernel_update_el, el.hpp:3-45
+ *   PFC_PROP_RELAX_EXP      its exponential form psi^' = E psi^ + Q N^, L = (1 - k^2)^2 +
+ *                           C - eps -- el-exp.hpp:3-60
+ * The relaxations move the k = 0 mode and take no noise (namp must be 0); for them
+ * *max_change (may be NULL) receives max_k |psi^'_k - psi^_k| of the last step, the value
+ * call_kernel_update_el returns (el.hpp:23-45), as a float.  The exponentials are
+ * evaluated in the field's precision. */
+typedef enum pfc_propagator {
+    PFC_PROP_CONSERVED = 0,
+    PFC_PROP_CONSERVED_EXP = 1,
+    PFC_PROP_RELAX = 2,
+    PFC_PROP_RELAX_EXP = 3
+} pfc_propagator;
+pfc_status pfc_step_prop(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params* params, int propagator,
+                         double* max_change);
+
 /* ---- ensembles (no counterpart in mcstar-libs, whose drivers run one field per process):
  * n independent fields, each with its own context (contexts and buffers must not be
  * shared between members), shape, precision and parameters, advanced together.

@@ -6,6 +6,7 @@
 #include <new>
 #include <string>
 #include <vector>
+#include "bulk.cuh"
 #include "pfc_ctx.h"
 
 using namespace pfc;
@@ -189,6 +190,9 @@ ZPropArgs zargs(const pfc_ctx* c, const pfc_step_params* p) {
     za.dev_counter = nullptr;
     za.use_noise = p->namp != 0.0;
     za.final_step = 0;
+    za.prop = PFC_PROP_CONSERVED;
+    za.maxc = nullptr;
+    za.margs = nullptr;
     return za;
 }
 
@@ -266,7 +270,7 @@ cudaError_t step_xy(pfc_ctx* ctx, void* kpsi, const pfc_step_params* p, bool las
     return traced(ctx, 1, ctx->ny > 1 ? 3 : 1, [&] {
         cudaError_t e;
         if (ctx->ny > 1) e = launch_cols(ctx, 1, 1, A, B, 1.0);
-        else e = cudaMemcpyAsync(B, A, ctx->state_bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+        else e = cudaMemcpyAsync(B, A, ctx->state_bytes * ctx->batch, cudaMemcpyDeviceToDevice, ctx->stream);
         if (e) return e;
         if ((e = launch_rows_nonlin(ctx, B, nullptr, mul, p->C, p->mu))) return e;
         return ctx->ny > 1 ? launch_cols(ctx, 1, -1, B, B, 1.0) : cudaSuccess;
@@ -295,14 +299,27 @@ cudaError_t step_z(pfc_ctx* ctx, void* kpsi, const ZPropArgs& za) {
 }  // namespace
 
 // ---- ensembles: many independent fields advanced by one CUDA graph launch -------------------
+// Members are grouped into classes of equal shape, precision, kernel schedules and shared
+// step parameters (dt, C, mu, lengths, noise on or off).  A class steps all of its members
+// with one launch per pass: its context has the members' shape with batch = members, and
+// its buffers hold every member's state and workspaces one field apart (the kernels take
+// the field from grid z).  eps, the noise amplitude, the seed and the noise counter are per
+// member (a device table).  The graph holds one branch per class.
 struct pfc_ensemble {
     std::vector<pfc_ctx*> ctx;
     std::vector<void*> kpsi;
     std::vector<pfc_step_params> p;
-    std::vector<cudaStream_t> st;
-    std::vector<cudaEvent_t> join;
+    struct Class {
+        pfc_ctx* cc = nullptr;              // the class context (batch = members)
+        std::vector<int> members;           // member indices, in batch order
+        void* state = nullptr;              // the members' psi^ buffers (the kpsi role), one field apart
+        MemberArgs* margs = nullptr;        // per-member eps, noise amplitude, seed (device)
+        unsigned long long* ctr = nullptr;  // per-member noise counters (device)
+        cudaStream_t st = nullptr;
+        cudaEvent_t join = nullptr;
+    };
+    std::vector<Class> cls;
     cudaEvent_t fork = nullptr;
-    unsigned long long* ctr = nullptr;  // device noise counters, one per member
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int steps_per_graph = 1;
@@ -314,13 +331,48 @@ void free_ensemble(pfc_ensemble* e) {
     if (!e) return;
     if (e->exec) cudaGraphExecDestroy(e->exec);
     if (e->graph) cudaGraphDestroy(e->graph);
-    for (cudaEvent_t v : e->join)
-        if (v) cudaEventDestroy(v);
+    for (auto& k : e->cls) {
+        if (k.join) cudaEventDestroy(k.join);
+        if (k.st) cudaStreamDestroy(k.st);
+        if (k.state) cudaFree(k.state);
+        if (k.margs) cudaFree(k.margs);
+        if (k.ctr) cudaFree(k.ctr);
+        if (k.cc) free_ctx(k.cc);
+    }
     if (e->fork) cudaEventDestroy(e->fork);
-    for (cudaStream_t s : e->st)
-        if (s) cudaStreamDestroy(s);
-    if (e->ctr) cudaFree(e->ctr);
     delete e;
+}
+
+// Members that may share a class: same shape, precision, schedules and shared parameters.
+bool same_class(const pfc_ctx* a, const pfc_step_params& pa, const pfc_ctx* b, const pfc_step_params& pb) {
+    const pfc_options &oa = a->opt, &ob = b->opt;
+    return a->nx == b->nx && a->ny == b->ny && a->nz == b->nz && a->dtype == b->dtype && oa.z_carry == ob.z_carry &&
+           oa.x_pair == ob.x_pair && oa.tiled == ob.tiled && oa.radix_order == ob.radix_order &&
+           std::memcmp(oa.tile_shift, ob.tile_shift, sizeof(oa.tile_shift)) == 0 && pa.dt == pb.dt && pa.C == pb.C &&
+           pa.mu == pb.mu && pa.lx == pb.lx && pa.ly == pb.ly && pa.lz == pb.lz && (pa.namp != 0.0) == (pb.namp != 0.0);
+}
+
+// A context of the shape and schedules of `like` holding m fields (batch = m).
+cudaError_t make_class_context(const pfc_ctx* like, int m, pfc_ctx** out) {
+    pfc_desc d{like->nx, like->ny, like->nz, like->dtype};
+    pfc_ctx* c = nullptr;
+    if (pfc_create_with(&d, &like->opt, &c) != PFC_OK) return cudaErrorMemoryAllocation;
+    cudaFree(c->work);
+    cudaFree(c->work2);
+    cudaFree(c->k0);
+    c->work = c->work2 = nullptr;
+    c->k0 = nullptr;
+    cudaError_t e = cudaMalloc(&c->work, c->state_bytes * m);
+    if (!e) e = cudaMalloc(&c->work2, c->state_bytes * m);
+    if (!e) e = cudaMalloc((void**)&c->k0, sizeof(double2) * m);
+    if (e) {
+        free_ctx(c);
+        return e;
+    }
+    c->batch = m;
+    c->mstride = (int64_t)c->n_cmpl;
+    *out = c;
+    return cudaSuccess;
 }
 }  // namespace
 
@@ -687,22 +739,42 @@ pfc_status pfc_bond_reserve(pfc_ctx* ctx, int max_atoms, long long max_pairs) {
 
 // ---- stepper ------------------------------------------------------------------------------
 pfc_status pfc_step(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params* p) {
+    return pfc_step_prop(ctx, kpsi, nsteps, p, PFC_PROP_CONSERVED, nullptr);
+}
+
+pfc_status pfc_step_prop(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params* p, int propagator,
+                         double* max_change) {
     PFC_CHECK_CTX();
     if (!kpsi || !p || nsteps < 0) return fail(ctx, PFC_ERR_INVALID, "pfc_step: bad arguments");
+    if (propagator < PFC_PROP_CONSERVED || propagator > PFC_PROP_RELAX_EXP)
+        return fail(ctx, PFC_ERR_INVALID, "pfc_step_prop: unknown propagator");
+    const bool relax = propagator == PFC_PROP_RELAX || propagator == PFC_PROP_RELAX_EXP;
+    if (relax && p->namp != 0.0)
+        return fail(ctx, PFC_ERR_INVALID, "pfc_step_prop: the relaxation propagators take no noise (el.hpp)");
+    if (max_change) *max_change = 0.0;
     if (nsteps == 0) return PFC_OK;
     ZPropArgs za = zargs(ctx, p);
-    PFC_CUDA(cudaMemsetAsync(ctx->flag, 0, sizeof(int), ctx->stream), "pfc_step flag");
+    za.prop = propagator;
+    // flag[0]: the watchdog and wait status; flag[2]: the last step's largest mode change
+    PFC_CUDA(cudaMemsetAsync(ctx->flag, 0, 3 * sizeof(int), ctx->stream), "pfc_step flag");
     PFC_CUDA(step_entry(ctx, kpsi), "pfc_step entry");
     for (int t = 0; t < nsteps; ++t) {
         PFC_CUDA(step_xy(ctx, kpsi, p, t == nsteps - 1), "pfc_step xy");
         za.counter = p->counter + (uint64_t)t;
         za.final_step = (t == nsteps - 1);  // the last step writes psi^ itself
+        za.maxc = relax && za.final_step ? reinterpret_cast<unsigned*>(ctx->flag + 2) : nullptr;
         PFC_CUDA(step_z(ctx, kpsi, za), "pfc_step z");
     }
-    int flag = 0;
-    PFC_CUDA(cudaMemcpyAsync(&flag, ctx->flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "pfc_step copy flag");
+    int flag[3] = {0, 0, 0};
+    PFC_CUDA(cudaMemcpyAsync(flag, ctx->flag, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream), "pfc_step copy flag");
     PFC_CUDA(cudaStreamSynchronize(ctx->stream), "pfc_step sync");
-    if (flag) return fail(ctx, PFC_ERR_NONFINITE, "pfc_step: non-finite value in the state");
+    if (flag[0] & kFlagWaitTimeout) return fail(ctx, PFC_ERR_CUDA, "pfc_step: a device wait timed out");
+    if (flag[0]) return fail(ctx, PFC_ERR_NONFINITE, "pfc_step: non-finite value in the state");
+    if (max_change) {
+        float m;
+        std::memcpy(&m, &flag[2], sizeof(float));
+        *max_change = (double)m;
+    }
     return PFC_OK;
 }
 
@@ -921,49 +993,71 @@ pfc_status pfc_ensemble_create(int n, pfc_ctx* const* ctxs, void* const* kpsis, 
     e->kpsi.assign(kpsis, kpsis + n);
     e->p.assign(params, params + n);
     e->steps_per_graph = steps_per_graph;
-    e->st.assign(n, nullptr);
-    e->join.assign(n, nullptr);
-    cudaError_t ce = cudaMalloc(&e->ctr, sizeof(unsigned long long) * n);
-    for (int i = 0; i < n && !ce; ++i) {
-        ce = cudaStreamCreateWithFlags(&e->st[i], cudaStreamNonBlocking);
-        if (!ce) ce = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming);
+    for (int i = 0; i < n; ++i) {
+        bool placed = false;
+        for (auto& k : e->cls) {
+            const int j = k.members[0];
+            if (same_class(e->ctx[j], e->p[j], e->ctx[i], e->p[i])) {
+                k.members.push_back(i);
+                placed = true;
+                break;
+            }
+        }
+        if (!placed) {
+            e->cls.emplace_back();
+            e->cls.back().members.push_back(i);
+        }
+    }
+    cudaError_t ce = cudaSuccess;
+    for (auto& k : e->cls) {
+        if (ce) break;
+        const int m = (int)k.members.size();
+        const pfc_ctx* like = e->ctx[k.members[0]];
+        ce = make_class_context(like, m, &k.cc);
+        if (!ce) ce = cudaMalloc(&k.state, like->state_bytes * m);
+        if (!ce) ce = cudaMalloc((void**)&k.margs, sizeof(MemberArgs) * m);
+        if (!ce) ce = cudaMalloc((void**)&k.ctr, sizeof(unsigned long long) * m);
+        if (!ce) {
+            std::vector<MemberArgs> h(m);
+            for (int q = 0; q < m; ++q) {
+                const int i = k.members[q];
+                const ZPropArgs za = zargs(e->ctx[i], &e->p[i]);
+                h[q] = MemberArgs{za.eps, za.namp_eff, za.seed};
+            }
+            ce = cudaMemcpy(k.margs, h.data(), sizeof(MemberArgs) * m, cudaMemcpyHostToDevice);
+        }
+        if (!ce) ce = cudaStreamCreateWithFlags(&k.st, cudaStreamNonBlocking);
+        if (!ce) ce = cudaEventCreateWithFlags(&k.join, cudaEventDisableTiming);
     }
     if (!ce) ce = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
     cudaStream_t cap = nullptr;
     if (!ce) ce = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
-    std::vector<cudaStream_t> saved(n);
-    std::vector<bool> prof(n);
-    for (int i = 0; i < n; ++i) {
-        saved[i] = e->ctx[i]->stream;
-        prof[i] = e->ctx[i]->prof_on;
-        e->ctx[i]->prof_on = false;  // no event brackets inside the graph
-    }
-    // One graph: a fork, steps_per_graph steps of every member on its own branch, a join.
+    // One graph: a fork, steps_per_graph steps of every class on its own branch (one launch
+    // per pass for all of the class's members), a join.
     if (!ce) ce = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (!ce) {
         cudaError_t ie = cudaEventRecord(e->fork, cap);
-        for (int i = 0; i < n && !ie; ++i) {
-            pfc_ctx* c = e->ctx[i];
-            c->stream = e->st[i];
-            ie = cudaStreamWaitEvent(e->st[i], e->fork, 0);
-            ZPropArgs za = zargs(c, &e->p[i]);
-            za.dev_counter = e->ctr + i;
+        for (auto& k : e->cls) {
+            if (ie) break;
+            pfc_ctx* c = k.cc;
+            c->stream = k.st;
+            ie = cudaStreamWaitEvent(k.st, e->fork, 0);
+            const pfc_step_params& p0 = e->p[k.members[0]];
+            ZPropArgs za = zargs(c, &p0);
+            za.dev_counter = k.ctr;
+            za.margs = k.margs;
             for (int s = 0; s < steps_per_graph && !ie; ++s) {
-                ie = step_xy(c, e->kpsi[i], &e->p[i], false);
-                if (!ie) ie = step_z(c, e->kpsi[i], za);
-                if (!ie) ie = launch_counter(e->st[i], e->ctr + i, 0, 0);
+                ie = step_xy(c, k.state, &p0, false);
+                if (!ie) ie = step_z(c, k.state, za);
+                if (!ie) ie = launch_counter(k.st, k.ctr, 0, 0, (int)k.members.size());
             }
-            if (!ie) ie = cudaEventRecord(e->join[i], e->st[i]);
-            if (!ie) ie = cudaStreamWaitEvent(cap, e->join[i], 0);
+            if (!ie) ie = cudaEventRecord(k.join, k.st);
+            if (!ie) ie = cudaStreamWaitEvent(cap, k.join, 0);
         }
         ce = cudaStreamEndCapture(cap, &e->graph);
         if (!ce) ce = ie;
     }
     if (!ce) ce = cudaGraphInstantiate(&e->exec, e->graph, 0);
-    for (int i = 0; i < n; ++i) {
-        e->ctx[i]->stream = saved[i];
-        e->ctx[i]->prof_on = prof[i];
-    }
     if (cap) cudaStreamDestroy(cap);
     if (ce) {
         cudaGetLastError();
@@ -984,20 +1078,41 @@ pfc_status pfc_ensemble_run(pfc_ensemble* e, int nsteps, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     const int n = (int)e->ctx.size();
     std::vector<cudaStream_t> saved(n);
+    for (int i = 0; i < n; ++i) saved[i] = e->ctx[i]->stream;
     cudaError_t ce = cudaSuccess;
-    for (int i = 0; i < n && !ce; ++i) {
-        pfc_ctx* c = e->ctx[i];
-        saved[i] = c->stream;
-        c->stream = st;
-        ce = cudaMemsetAsync(c->flag, 0, sizeof(int), st);
-        if (!ce) ce = launch_counter(st, e->ctr + i, e->p[i].counter, 1);
-        if (!ce) ce = step_entry(c, e->kpsi[i]);
+    // each member to its carried form (its own context), then into its class's slot: the
+    // psi^ buffer, work2 (the carried field of the tiled and psi^-carrying schedules) and k0
+    for (auto& k : e->cls) {
+        if (ce) break;
+        const size_t S = k.cc->state_bytes;
+        ce = cudaMemsetAsync(k.cc->flag, 0, sizeof(int), st);
+        for (int q = 0; q < (int)k.members.size() && !ce; ++q) {
+            const int i = k.members[q];
+            pfc_ctx* c = e->ctx[i];
+            c->stream = st;
+            ce = step_entry(c, e->kpsi[i]);
+            if (!ce) ce = cudaMemcpyAsync((char*)k.state + q * S, e->kpsi[i], S, cudaMemcpyDeviceToDevice, st);
+            if (!ce) ce = cudaMemcpyAsync((char*)k.cc->work2 + q * S, c->work2, S, cudaMemcpyDeviceToDevice, st);
+            if (!ce) ce = cudaMemcpyAsync(k.cc->k0 + q, c->k0, sizeof(double2), cudaMemcpyDeviceToDevice, st);
+            if (!ce) ce = launch_counter(st, k.ctr + q, e->p[i].counter, 1);
+        }
     }
     for (int r = 0; r < nsteps / e->steps_per_graph && !ce; ++r) ce = cudaGraphLaunch(e->exec, st);
-    for (int i = 0; i < n && !ce; ++i) ce = step_exit(e->ctx[i], e->kpsi[i]);
-    std::vector<int> flags(n, 0);
-    for (int i = 0; i < n && !ce; ++i)
-        ce = cudaMemcpyAsync(&flags[i], e->ctx[i]->flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+    // back from the class slots, then each member to psi^
+    for (auto& k : e->cls) {
+        if (ce) break;
+        const size_t S = k.cc->state_bytes;
+        for (int q = 0; q < (int)k.members.size() && !ce; ++q) {
+            const int i = k.members[q];
+            pfc_ctx* c = e->ctx[i];
+            ce = cudaMemcpyAsync(e->kpsi[i], (char*)k.state + q * S, S, cudaMemcpyDeviceToDevice, st);
+            if (!ce) ce = cudaMemcpyAsync(c->work2, (char*)k.cc->work2 + q * S, S, cudaMemcpyDeviceToDevice, st);
+            if (!ce) ce = step_exit(c, e->kpsi[i]);
+        }
+    }
+    std::vector<int> flags(e->cls.size(), 0);
+    for (size_t k = 0; k < e->cls.size() && !ce; ++k)
+        ce = cudaMemcpyAsync(&flags[k], e->cls[k].cc->flag, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (!ce) ce = cudaStreamSynchronize(st);
     for (int i = 0; i < n; ++i) e->ctx[i]->stream = saved[i];
     if (ce) {
@@ -1005,9 +1120,10 @@ pfc_status pfc_ensemble_run(pfc_ensemble* e, int nsteps, void* stream) {
         return PFC_ERR_CUDA;
     }
     for (int i = 0; i < n; ++i) e->p[i].counter += (uint64_t)nsteps;
-    for (int i = 0; i < n; ++i)
-        if (flags[i]) {
-            e->err = "pfc_ensemble_run: non-finite value in member " + std::to_string(i);
+    for (size_t k = 0; k < e->cls.size(); ++k)
+        if (flags[k]) {
+            e->err = "pfc_ensemble_run: non-finite value in member " + std::to_string(e->cls[k].members[0]) +
+                     (e->cls[k].members.size() > 1 ? " or another member of its shape" : "");
             return PFC_ERR_NONFINITE;
         }
     return PFC_OK;

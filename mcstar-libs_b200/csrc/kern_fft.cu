@@ -15,7 +15,9 @@ namespace {
 template <typename T, int DIR>
 __global__ void __launch_bounds__(256) k_cols(const cx<T>* __restrict__ in, cx<T>* out, int ni, int64_t es,
                                               int64_t os, LinePlan p, const cx<T>* __restrict__ tw, int tile,
-                                              T scale) {
+                                              T scale, int64_t ms) {
+    in += blockIdx.z * ms;  // fields of a batch (grid z)
+    out += blockIdx.z * ms;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
     const int n = p.n;
@@ -126,7 +128,9 @@ __device__ __forceinline__ T cubic(T v, T mul, T C, T mu) {
 template <typename T>
 __global__ void __launch_bounds__(256) k_rows_nonlin(cx<T>* buf, const T* __restrict__ pot, int nrows, int nx,
                                                      LinePlan p, const cx<T>* __restrict__ tw,
-                                                     const cx<T>* __restrict__ post, int rpc, T mul, T C, T mu) {
+                                                     const cx<T>* __restrict__ post, int rpc, T mul, T C, T mu,
+                                                     int64_t ms) {
+    buf += blockIdx.z * ms;  // fields of a batch (grid z; no potential then)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
     const int L = p.n;
@@ -186,12 +190,26 @@ struct ZArgsT {
     uint64_t seed, counter;
     const unsigned long long* dev_counter;  // read instead of counter when set
     int use_noise, final_step;
+    unsigned* maxc;                         // relaxations: max |psi^' - psi^| (float bits), or null
+    const MemberArgs* margs;                // batched fields: per-field eps, noise amplitude, seed
 };
 
-template <typename T>
+template <typename T, int PROP>
 __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict__ B, int nx, int ny, int nz,
                                                LinePlan p, const cx<T>* __restrict__ tw, int tile, ZArgsT<T> a,
-                                               const double2* __restrict__ k0, int* flag, int col0, int col_end) {
+                                               const double2* __restrict__ k0, int* flag, int col0, int col_end,
+                                               int64_t ms) {
+    // fields of a batch (grid z): their own state, k0, noise counter and parameters
+    A += blockIdx.z * ms;
+    B += blockIdx.z * ms;
+    k0 += blockIdx.z;
+    if (a.dev_counter) a.dev_counter += blockIdx.z;
+    if (a.margs) {
+        const MemberArgs m = a.margs[blockIdx.z];
+        a.eps = (T)m.eps;
+        a.namp_eff = (T)m.namp_eff;
+        a.seed = m.seed;
+    }
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int bad;
     cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
@@ -215,6 +233,7 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
     cx<T>* other = (r == b0) ? b1 : b0;
     const T k1 = kwave<T>(ky, ny, a.ly);
     const T deps = T(1) + a.C - a.eps;
+    float mc = 0.f;
     for (int e = threadIdx.x; e < nt * n; e += blockDim.x) {
         const int i = e / n, kz = e - i * n;
         const int kx = i0 + i;
@@ -222,23 +241,42 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
         const cx<T> nl = r[(tile + i) * n + kz];
         const T kk0 = kwave<T>(kx, nx, a.lx), kk2 = kwave<T>(kz, nz, a.lz);
         const T dopx = -kk0 * kk0 - k1 * k1 - kk2 * kk2;
-        const T dopy = dopx * dopx;
-        const T denom = T(1) - a.dt * (deps * dopx + T(2) * dopy + dopx * dopy);
-        if (kx == 0 && ky == 0 && kz == 0) psi = mkc<T>((T)k0->x, (T)k0->y);
-        const T f = a.dt * dopx;
-        cx<T> num = mkc<T>(psi.x + f * nl.x, psi.y + f * nl.y);
-        if (a.use_noise) {
-            const T kabs = sqrt(-dopx);
-            const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
-            const cx<T> xi = kspace_noise<T>(kx, ky, kz, nx, ny, nz, a.seed, ctr);
-            const T g = a.dt * a.namp_eff * kabs;
-            num.x += g * xi.x;
-            num.y += g * xi.y;
+        cx<T> v;
+        if constexpr (PROP == kPropConserved) {
+            const T dopy = dopx * dopx;
+            const T denom = T(1) - a.dt * (deps * dopx + T(2) * dopy + dopx * dopy);
+            if (kx == 0 && ky == 0 && kz == 0) psi = mkc<T>((T)k0->x, (T)k0->y);
+            const T f = a.dt * dopx;
+            cx<T> num = mkc<T>(psi.x + f * nl.x, psi.y + f * nl.y);
+            if (a.use_noise) {
+                const T kabs = sqrt(-dopx);
+                const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
+                const cx<T> xi = kspace_noise<T>(kx, ky, kz, nx, ny, nz, a.seed, ctr);
+                const T g = a.dt * a.namp_eff * kabs;
+                num.x += g * xi.x;
+                num.y += g * xi.y;
+            }
+            v = mkc<T>(num.x / denom, num.y / denom);
+        } else {
+            if (prop_conserved<PROP>() && kx == 0 && ky == 0 && kz == 0) psi = mkc<T>((T)k0->x, (T)k0->y);
+            T ca, cb, cg;
+            prop_coef<PROP, T>(dopx, a.dt, deps, ca, cb, cg);
+            v = mkc<T>(ca * psi.x + cb * nl.x, ca * psi.y + cb * nl.y);
+            if (prop_conserved<PROP>() && a.use_noise) {
+                const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
+                const cx<T> xi = kspace_noise<T>(kx, ky, kz, nx, ny, nz, a.seed, ctr);
+                v.x += a.namp_eff * cg * xi.x;
+                v.y += a.namp_eff * cg * xi.y;
+            }
+            if (!prop_conserved<PROP>()) {
+                const T dx = v.x - psi.x, dy = v.y - psi.y;
+                mc = fmaxf(mc, (float)sqrt(dx * dx + dy * dy));
+            }
         }
-        const cx<T> v = mkc<T>(num.x / denom, num.y / denom);
         if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
         r[i * n + kz] = v;
     }
+    if (!prop_conserved<PROP>() && a.maxc) fold_max_change(mc, a.maxc);
     __syncthreads();
     if (threadIdx.x == 0 && bad) atomicOr(flag, 1);
     cx<T>* outb = r;
@@ -262,7 +300,11 @@ cudaError_t set_attrs_T(const pfc_ctx* c) {
     if ((e = cudaFuncSetAttribute(k_rows_r2c<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
     if ((e = cudaFuncSetAttribute(k_rows_c2r<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
     if ((e = cudaFuncSetAttribute(k_rows_nonlin<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
-    if ((e = cudaFuncSetAttribute(k_zprop<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
+    if ((e = cudaFuncSetAttribute(k_zprop<T, kPropConserved>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
+    if ((e = cudaFuncSetAttribute(k_zprop<T, kPropConservedExp>, cudaFuncAttributeMaxDynamicSharedMemorySize, m)))
+        return e;
+    if ((e = cudaFuncSetAttribute(k_zprop<T, kPropRelax>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
+    if ((e = cudaFuncSetAttribute(k_zprop<T, kPropRelaxExp>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
     (void)c;
     return cudaSuccess;
 }
@@ -276,14 +318,14 @@ cudaError_t cols_T(const pfc_ctx* c, int axis, int dir, const void* in, void* ou
     int no;
     if (axis == 1) { es = c->nxh; os = (int64_t)c->ny * c->nxh; no = c->nz; }
     else { es = (int64_t)c->ny * c->nxh; os = c->nxh; no = c->ny; }
-    dim3 grid((c->nxh + ap.tile - 1) / ap.tile, no);
+    dim3 grid((c->nxh + ap.tile - 1) / ap.tile, no, c->batch);
     const cx<T>* tw = reinterpret_cast<const cx<T>*>(c->tw);
     if (dir < 0)
         k_cols<T, -1><<<grid, 256, ap.smem, c->stream>>>((const cx<T>*)in, (cx<T>*)out, c->nxh, es, os, ap.plan, tw,
-                                                           ap.tile, (T)scale);
+                                                           ap.tile, (T)scale, c->mstride);
     else
         k_cols<T, 1><<<grid, 256, ap.smem, c->stream>>>((const cx<T>*)in, (cx<T>*)out, c->nxh, es, os, ap.plan, tw,
-                                                          ap.tile, (T)scale);
+                                                          ap.tile, (T)scale, c->mstride);
     return cudaGetLastError();
 }
 
@@ -330,37 +372,45 @@ cudaError_t launch_rows_c2r(const pfc_ctx* c, const void* in, void* out) {
 
 cudaError_t launch_rows_nonlin(const pfc_ctx* c, void* buf, const void* pot, double mul, double C, double mu) {
     const int nrows = c->ny * c->nz;
-    dim3 grid((nrows + c->px.tile - 1) / c->px.tile);
+    dim3 grid((nrows + c->px.tile - 1) / c->px.tile, 1, c->batch);
+    if (pot && c->batch > 1) return cudaErrorNotSupported;
     if (c->dtype == PFC_F64) {
         const cx<double>* tw = (const cx<double>*)c->tw;
         k_rows_nonlin<double><<<grid, 256, c->px.smem, c->stream>>>((cx<double>*)buf, (const double*)pot, nrows,
                                                                      c->nx, c->px.plan, tw, tw + c->post_off,
-                                                                     c->px.tile, mul, C, mu);
+                                                                     c->px.tile, mul, C, mu, c->mstride);
     } else {
         const cx<float>* tw = (const cx<float>*)c->tw;
         k_rows_nonlin<float><<<grid, 256, c->px.smem, c->stream>>>((cx<float>*)buf, (const float*)pot, nrows, c->nx,
                                                                     c->px.plan, tw, tw + c->post_off, c->px.tile,
-                                                                    (float)mul, (float)C, (float)mu);
+                                                                    (float)mul, (float)C, (float)mu, c->mstride);
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_zprop_cols(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int col0, int ncols) {
+template <typename T, int PROP>
+void zprop_T(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int col0, int ncols) {
     const int tile = c->pzprop.tile;
-    dim3 grid((ncols + tile - 1) / tile, c->ny);
-    const int col_end = col0 + ncols;
-    if (c->dtype == PFC_F64) {
-        ZArgsT<double> t{a.dt,   a.eps,     a.C,         a.namp_eff, a.lx,        a.ly,
-                         a.lz,   a.seed,    a.counter,   a.dev_counter, a.use_noise, a.final_step};
-        k_zprop<double><<<grid, 256, c->pzprop.smem, c->stream>>>((cx<double>*)A, (const cx<double>*)B, c->nx, c->ny,
-                                                                   c->nz, c->pz.plan, (const cx<double>*)c->tw, tile,
-                                                                   t, c->k0, c->flag, col0, col_end);
-    } else {
-        ZArgsT<float> t{(float)a.dt, (float)a.eps, (float)a.C, (float)a.namp_eff, (float)a.lx, (float)a.ly,
-                        (float)a.lz, a.seed, a.counter, a.dev_counter, a.use_noise, a.final_step};
-        k_zprop<float><<<grid, 256, c->pzprop.smem, c->stream>>>((cx<float>*)A, (const cx<float>*)B, c->nx, c->ny,
-                                                                  c->nz, c->pz.plan, (const cx<float>*)c->tw, tile, t,
-                                                                  c->k0, c->flag, col0, col_end);
+    dim3 grid((ncols + tile - 1) / tile, c->ny, c->batch);
+    ZArgsT<T> t{(T)a.dt, (T)a.eps, (T)a.C, (T)a.namp_eff, (T)a.lx, (T)a.ly, (T)a.lz, a.seed, a.counter,
+                a.dev_counter, a.use_noise, a.final_step, a.maxc, a.margs};
+    k_zprop<T, PROP><<<grid, 256, c->pzprop.smem, c->stream>>>((cx<T>*)A, (const cx<T>*)B, c->nx, c->ny, c->nz,
+                                                                c->pz.plan, (const cx<T>*)c->tw, tile, t, c->k0,
+                                                                c->flag, col0, col0 + ncols, c->mstride);
+}
+
+template <int PROP>
+void zprop_dt(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int col0, int ncols) {
+    if (c->dtype == PFC_F64) zprop_T<double, PROP>(c, A, B, a, col0, ncols);
+    else zprop_T<float, PROP>(c, A, B, a, col0, ncols);
+}
+
+cudaError_t launch_zprop_cols(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int col0, int ncols) {
+    switch (a.prop) {
+        case kPropConservedExp: zprop_dt<kPropConservedExp>(c, A, B, a, col0, ncols); break;
+        case kPropRelax: zprop_dt<kPropRelax>(c, A, B, a, col0, ncols); break;
+        case kPropRelaxExp: zprop_dt<kPropRelaxExp>(c, A, B, a, col0, ncols); break;
+        default: zprop_dt<kPropConserved>(c, A, B, a, col0, ncols);
     }
     return cudaGetLastError();
 }

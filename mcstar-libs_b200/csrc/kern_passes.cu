@@ -32,12 +32,14 @@ struct YCfg {
 template <class Y, int DIR, bool kZ>
 __global__ void __launch_bounds__(Y::T, Y::MINB)
     k_ycol(const float2* in, float2* out, int nxh, int ny, int nz, int lay, const float2* __restrict__ twg,
-           float scale) {
+           float scale, int64_t ms) {
     // the columns of NY elements of kx tile blockIdx.x at plane blockIdx.y: y columns of
     // z-plane blockIdx.y (kZ false) or z columns at ky = blockIdx.y (kZ); lay & 3: the
     // layout of the input, lay >> 2: of the output (col_addr).  With the standard layout on
-    // both sides, in may equal out.
+    // both sides, in may equal out.  ms: elements between the fields of a batch (grid z).
     constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P, U = Y::U;
+    in += blockIdx.z * ms;
+    out += blockIdx.z * ms;
     extern __shared__ __align__(16) float2 sm[];
     float2* xb = sm;
     float2* tw = sm + Y::XB;
@@ -79,8 +81,11 @@ struct YCfg3 {
 // (lay as k_ycol: the layouts of in and out, y columns of z-plane blockIdx.y)
 template <class Y, int DIR>
 __global__ void __launch_bounds__(Y::T, Y::MINB)
-    k_ycol3(const float2* in, float2* out, int nxh, int nz, int lay, const float2* __restrict__ twg, float scale) {
+    k_ycol3(const float2* in, float2* out, int nxh, int nz, int lay, const float2* __restrict__ twg, float scale,
+            int64_t ms) {
     constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P;
+    in += blockIdx.z * ms;  // fields of a batch (grid z)
+    out += blockIdx.z * ms;
     extern __shared__ __align__(16) float2 sm[];
     float2* xb = sm;
     float2* tw = sm + Y::XB;  // W_NY^m, then -W_NY^m (fft_d1_to_d3)
@@ -202,8 +207,10 @@ __device__ __forceinline__ void row_tiles_r2c(const float2* rb, const float2* tw
 template <class X, int MODE>
 __global__ void __launch_bounds__(X::T, X::MINB)
     k_xrow(const float2* in, float2* out, const float* __restrict__ pot, int nrows, const float2* __restrict__ twg,
-           float mul, float Cc, float mu) {
+           float mul, float Cc, float mu, int64_t ms) {
     constexpr int NX = X::NX, M = X::M, NXH = X::NXH, E = X::E, P = X::P, U = X::U, R = X::R, LDR = X::LDR;
+    in += blockIdx.z * ms;  // fields of a batch (grid z; no potential then)
+    out += blockIdx.z * ms;
     constexpr int LIN = MODE == 1 ? M : NXH;  // input row length (float2)
     extern __shared__ __align__(16) float2 sm[];
     float2* rb = sm;
@@ -319,7 +326,7 @@ struct XPCfg {
 
 template <class X>
 __global__ void __launch_bounds__(X::T, 4) k_xpair(float2* g, int nrows, const float2* __restrict__ twg, float mul,
-                                                   float Cc, float mu) {
+                                                   float Cc, float mu, int64_t ms) {
     constexpr int NX = X::NX, E = X::E, P = X::P, NG = X::NG, T = X::T, R = X::R, NXH = X::NXH;
     constexpr int FT = (NX / 2) / kTileW;  // whole tiles; the last tile holds kx = NX/2 alone
     extern __shared__ __align__(16) float2 sm[];
@@ -327,6 +334,7 @@ __global__ void __launch_bounds__(X::T, 4) k_xpair(float2* g, int nrows, const f
     float2* tw = sm + X::BUF;
     float4* rows4 = reinterpret_cast<float4*>(buf);  // [pair][kx]: {row a, row b}
     const int tid = threadIdx.x;
+    g += blockIdx.z * ms;  // fields of a batch (grid z)
     for (int i = tid; i < NX; i += T) {
         const float2 w = twg[i];
         tw[i] = w;
@@ -398,7 +406,8 @@ template <class X>
 cudaError_t xplaunch(const pfc_ctx* c, void* b, double mul, double C, double mu, int nrows) {
     if (nrows % X::R) return cudaErrorNotSupported;
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->xpair_tw_off;
-    k_xpair<X><<<nrows / X::R, X::T, X::SMEM, c->stream>>>((float2*)b, nrows, tw, (float)mul, (float)C, (float)mu);
+    k_xpair<X><<<dim3(nrows / X::R, 1, c->batch), X::T, X::SMEM, c->stream>>>((float2*)b, nrows, tw, (float)mul,
+                                                                              (float)C, (float)mu, c->mstride);
     return cudaGetLastError();
 }
 
@@ -413,14 +422,14 @@ cudaError_t y3attr() {
 }
 template <class Y>
 cudaError_t y3launch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs, int lay) {
-    dim3 grid((c->nxh + Y::TX - 1) / Y::TX, nzs);
+    dim3 grid((c->nxh + Y::TX - 1) / Y::TX, nzs, c->batch);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->ypass_tw_off;
     if (dir > 0)
         k_ycol3<Y, 1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->nz, lay, tw,
-                                                          (float)scale);
+                                                          (float)scale, c->mstride);
     else
         k_ycol3<Y, -1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->nz, lay, tw,
-                                                           (float)scale);
+                                                           (float)scale, c->mstride);
     return cudaGetLastError();
 }
 using Y256 = YCfg<256, 16, 8>;
@@ -453,14 +462,14 @@ cudaError_t xattr() {
 template <class Y, bool kZ>
 cudaError_t collaunch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int planes, int lay,
                       int tw_off) {
-    dim3 grid((c->nxh + Y::TX - 1) / Y::TX, planes);
+    dim3 grid((c->nxh + Y::TX - 1) / Y::TX, planes, c->batch);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + tw_off;
     if (dir > 0)
         k_ycol<Y, 1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->ny, c->nz,
-                                                             lay, tw, (float)scale);
+                                                             lay, tw, (float)scale, c->mstride);
     else
         k_ycol<Y, -1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->ny, c->nz,
-                                                              lay, tw, (float)scale);
+                                                              lay, tw, (float)scale, c->mstride);
     return cudaGetLastError();
 }
 template <class Y>
@@ -474,11 +483,12 @@ cudaError_t zlaunch_fft(const pfc_ctx* c, int dir, const void* in, void* out, do
 template <class X, int MODE>
 cudaError_t xlaunch(const pfc_ctx* c, const void* in, void* out, const void* pot, double mul, double C, double mu,
                     int nrows) {
-    dim3 grid((nrows + X::R - 1) / X::R);
+    dim3 grid((nrows + X::R - 1) / X::R, 1, c->batch);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->xpass_tw_off;
     if (MODE == 3 && nrows % X::R) return cudaErrorNotSupported;  // whole tiles of rows
+    if (pot && c->batch > 1) return cudaErrorNotSupported;
     k_xrow<X, MODE><<<grid, X::T, X::SMEM, c->stream>>>((const float2*)in, (float2*)out, (const float*)pot, nrows, tw,
-                                                        (float)mul, (float)C, (float)mu);
+                                                        (float)mul, (float)C, (float)mu, c->mstride);
     return cudaGetLastError();
 }
 

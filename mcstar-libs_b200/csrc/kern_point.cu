@@ -181,9 +181,11 @@ __global__ void k_k0_restore(cx<T>* __restrict__ kpsi, const double2* k0) {
     kpsi[0] = mkc<T>((T)k0->x, (T)k0->y);
 }
 
-__global__ void k_counter(unsigned long long* ctr, unsigned long long value, int set) {
-    if (set) *ctr = value;
-    else *ctr += 1ull;
+__global__ void k_counter(unsigned long long* ctr, int n, unsigned long long value, int set) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        if (set) ctr[i] = value;
+        else ctr[i] += 1ull;
+    }
 }
 
 }  // namespace
@@ -194,8 +196,8 @@ cudaError_t launch_k0_restore(const pfc_ctx* c, void* kpsi) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_counter(cudaStream_t st, unsigned long long* ctr, unsigned long long value, int set) {
-    k_counter<<<1, 1, 0, st>>>(ctr, value, set);
+cudaError_t launch_counter(cudaStream_t st, unsigned long long* ctr, unsigned long long value, int set, int n) {
+    k_counter<<<1, 128, 0, st>>>(ctr, n, value, set);
     return cudaGetLastError();
 }
 

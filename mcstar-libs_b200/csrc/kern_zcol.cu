@@ -8,6 +8,7 @@
 //
 //  k_zcol   one tile per CTA; both halves load and transform concurrently, N^ is
 //           handed over through shared memory, then the A half finishes alone.
+#include <type_traits>
 #include "bulk.cuh"
 #include "pfc_ctx.h"
 #include "regfft.cuh"
@@ -20,7 +21,21 @@ struct ZArgsF {
     uint64_t seed, counter;
     const unsigned long long* dev_counter;      // read instead of counter when set
     int use_noise, final_step;
+    unsigned* maxc;                             // relaxations: max |psi^' - psi^| (float bits), or null
+    const MemberArgs* margs;                    // batched fields: per-field eps, noise amplitude, seed
 };
+
+// The field of a batch this CTA steps (grid z): its noise counter and parameters (the
+// kernels also take its k0 slot, k0 + blockIdx.z).
+__device__ __forceinline__ void take_member(ZArgsF& a) {
+    if (a.dev_counter) a.dev_counter += blockIdx.z;
+    if (a.margs) {
+        const MemberArgs m = a.margs[blockIdx.z];
+        a.eps = (float)m.eps;
+        a.namp_eff = (float)m.namp_eff;
+        a.seed = m.seed;
+    }
+}
 
 template <int NZ_, int E_, int TX_>
 struct ZCfg {
@@ -98,7 +113,7 @@ __device__ __forceinline__ void watch(const float2 (&v)[Z::E], bool all, bool va
 // the transforming threads (bar) first, for a scratch that is an exchange buffer other
 // threads may still be reading.  The k = 0 mode (register 0 of thread t = 0 in column
 // kx = 0 at ky = 0, where D = 1 and the noise vanishes) is set to the FP64 value k0.
-template <class Z, bool kPsiInV, bool kSync, class Bar, class OTHER, class SLOT>
+template <class Z, bool kPsiInV, bool kSync, int PROP, class Bar, class OTHER, class SLOT>
 __device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2* scratch, SLOT slot, const Bar& bar,
                                           const float* kz_tab, int kx, int ky, int t, int nx, int ny,
                                           const ZArgsF& a, const double2* k0) {
@@ -108,6 +123,7 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2
     const float k1y = (float)(ky < ny / 2 + 1 ? ky : ky - ny) * a.cky;
     const float kxy = k0x * k0x + k1y * k1y;
     const float deps = 1.0f + a.C - a.eps;
+    float mc = 0.f;
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
@@ -117,11 +133,21 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2
             const float2 n = kPsiInV ? other(kz) : v[u * P + k2];
             const float k2z = kz_tab[kz_slot(kz)];
             const float dopx = -kxy - k2z * k2z;
-            const float dopy = dopx * dopx;
-            const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
-            const float f = a.dt * dopx;
-            v[u * P + k2] = make_float2((psi.x + f * n.x) * inv, (psi.y + f * n.y) * inv);
+            if constexpr (PROP == kPropConserved) {
+                const float dopy = dopx * dopx;
+                const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
+                const float f = a.dt * dopx;
+                v[u * P + k2] = make_float2((psi.x + f * n.x) * inv, (psi.y + f * n.y) * inv);
+            } else {
+                float ca, cb, cg;
+                prop_coef<PROP, float>(dopx, a.dt, deps, ca, cb, cg);
+                const float2 w = make_float2(ca * psi.x + cb * n.x, ca * psi.y + cb * n.y);
+                if (!prop_conserved<PROP>())
+                    mc = fmaxf(mc, (w.x - psi.x) * (w.x - psi.x) + (w.y - psi.y) * (w.y - psi.y));
+                v[u * P + k2] = w;
+            }
         }
+    if (!prop_conserved<PROP>() && a.maxc) fold_max_change(sqrtf(mc), a.maxc);
     if (a.use_noise) {
         // conserved k-space noise, dt namp sqrt(N) |k| xi / D(k): a compact loop over this
         // thread's modes, staged through its own slots (kept out of the unrolled body)
@@ -136,10 +162,17 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2
             const int kz = (t * U + m / P) + E * (m % P);
             const float k2z = kz_tab[kz_slot(kz)];
             const float dopx = -kxy - k2z * k2z;
-            const float dopy = dopx * dopx;
-            const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
+            float g;
+            if constexpr (PROP == kPropConserved) {
+                const float dopy = dopx * dopx;
+                const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
+                g = a.dt * a.namp_eff * sqrtf(-dopx) * inv;
+            } else {
+                float ca, cb, cg;
+                prop_coef<PROP, float>(dopx, a.dt, deps, ca, cb, cg);
+                g = a.namp_eff * cg;
+            }
             const float2 xi = kspace_noise<float>(kx, ky, kz, nx, ny, NZ, a.seed, ctr);
-            const float g = a.dt * a.namp_eff * sqrtf(-dopx) * inv;
             float2 w = scratch[slot(kz)];
             w.x += g * xi.x;
             w.y += g * xi.y;
@@ -150,7 +183,7 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2
 #pragma unroll
             for (int k2 = 0; k2 < P; ++k2) v[u * P + k2] = scratch[slot((t * U + u) + E * k2)];
     }
-    if (kx == 0 && ky == 0 && t == 0) v[0] = make_float2((float)k0->x, (float)k0->y);
+    if (prop_conserved<PROP>() && kx == 0 && ky == 0 && t == 0) v[0] = make_float2((float)k0->x, (float)k0->y);
 }
 
 // A' (D1 after the inverse FFT, scaled) or psi^' (D2, last step) for the thread's column
@@ -172,12 +205,17 @@ __device__ __forceinline__ void store_state(float2 (&v)[Z::E], float2* A, int64_
 }
 
 // lay bits 0, 1, 2: A, B, O kx-tiled (col_addr); O may be A when their layouts agree.
-template <class Z>
+template <class Z, int PROP>
 __global__ void __launch_bounds__(Z::T, Z::MINB) k_zcol(const float2* A, const float2* __restrict__ B, float2* O,
                                                    int nx, int ny, int lay, ZArgsF a,
                                                    const double2* __restrict__ k0, int* flag,
-                                                   const float2* __restrict__ twg) {
+                                                   const float2* __restrict__ twg, int64_t ms) {
     constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, U = Z::U, TH = Z::TH;
+    A += blockIdx.z * ms;  // fields of a batch (grid z)
+    B += blockIdx.z * ms;
+    O += blockIdx.z * ms;
+    take_member(a);
+    k0 += blockIdx.z;
     extern __shared__ __align__(16) float2 sm[];
     float2* regA = sm;
     float2* regB = sm + Z::REG;
@@ -210,8 +248,8 @@ __global__ void __launch_bounds__(Z::T, Z::MINB) k_zcol(const float2* A, const f
     }
     __syncthreads();
     if (half != 0) return;
-    propagate<Z, true, true>(v, [&](int kz) { return regB[own(kz)]; }, regB, own, bar, kz_tab, kx, ky, t, nx, ny, a,
-                             k0);
+    propagate<Z, true, true, PROP>(v, [&](int kz) { return regB[own(kz)]; }, regB, own, bar, kz_tab, kx, ky, t, nx, ny,
+                                   a, k0);
     if (!a.final_step) fft_d2_to_d1<NZ, E, TX, 1, BarDyn, Z::PADG>(v, t, c, regA, tw, bar);
     watch<Z>(v, a.final_step, valid, flag);
     const ColAddr co = col_addr((lay & 4) ? 1 : 0, true, kx, ky, nxh, ny, NZ);
@@ -242,7 +280,7 @@ struct Z3Cfg {
 template <int E, bool kPadRows> __device__ __forceinline__ constexpr int d3_row(int r) {
     return kPadRows ? d3_off<E>(r) + (d3_off<E>(r) >> 7) : d3_off<E>(r);
 }
-template <class Z, bool kPsiInV, bool kSync, class Bar, bool kPadRows = false>
+template <class Z, bool kPsiInV, bool kSync, class Bar, bool kPadRows = false, int PROP = kPropConserved>
 __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int c, const Bar& bar,
                                            const float* kz_tab, int kx, int ky, int t, int nx, int ny,
                                            const ZArgsF& a, const double2* k0, float sc) {
@@ -256,6 +294,7 @@ __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int 
     const float k1y = (float)(ky < ny / 2 + 1 ? ky : ky - ny) * a.cky;
     const float kxy = k0x * k0x + k1y * k1y;
     const float deps = 1.0f + a.C - a.eps;
+    float mc = 0.f;
 #pragma unroll
     for (int r = 0; r < E; ++r) {
         const float2 o = trow[d3_row<E, kPadRows>(r) * TX];
@@ -263,11 +302,21 @@ __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int 
         const float2 n = kPsiInV ? o : v[r];
         const float k2z = tab[d3_off<E>(r) + (r >= E / 2 ? 2 : 0)];
         const float dopx = -kxy - k2z * k2z;
-        const float dopy = dopx * dopx;
-        const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy)) * sc;
-        const float f = a.dt * dopx;
-        v[r] = make_float2((psi.x + f * n.x) * inv, (psi.y + f * n.y) * inv);
+        if constexpr (PROP == kPropConserved) {
+            const float dopy = dopx * dopx;
+            const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy)) * sc;
+            const float f = a.dt * dopx;
+            v[r] = make_float2((psi.x + f * n.x) * inv, (psi.y + f * n.y) * inv);
+        } else {
+            float ca, cb, cg;
+            prop_coef<PROP, float>(dopx, a.dt, deps, ca, cb, cg);
+            const float2 w = make_float2(ca * psi.x + cb * n.x, ca * psi.y + cb * n.y);
+            if (!prop_conserved<PROP>())
+                mc = fmaxf(mc, (w.x - psi.x) * (w.x - psi.x) + (w.y - psi.y) * (w.y - psi.y));
+            v[r] = make_float2(w.x * sc, w.y * sc);
+        }
     }
+    if (!prop_conserved<PROP>() && a.maxc) fold_max_change(sqrtf(mc), a.maxc);
     if (a.use_noise) {
         if (kSync) bar.sync();
         const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
@@ -280,10 +329,17 @@ __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int 
             const int kz = kzb + off;
             const float k2z = tab[off + (r >= E / 2 ? 2 : 0)];
             const float dopx = -kxy - k2z * k2z;
-            const float dopy = dopx * dopx;
-            const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy)) * sc;
+            float g;
+            if constexpr (PROP == kPropConserved) {
+                const float dopy = dopx * dopx;
+                const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy)) * sc;
+                g = a.dt * a.namp_eff * sqrtf(-dopx) * inv;
+            } else {
+                float ca, cb, cg;
+                prop_coef<PROP, float>(dopx, a.dt, deps, ca, cb, cg);
+                g = a.namp_eff * cg * sc;
+            }
             const float2 xi = kspace_noise<float>(kx, ky, kz, nx, ny, NZ, a.seed, ctr);
-            const float g = a.dt * a.namp_eff * sqrtf(-dopx) * inv;
             float2 w = trow[row * TX];
             w.x += g * xi.x;
             w.y += g * xi.y;
@@ -292,15 +348,21 @@ __device__ __forceinline__ void propagate3(float2 (&v)[Z::E], float2* tile, int 
 #pragma unroll
         for (int r = 0; r < E; ++r) v[r] = trow[d3_row<E, kPadRows>(r) * TX];
     }
-    if (kx == 0 && ky == 0 && t == 0) v[0] = make_float2((float)k0->x * sc, (float)k0->y * sc);  // kz = 0 at r = 0
+    if (prop_conserved<PROP>() && kx == 0 && ky == 0 && t == 0)
+        v[0] = make_float2((float)k0->x * sc, (float)k0->y * sc);  // kz = 0 at r = 0
 }
 
 // LAY: the layouts of A, B, O as k_zcol's lay, fixed at compile time (0, 1 or 7)
-template <class Z, int LAY>
+template <class Z, int LAY, int PROP>
 __global__ void __launch_bounds__(Z::T, 2) k_zcol3(const float2* A, const float2* __restrict__ B, float2* O, int nx,
                                                     int ny, ZArgsF a, const double2* __restrict__ k0, int* flag,
-                                                    const float2* __restrict__ twg) {
+                                                    const float2* __restrict__ twg, int64_t ms) {
     constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, TH = Z::TH;
+    A += blockIdx.z * ms;  // fields of a batch (grid z)
+    B += blockIdx.z * ms;
+    O += blockIdx.z * ms;
+    take_member(a);
+    k0 += blockIdx.z;
     extern __shared__ __align__(16) float2 sm[];
     float2* regA = sm;
     float2* regB = sm + Z::REG;
@@ -334,8 +396,8 @@ __global__ void __launch_bounds__(Z::T, 2) k_zcol3(const float2* A, const float2
     }
     __syncthreads();
     if (half != 0) return;
-    propagate3<Z, true, false>(v, regB, c, bar, kz_tab, kx, ky, t, nx, ny, a, k0,
-                               a.final_step ? 1.0f : 1.0f / (float)NZ);
+    propagate3<Z, true, false, BarDyn, false, PROP>(v, regB, c, bar, kz_tab, kx, ky, t, nx, ny, a, k0,
+                                                    a.final_step ? 1.0f : 1.0f / (float)NZ);
     if (!a.final_step) fft_d3_to_d1<NZ, E, TX, 1, BarDyn>(v, t, c, regA, tw, bar);
     watch<Z>(v, a.final_step, valid, flag);
     if (!valid) return;
@@ -365,12 +427,17 @@ __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_grou
 // A' = IFFT_z(psi^')/nz.  Two z transforms per column instead of k_zcol's three, no FP32
 // round trip of the state per step (its rounding matches the reference's k-space
 // update), and one more read and write of the state.
-template <class Z>
+template <class Z, int PROP>
 __global__ void __launch_bounds__(Z::TH, Z::CMINB) k_zcarry(float2* kpsi, float2* A, const float2* __restrict__ B, int nx,
                                                       int ny, ZArgsF a, const double2* __restrict__ k0, int* flag,
-                                                      const float2* __restrict__ twg) {
+                                                      const float2* __restrict__ twg, int64_t ms) {
     constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, TH = Z::TH;
     static_assert(TX == 8 && (Z::U == 1 || Z::U == 2), "staging swizzle assumes 8 columns per tile");
+    kpsi += blockIdx.z * ms;  // fields of a batch (grid z)
+    A += blockIdx.z * ms;
+    B += blockIdx.z * ms;
+    take_member(a);
+    k0 += blockIdx.z;
     extern __shared__ __align__(16) float2 sm[];
     float2* xb = sm;
     float2* stg = sm + Z::REG;
@@ -401,8 +468,8 @@ __global__ void __launch_bounds__(Z::TH, Z::CMINB) k_zcarry(float2* kpsi, float2
     __syncthreads();  // psi^ staged by the other threads of the column is visible
     // the noise pass stages through the thread's own psi^ slots, read only by itself
     auto own = [&](int kz) { return stg_row<Z>(kz) * TX + c; };
-    propagate<Z, false, false>(v, [&](int kz) { return stg[own(kz)]; }, stg, own, BarCta{}, kz_tab, kx, ky, t, nx, ny,
-                               a, k0);
+    propagate<Z, false, false, PROP>(v, [&](int kz) { return stg[own(kz)]; }, stg, own, BarCta{}, kz_tab, kx, ky, t, nx,
+                                     ny, a, k0);
     if (a.final_step) watch<Z>(v, true, valid, flag);
     store_state<Z>(v, kpsi, base, zs, t, valid, true);
     if (a.final_step) return;
@@ -419,13 +486,19 @@ __global__ void __launch_bounds__(Z::TH, Z::CMINB) k_zcarry(float2* kpsi, float2
 // memory: the exchange buffer, the stage [kz][c] (a warp's four modes per register have
 // two even and two odd kz: no bank conflicts), the tail.
 // kt0: the kx tile of blockIdx.x = 0 (a launch may cover only some tiles).
-template <class Z, bool kLast>
+template <class Z, bool kLast, int PROP>
 __global__ void __launch_bounds__(Z::TH, 3) k_zcarry3(const float2* psi_in, const float2* B, float2* psi_out,
                                                        float2* A, int nx, int ny, ZArgsF a,
                                                        const double2* __restrict__ k0, int* flag,
-                                                       const float2* __restrict__ twg, int kt0) {
+                                                       const float2* __restrict__ twg, int kt0, int64_t ms) {
     constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, TH = Z::TH;
     static_assert(TX == kTileW, "the tiles of the z-tiled layout");
+    psi_in += blockIdx.z * ms;  // fields of a batch (grid z)
+    B += blockIdx.z * ms;
+    psi_out += blockIdx.z * ms;
+    if (A) A += blockIdx.z * ms;
+    take_member(a);
+    k0 += blockIdx.z;
     extern __shared__ __align__(16) float2 sm[];
     float2* xb = sm;
     float2* stg = sm + Z::REG;
@@ -455,7 +528,7 @@ __global__ void __launch_bounds__(Z::TH, 3) k_zcarry3(const float2* psi_in, cons
     fft_d1_to_d3<NZ, E, TX, -1>(v, t, c, xb, tw);
     cp_wait_all();
     __syncthreads();  // psi^ staged by the other threads of the column is visible
-    propagate3<Z, false, false>(v, stg, c, BarCta{}, kz_tab, kx, ky, t, nx, ny, a, k0, 1.0f);
+    propagate3<Z, false, false, BarCta, false, PROP>(v, stg, c, BarCta{}, kz_tab, kx, ky, t, nx, ny, a, k0, 1.0f);
     const int p = t >> 1, h = t & 1;
     if (kLast) watch<Z>(v, true, valid, flag);
     if (valid) {
@@ -496,13 +569,17 @@ struct ZBulkCfg {
     static_assert(XB == NZ * TX && NZ % PIECE == 0 && TX == kTileW, "shape");
 };
 
-template <class Z>
+template <class Z, int PROP>
 __global__ void __launch_bounds__(Z::TH, 3) k_zbulk(float2* psi, float2* BA, int nx, int ny, ZArgsF a,
                                                      const double2* __restrict__ k0, int* flag,
-                                                     const float2* __restrict__ twg) {
+                                                     const float2* __restrict__ twg, int64_t ms) {
+    psi += blockIdx.z * ms;  // fields of a batch (grid z)
+    BA += blockIdx.z * ms;
+    take_member(a);
+    k0 += blockIdx.z;
     using C = ZBulkCfg<Z>;
     constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, TH = Z::TH;
-    extern __shared__ __align__(128) float2 sm[];
+    extern __shared__ __align__(16) float2 sm[];
     float2* stp = sm;
     float2* xb = sm + C::STP;
     float2* tw = xb + C::XB;
@@ -536,7 +613,7 @@ __global__ void __launch_bounds__(Z::TH, 3) k_zbulk(float2* psi, float2* BA, int
     for (int j = 0; j < E; ++j) v[j] = xb[(t + P * j) * TX + c];
     // (fft_d1_to_d3 synchronises before its first write to xb)
     fft_d1_to_d3<NZ, E, TX, -1, BarCta, true, 0>(v, t, c, xb, tw);
-    propagate3<Z, false, false, BarCta, true>(v, stp, c, BarCta{}, kz_tab, kx, ky, t, nx, ny, a, k0, 1.0f);
+    propagate3<Z, false, false, BarCta, true, PROP>(v, stp, c, BarCta{}, kz_tab, kx, ky, t, nx, ny, a, k0, 1.0f);
     // psi^' replaced psi^ in each thread's own slots: hand them to the async proxy
     fence_async_smem();
     __syncthreads();
@@ -579,35 +656,62 @@ using Z256 = ZCfg<256, 16, 8>;
 using Z128 = ZCfg<128, 16, 8>;
 using Z64 = ZCfg<64, 8, 8>;
 
+// The propagator of a launch as a compile-time constant: f(std::integral_constant<int, PROP>).
+template <class F>
+cudaError_t by_prop(int prop, F&& f) {
+    switch (prop) {
+        case kPropConservedExp: return f(std::integral_constant<int, kPropConservedExp>{});
+        case kPropRelax: return f(std::integral_constant<int, kPropRelax>{});
+        case kPropRelaxExp: return f(std::integral_constant<int, kPropRelaxExp>{});
+        default: return f(std::integral_constant<int, kPropConserved>{});
+    }
+}
+// f(k) for the kernel of every propagator (attribute set-up)
+template <class F>
+cudaError_t each_prop(F&& f) {
+    cudaError_t e = cudaSuccess;
+    for (int p = 0; p < 4 && !e; ++p) e = by_prop(p, f);
+    return e;
+}
+
 template <class Z>
 cudaError_t zattr() {
-    cudaError_t e = cudaFuncSetAttribute(k_zcol<Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Z::SMEM);
-    if (e) return e;
-    return cudaFuncSetAttribute(k_zcarry<Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Z::SMEM_CARRY);
+    return each_prop([](auto P) {
+        cudaError_t e = cudaFuncSetAttribute(k_zcol<Z, P.value>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)Z::SMEM);
+        if (e) return e;
+        return cudaFuncSetAttribute(k_zcarry<Z, P.value>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)Z::SMEM_CARRY);
+    });
 }
 
 ZArgsF zargs_f(const ZPropArgs& p) {
     const double tp = 6.283185307179586232;
     return ZArgsF{(float)p.dt, (float)p.eps, (float)p.C, (float)p.namp_eff, (float)(tp / p.lx), (float)(tp / p.ly),
-                  (float)(tp / p.lz), p.seed, p.counter, p.dev_counter, p.use_noise, p.final_step};
+                  (float)(tp / p.lz), p.seed, p.counter, p.dev_counter, p.use_noise, p.final_step, p.maxc, p.margs};
 }
 
 template <class Z>
 cudaError_t zlaunch_carry(const pfc_ctx* c, void* kpsi, void* A, const void* B, const ZPropArgs& p) {
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
-    dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny);
-    k_zcarry<Z><<<grid, Z::TH, Z::SMEM_CARRY, c->stream>>>((float2*)kpsi, (float2*)A, (const float2*)B, c->nx, c->ny,
-                                                           zargs_f(p), c->k0, c->flag, tw);
-    return cudaGetLastError();
+    dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny, c->batch);
+    return by_prop(p.prop, [&](auto P) {
+        k_zcarry<Z, P.value><<<grid, Z::TH, Z::SMEM_CARRY, c->stream>>>(
+            (float2*)kpsi, (float2*)A, (const float2*)B, c->nx, c->ny, zargs_f(p), c->k0, c->flag, tw, c->mstride);
+        return cudaGetLastError();
+    });
 }
 
 template <class Z>
 cudaError_t zlaunch(const pfc_ctx* c, const void* A, const void* B, void* O, const ZPropArgs& p, int lay) {
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
-    dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny);
-    k_zcol<Z><<<grid, Z::T, Z::SMEM, c->stream>>>((const float2*)A, (const float2*)B, (float2*)O, c->nx, c->ny, lay,
-                                                   zargs_f(p), c->k0, c->flag, tw);
-    return cudaGetLastError();
+    dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny, c->batch);
+    return by_prop(p.prop, [&](auto P) {
+        k_zcol<Z, P.value><<<grid, Z::T, Z::SMEM, c->stream>>>((const float2*)A, (const float2*)B, (float2*)O, c->nx,
+                                                                c->ny, lay, zargs_f(p), c->k0, c->flag, tw,
+                                                                c->mstride);
+        return cudaGetLastError();
+    });
 }
 
 }  // namespace
@@ -632,26 +736,19 @@ cudaError_t set_zcol_attributes(const pfc_ctx* c) {
         case 2: return zattr<Z256>();
         case 3: return zattr<Z128>();
         case 4: return zattr<Z64>();
-        case 6: {
-            cudaError_t e = cudaFuncSetAttribute(k_zcol3<Z3_512, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)Z3_512::SMEM);
-            if (!e)
-                e = cudaFuncSetAttribute(k_zcol3<Z3_512, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)Z3_512::SMEM);
-            if (!e)
-                e = cudaFuncSetAttribute(k_zcol3<Z3_512, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)Z3_512::SMEM);
-            if (!e)
-                e = cudaFuncSetAttribute(k_zcarry3<Z3_512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)Z3_512::SMEM_CARRY);
-            if (!e)
-                e = cudaFuncSetAttribute(k_zcarry3<Z3_512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)Z3_512::SMEM_CARRY);
-            if (!e)
-                e = cudaFuncSetAttribute(k_zbulk<Z3_512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)ZBulkCfg<Z3_512>::SMEM);
-            return e;
-        }
+        case 6:
+            return each_prop([](auto P) {
+                using Z = Z3_512;
+                const int sm = (int)Z::SMEM, smc = (int)Z::SMEM_CARRY, smb = (int)ZBulkCfg<Z>::SMEM;
+                const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+                cudaError_t e = cudaFuncSetAttribute(k_zcol3<Z, 0, P.value>, attr, sm);
+                if (!e) e = cudaFuncSetAttribute(k_zcol3<Z, 1, P.value>, attr, sm);
+                if (!e) e = cudaFuncSetAttribute(k_zcol3<Z, 7, P.value>, attr, sm);
+                if (!e) e = cudaFuncSetAttribute(k_zcarry3<Z, false, P.value>, attr, smc);
+                if (!e) e = cudaFuncSetAttribute(k_zcarry3<Z, true, P.value>, attr, smc);
+                if (!e) e = cudaFuncSetAttribute(k_zbulk<Z, P.value>, attr, smb);
+                return e;
+            });
     }
     return cudaSuccess;
 }
@@ -673,24 +770,26 @@ cudaError_t launch_zcarry_tiled(const pfc_ctx* c, const void* psi_in, const void
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
     const ZArgsF za = zargs_f(a);
     const int ntx = (c->nxh + Z::TX - 1) / Z::TX;
-    if (a.final_step) {
-        k_zcarry3<Z, true><<<dim3(ntx, c->ny), Z::TH, Z::SMEM_CARRY, c->stream>>>(
-            (const float2*)psi_in, (const float2*)B, (float2*)psi_out, (float2*)A, c->nx, c->ny, za, c->k0, c->flag,
-            tw, 0);
+    return by_prop(a.prop, [&](auto P) {
+        if (a.final_step) {
+            k_zcarry3<Z, true, P.value><<<dim3(ntx, c->ny, c->batch), Z::TH, Z::SMEM_CARRY, c->stream>>>(
+                (const float2*)psi_in, (const float2*)B, (float2*)psi_out, (float2*)A, c->nx, c->ny, za, c->k0,
+                c->flag, tw, 0, c->mstride);
+            return cudaGetLastError();
+        }
+        // whole tiles with bulk copies (psi^ in place, A' over B); the partial last tile with
+        // per-thread accesses
+        const int full = c->nxh / Z::TX;
+        if (psi_in != psi_out || B != A) return cudaErrorNotSupported;
+        if (full > 0)
+            k_zbulk<Z, P.value><<<dim3(full, c->ny, c->batch), Z::TH, ZBulkCfg<Z>::SMEM, c->stream>>>(
+                (float2*)psi_out, (float2*)A, c->nx, c->ny, za, c->k0, c->flag, tw, c->mstride);
+        if (full < ntx)
+            k_zcarry3<Z, false, P.value><<<dim3(ntx - full, c->ny, c->batch), Z::TH, Z::SMEM_CARRY, c->stream>>>(
+                (const float2*)psi_in, (const float2*)B, (float2*)psi_out, (float2*)A, c->nx, c->ny, za, c->k0,
+                c->flag, tw, full, c->mstride);
         return cudaGetLastError();
-    }
-    // whole tiles with bulk copies (psi^ in place, A' over B); the partial last tile with
-    // per-thread accesses
-    const int full = c->nxh / Z::TX;
-    if (psi_in != psi_out || B != A) return cudaErrorNotSupported;
-    if (full > 0)
-        k_zbulk<Z><<<dim3(full, c->ny), Z::TH, ZBulkCfg<Z>::SMEM, c->stream>>>((float2*)psi_out, (float2*)A, c->nx,
-                                                                                 c->ny, za, c->k0, c->flag, tw);
-    if (full < ntx)
-        k_zcarry3<Z, false><<<dim3(ntx - full, c->ny), Z::TH, Z::SMEM_CARRY, c->stream>>>(
-            (const float2*)psi_in, (const float2*)B, (float2*)psi_out, (float2*)A, c->nx, c->ny, za, c->k0, c->flag,
-            tw, full);
-    return cudaGetLastError();
+    });
 }
 
 cudaError_t launch_relayout(const pfc_ctx* c, const void* in, void* out, int to_tiled) {
@@ -705,12 +804,14 @@ cudaError_t launch_zcol(const pfc_ctx* c, const void* A, const void* B, void* O,
         case 6: {
             using Z = Z3_512;
             const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
-            dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny);
-            auto k = lay == 7 ? k_zcol3<Z, 7> : lay == 1 ? k_zcol3<Z, 1> : k_zcol3<Z, 0>;
+            dim3 grid((c->nxh + Z::TX - 1) / Z::TX, c->ny, c->batch);
             if (lay != 0 && lay != 1 && lay != 7) return cudaErrorNotSupported;
-            k<<<grid, Z::T, Z::SMEM, c->stream>>>((const float2*)A, (const float2*)B, (float2*)O, c->nx, c->ny,
-                                                  zargs_f(a), c->k0, c->flag, tw);
-            return cudaGetLastError();
+            return by_prop(a.prop, [&](auto P) {
+                auto k = lay == 7 ? k_zcol3<Z, 7, P.value> : lay == 1 ? k_zcol3<Z, 1, P.value> : k_zcol3<Z, 0, P.value>;
+                k<<<grid, Z::T, Z::SMEM, c->stream>>>((const float2*)A, (const float2*)B, (float2*)O, c->nx, c->ny,
+                                                      zargs_f(a), c->k0, c->flag, tw, c->mstride);
+                return cudaGetLastError();
+            });
         }
         case 1: return zlaunch<Z512>(c, A, B, O, a, lay);
         case 2: return zlaunch<Z256>(c, A, B, O, a, lay);

@@ -61,6 +61,10 @@ struct pfc_ctx {
                                   // the x pass field row-tiled in work, the z pass input B z-tiled
                                   // in the caller's psi^ buffer
     int num_sms;                  // multiprocessors of the device the context was made on
+    // batched fields (ensembles): the step's kernels run over `batch` fields of this shape
+    // stored mstride complex elements apart (grid z = field); 1 and 0 for a single field
+    int batch = 1;
+    int64_t mstride = 0;
     int zcol_tw_off;              // twiddles of the register z kernel: W_nz^m
     int fused_y, fused_x;         // register y / x pass variants (0: none)
     int fused_zfft;               // register column kernel variant for plain z transforms (0: none)
@@ -109,6 +113,11 @@ struct ZPropArgs {
     const unsigned long long* dev_counter;
     int use_noise;
     int final_step;
+    int prop;        // kPropConserved, kPropConservedExp, kPropRelax, kPropRelaxExp (pfc_internal.cuh)
+    unsigned* maxc;  // relaxations: the largest |psi^' - psi^| of the step (float bits), or null
+    // batched fields: per-field eps, noise amplitude and seed (null: the values above for
+    // every field); k0 and dev_counter then hold one entry per field
+    const MemberArgs* margs;
 };
 cudaError_t launch_zprop(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a);
 // the general z pass over the kx columns [col0, col0 + ncols)
@@ -176,8 +185,8 @@ cudaError_t launch_noise_kspace(const pfc_ctx* c, void* arr, uint64_t seed, uint
 cudaError_t launch_noise_real(const pfc_ctx* c, void* arr, double sigma, uint64_t seed, uint64_t counter);
 cudaError_t launch_k0_save(const pfc_ctx* c, const void* kpsi);
 cudaError_t launch_k0_restore(const pfc_ctx* c, void* kpsi);
-// set (set != 0) or increment a device-side step counter
-cudaError_t launch_counter(cudaStream_t st, unsigned long long* ctr, unsigned long long value, int set);
+// set (set != 0) or increment n device-side step counters
+cudaError_t launch_counter(cudaStream_t st, unsigned long long* ctr, unsigned long long value, int set, int n = 1);
 // reduce the kRedBlocks partials in c->red into c->red[kRedBlocks + slot]
 cudaError_t launch_reduce_final(const pfc_ctx* c, int slot, double scale);
 

@@ -201,6 +201,74 @@ template <typename T> __device__ __forceinline__ T kwave(int i, int n, T len) {
 }
 
 // ---------------------------------------------------------------------------------
+// The stepper's propagators: the reference's update kernels as the per-mode map
+// psi^' = a psi^ + b N^ + g namp_eff xi^, with dopx = -k^2, dopy = k^4 and the split
+// deps = 1 + C - eps (C = 1 is the reference's split: psi3_split.hpp subtracts psi):
+//  kPropConserved     semi-implicit conserved (eom.hpp:60-72): D = 1 - dt (deps dopx + 2 dopy
+//                     + dopx dopy); a = 1/D, b = dt dopx / D, g = dt |k| / D
+//  kPropConservedExp  exponential time differencing (eom-exp.hpp:3-60): L = -dopx (deps +
+//                     2 dopx + dopy), E = exp(-L dt), Q = (E - 1)/L (-dt where L = 0, as
+//                     kernel_init_eom_op); a = E, b = -dopx Q, g = -|k| Q
+//  kPropRelax         non-conserved relaxation (el.hpp:3-45): D = 1 + dt (deps + 2 dopx +
+//                     dopy); a = 1/D, b = -dt / D; no noise
+//  kPropRelaxExp      its exponential form (el-exp.hpp:3-60): L = deps + 2 dopx + dopy,
+//                     E = exp(-L dt), Q = (E - 1)/L (-dt where L = 0); a = E, b = Q; no noise
+// The conserved propagators leave the k = 0 mode unchanged (the stepper restores it from
+// FP64); the relaxations move it.
+enum { kPropConserved = 0, kPropConservedExp = 1, kPropRelax = 2, kPropRelaxExp = 3 };
+template <int PROP> __host__ __device__ constexpr bool prop_conserved() {
+    return PROP == kPropConserved || PROP == kPropConservedExp;
+}
+
+// Per-field parameters of a batch of fields stepped by one launch (grid z = field).
+struct MemberArgs {
+    double eps, namp_eff;
+    uint64_t seed;
+};
+
+template <typename T> __device__ __forceinline__ T dev_exp(T x);
+template <> __device__ __forceinline__ float dev_exp<float>(float x) { return expf(x); }
+template <> __device__ __forceinline__ double dev_exp<double>(double x) { return exp(x); }
+
+// a, b and g (see above) of the propagators other than kPropConserved, whose kernels keep
+// their own arithmetic
+template <int PROP, typename T>
+__device__ __forceinline__ void prop_coef(T dopx, T dt, T deps, T& a, T& b, T& g) {
+    const T dopy = dopx * dopx;
+    if constexpr (PROP == kPropConservedExp) {
+        const T lin = -dopx * (deps + T(2) * dopx + dopy);
+        const T e = dev_exp<T>(-lin * dt);
+        T q = (e - T(1)) / lin;
+        if (q != q) q = -dt;
+        a = e;
+        b = -dopx * q;
+        g = -sqrt(-dopx) * q;
+    } else if constexpr (PROP == kPropRelax) {
+        const T inv = T(1) / (T(1) + dt * (deps + T(2) * dopx + dopy));
+        a = inv;
+        b = -dt * inv;
+        g = T(0);
+    } else {
+        const T lin = deps + T(2) * dopx + dopy;
+        const T e = dev_exp<T>(-lin * dt);
+        T q = (e - T(1)) / lin;
+        if (q != q) q = -dt;
+        a = e;
+        b = q;
+        g = T(0);
+    }
+}
+
+// The largest |psi^' - psi^| of a relaxation step: a warp's maximum, folded into *out
+// (float bits of a non-negative value: their integer order is the value order).  Every
+// lane of the warp calls it.
+__device__ __forceinline__ void fold_max_change(float m, unsigned* out) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(out, __float_as_uint(m));
+}
+
+// ---------------------------------------------------------------------------------
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as
 // 1, 2, 3", SC'11): 10 rounds of two 32x32->64 multiplies with Weyl key bumps.
 // ---------------------------------------------------------------------------------

@@ -30,8 +30,11 @@ EXPORTED = (
     "pfc_update_el", "pfc_init_el_op", "pfc_update_el_exp", "pfc_update_eom_py", "pfc_update_eom_hpfcnoise",
     "pfc_gaussian_init", "pfc_kmult_real", "pfc_kmult_imag", "pfc_square", "pfc_write_lowpass_2d",
     "pfc_amplitude_lowpass", "pfc_bond_reserve", "pfc_default_options", "pfc_create_with", "pfc_get_options",
-    "pfc_tune",
+    "pfc_tune", "pfc_step_prop",
 )
+
+# pfc_propagator
+PROPAGATORS = {"conserved": 0, "conserved_exp": 1, "relax": 2, "relax_exp": 3}
 
 
 class PfcError(RuntimeError):
@@ -114,6 +117,7 @@ _SIGS = {
     "pfc_bond_order": ([_P, _P, _I, _D, _D, _D, _D, _D, _D, _P, _I, ctypes.POINTER(_I)], _I),
     "pfc_bond_reserve": ([_P, _I, ctypes.c_longlong], _I),
     "pfc_step": ([_P, _P, _I, ctypes.POINTER(PfcStepParams)], _I),
+    "pfc_step_prop": ([_P, _P, _I, ctypes.POINTER(PfcStepParams), _I, ctypes.POINTER(_D)], _I),
     "pfc_free_energy": ([_P, _P, _D, _D, _D, _D, _D, _D, _D, ctypes.POINTER(_D)], _I),
     "pfc_profile_enable": ([_P, _I], _I),
     "pfc_profile_read": ([_P, ctypes.POINTER(PfcProfile)], _I),

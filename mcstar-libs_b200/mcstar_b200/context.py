@@ -209,10 +209,16 @@ class Context:
         check(lib().pfc_bond_reserve(self._h, int(max_atoms), int(max_pairs)), self._h, "pfc_bond_reserve")
 
     # -- stepper ------------------------------------------------------------------------
-    def step(self, kpsi, nsteps, dt, eps, lens, mu=0.0, C=1.0, namp=0.0, seed=0, counter=0):
+    def step(self, kpsi, nsteps, dt, eps, lens, mu=0.0, C=1.0, namp=0.0, seed=0, counter=0, propagator="conserved"):
+        """nsteps fused steps (pfc_step_prop); propagator: "conserved" (eom.hpp),
+        "conserved_exp" (eom-exp.hpp), "relax" (el.hpp), "relax_exp" (el-exp.hpp).  Returns
+        the last step's largest mode change for the relaxations, else 0."""
         p = PfcStepParams(float(dt), float(eps), float(mu), float(C), float(namp), float(lens[0]),
                           float(lens[1]), float(lens[2]), int(seed), int(counter))
-        self._call("pfc_step", _ptr(kpsi), int(nsteps), ctypes.byref(p))
+        m = ctypes.c_double(0.0)
+        self._call("pfc_step_prop", _ptr(kpsi), int(nsteps), ctypes.byref(p), _lib.PROPAGATORS[propagator],
+                   ctypes.byref(m))
+        return m.value
 
     # -- reverse mode --------------------------------------------------------------------
     def adjoint_workspace(self):

@@ -95,10 +95,13 @@ class Stepper:
         self.kpsi.copy_(torch.from_numpy(np.ascontiguousarray(k).view(self.dtype).ravel()))
 
     # -- dynamics and observables --------------------------------------------------------------
-    def step(self, nsteps):
-        self.ctx.step(self.kpsi, nsteps, self.dt, self.eps, self.lens, mu=self.mu, C=self.C, namp=self.namp,
-                      seed=self.seed, counter=self.counter)
+    def step(self, nsteps, propagator="conserved"):
+        """Advances nsteps fused steps; returns the last step's largest mode change for the
+        relaxation propagators (else 0)."""
+        m = self.ctx.step(self.kpsi, nsteps, self.dt, self.eps, self.lens, mu=self.mu, C=self.C, namp=self.namp,
+                          seed=self.seed, counter=self.counter, propagator=propagator)
         self.counter += int(nsteps)
+        return m
 
     def free_energy(self):
         return self.ctx.free_energy(self.kpsi, self.eps, self.lens, self.hh)

@@ -22,7 +22,8 @@ What each function restates (reference paths relative to the mcstar-libs root):
 * ``bond_order``         -- ``bond_order_analysis`` and helpers,
                             bond-order-analysis/bond-order.cpp:53-349
 * ``step``               -- the driver loop of one conserved step (copy, C2R,
-                            psi3_split(norm), R2C, [noise], update_eom)
+                            psi3_split(norm), R2C, [noise], update_eom), or with the
+                            updates of eom-exp.hpp, el.hpp, el-exp.hpp (``propagate``)
 * ``fill_kspace``        -- the k-space noise contract of ``NoiseHostApi::fill_kspace``
                             (cuda/noise.hpp:7-142): complex normal modes with
                             E|xi|^2 = 1, Hermitian pairs on the i0 = 0 and i0 = nx/2
@@ -425,17 +426,54 @@ def fill_real(n, sigma, seed, counter, dtype=np.float32):
 # ----------------------------------------------------------------------------------
 # the step
 # ----------------------------------------------------------------------------------
+def propagate(kpsi, knl, knoise, namp, dt, eps, lens, shape_xyz, C, propagator):
+    """One update of the fused stepper's other propagators, in full precision (the fused
+    kernels evaluate exp in the field's precision), with the stabilisation C
+    (deps = 1 + C - eps; C = 1 is the reference's split):
+      "conserved_exp"  eom-exp.hpp:3-60   psi^' = E psi^ - dop.x Q N^ - namp sqrt(N) |k| Q xi^,
+                       L = -dop.x (deps + 2 dop.x + dop.y), E = exp(-L dt), Q = (E-1)/L (-dt at L = 0)
+      "relax"          el.hpp:3-25         psi^' = (psi^ - dt N^) / (1 + dt (deps + 2 dop.x + dop.y))
+      "relax_exp"      el-exp.hpp:3-40     psi^' = E psi^ + Q N^, L = deps + 2 dop.x + dop.y
+    Returns (psi^', max_k |psi^' - psi^|)."""
+    dx, dy = _dops(shape_xyz, lens)
+    deps = 1.0 + C - eps
+    if propagator == "conserved_exp":
+        lin = -dx * (deps + 2.0 * dx + dy)
+        e = np.exp(-lin * dt)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            q = (e - 1.0) / lin
+        q = np.where(np.isnan(q), -dt, q)
+        new = e * kpsi - dx * q * knl
+        if knoise is not None:
+            nx, ny, nz = shape_xyz
+            new = new - namp * np.sqrt(float(nx * ny * nz)) * np.sqrt(-dx) * q * knoise
+    elif propagator == "relax":
+        new = (kpsi - dt * knl) / (1.0 + dt * (deps + 2.0 * dx + dy))
+    elif propagator == "relax_exp":
+        lin = deps + 2.0 * dx + dy
+        e = np.exp(-lin * dt)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            q = (e - 1.0) / lin
+        new = e * kpsi + np.where(np.isnan(q), -dt, q) * knl
+    else:
+        raise ValueError(propagator)
+    return new, float(np.max(np.abs(new - kpsi)))
+
+
 def step(kpsi, nsteps, dt, eps, lens, shape_xyz, mu=0.0, C=1.0, namp=0.0,
-         seed=0, counter0=0, workers=None, dtype=np.float64, noise_dtype=None, ref_float_sqrt=False):
-    """nsteps conserved semi-implicit steps: the driver loop of the reference
-    (copy, C2R, psi3_split(norm=True), R2C, [fill_kspace], update_eom).
-    noise_dtype selects the precision of the Philox draw (that of the field being
-    compared); the fused stepper evaluates sqrt(N) and |k| in full precision, hence
-    ref_float_sqrt=False by default here."""
+         seed=0, counter0=0, workers=None, dtype=np.float64, noise_dtype=None, ref_float_sqrt=False,
+         propagator="conserved", return_max_change=False):
+    """nsteps steps of the driver loop of the reference (copy, C2R, psi3_split(norm=True),
+    R2C, [fill_kspace], update): the conserved semi-implicit update (eom.hpp:60-72) or,
+    with `propagator`, one of the updates of ``propagate``.  noise_dtype selects the
+    precision of the Philox draw (that of the field being compared); the fused stepper
+    evaluates sqrt(N) and |k| in full precision, hence ref_float_sqrt=False by default
+    here.  return_max_change: also return the last step's max_k |psi^' - psi^|."""
     real_t = np.dtype(dtype)
     cmpl_t = np.complex128 if real_t == np.float64 else np.complex64
     noise_t = real_t if noise_dtype is None else np.dtype(noise_dtype)
     kpsi = kpsi.astype(cmpl_t)
+    change = 0.0
     for t in range(nsteps):
         psi = c2r(kpsi, shape_xyz, workers=workers).astype(real_t)
         nl = psi3_split(psi, None, mu, norm=True, C=C).astype(real_t)
@@ -443,9 +481,13 @@ def step(kpsi, nsteps, dt, eps, lens, shape_xyz, mu=0.0, C=1.0, namp=0.0,
         knoise = None
         if namp != 0.0:
             knoise = fill_kspace(shape_xyz, seed, counter0 + t, dtype=noise_t)
-        kpsi = update_eom(kpsi, knl, knoise, namp, dt, eps, lens, shape_xyz, C=C,
-                          ref_float_sqrt=ref_float_sqrt).astype(cmpl_t)
-    return kpsi
+        if propagator == "conserved":
+            new = update_eom(kpsi, knl, knoise, namp, dt, eps, lens, shape_xyz, C=C, ref_float_sqrt=ref_float_sqrt)
+        else:
+            new, change = propagate(kpsi.astype(np.complex128), knl.astype(np.complex128), knoise, namp, dt, eps,
+                                    lens, shape_xyz, C, propagator)
+        kpsi = new.astype(cmpl_t)
+    return (kpsi, change) if return_max_change else kpsi
 
 
 # ----------------------------------------------------------------------------------

@@ -11,11 +11,17 @@ pytestmark = pytest.mark.gpu
 
 
 def _members():
+    """Members of mixed shapes; several share a shape (and so one batched launch per pass)
+    with their own eps, psi0, noise amplitude and seed."""
     mk = lambda shape, eps, psi0, seed, namp: dict(shape=shape, dx=math.pi / 4, dt=0.5, eps=eps, psi0=psi0,
                                                    seed=seed, namp=namp)
     return [mk((64, 64, 1), 0.25, -0.25, 11, 0.03), mk((32, 32, 32), 0.3, -0.2, 12, 0.05),
             mk((48, 40, 30), 0.2, -0.3, 13, 0.0), mk((96, 96, 1), 0.35, -0.18, 14, 0.02),
-            mk((64, 64, 64), 0.3, -0.2, 15, 0.0)]
+            mk((64, 64, 64), 0.3, -0.2, 15, 0.0), mk((64, 64, 1), 0.15, -0.3, 16, 0.01),
+            mk((64, 64, 1), 0.4, -0.2, 17, 0.05), mk((32, 32, 32), 0.2, -0.25, 18, 0.02),
+            mk((48, 40, 30), 0.35, -0.2, 19, 0.0), mk((64, 64, 64), 0.2, -0.3, 20, 0.0),
+            mk((64, 64, 64), 0.25, -0.22, 21, 0.02), mk((32, 16, 512), 0.3, -0.2, 22, 0.01),
+            mk((32, 16, 512), 0.25, -0.25, 23, 0.02)]
 
 
 @pytest.mark.parametrize("spg", [1, 3])

@@ -1,0 +1,52 @@
+"""The fused stepper with the reference's other update kernels in its propagator slot
+(pfc_step_prop): exponential time differencing of the conserved equation (eom-exp.hpp),
+the non-conserved relaxation (el.hpp) and its exponential form (el-exp.hpp).  Each is
+checked against the oracle's driver loop (C2R, psi3_split, R2C, update) on every kernel
+family of the stepper: the general passes (FP64 and odd shapes), the register passes
+(standard and kx-tiled layouts), the 512-point z kernels carrying A or psi^ -- and the
+relaxations' largest mode change against the oracle's (call_kernel_update_el)."""
+import math
+
+import numpy as np
+import pytest
+
+import pfc_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+CASES = [((16, 12, 10), np.float64, None), ((24, 20, 1), np.float64, None), ((48, 40, 30), np.float32, None),
+         ((64, 64, 64), np.float32, None), ((32, 16, 128), np.float32, None), ((64, 64, 512), np.float32, None),
+         ((64, 64, 512), np.float32, dict(z_carry=1)), ((128, 64, 256), np.float32, dict(tiled=0))]
+
+
+@pytest.mark.parametrize("propagator", ["conserved_exp", "relax", "relax_exp"])
+@pytest.mark.parametrize("shape,dtype,options", CASES, ids=lambda v: str(v))
+def test_fused_propagators_match_oracle(shape, dtype, options, propagator):
+    from mcstar_b200 import Stepper
+    nx, ny, nz = shape
+    namp = 0.03 if propagator == "conserved_exp" else 0.0
+    st = Stepper(shape, math.pi / 4, 0.3, 0.3, dtype=dtype, namp=namp, seed=21, mu=0.05, options=options)
+    k = O.r2c(-0.2 + 0.1 * np.random.default_rng(2).uniform(-1, 1, (nz, ny, nx)))
+    st.set_kspace(k.astype(np.complex64 if dtype == np.float32 else np.complex128))
+    change = st.step(5, propagator=propagator)
+    want, want_change = O.step(k, 5, 0.3, 0.3, st.lens, shape, mu=0.05, namp=namp, seed=21, noise_dtype=dtype,
+                               propagator=propagator, return_max_change=True)
+    got = st.kspace()
+    tol = 2e-6 if dtype == np.float32 else 1e-12
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) < tol
+    if propagator == "conserved_exp":
+        assert change == 0.0
+        assert got.flat[0] == k.astype(got.dtype).flat[0]  # the mean density is carried exactly
+    else:
+        # the relaxation moves the k = 0 mode; its largest change is reported (a float)
+        rel = 1e-3 if dtype == np.float32 else 1e-6
+        assert want_change > 0 and abs(change - want_change) <= rel * want_change
+
+
+def test_relaxation_rejects_noise():
+    from mcstar_b200 import PfcError, Stepper
+    st = Stepper((16, 16, 16), math.pi / 4, 0.3, 0.3, dtype=np.float64, namp=0.1)
+    st.set_kspace(O.r2c(np.full((16, 16, 16), -0.2)))
+    with pytest.raises(PfcError) as e:
+        st.step(1, propagator="relax")
+    assert e.value.status == 1
