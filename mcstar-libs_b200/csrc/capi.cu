@@ -108,7 +108,8 @@ void free_ctx(pfc_ctx* c) {
     if (!c) return;
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     void* ptrs[] = {c->tw,          c->work,         c->work2,        c->red,       c->k0,
-                    c->flag,        c->peak_counts,  c->peak_offsets, c->bond_scratch, c->bond_pairs};
+                    c->flag,        c->peak_counts,  c->peak_offsets, c->bond_scratch, c->bond_pairs,
+                    c->peak_mask};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete c;
@@ -537,7 +538,7 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
         free_ctx(c);
         return PFC_ERR_UNSUPPORTED;
     }
-    c->n_peak_blocks = (int)((c->n_real + kPeakBlock - 1) / kPeakBlock);
+    c->n_peak_blocks = peak_chunks(c->nx, c->ny, c->nz);
     // bond order starts with room for 4096 atoms and 64 neighbours each; pfc_bond_order
     // grows both when a call needs more (pfc_bond_reserve does it up front)
     c->max_atoms = 4096;
@@ -554,6 +555,7 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
     alloc((void**)&c->red, sizeof(double) * (kRedBlocks + 8));
     alloc((void**)&c->k0, sizeof(double2));
     alloc((void**)&c->flag, sizeof(int) * 4);
+    alloc((void**)&c->peak_mask, sizeof(uint32_t) * (size_t)peak_mask_words(c->nx, c->ny, c->nz));
     alloc((void**)&c->peak_counts, sizeof(int) * c->n_peak_blocks);
     alloc((void**)&c->peak_offsets, sizeof(int) * (c->n_peak_blocks + 1));
     alloc(&c->bond_scratch, c->bond_scratch_bytes);
@@ -605,7 +607,8 @@ size_t pfc_state_bytes(const pfc_ctx* ctx) { return ctx ? ctx->state_bytes : 0; 
 size_t pfc_workspace_bytes(const pfc_ctx* ctx) {
     if (!ctx) return 0;
     return 2 * ctx->state_bytes + ctx->bond_scratch_bytes + sizeof(int) * (size_t)ctx->max_pairs +
-           sizeof(double) * (kRedBlocks + 8) + sizeof(int) * (2 * ctx->n_peak_blocks + 1);
+           sizeof(double) * (kRedBlocks + 8) + sizeof(int) * (2 * ctx->n_peak_blocks + 1) +
+           sizeof(uint32_t) * (size_t)peak_mask_words(ctx->nx, ctx->ny, ctx->nz);
 }
 
 // ---- FFT ------------------------------------------------------------------------------

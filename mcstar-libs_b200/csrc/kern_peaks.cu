@@ -1,9 +1,12 @@
 // Local-maximum peak finding (cuda/kernels/findpeaks.hpp:7-29, findpeaks_2d.hpp:7-27).
 // A cell is a peak when it is strictly greater than all 26 (3D) or 8 (2D) periodic
-// neighbours and >= ths.  Deterministic compaction: pass 1 counts peaks per block of
-// kPeakBlock consecutive cells (__syncthreads_count), one block scans the counts,
-// pass 2 writes each peak at block offset + warp-ballot rank.  Blocks cover linear
-// index ranges in order, so the output is sorted by linear index.
+// neighbours and >= ths.  Output sorted by linear index (deterministic).
+//
+// Two implementations: the context's (k_peaks_mark ... k_peaks_emit below: the stencil once
+// per cell in shared memory, a bit mask, a compaction of the bits), and the one of the
+// entry point without allocation, whose scratch must stay small (pass 1 counts peaks per
+// block of kPeakBlock consecutive cells, one block scans the counts, pass 2 evaluates the
+// stencil again and writes each peak at block offset + warp-ballot rank).
 #include <cuda.h>
 #include <cstdio>
 #include <mutex>
@@ -119,14 +122,183 @@ cudaError_t peaks_raw(const void* psi, int nx, int ny, int nz, double ths, int* 
     return cudaSuccess;
 }
 
+// ---------------------------------------------------------------------------------------
+// The context's peak finder: the stencil is evaluated once per cell, in shared memory, and
+// leaves one bit per cell; the compaction then reads only the bits.
+//
+//  k_peaks_mark   a CTA of 32 x 8 threads owns a tile of 32 x 8 cells of kZC consecutive
+//                 z-planes.  Plane by plane (with one halo plane below and above) it stages
+//                 the tile and its periodic halo, 34 x 10 values, in shared memory; each
+//                 thread forms the maximum M9 of its 3 x 3 in-plane neighbourhood and the
+//                 maximum N8 of the 8 in-plane neighbours.  A cell of plane z is a peak when
+//                 psi > max(M9(z-1), N8(z), M9(z+1)) (26 neighbours; 2D: N8 alone) and
+//                 psi >= ths.  The maxima propagate NaN, so a NaN anywhere in the
+//                 neighbourhood makes the strict comparison false, exactly as the 26
+//                 comparisons of the reference (findpeaks.hpp:7-29, findpeaks_2d.hpp:7-27).
+//                 Bit x % 32 of word (z, y, x / 32) is the cell (x, y, z): one warp ballot
+//                 per row segment.
+//  k_words_count  per chunk of kChunkWords words (256 threads x 32 consecutive words): the
+//                 number of set bits.
+//  k_scan         (above) exclusive scan of the chunk counts.
+//  k_peaks_emit   per chunk: each thread's words, a block scan of their bit counts, and one
+//                 record per set bit at chunk offset + rank -- in linear-index order.
+// ---------------------------------------------------------------------------------------
+constexpr int kTX = 32, kTY = 8, kZC = 16;
+constexpr int kChunkWords = 256 * 32;
+
+__device__ __forceinline__ float nmax(float a, float b) {
+    float r;
+    asm("max.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ double nmax(double a, double b) { return (a != a || b != b) ? a + b : fmax(a, b); }
+
+template <typename T, bool D3>
+__global__ void __launch_bounds__(kTX * kTY) k_peaks_mark(const T* __restrict__ psi, int nx, int ny, int nz, T ths,
+                                                          uint32_t* __restrict__ mask, int wpr) {
+    __shared__ T S[kTY + 2][kTX + 2];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
+    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
+    const int z0 = D3 ? blockIdx.z * kZC : 0;
+    const int zend = D3 ? min(z0 + kZC, nz) : 1;
+    const int x = x0 + tx, y = y0 + ty;
+    const bool inside = x < nx && y < ny;
+    // the tile and its halo, (kTY + 2)(kTX + 2) = 340 values over 256 threads; cells of a
+    // partial tile past the grid's edge only fill the tile (no cell inside reads them)
+    auto stage = [&](int zp) {
+        const int zz = D3 ? (zp < 0 ? zp + nz : (zp >= nz ? zp - nz : zp)) : 0;
+        const T* plane = psi + (int64_t)zz * ny * nx;
+        for (int i = tid; i < (kTY + 2) * (kTX + 2); i += kTX * kTY) {
+            const int r = i / (kTX + 2), q = i - r * (kTX + 2);
+            int gy = y0 + r - 1, gx = x0 + q - 1;
+            gy = gy < 0 ? gy + ny : (gy >= ny ? gy - ny : gy);
+            gx = gx < 0 ? gx + nx : (gx >= nx ? gx - nx : gx);
+            S[r][q] = (gy < ny && gx < nx) ? plane[(int64_t)gy * nx + gx] : T(0);
+        }
+    };
+    T m9_prev = T(0), m9_cur = T(0), n8_cur = T(0), v_cur = T(0);
+    const int zfirst = D3 ? z0 - 1 : 0, zlast = D3 ? zend : 0;
+    for (int zp = zfirst; zp <= zlast; ++zp) {
+        __syncthreads();  // the previous plane's reads are done
+        stage(zp);
+        __syncthreads();
+        const T r0 = nmax(nmax(S[ty][tx], S[ty][tx + 1]), S[ty][tx + 2]);
+        const T r2 = nmax(nmax(S[ty + 2][tx], S[ty + 2][tx + 1]), S[ty + 2][tx + 2]);
+        const T v = S[ty + 1][tx + 1];
+        const T n8 = nmax(nmax(r0, r2), nmax(S[ty + 1][tx], S[ty + 1][tx + 2]));
+        const T m9 = nmax(n8, v);
+        if (D3 && zp >= z0 + 1) {
+            // the cell of plane zp - 1 has all of its neighbours: M9(zp - 2), N8(zp - 1), M9(zp)
+            const T m = nmax(nmax(m9_prev, n8_cur), m9);
+            const bool pk = inside && v_cur > m && v_cur >= ths;
+            const unsigned b = __ballot_sync(0xffffffffu, pk);
+            if (tx == 0 && y < ny) mask[((int64_t)(zp - 1) * ny + y) * wpr + blockIdx.x] = b;
+        }
+        if (!D3) {
+            const bool pk = inside && v > n8 && v >= ths;
+            const unsigned b = __ballot_sync(0xffffffffu, pk);
+            if (tx == 0 && y < ny) mask[(int64_t)y * wpr + blockIdx.x] = b;
+        }
+        m9_prev = m9_cur;
+        m9_cur = m9;
+        n8_cur = n8;
+        v_cur = v;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_words_count(const uint32_t* __restrict__ mask, int64_t nwords,
+                                                     int* __restrict__ counts) {
+    __shared__ int ws[8];
+    const int64_t w0 = (int64_t)blockIdx.x * kChunkWords + (int64_t)threadIdx.x * 32;
+    int c = 0;
+    for (int i = 0; i < 32; ++i)
+        if (w0 + i < nwords) c += __popc(mask[w0 + i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int i = 0; i < 8; ++i) t += ws[i];
+        counts[blockIdx.x] = t;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_peaks_emit(const T* __restrict__ psi, const uint32_t* __restrict__ mask,
+                                                    int64_t nwords, int nx, int ny, int wpr,
+                                                    const int* __restrict__ offsets, MaxRec<T>* __restrict__ out,
+                                                    int capacity) {
+    __shared__ int ws[8];
+    const int64_t w0 = (int64_t)blockIdx.x * kChunkWords + (int64_t)threadIdx.x * 32;
+    int c = 0;
+    for (int i = 0; i < 32; ++i)
+        if (w0 + i < nwords) c += __popc(mask[w0 + i]);
+    // exclusive scan of c over the block
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+    }
+    if (lane == 31) ws[warp] = incl;
+    __syncthreads();
+    int pos = offsets[blockIdx.x] + incl - c;
+    for (int w = 0; w < warp; ++w) pos += ws[w];
+    if (c == 0) return;
+    for (int i = 0; i < 32 && w0 + i < nwords; ++i) {
+        uint32_t b = mask[w0 + i];
+        const int64_t row = (w0 + i) / wpr;
+        const int xb = (int)((w0 + i) - row * wpr) * 32;
+        while (b) {
+            const int bit = __ffs(b) - 1;
+            b &= b - 1;
+            if (pos < capacity) {
+                const int xx = xb + bit;
+                MaxRec<T> rec = {};
+                rec.i0 = (T)xx;
+                rec.i1 = (T)(int)(row % ny);
+                rec.i2 = (T)(int)(row / ny);
+                rec.field = (float)psi[row * nx + xx];
+                out[pos] = rec;
+            }
+            ++pos;
+        }
+    }
+}
+
+template <typename T>
+cudaError_t peaks_ctx(const pfc_ctx* c, const void* psi, double ths, void* out, int capacity) {
+    const bool d3 = c->nz > 1;
+    const int wpr = (c->nx + 31) / 32;
+    const int64_t nwords = (int64_t)c->nz * c->ny * wpr;
+    const int nchunks = (int)((nwords + kChunkWords - 1) / kChunkWords);
+    dim3 grid(wpr, (c->ny + kTY - 1) / kTY, d3 ? (c->nz + kZC - 1) / kZC : 1);
+    if (d3)
+        k_peaks_mark<T, true><<<grid, dim3(kTX, kTY), 0, c->stream>>>((const T*)psi, c->nx, c->ny, c->nz, (T)ths,
+                                                                       c->peak_mask, wpr);
+    else
+        k_peaks_mark<T, false><<<grid, dim3(kTX, kTY), 0, c->stream>>>((const T*)psi, c->nx, c->ny, c->nz, (T)ths,
+                                                                        c->peak_mask, wpr);
+    k_words_count<<<nchunks, 256, 0, c->stream>>>(c->peak_mask, nwords, c->peak_counts);
+    k_scan<<<1, 1024, 0, c->stream>>>(c->peak_counts, nchunks, c->peak_offsets);
+    if (capacity > 0 && out)
+        k_peaks_emit<T><<<nchunks, 256, 0, c->stream>>>((const T*)psi, c->peak_mask, nwords, c->nx, c->ny, wpr,
+                                                        c->peak_offsets, (MaxRec<T>*)out, capacity);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
+int64_t peak_mask_words(int nx, int ny, int nz) { return (int64_t)nz * ny * ((nx + 31) / 32); }
+int peak_chunks(int nx, int ny, int nz) {
+    return (int)((peak_mask_words(nx, ny, nz) + kChunkWords - 1) / kChunkWords);
+}
+
 cudaError_t launch_findpeaks(const pfc_ctx* c, const void* psi, double ths, void* out, int capacity) {
-    return c->dtype == PFC_F64
-               ? peaks_raw<double>(psi, c->nx, c->ny, c->nz, ths, c->peak_counts, c->peak_offsets, out, capacity,
-                                   c->stream)
-               : peaks_raw<float>(psi, c->nx, c->ny, c->nz, ths, c->peak_counts, c->peak_offsets, out, capacity,
-                                  c->stream);
+    return c->dtype == PFC_F64 ? peaks_ctx<double>(c, psi, ths, out, capacity)
+                               : peaks_ctx<float>(c, psi, ths, out, capacity);
 }
 
 }  // namespace pfc

@@ -44,9 +44,10 @@ struct pfc_ctx {
     double* red;                  // kRedBlocks partial sums + 4 results
     double2* k0;                  // FP64 k = 0 mode carried by the stepper
     int* flag;                    // device status word of the stepper (non-finite watchdog)
-    int* peak_counts;             // per-block peak counts (kPeakBlock cells per block)
+    uint32_t* peak_mask;          // one bit per cell (peak finder)
+    int* peak_counts;             // set bits per chunk of the mask
     int* peak_offsets;            // exclusive scan of peak_counts (+ total)
-    int n_peak_blocks;
+    int n_peak_blocks;            // chunks
     // bond order: per-atom scratch for max_atoms atoms and the neighbour lists (max_pairs
     // entries), both grown by pfc_bond_order / pfc_bond_reserve when a call needs more
     int max_atoms;
@@ -191,6 +192,8 @@ cudaError_t launch_counter(cudaStream_t st, unsigned long long* ctr, unsigned lo
 cudaError_t launch_reduce_final(const pfc_ctx* c, int slot, double scale);
 
 // ---- peaks (kern_peaks.cu) ----
+int64_t peak_mask_words(int nx, int ny, int nz);
+int peak_chunks(int nx, int ny, int nz);
 cudaError_t launch_findpeaks(const pfc_ctx* c, const void* psi, double ths, void* out, int capacity);
 
 // ---- bond order (kern_bond.cu) ----
