@@ -614,7 +614,13 @@ __global__ void __launch_bounds__(Z::TH, 3) k_zbulk(float2* psi, float2* BA, int
     // (fft_d1_to_d3 synchronises before its first write to xb)
     fft_d1_to_d3<NZ, E, TX, -1, BarCta, true, 0>(v, t, c, xb, tw);
     propagate3<Z, false, false, BarCta, true, PROP>(v, stp, c, BarCta{}, kz_tab, kx, ky, t, nx, ny, a, k0, 1.0f);
-    // psi^' replaced psi^ in each thread's own slots: hand them to the async proxy
+    {
+        // psi^' over psi^ in the thread's own slots (the rows it read), then to the async proxy
+        const int p = t >> 1, h = t & 1;
+        float2* trow = stp + (p + h * (C::PIECE + 1)) * TX + c;
+#pragma unroll
+        for (int r = 0; r < E; ++r) trow[d3_row<E, true>(r) * TX] = v[r];
+    }
     fence_async_smem();
     __syncthreads();
     if (tid == 0) {
