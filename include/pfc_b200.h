@@ -294,6 +294,28 @@ pfc_status  pfc_ensemble_run(pfc_ensemble* e, int nsteps, void* cuda_stream);
 pfc_status  pfc_ensemble_destroy(pfc_ensemble* e);
 const char* pfc_ensemble_last_error(const pfc_ensemble* e);
 
+/* ---- slab-decomposed steps (no counterpart in mcstar-libs, whose drivers run one field per
+ * GPU through cuFFT): a field of nx x NY x NZ spread over G processes, each holding a
+ * ky-slab of NY / G rows between steps and a z-slab of NZ / G planes inside a step.  Rank r
+ * makes a ky-slab context of shape (nx, NY / G, NZ) and a z-slab context of shape
+ * (nx, NY, NZ / G), both of the field's precision, and steps its ky-slab A with
+ *   once:      pfc_slab_zinv(ky_ctx, kpsi_slab, A, ky0)        A = IFFT_z(psi^) / NZ
+ *   per step:  all-to-all A: ky-slabs -> z-slabs (the caller, e.g. NCCL all-to-all)
+ *              pfc_slab_xy(z_ctx, A_z, B_z, C, mu)              B = FFT_xy(cubic(IFFT_xy(A) / (nx NY)))
+ *              all-to-all B: z-slabs -> ky-slabs
+ *              pfc_slab_zpass(ky_ctx, A, B, p, ky0, NY, last)   N^ = FFT_z(B), the update with the
+ *                                                               field's wavenumbers and noise keys,
+ *                                                               A' = IFFT_z(psi^')/NZ, or psi^' in A
+ *                                                               on the last step (then synchronises)
+ * ky0 is the rank's first global ky row; p carries the field's lengths.  Slab buffers are
+ * standard-layout half spectra of the slab shape (pfc_state_bytes of its context).  The
+ * result equals pfc_step on the whole field up to rounding; the noise of mode k is the
+ * whole field's (keys of global indices).  The z pass runs the general kernels. */
+pfc_status pfc_slab_zinv(pfc_ctx* ky_ctx, const void* kpsi, void* A, int ky0);
+pfc_status pfc_slab_xy(pfc_ctx* z_ctx, const void* A, void* B, double C, double mu);
+pfc_status pfc_slab_zpass(pfc_ctx* ky_ctx, void* A, const void* B, const pfc_step_params* params, int ky0,
+                          int ny_global, int final_step);
+
 /* Free energy F = h^3 sum 1/2 psi ((1+lap)^2 - eps) psi + 1/4 psi^4 of the state kpsi,
  * computed as the reference does (eom.hpp:88-141: L^psi^, C2R, norm, calc_fen) with an
  * FP64 deterministic sum.  Does not modify kpsi. */

@@ -194,6 +194,8 @@ ZPropArgs zargs(const pfc_ctx* c, const pfc_step_params* p) {
     za.prop = PFC_PROP_CONSERVED;
     za.maxc = nullptr;
     za.margs = nullptr;
+    za.ky0 = 0;
+    za.ny_global = 0;
     return za;
 }
 
@@ -778,6 +780,58 @@ pfc_status pfc_step_prop(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_pa
         std::memcpy(&m, &flag[2], sizeof(float));
         *max_change = (double)m;
     }
+    return PFC_OK;
+}
+
+// ---- slab-decomposed steps of fields spread over several processes --------------------------
+pfc_status pfc_slab_zinv(pfc_ctx* ctx, const void* kpsi, void* A, int ky0) {
+    PFC_CHECK_CTX();
+    if (!kpsi || !A || kpsi == A || ky0 < 0) return fail(ctx, PFC_ERR_INVALID, "pfc_slab_zinv: bad arguments");
+    if (ky0 == 0) PFC_CUDA(launch_k0_save(ctx, kpsi), "pfc_slab_zinv k0");
+    if (ctx->nz > 1) {
+        PFC_CUDA(zcols(ctx, 1, kpsi, A, 1.0 / ctx->nz), "pfc_slab_zinv");
+    } else {
+        PFC_CUDA(cudaMemcpyAsync(A, kpsi, ctx->state_bytes, cudaMemcpyDeviceToDevice, ctx->stream), "pfc_slab_zinv");
+    }
+    return PFC_OK;
+}
+
+pfc_status pfc_slab_xy(pfc_ctx* ctx, const void* A, void* B, double C, double mu) {
+    PFC_CHECK_CTX();
+    if (!A || !B || A == B) return fail(ctx, PFC_ERR_INVALID, "pfc_slab_xy: bad arguments");
+    const double mul = 1.0 / ((double)ctx->nx * (double)ctx->ny);
+    if (ctx->xy_mode == 2) {
+        PFC_CUDA(launch_ypass(ctx, 1, A, B, 1.0, ctx->nz), "pfc_slab_xy y");
+        PFC_CUDA(launch_xpass(ctx, B, nullptr, mul, C, mu, ctx->nz), "pfc_slab_xy x");
+        PFC_CUDA(launch_ypass(ctx, -1, B, B, 1.0, ctx->nz), "pfc_slab_xy y");
+    } else {
+        if (ctx->ny > 1) PFC_CUDA(launch_cols(ctx, 1, 1, A, B, 1.0), "pfc_slab_xy y");
+        else PFC_CUDA(cudaMemcpyAsync(B, A, ctx->state_bytes, cudaMemcpyDeviceToDevice, ctx->stream), "pfc_slab_xy");
+        PFC_CUDA(launch_rows_nonlin(ctx, B, nullptr, mul, C, mu), "pfc_slab_xy x");
+        if (ctx->ny > 1) PFC_CUDA(launch_cols(ctx, 1, -1, B, B, 1.0), "pfc_slab_xy y");
+    }
+    ctx->launches += 3;
+    return PFC_OK;
+}
+
+pfc_status pfc_slab_zpass(pfc_ctx* ctx, void* A, const void* B, const pfc_step_params* p, int ky0, int ny_global,
+                          int final_step) {
+    PFC_CHECK_CTX();
+    if (!A || !B || !p || ky0 < 0 || ny_global < ctx->ny || ky0 + ctx->ny > ny_global)
+        return fail(ctx, PFC_ERR_INVALID, "pfc_slab_zpass: bad arguments");
+    ZPropArgs za = zargs(ctx, p);
+    // the noise amplitude of the whole field: sqrt(N) of its nx ny_global nz cells
+    za.namp_eff = p->namp * std::sqrt((double)ctx->nx * (double)ny_global * (double)ctx->nz);
+    za.ky0 = ky0;
+    za.ny_global = ny_global;
+    za.final_step = final_step != 0;
+    PFC_CUDA(launch_zprop(ctx, A, B, za), "pfc_slab_zpass");
+    ctx->launches += 1;
+    if (!final_step) return PFC_OK;
+    int flag = 0;
+    PFC_CUDA(cudaMemcpyAsync(&flag, ctx->flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "pfc_slab_zpass");
+    PFC_CUDA(cudaStreamSynchronize(ctx->stream), "pfc_slab_zpass sync");
+    if (flag) return fail(ctx, PFC_ERR_NONFINITE, "pfc_slab_zpass: non-finite value in the state");
     return PFC_OK;
 }
 

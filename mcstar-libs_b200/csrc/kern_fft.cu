@@ -192,6 +192,7 @@ struct ZArgsT {
     int use_noise, final_step;
     unsigned* maxc;                         // relaxations: max |psi^' - psi^| (float bits), or null
     const MemberArgs* margs;                // batched fields: per-field eps, noise amplitude, seed
+    int ky0, nyg;                           // a ky-slab: the field's first row here and its row count
 };
 
 template <typename T, int PROP>
@@ -231,7 +232,9 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
     __syncthreads();
     cx<T>* r = stockham_lines<T, -1>(b0, b1, 2 * tile, n, p, tw);
     cx<T>* other = (r == b0) ? b1 : b0;
-    const T k1 = kwave<T>(ky, ny, a.ly);
+    // a ky-slab of a larger field: wavenumbers, the k = 0 mode and the noise keys of the field
+    const int kyg = ky + a.ky0;
+    const T k1 = kwave<T>(kyg, a.nyg, a.ly);
     const T deps = T(1) + a.C - a.eps;
     float mc = 0.f;
     for (int e = threadIdx.x; e < nt * n; e += blockDim.x) {
@@ -245,26 +248,26 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
         if constexpr (PROP == kPropConserved) {
             const T dopy = dopx * dopx;
             const T denom = T(1) - a.dt * (deps * dopx + T(2) * dopy + dopx * dopy);
-            if (kx == 0 && ky == 0 && kz == 0) psi = mkc<T>((T)k0->x, (T)k0->y);
+            if (kx == 0 && kyg == 0 && kz == 0) psi = mkc<T>((T)k0->x, (T)k0->y);
             const T f = a.dt * dopx;
             cx<T> num = mkc<T>(psi.x + f * nl.x, psi.y + f * nl.y);
             if (a.use_noise) {
                 const T kabs = sqrt(-dopx);
                 const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
-                const cx<T> xi = kspace_noise<T>(kx, ky, kz, nx, ny, nz, a.seed, ctr);
+                const cx<T> xi = kspace_noise<T>(kx, kyg, kz, nx, a.nyg, nz, a.seed, ctr);
                 const T g = a.dt * a.namp_eff * kabs;
                 num.x += g * xi.x;
                 num.y += g * xi.y;
             }
             v = mkc<T>(num.x / denom, num.y / denom);
         } else {
-            if (prop_conserved<PROP>() && kx == 0 && ky == 0 && kz == 0) psi = mkc<T>((T)k0->x, (T)k0->y);
+            if (prop_conserved<PROP>() && kx == 0 && kyg == 0 && kz == 0) psi = mkc<T>((T)k0->x, (T)k0->y);
             T ca, cb, cg;
             prop_coef<PROP, T>(dopx, a.dt, deps, ca, cb, cg);
             v = mkc<T>(ca * psi.x + cb * nl.x, ca * psi.y + cb * nl.y);
             if (prop_conserved<PROP>() && a.use_noise) {
                 const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
-                const cx<T> xi = kspace_noise<T>(kx, ky, kz, nx, ny, nz, a.seed, ctr);
+                const cx<T> xi = kspace_noise<T>(kx, kyg, kz, nx, a.nyg, nz, a.seed, ctr);
                 v.x += a.namp_eff * cg * xi.x;
                 v.y += a.namp_eff * cg * xi.y;
             }
@@ -392,8 +395,10 @@ template <typename T, int PROP>
 void zprop_T(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int col0, int ncols) {
     const int tile = c->pzprop.tile;
     dim3 grid((ncols + tile - 1) / tile, c->ny, c->batch);
-    ZArgsT<T> t{(T)a.dt, (T)a.eps, (T)a.C, (T)a.namp_eff, (T)a.lx, (T)a.ly, (T)a.lz, a.seed, a.counter,
-                a.dev_counter, a.use_noise, a.final_step, a.maxc, a.margs};
+    ZArgsT<T> t{(T)a.dt,      (T)a.eps,    (T)a.C,      (T)a.namp_eff,
+                (T)a.lx,      (T)a.ly,     (T)a.lz,     a.seed,
+                a.counter,    a.dev_counter, a.use_noise, a.final_step,
+                a.maxc,       a.margs,     a.ky0,       a.ny_global > 0 ? a.ny_global : c->ny};
     k_zprop<T, PROP><<<grid, 256, c->pzprop.smem, c->stream>>>((cx<T>*)A, (const cx<T>*)B, c->nx, c->ny, c->nz,
                                                                 c->pz.plan, (const cx<T>*)c->tw, tile, t, c->k0,
                                                                 c->flag, col0, col0 + ncols, c->mstride);

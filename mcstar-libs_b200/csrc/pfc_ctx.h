@@ -119,6 +119,9 @@ struct ZPropArgs {
     // batched fields: per-field eps, noise amplitude and seed (null: the values above for
     // every field); k0 and dev_counter then hold one entry per field
     const MemberArgs* margs;
+    // a ky-slab of a larger field (slab-decomposed steps; the general z pass only): this
+    // context's ky = 0 is the field's ky0, of ny_global rows (0, 0: the context's own field)
+    int ky0, ny_global;
 };
 cudaError_t launch_zprop(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a);
 // the general z pass over the kx columns [col0, col0 + ncols)
