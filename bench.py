@@ -151,7 +151,7 @@ def kernel_table(prof, S, steps):
         add("k_cols+k_rows_nonlin+k_cols", 1, 6.0 * S)
     if prof["z_mode"] in (2, 4):
         # psi^ and B read, psi^' and A' written; the last step of a run writes psi^' only
-        add("k_zcarry3" if prof["z_mode"] == 4 else "k_zcarry", 2, (4.0 * (steps - 1) + 3.0) / steps * S)
+        add("k_zbulk" if prof["z_mode"] == 4 else "k_zcarry", 2, (4.0 * (steps - 1) + 3.0) / steps * S)
     else:
         name = "k_zprop" if prof["z_mode"] == 0 else ("k_zcol3" if prof.get("z_variant") == 6 else "k_zcol")
         add(name, 2, 3.0 * S)
@@ -479,6 +479,8 @@ def run_b200(args, ws, rank, local):
     d = kern[dom]
     achieved = d["bytes_per_launch"] / (d["ms_per_launch"] / 1e3) / 1e9
     step_bytes = sum(k["bytes_per_launch"] * k["launches"] for k in kern.values()) / args.steps
+    # the step's fraction of the roofline with the minimum traffic a step can have (two
+    # read+write passes of the half spectrum, 4 S bytes), beside the traffic of this design
     roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
             "peak_kind": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)", "unit": "GB/s",
             "frac": round(achieved / peak, 4), "algorithmic_bytes_per_launch": d["bytes_per_launch"],
@@ -486,6 +488,7 @@ def run_b200(args, ws, rank, local):
             "traffic": ncu_traffic(dom, n),
             "step_bytes_alg": step_bytes,
             "step_frac": round(step_bytes * (value / ws) / 1e9 / peak, 4),
+            "step_frac_4S": round(4.0 * S * (value / ws) / 1e9 / peak, 4),
             "kernels": {k: {"ms_per_launch": round(v["ms_per_launch"], 5), "launches": v["launches"],
                             "share": round(v["ms_total"] / max(1e-9, prof["ms"][1] + prof["ms"][2]), 4),
                             "alg_bytes_per_launch": v["bytes_per_launch"],

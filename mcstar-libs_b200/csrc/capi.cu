@@ -75,9 +75,6 @@ bool make_plan(int n, LinePlan& p, std::vector<std::complex<double>>& tab, int o
     return true;
 }
 
-// The z pass carries psi^ itself unless the options say otherwise.
-constexpr bool kCarryPsiDefault = false;
-
 int pow2_floor(size_t v, int cap) {
     int t = 1;
     while (t * 2 <= cap && (size_t)(t * 2) <= v) t *= 2;
@@ -474,13 +471,14 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
         roots(c->nx / 2, c->nx / 2);
         roots(c->nx, c->nx / 2 + 1);
     }
-    // the row-pair x pass where it exists, unless the options ask for single rows
+    // the row-pair x pass where the options ask for it (measured no faster than single rows
+    // at 512^3: 0.344 against 0.333 ms)
     c->xpair = c->fused_x ? xpair_variant(c->nx, c->dtype) : 0;
     if (o.x_pair == 1 && !c->xpair) {
         free_ctx(c);
         return PFC_ERR_UNSUPPORTED;
     }
-    if (o.x_pair == 0) c->xpair = 0;
+    if (o.x_pair != 1) c->xpair = 0;
     c->xpair_tw_off = (int)tab.size();
     if (c->xpair) roots(c->nx, c->nx);
     // (its line stride ny (nx/2+1) is a 32-bit int)
@@ -496,8 +494,7 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
         free_ctx(c);
         return PFC_ERR_UNSUPPORTED;
     }
-    const bool carry = c->fused_z && (o.z_carry == 1 || (o.z_carry == -1 && kCarryPsiDefault));
-    // kx-tiled fields (measured faster: whole-block z and y columns); PFC_TILED=0 keeps the
+    // kx-tiled fields (measured faster: whole-block z and y columns); tiled = 0 keeps the
     // standard layout.  Needs the register y, x, z passes, whole fields, and the register
     // column kernel for the entry / exit z transforms.
     c->tiled = c->fused_z && c->fused_zfft && c->xy_mode == 2 && c->fused_y;
@@ -506,6 +503,11 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
         return PFC_ERR_UNSUPPORTED;
     }
     if (o.tiled == 0) c->tiled = 0;
+    // The library carries psi^ where the tiled bulk-copy z kernel exists (nz = 512): faster
+    // (two z transforms; 0.344 against 0.447 ms at 512^3) and no FP32 round trip of the state
+    // through IFFT_z / FFT_z each step (its FP32 error against FP64 is the reference cuFFT
+    // path's or lower at 1, 10, 100, 1000 steps); elsewhere A.
+    const bool carry = c->fused_z && (o.z_carry == 1 || (o.z_carry == -1 && c->tiled && c->fused_z == 6));
     // psi^ carried: tiled, with the 16-values-per-thread kernel (nz 512); standard layout,
     // with the square split.  A tiled context whose z length has no tiled psi^-carrying
     // kernel carries A unless the options ask for psi^ (then the layout is standard).

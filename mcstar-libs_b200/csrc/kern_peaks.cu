@@ -137,11 +137,12 @@ cudaError_t peaks_raw(const void* psi, int nx, int ny, int nz, double ths, int* 
 //                 comparisons of the reference (findpeaks.hpp:7-29, findpeaks_2d.hpp:7-27).
 //                 Bit x % 32 of word (z, y, x / 32) is the cell (x, y, z): one warp ballot
 //                 per row segment.
-//  k_words_count  per chunk of kChunkWords words (256 threads x 32 consecutive words): the
-//                 number of set bits.
+//  k_words_count  per chunk of kChunkWords words (eight warps of 1024 consecutive words, one
+//                 word per lane and iteration): the number of set bits.
 //  k_scan         (above) exclusive scan of the chunk counts.
-//  k_peaks_emit   per chunk: each thread's words, a block scan of their bit counts, and one
-//                 record per set bit at chunk offset + rank -- in linear-index order.
+//  k_peaks_emit   per chunk: the warps' bit counts, then per iteration a warp scan of the
+//                 32 words' counts and one record per set bit at its rank -- in
+//                 linear-index order.
 // ---------------------------------------------------------------------------------------
 constexpr int kTX = 32, kTY = 8, kZC = 16;
 constexpr int kChunkWords = 256 * 32;
@@ -163,17 +164,31 @@ __global__ void __launch_bounds__(kTX * kTY) k_peaks_mark(const T* __restrict__ 
     const int zend = D3 ? min(z0 + kZC, nz) : 1;
     const int x = x0 + tx, y = y0 + ty;
     const bool inside = x < nx && y < ny;
-    // the tile and its halo, (kTY + 2)(kTX + 2) = 340 values over 256 threads; cells of a
-    // partial tile past the grid's edge only fill the tile (no cell inside reads them)
-    auto stage = [&](int zp) {
-        const int zz = D3 ? (zp < 0 ? zp + nz : (zp >= nz ? zp - nz : zp)) : 0;
-        const T* plane = psi + (int64_t)zz * ny * nx;
-        for (int i = tid; i < (kTY + 2) * (kTX + 2); i += kTX * kTY) {
+    // the tile and its halo, (kTY + 2)(kTX + 2) = 340 values: at most two per thread, at
+    // in-plane offsets fixed for every plane (periodic wrap done once).  Cells of a partial
+    // tile past the grid's edge only fill the tile (no cell inside reads them): offset -1.
+    constexpr int kHalo = (kTY + 2) * (kTX + 2);
+    int off[2];
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+        const int i = tid + m * kTX * kTY;
+        off[m] = -1;
+        if (i < kHalo) {
             const int r = i / (kTX + 2), q = i - r * (kTX + 2);
             int gy = y0 + r - 1, gx = x0 + q - 1;
             gy = gy < 0 ? gy + ny : (gy >= ny ? gy - ny : gy);
             gx = gx < 0 ? gx + nx : (gx >= nx ? gx - nx : gx);
-            S[r][q] = (gy < ny && gx < nx) ? plane[(int64_t)gy * nx + gx] : T(0);
+            if (gy < ny && gx < nx) off[m] = gy * nx + gx;
+        }
+    }
+    T* Sf = &S[0][0];
+    auto stage = [&](int zp) {
+        const int zz = D3 ? (zp < 0 ? zp + nz : (zp >= nz ? zp - nz : zp)) : 0;
+        const T* plane = psi + (int64_t)zz * ny * nx;
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            const int i = tid + m * kTX * kTY;
+            if (i < kHalo) Sf[i] = off[m] >= 0 ? plane[off[m]] : T(0);
         }
     };
     T m9_prev = T(0), m9_cur = T(0), n8_cur = T(0), v_cur = T(0);
@@ -206,16 +221,35 @@ __global__ void __launch_bounds__(kTX * kTY) k_peaks_mark(const T* __restrict__ 
     }
 }
 
+// A chunk of kChunkWords mask words per block: warp w takes words [w 1024, (w + 1) 1024) of
+// the chunk, 32 consecutive words (one per lane) per iteration -- coalesced.
+__device__ __forceinline__ int warp_incl_scan(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    return v;
+}
+__device__ __forceinline__ int warp_sum(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 __global__ void __launch_bounds__(256) k_words_count(const uint32_t* __restrict__ mask, int64_t nwords,
                                                      int* __restrict__ counts) {
     __shared__ int ws[8];
-    const int64_t w0 = (int64_t)blockIdx.x * kChunkWords + (int64_t)threadIdx.x * 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t w0 = (int64_t)blockIdx.x * kChunkWords + warp * 1024 + lane;
     int c = 0;
-    for (int i = 0; i < 32; ++i)
-        if (w0 + i < nwords) c += __popc(mask[w0 + i]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+#pragma unroll 8
+    for (int it = 0; it < 32; ++it) {
+        const int64_t w = w0 + it * 32;
+        if (w < nwords) c += __popc(mask[w]);
+    }
+    c = warp_sum(c);
+    if (lane == 0) ws[warp] = c;
     __syncthreads();
     if (threadIdx.x == 0) {
         int t = 0;
@@ -230,40 +264,45 @@ __global__ void __launch_bounds__(256) k_peaks_emit(const T* __restrict__ psi, c
                                                     const int* __restrict__ offsets, MaxRec<T>* __restrict__ out,
                                                     int capacity) {
     __shared__ int ws[8];
-    const int64_t w0 = (int64_t)blockIdx.x * kChunkWords + (int64_t)threadIdx.x * 32;
-    int c = 0;
-    for (int i = 0; i < 32; ++i)
-        if (w0 + i < nwords) c += __popc(mask[w0 + i]);
-    // exclusive scan of c over the block
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int incl = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int u = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += u;
+    const int64_t w0 = (int64_t)blockIdx.x * kChunkWords + warp * 1024 + lane;
+    int c = 0;
+#pragma unroll 8
+    for (int it = 0; it < 32; ++it) {
+        const int64_t w = w0 + it * 32;
+        if (w < nwords) c += __popc(mask[w]);
     }
-    if (lane == 31) ws[warp] = incl;
+    c = warp_sum(c);
+    if (lane == 0) ws[warp] = c;
     __syncthreads();
-    int pos = offsets[blockIdx.x] + incl - c;
-    for (int w = 0; w < warp; ++w) pos += ws[w];
-    if (c == 0) return;
-    for (int i = 0; i < 32 && w0 + i < nwords; ++i) {
-        uint32_t b = mask[w0 + i];
-        const int64_t row = (w0 + i) / wpr;
-        const int xb = (int)((w0 + i) - row * wpr) * 32;
-        while (b) {
-            const int bit = __ffs(b) - 1;
-            b &= b - 1;
-            if (pos < capacity) {
-                const int xx = xb + bit;
-                MaxRec<T> rec = {};
-                rec.i0 = (T)xx;
-                rec.i1 = (T)(int)(row % ny);
-                rec.i2 = (T)(int)(row / ny);
-                rec.field = (float)psi[row * nx + xx];
-                out[pos] = rec;
+    if (c == 0) return;  // (warp-uniform)
+    int base = offsets[blockIdx.x];
+    for (int w = 0; w < warp; ++w) base += ws[w];
+    for (int it = 0; it < 32; ++it) {
+        const int64_t w = w0 + it * 32;
+        const uint32_t word = w < nwords ? mask[w] : 0u;
+        const int n = __popc(word);
+        const int incl = warp_incl_scan(n, lane);
+        int pos = base + incl - n;
+        base += __shfl_sync(0xffffffffu, incl, 31);
+        uint32_t b = word;
+        if (b) {
+            const int64_t row = w / wpr;
+            const int xb = (int)(w - row * wpr) * 32;
+            while (b) {
+                const int bit = __ffs(b) - 1;
+                b &= b - 1;
+                if (pos < capacity) {
+                    const int xx = xb + bit;
+                    MaxRec<T> rec = {};
+                    rec.i0 = (T)xx;
+                    rec.i1 = (T)(int)(row % ny);
+                    rec.i2 = (T)(int)(row / ny);
+                    rec.field = (float)psi[row * nx + xx];
+                    out[pos] = rec;
+                }
+                ++pos;
             }
-            ++pos;
         }
     }
 }
