@@ -182,20 +182,38 @@ __global__ void __launch_bounds__(kTX * kTY) k_peaks_mark(const T* __restrict__ 
         }
     }
     T* Sf = &S[0][0];
-    auto stage = [&](int zp) {
+    // Planes are loaded kAhead planes ahead of their use into registers, so that the loads of
+    // later planes are in flight while a plane is compared (the plane loop is otherwise a
+    // chain of load latencies and barriers).
+    constexpr int kAhead = 4;
+    T ring[kAhead][2];
+    auto load = [&](int zp, T (&dst)[2]) {
         const int zz = D3 ? (zp < 0 ? zp + nz : (zp >= nz ? zp - nz : zp)) : 0;
         const T* plane = psi + (int64_t)zz * ny * nx;
 #pragma unroll
-        for (int m = 0; m < 2; ++m) {
-            const int i = tid + m * kTX * kTY;
-            if (i < kHalo) Sf[i] = off[m] >= 0 ? plane[off[m]] : T(0);
-        }
+        for (int m = 0; m < 2; ++m) dst[m] = off[m] >= 0 ? plane[off[m]] : T(0);
     };
     T m9_prev = T(0), m9_cur = T(0), n8_cur = T(0), v_cur = T(0);
     const int zfirst = D3 ? z0 - 1 : 0, zlast = D3 ? zend : 0;
+#pragma unroll
+    for (int a = 0; a < kAhead; ++a)
+        if (zfirst + a <= zlast) load(zfirst + a, ring[a]);
     for (int zp = zfirst; zp <= zlast; ++zp) {
+        const int slot = (zp - zfirst) % kAhead;
         __syncthreads();  // the previous plane's reads are done
-        stage(zp);
+        T cur[2];
+#pragma unroll
+        for (int a = 0; a < kAhead; ++a)
+            if (a == slot) {
+                cur[0] = ring[a][0];
+                cur[1] = ring[a][1];
+                if (zp + kAhead <= zlast) load(zp + kAhead, ring[a]);
+            }
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            const int i = tid + m * kTX * kTY;
+            if (i < kHalo) Sf[i] = cur[m];
+        }
         __syncthreads();
         const T r0 = nmax(nmax(S[ty][tx], S[ty][tx + 1]), S[ty][tx + 2]);
         const T r2 = nmax(nmax(S[ty + 2][tx], S[ty + 2][tx + 1]), S[ty + 2][tx + 2]);
