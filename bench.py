@@ -126,7 +126,10 @@ def ncu_traffic(kernel, size):
         return None
 
 
-def kernel_table(prof, S, steps):
+X_KERNELS = {0: "k_xrow", 1: "k_xpair", 2: "k_xlane"}
+
+
+def kernel_table(prof, S, steps, x_kernel=0):
     """Per-kernel device time of the timed region (the library's CUDA-event brackets on
     its stream) with the algorithmic HBM bytes of one launch, S = bytes of one
     half-spectrum field: every pass reads each input field once and writes each output
@@ -142,7 +145,7 @@ def kernel_table(prof, S, steps):
     if prof["xy_mode"] == 2 and prof["calls"][3]:
         # y-inverse A -> B, y-forward B -> B
         add("k_ycol3" if prof.get("y_variant") in (6, 7, 8) else "k_ycol", 3, 2.0 * S)
-        add("k_xrow", 4, 2.0 * S)  # C2R, cubic term, R2C of every row, in place
+        add(X_KERNELS.get(x_kernel, "k_xrow"), 4, 2.0 * S)  # C2R, cubic term, R2C of every row, in place
     elif prof["xy_mode"] == 2:
         add("k_ycol+k_xrow+k_ycol (z slabs)", 1, 6.0 * S)
     elif prof["xy_mode"] == 1:
@@ -474,7 +477,7 @@ def run_b200(args, ws, rank, local):
     cells = n ** 3
     # ---- roofline of the dominant kernel family -------------------------------------------------
     peak, peak_kind = measured_peak()
-    kern = kernel_table(prof, S, args.steps)
+    kern = kernel_table(prof, S, args.steps, ctx.options.get("x_kernel", 0))
     dom = max(kern, key=lambda k: kern[k]["ms_total"])
     d = kern[dom]
     achieved = d["bytes_per_launch"] / (d["ms_per_launch"] / 1e3) / 1e9

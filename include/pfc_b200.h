@@ -66,8 +66,11 @@ pfc_status  pfc_destroy(pfc_ctx* ctx);
  *   z_carry      the state the stepper's z pass carries between steps: 0 A = IFFT_z(psi^)/nz
  *                (three z transforms, three field sweeps), 1 psi^ itself (two transforms,
  *                four sweeps); -1 the library's choice
- *   x_pair       the register x pass: 0 one row per transform, 1 row pairs packed into one
- *                complex transform (nx = 128, 512); -1 the library's choice
+ *   x_kernel     the register x pass of the kx-tiled layout: 0 one row per transform over
+ *                16 lanes per row and 16 rows per CTA with a shared-memory row stage, 1 row
+ *                pairs packed into one complex transform (nx = 128, 512), 2 one row per
+ *                half-warp straight from and to global memory (nx = 512); -1 the library's
+ *                choice
  *   tiled        the register passes' field layout: 0 the reference layout, 1 kx tiles of
  *                8 columns (contiguous z and y column blocks); -1 the library's choice
  *   radix_order  the general (mixed-radix Stockham) passes: 0 radix 8 first, 1 radices 4
@@ -83,7 +86,7 @@ pfc_status  pfc_destroy(pfc_ctx* ctx);
  * and destroys contexts and allocates device memory (setup time, not the step). */
 typedef struct pfc_options {
     int z_carry;
-    int x_pair;
+    int x_kernel;
     int tiled;
     int radix_order;
     int tile_shift[4];
@@ -280,8 +283,12 @@ pfc_status pfc_step_prop(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_pa
 /* ---- ensembles (no counterpart in mcstar-libs, whose drivers run one field per process):
  * n independent fields, each with its own context (contexts and buffers must not be
  * shared between members), shape, precision and parameters, advanced together.
- * pfc_ensemble_create captures steps_per_graph steps of every member into one CUDA graph
- * (one branch per member, so members of different sizes run concurrently);
+ * pfc_ensemble_create sorts the members into classes -- same shape, precision, kernel
+ * schedules and shared parameters (dt, C, mu, box lengths, noise on or off) -- and steps the
+ * members of a class as one batch: every pass of the step is one launch over all of them
+ * (per-member eps, noise amplitude, seed and counter in a device table).  It captures
+ * steps_per_graph steps of every class into one CUDA graph, one branch per class, so
+ * classes of different sizes run concurrently;
  * pfc_ensemble_run(e, nsteps, stream) converts every member into the stepper's carried
  * form, replays the graph nsteps / steps_per_graph times (nsteps must be a multiple) and
  * converts back, then checks every member's non-finite watchdog.  Each member's noise

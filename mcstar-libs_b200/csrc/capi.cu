@@ -347,7 +347,7 @@ void free_ensemble(pfc_ensemble* e) {
 bool same_class(const pfc_ctx* a, const pfc_step_params& pa, const pfc_ctx* b, const pfc_step_params& pb) {
     const pfc_options &oa = a->opt, &ob = b->opt;
     return a->nx == b->nx && a->ny == b->ny && a->nz == b->nz && a->dtype == b->dtype && oa.z_carry == ob.z_carry &&
-           oa.x_pair == ob.x_pair && oa.tiled == ob.tiled && oa.radix_order == ob.radix_order &&
+           oa.x_kernel == ob.x_kernel && oa.tiled == ob.tiled && oa.radix_order == ob.radix_order &&
            std::memcmp(oa.tile_shift, ob.tile_shift, sizeof(oa.tile_shift)) == 0 && pa.dt == pb.dt && pa.C == pb.C &&
            pa.mu == pb.mu && pa.lx == pb.lx && pa.ly == pb.ly && pa.lz == pb.lz && (pa.namp != 0.0) == (pb.namp != 0.0);
 }
@@ -396,7 +396,7 @@ const char* pfc_last_error(const pfc_ctx* ctx) { return ctx ? ctx->err.c_str() :
 pfc_status pfc_default_options(pfc_options* o) {
     if (!o) return PFC_ERR_INVALID;
     o->z_carry = -1;
-    o->x_pair = -1;
+    o->x_kernel = -1;
     o->tiled = -1;
     o->radix_order = 0;
     for (int i = 0; i < 4; ++i) o->tile_shift[i] = 0;
@@ -417,7 +417,7 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
     pfc_options o;
     pfc_default_options(&o);
     if (opts) o = *opts;
-    if (o.z_carry < -1 || o.z_carry > 1 || o.x_pair < -1 || o.x_pair > 1 || o.tiled < -1 || o.tiled > 1 ||
+    if (o.z_carry < -1 || o.z_carry > 1 || o.x_kernel < -1 || o.x_kernel > 2 || o.tiled < -1 || o.tiled > 1 ||
         o.radix_order < 0 || o.radix_order > 2)
         return PFC_ERR_INVALID;
     for (int i = 0; i < 4; ++i)
@@ -471,16 +471,18 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
         roots(c->nx / 2, c->nx / 2);
         roots(c->nx, c->nx / 2 + 1);
     }
-    // the row-pair x pass where the options ask for it (measured no faster than single rows
-    // at 512^3: 0.344 against 0.333 ms)
-    c->xpair = c->fused_x ? xpair_variant(c->nx, c->dtype) : 0;
-    if (o.x_pair == 1 && !c->xpair) {
-        free_ctx(c);
-        return PFC_ERR_UNSUPPORTED;
+    // the kernel of the row-tiled x pass: rows (0), row pairs (1) or a row per half-warp (2),
+    // among those the length has
+    {
+        const int have = c->fused_x ? xkernel_variants(c->nx, c->dtype) : 1;
+        if (o.x_kernel > 0 && !((have >> o.x_kernel) & 1)) {
+            free_ctx(c);
+            return PFC_ERR_UNSUPPORTED;
+        }
+        c->xkern = o.x_kernel >= 0 ? o.x_kernel : default_xkernel(have);
     }
-    if (o.x_pair != 1) c->xpair = 0;
     c->xpair_tw_off = (int)tab.size();
-    if (c->xpair) roots(c->nx, c->nx);
+    if (c->xkern == 1) roots(c->nx, c->nx);
     // (its line stride ny (nx/2+1) is a 32-bit int)
     c->fused_zfft = c->nz > 1 && c->n_cmpl < (1ull << 31) ? fused_zfft_variant(c->nz, c->dtype) : 0;
     c->zfft_tw_off = (int)tab.size();
@@ -588,7 +590,7 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
     // the options in effect (the library's choices filled in)
     c->opt = o;
     c->opt.z_carry = c->z_carry ? 1 : 0;
-    c->opt.x_pair = c->xpair ? 1 : 0;
+    c->opt.x_kernel = c->xkern;
     c->opt.tiled = c->tiled ? 1 : 0;
     *out = c;
     return PFC_OK;

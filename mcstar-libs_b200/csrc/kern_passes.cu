@@ -395,6 +395,112 @@ __global__ void __launch_bounds__(X::T, 4) k_xpair(float2* g, int nrows, const f
     }
 }
 
+// The x pass with each row on one half-warp (row-tiled layout, nx = 2 P^2 real points with
+// P = 16 lanes per row: 512).  Lane t of a row holds modes kx = t + P j (j < E = P), the
+// four-step transforms' D1 = D2 distribution, so nothing is staged through shared memory
+// but the transposes of the two transforms:
+//  - load: mode kx and its split partner nx/2 - kx straight from global memory (the
+//    partner's lines are the ones another j of the same row loads, served by L1);
+//  - C2R: c2r_pre_f, the nx/2-point inverse FFT (one transpose), cubic term, forward FFT
+//    (one transpose), all exchanges within the half-warp (__syncwarp only);
+//  - store: the R2C merge partner Y[(nx/2 - kx) mod nx/2] is register 15 - j of lane 16 - t
+//    (lane 0: its own register (16 - j) mod 16), fetched by warp shuffle; the merged modes go
+//    straight to global memory.
+// Exchange slots of a row: (a, b) -> a (P + 1) + b, so both the writes (b = t) and the reads
+// (a = t) of a half-warp fall on 16 distinct 8-byte bank pairs.  The stage twiddles W^{t k1}
+// sit in a [k1][t] table (a half-warp reads 16 consecutive entries).  A CTA holds 16 rows:
+// one 1 KB block of each kx tile of the row-tiled field.
+template <int NX_>
+struct XLCfg {
+    static constexpr int NX = NX_, M = NX / 2, P = 16, E = M / P, R = 16, T = R * P;
+    static constexpr int LDA = P + 1, LDG = E * LDA;  // exchange: a stride, row stride
+    static constexpr int XB = R * LDG;
+    static constexpr size_t SMEM = (size_t)(XB + E * P + M + 1) * sizeof(float2);
+    static_assert(E == P && M % kTileW == 0 && P == 2 * kTileW, "shape");
+};
+
+template <class X>
+__global__ void __launch_bounds__(X::T, 3) k_xlane(float2* g, int nrows, const float2* __restrict__ twg, float mul,
+                                                   float Cc, float mu, int64_t ms) {
+    constexpr int M = X::M, E = X::E, P = X::P, R = X::R, LDA = X::LDA, FT = M / kTileW;
+    g += blockIdx.z * ms;  // fields of a batch (grid z)
+    extern __shared__ __align__(16) float2 sm[];
+    float2* tw2 = sm + X::XB;  // [k1][t]: W_M^{t k1}
+    float2* twP = tw2 + E * P; // W_NX^k, k <= M
+    const int tid = threadIdx.x;
+    for (int i = tid; i < E * P; i += X::T) tw2[i] = twg[(i % P) * (i / P)];
+    for (int i = tid; i <= M; i += X::T) twP[i] = twg[M + i];
+    const int t = tid % P, rl = tid / P;
+    float2* xr = sm + rl * X::LDG;
+    const int64_t ts = (int64_t)kTileW * nrows;  // elements between tiles
+    const int64_t rowoff = (int64_t)(blockIdx.x * R + rl) * kTileW;
+    float2* gl = g + rowoff + (t & (kTileW - 1)) + (t / kTileW) * ts;  // mode t of the row
+    float2* gnyq = g + FT * ts + blockIdx.x * R + rl;                   // mode M (tile of width 1)
+    __syncthreads();
+    float2 v[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+        const int k = t + P * j, km = M - k;  // km in [1, M]
+        const float2 xk = gl[(2 * j) * ts];
+        const float2 xm = km == M ? *gnyq : g[(km / kTileW) * ts + rowoff + (km & (kTileW - 1))];
+        v[j] = c2r_pre_f(xk, xm, twP[k]);
+    }
+    // inverse transform, D1 -> D2 (thread t: pair n = t + P k2 at register k2)
+    RF<E, 1>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < E; ++k1) {
+        float2 w = tw2[k1 * P + t];
+        w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < E; ++k1) xr[k1 * LDA + t] = v[k1];
+    __syncwarp();
+#pragma unroll
+    for (int tt = 0; tt < P; ++tt) v[tt] = xr[t * LDA + tt];
+    RF<P, 1>::run(v);
+#pragma unroll
+    for (int k2 = 0; k2 < P; ++k2) {
+        const float a = v[k2].x * mul, b = v[k2].y * mul;
+        v[k2] = make_float2(a * a * a - Cc * a - mu, b * b * b - Cc * b - mu);
+    }
+    // forward transform, D2 -> D1
+    RF<P, -1>::run(v);
+#pragma unroll
+    for (int k2 = 1; k2 < P; ++k2) v[k2] = cmul(v[k2], tw2[k2 * P + t]);
+    __syncwarp();  // the first exchange's reads are done
+#pragma unroll
+    for (int k2 = 0; k2 < P; ++k2) xr[t * LDA + k2] = v[k2];
+    __syncwarp();
+#pragma unroll
+    for (int n1 = 0; n1 < E; ++n1) v[n1] = xr[n1 * LDA + t];
+    RF<E, -1>::run(v);
+    // merge and store: Y[k] here, Y[(M - k) mod M] from lane 16 - t (lane 0: itself)
+    const int src = (threadIdx.x & 31 & ~(P - 1)) | ((P - t) & (P - 1));
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+        const float2 s = v[E - 1 - j];
+        float2 ym = make_float2(__shfl_sync(0xffffffffu, s.x, src), __shfl_sync(0xffffffffu, s.y, src));
+        if (t == 0) ym = v[(E - j) & (E - 1)];
+        gl[(2 * j) * ts] = r2c_post_f(v[j], ym, twP[t + P * j]);
+    }
+    if (t == 0) *gnyq = make_float2(v[0].x - v[0].y, 0.f);
+}
+
+template <class X>
+cudaError_t xlattr() {
+    return cudaFuncSetAttribute(k_xlane<X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)X::SMEM);
+}
+template <class X>
+cudaError_t xllaunch(const pfc_ctx* c, void* b, double mul, double C, double mu, int nrows) {
+    if (nrows % X::R) return cudaErrorNotSupported;
+    const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->xpass_tw_off;
+    k_xlane<X><<<dim3(nrows / X::R, 1, c->batch), X::T, X::SMEM, c->stream>>>((float2*)b, nrows, tw, (float)mul,
+                                                                              (float)C, (float)mu, c->mstride);
+    return cudaGetLastError();
+}
+using XL512 = XLCfg<512>;
+
 using XP512 = XPCfg<512, 16>;
 using XP128 = XPCfg<128, 8>;
 
@@ -533,7 +639,8 @@ cudaError_t set_pass_attributes(const pfc_ctx* c) {
         case 4: e = xattr<X64>(); break;
         case 5: e = xattr<X512h>(); break;
     }
-    if (!e && c->xpair) e = c->nx == 512 ? xpattr<XP512>() : xpattr<XP128>();
+    if (!e && c->xkern == 1) e = c->nx == 512 ? xpattr<XP512>() : xpattr<XP128>();
+    if (!e && c->xkern == 2) e = xlattr<XL512>();
     return e;
 }
 
@@ -563,12 +670,13 @@ cudaError_t xdispatch(const pfc_ctx* c, const void* in, void* out, const void* p
 cudaError_t launch_xpass(const pfc_ctx* c, void* b, const void* pot, double mul, double C, double mu, int nzs,
                          int lay) {
     if (lay == 2 && nzs != c->nz) return cudaErrorNotSupported;
-    if (lay == 2 && !pot && c->xpair) {
+    if (lay == 2 && !pot && c->xkern == 1) {
         switch (c->nx) {
             case 512: return xplaunch<XP512>(c, b, mul, C, mu, nzs * c->ny);
             case 128: return xplaunch<XP128>(c, b, mul, C, mu, nzs * c->ny);
         }
     }
+    if (lay == 2 && !pot && c->xkern == 2 && c->nx == 512) return xllaunch<XL512>(c, b, mul, C, mu, nzs * c->ny);
     if (lay == 2) return xdispatch<3>(c, b, b, pot, mul, C, mu, nzs * c->ny);
     if (lay != 0) return cudaErrorNotSupported;
     return xdispatch<0>(c, b, b, pot, mul, C, mu, nzs * c->ny);
@@ -599,8 +707,14 @@ cudaError_t set_zfft_attributes(const pfc_ctx* c) {
     }
     return cudaSuccess;
 }
-// the packed row-pair x pass exists for nx = 2 E^2 (128 and 512)
-int xpair_variant(int nx, int dtype) { return dtype == PFC_F32 && (nx == 512 || nx == 128) ? 1 : 0; }
+// the packed row-pair x pass exists for nx = 2 E^2 (128 and 512), the row per half-warp for 512
+int xkernel_variants(int nx, int dtype) {
+    if (dtype != PFC_F32) return 1;
+    return 1 | (nx == 512 || nx == 128 ? 2 : 0) | (nx == 512 ? 4 : 0);
+}
+// k_xlane where the length has it (512: 0.309 against 0.338 ms for k_xrow and 0.348 for
+// k_xpair per 512^3 pass), else k_xrow
+int default_xkernel(int variants) { return (variants & 4) ? 2 : 0; }
 
 cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay) {
     switch (c->fused_zfft) {

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <mutex>
 #include "pfc_ctx.h"
+#include <type_traits>
 
 namespace pfc {
 namespace {
@@ -239,6 +240,89 @@ __global__ void __launch_bounds__(kTX * kTY) k_peaks_mark(const T* __restrict__ 
     }
 }
 
+// The same stencil for FP32 3D fields with nx a multiple of 128 and ny of 16, at fewer
+// instructions per cell: a CTA of 18 warps owns 128 x 16 cells of kZC4 consecutive planes.
+// Warp w holds row y0 + w - 1 (w = 0 and 17 are the periodic halo rows), lane L the four
+// cells x0 + 4L .. 4L + 3 (one 16-byte load per plane).  In a plane each lane forms, per
+// cell, lr = max of its two x neighbours (the outer ones by warp shuffle, the warp's edges
+// loaded by lanes 0 and 31) and h = max(lr, psi); h goes to shared memory (double-buffered,
+// one barrier per plane), and the interior warps read the rows above and below:
+// M9 = max(h(y-1), h, h(y+1)), N8 = max(h(y-1), h(y+1), lr).  The 3D test and the NaN
+// semantics are k_peaks_mark's.  The four bits of a lane are OR-ed over the eight lanes of
+// a mask word by three shuffles.  Loads run two planes ahead of their use.
+constexpr int kZC4 = 32, kRows4 = 16;
+
+__device__ __forceinline__ float4 nmax4(float4 a, float4 b) {
+    return make_float4(nmax(a.x, b.x), nmax(a.y, b.y), nmax(a.z, b.z), nmax(a.w, b.w));
+}
+
+struct Plane4 {
+    float4 q;  // the lane's four cells
+    float e;   // lane 0: the cell left of the warp's row segment; lane 31: the cell right of it
+};
+
+__global__ void __launch_bounds__(32 * (kRows4 + 2), 2)
+    k_peaks_mark4(const float* __restrict__ psi, int nx, int ny, int nz, float ths, uint32_t* __restrict__ mask,
+                  int wpr) {
+    __shared__ float4 H[2][kRows4 + 2][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int x0 = blockIdx.x * 128, y0 = blockIdx.y * kRows4, z0 = blockIdx.z * kZC4;
+    const int zend = min(z0 + kZC4, nz);
+    int y = y0 + w - 1;
+    y = y < 0 ? y + ny : (y >= ny ? y - ny : y);
+    const float* rowp = psi + (int64_t)y * nx + x0 + 4 * lane;  // the lane's cells in plane 0
+    // the edge cell of lanes 0 and 31, relative to rowp (periodic in x)
+    const bool edge = lane == 0 || lane == 31;
+    const int eoff = lane == 0 ? (x0 == 0 ? nx - 1 : -1) : (x0 + 128 == nx ? -x0 - 124 : 4);
+    const int64_t plane = (int64_t)ny * nx;
+    auto load = [&](int zp) {
+        const int zz = zp < 0 ? zp + nz : (zp >= nz ? zp - nz : zp);
+        const float* p = rowp + zz * plane;
+        Plane4 o;
+        o.q = *reinterpret_cast<const float4*>(p);
+        o.e = edge ? p[eoff] : 0.f;
+        return o;
+    };
+    const bool interior = w >= 1 && w <= kRows4;
+    float4 m9p = make_float4(0.f, 0.f, 0.f, 0.f), m9c = m9p, n8c = m9p, vc = m9p;
+    const int zfirst = z0 - 1, zlast = zend;
+    Plane4 a = load(zfirst), b = load(zfirst + 1);
+    for (int zp = zfirst; zp <= zlast; ++zp) {
+        const Plane4 cur = a;
+        a = b;
+        if (zp + 2 <= zlast) b = load(zp + 2);
+        const float4 q = cur.q;
+        float left = __shfl_up_sync(0xffffffffu, q.w, 1), right = __shfl_down_sync(0xffffffffu, q.x, 1);
+        if (lane == 0) left = cur.e;
+        if (lane == 31) right = cur.e;
+        const float4 lr = make_float4(nmax(left, q.y), nmax(q.x, q.z), nmax(q.y, q.w), nmax(q.z, right));
+        const float4 h = nmax4(lr, q);
+        const int buf = (zp - zfirst) & 1;
+        H[buf][w][lane] = h;
+        __syncthreads();
+        if (interior) {
+            const float4 up = H[buf][w - 1][lane], dn = H[buf][w + 1][lane];
+            const float4 ud = nmax4(up, dn);
+            const float4 m9 = nmax4(ud, h), n8 = nmax4(ud, lr);
+            if (zp >= z0 + 1) {
+                // the cells of plane zp - 1: M9(zp - 2), N8(zp - 1), M9(zp)
+                const float4 m = nmax4(nmax4(m9p, n8c), m9);
+                uint32_t nib = (vc.x > m.x && vc.x >= ths ? 1u : 0u) | (vc.y > m.y && vc.y >= ths ? 2u : 0u) |
+                               (vc.z > m.z && vc.z >= ths ? 4u : 0u) | (vc.w > m.w && vc.w >= ths ? 8u : 0u);
+                nib <<= 4 * (lane & 7);
+                nib |= __shfl_xor_sync(0xffffffffu, nib, 1);
+                nib |= __shfl_xor_sync(0xffffffffu, nib, 2);
+                nib |= __shfl_xor_sync(0xffffffffu, nib, 4);
+                if ((lane & 7) == 0) mask[((int64_t)(zp - 1) * ny + y) * wpr + (x0 >> 5) + (lane >> 3)] = nib;
+            }
+            m9p = m9c;
+            m9c = m9;
+            n8c = n8;
+            vc = q;
+        }
+    }
+}
+
 // A chunk of kChunkWords mask words per block: warp w takes words [w 1024, (w + 1) 1024) of
 // the chunk, 32 consecutive words (one per lane) per iteration -- coalesced.
 __device__ __forceinline__ int warp_incl_scan(int v, int lane) {
@@ -332,7 +416,11 @@ cudaError_t peaks_ctx(const pfc_ctx* c, const void* psi, double ths, void* out, 
     const int64_t nwords = (int64_t)c->nz * c->ny * wpr;
     const int nchunks = (int)((nwords + kChunkWords - 1) / kChunkWords);
     dim3 grid(wpr, (c->ny + kTY - 1) / kTY, d3 ? (c->nz + kZC - 1) / kZC : 1);
-    if (d3)
+    if (std::is_same<T, float>::value && d3 && c->nx % 128 == 0 && c->ny % kRows4 == 0 &&
+        ((uintptr_t)psi & 15) == 0)
+        k_peaks_mark4<<<dim3(c->nx / 128, c->ny / kRows4, (c->nz + kZC4 - 1) / kZC4), 32 * (kRows4 + 2), 0,
+                        c->stream>>>((const float*)psi, c->nx, c->ny, c->nz, (float)ths, c->peak_mask, wpr);
+    else if (d3)
         k_peaks_mark<T, true><<<grid, dim3(kTX, kTY), 0, c->stream>>>((const T*)psi, c->nx, c->ny, c->nz, (T)ths,
                                                                        c->peak_mask, wpr);
     else

@@ -72,7 +72,7 @@ struct pfc_ctx {
     int zfft_tw_off;              // W_nz^m of the plain z transforms
     int ypass_tw_off;             // W_ny^m
     int xpass_tw_off;             // W_{nx/2}^m, then W_nx^k (k <= nx/2)
-    int xpair;                    // the row-tiled x pass on row pairs (k_xpair) for this nx
+    int xkern;                    // the row-tiled x pass: 0 k_xrow, 1 k_xpair (row pairs), 2 k_xlane
     int xpair_tw_off;             // W_nx^m, m < nx
     int xy_mode;                  // 0 general passes, 2 register y/x/y passes
     // tracing (pfc_profile_enable / pfc_profile_read)
@@ -130,7 +130,9 @@ cudaError_t launch_zprop_cols(const pfc_ctx* c, void* A, const void* B, const ZP
 // ---- register-resident y and x passes (kern_passes.cu) ----
 int fused_y_variant(int ny, int dtype);
 int fused_x_variant(int nx, int dtype);
-int xpair_variant(int nx, int dtype);
+// the row-tiled x kernels this nx has (bit i: x kernel i; bit 0 always) and the default among them
+int xkernel_variants(int nx, int dtype);
+int default_xkernel(int variants);
 cudaError_t set_pass_attributes(const pfc_ctx* c);
 // y FFT of nzs consecutive planes starting at in / out (in may equal out); lay & 3 / lay
 // >> 2: the layouts of in / out (col_addr; tiled: whole fields only, not in place)

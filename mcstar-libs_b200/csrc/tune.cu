@@ -46,7 +46,7 @@ std::string device_key(const pfc_desc* d) {
 
 std::string options_json(const pfc_options& o, double ms) {
     std::ostringstream s;
-    s << "{\"z_carry\": " << o.z_carry << ", \"x_pair\": " << o.x_pair << ", \"tiled\": " << o.tiled
+    s << "{\"z_carry\": " << o.z_carry << ", \"x_kernel\": " << o.x_kernel << ", \"tiled\": " << o.tiled
       << ", \"radix_order\": " << o.radix_order << ", \"tile_shift\": [" << o.tile_shift[0] << ", " << o.tile_shift[1]
       << ", " << o.tile_shift[2] << ", " << o.tile_shift[3] << "], \"ms_per_step\": " << ms << "}";
     return s.str();
@@ -96,7 +96,7 @@ bool field_int(const std::string& obj, const char* name, int* v) {
 
 bool parse_entry(const std::string& obj, pfc_options* o, double* ms) {
     pfc_default_options(o);
-    if (!field_int(obj, "z_carry", &o->z_carry) || !field_int(obj, "x_pair", &o->x_pair) ||
+    if (!field_int(obj, "z_carry", &o->z_carry) || !field_int(obj, "x_kernel", &o->x_kernel) ||
         !field_int(obj, "tiled", &o->tiled) || !field_int(obj, "radix_order", &o->radix_order))
         return false;
     const size_t p = obj.find("\"tile_shift\":");
@@ -181,14 +181,15 @@ extern "C" pfc_status pfc_tune(const pfc_desc* d, const char* cache_path, pfc_op
     // which options touch a kernel of this shape: ask a context with the library's choice
     pfc_options cur;
     pfc_default_options(&cur);
-    bool general = false, zreg = false, xpair = false, tiled_ok = false;
+    bool general = false, zreg = false, tiled_ok = false;
+    int xks = 1;
     {
         pfc_ctx* c = nullptr;
         pfc_status s = pfc_create_with(d, &cur, &c);
         if (s != PFC_OK) return s;
         general = c->xy_mode != 2 || (c->nz > 1 && !c->fused_z);
         zreg = c->fused_z != 0;
-        xpair = c->fused_x && pfc::xpair_variant(c->nx, c->dtype);
+        xks = c->fused_x ? pfc::xkernel_variants(c->nx, c->dtype) : 1;
         tiled_ok = c->fused_z && c->fused_zfft && c->xy_mode == 2 && c->fused_y;
         pfc_get_options(c, &cur);  // the library's choices, explicit
         pfc_destroy(c);
@@ -203,7 +204,12 @@ extern "C" pfc_status pfc_tune(const pfc_desc* d, const char* cache_path, pfc_op
     }
     std::vector<Knob> knobs;
     if (zreg) knobs.push_back({"z_carry", &cur.z_carry, {0, 1}});
-    if (xpair) knobs.push_back({"x_pair", &cur.x_pair, {0, 1}});
+    if (xks > 1) {
+        Knob k{"x_kernel", &cur.x_kernel, {}};
+        for (int v = 0; v < 3; ++v)
+            if ((xks >> v) & 1) k.values.push_back(v);
+        knobs.push_back(k);
+    }
     if (tiled_ok) knobs.push_back({"tiled", &cur.tiled, {0, 1}});
     if (general) {
         knobs.push_back({"radix_order", &cur.radix_order, {0, 1, 2}});

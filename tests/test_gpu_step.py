@@ -56,15 +56,16 @@ def test_step_matches_oracle(shape, dtype, namp):
 
 VARIANT_SHAPES = [((64, 64, 64), 0.02), ((128, 128, 16), 0.0), ((32, 16, 128), 0.05), ((256, 256, 8), 0.0),
                   ((512, 512, 4), 0.0), ((16, 16, 512), 0.03), ((16, 8, 512), 0.0), ((64, 64, 512), 0.02),
-                  ((128, 64, 512), 0.0), ((48, 40, 30), 0.02), ((96, 80, 1), 0.0)]
-OPTIONS = [dict(z_carry=1), dict(z_carry=0), dict(tiled=0), dict(x_pair=0), dict(z_carry=1, tiled=0),
+                  ((128, 64, 512), 0.0), ((512, 64, 64), 0.02), ((512, 128, 64), 0.0), ((48, 40, 30), 0.02), ((96, 80, 1), 0.0)]
+OPTIONS = [dict(z_carry=1), dict(z_carry=0), dict(tiled=0), dict(x_kernel=0), dict(x_kernel=1), dict(x_kernel=2),
+           dict(x_kernel=2, z_carry=0), dict(z_carry=1, tiled=0),
            dict(radix_order=1), dict(radix_order=2), dict(tile_shift=[1, 2, 1, 2]), dict(tile_shift=[3, 3, 4, 3])]
 
 
 @pytest.mark.parametrize("options", OPTIONS, ids=lambda o: ",".join(f"{k}={v}" for k, v in o.items()))
 def test_step_kernel_schedules_match_oracle(options):
     """Every kernel schedule a context can be made with (pfc_options: the z pass carrying
-    psi^ or A, the standard or kx-tiled layout, single-row or row-pair x pass, the general
+    psi^ or A, the standard or kx-tiled layout, the three x kernels, the general
     passes' radix order and tiles) computes the same step.  Options a shape has no kernel
     for are refused at creation (PFC_ERR_UNSUPPORTED) and skipped."""
     from mcstar_b200 import PfcError, Stepper
