@@ -279,6 +279,15 @@ typedef enum pfc_propagator {
 } pfc_propagator;
 pfc_status pfc_step_prop(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params* params, int propagator,
                          double* max_change);
+/* pfc_step with the field in host memory: the driver's `d_arr << h_arr`, the steps and
+ * `h_arr << d_arr` (the copies of cuda/array_abstraction.hpp:86-96) as one call.  host_in
+ * holds psi^ (state layout, pfc_state_bytes(ctx) bytes; pinned memory for the copies to
+ * overlap), kpsi is the device state buffer (it holds psi^ at the end, as after pfc_step),
+ * host_out receives the final psi^ (may be host_in).  The copy in runs by ky chunks
+ * overlapped with the step's entry pass, the copy out by ky chunks overlapped with the last
+ * step's z pass.  Returns when host_out is written. */
+pfc_status pfc_step_host(pfc_ctx* ctx, const void* host_in, void* host_out, void* kpsi, int nsteps,
+                         const pfc_step_params* params);
 
 /* ---- ensembles (no counterpart in mcstar-libs, whose drivers run one field per process):
  * n independent fields, each with its own context (contexts and buffers must not be

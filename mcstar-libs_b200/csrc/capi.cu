@@ -104,6 +104,9 @@ pfc_status cuda_fail(pfc_ctx* c, cudaError_t e, const char* where) {
 void free_ctx(pfc_ctx* c) {
     if (!c) return;
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->host_ev)
+        if (e) cudaEventDestroy(e);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     void* ptrs[] = {c->tw,          c->work,         c->work2,        c->red,       c->k0,
                     c->flag,        c->peak_counts,  c->peak_offsets, c->bond_scratch, c->bond_pairs,
                     c->peak_mask};
@@ -529,15 +532,24 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
             cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
         cudaGetLastError();
     }
-    // tiles: two ping-pong buffers of `tile` lines per CTA, halved tile_shift times
+    // tiles: two ping-pong buffers of `tile` lines per CTA, halved tile_shift times; a pass
+    // with few lines takes smaller tiles, so that it still has two CTAs per SM
     auto shifted = [](int t, int sh) { return std::max(1, t >> sh); };
-    c->px.tile = shifted(pow2_floor((64 * 1024) / (2 * (size_t)lx * csz), 16), o.tile_shift[0]);
+    auto fit = [&](int t, int64_t lines) {
+        while (t > 1 && (lines + t - 1) / t < 2 * (int64_t)c->num_sms) t >>= 1;
+        return t;
+    };
+    const int64_t nyz = (int64_t)c->ny * c->nz;
+    c->px.tile = shifted(fit(pow2_floor((64 * 1024) / (2 * (size_t)lx * csz), 16), nyz), o.tile_shift[0]);
     c->px.smem = 2 * (size_t)c->px.tile * lx * csz;
-    c->py.tile = shifted(pow2_floor((64 * 1024) / (2 * (size_t)c->ny * csz), 16), o.tile_shift[1]);
+    c->py.tile = shifted(fit(pow2_floor((64 * 1024) / (2 * (size_t)c->ny * csz), 16), (int64_t)c->nxh * c->nz),
+                         o.tile_shift[1]);
     c->py.smem = 2 * (size_t)c->py.tile * c->ny * csz;
-    c->pz.tile = shifted(pow2_floor((64 * 1024) / (2 * (size_t)c->nz * csz), 16), o.tile_shift[2]);
+    c->pz.tile = shifted(fit(pow2_floor((64 * 1024) / (2 * (size_t)c->nz * csz), 16), (int64_t)c->nxh * c->ny),
+                         o.tile_shift[2]);
     c->pz.smem = 2 * (size_t)c->pz.tile * c->nz * csz;
-    c->pzprop.tile = shifted(pow2_floor((96 * 1024) / (4 * (size_t)c->nz * csz), 8), o.tile_shift[3]);
+    c->pzprop.tile = shifted(fit(pow2_floor((96 * 1024) / (4 * (size_t)c->nz * csz), 8), (int64_t)c->nxh * c->ny),
+                             o.tile_shift[3]);
     c->pzprop.smem = 4 * (size_t)c->pzprop.tile * c->nz * csz;
     if (c->px.smem > kMaxDynSmem || c->py.smem > kMaxDynSmem || c->pz.smem > kMaxDynSmem ||
         c->pzprop.smem > kMaxDynSmem) {
@@ -784,6 +796,90 @@ pfc_status pfc_step_prop(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_pa
         std::memcpy(&m, &flag[2], sizeof(float));
         *max_change = (double)m;
     }
+    return PFC_OK;
+}
+
+// ---- the step with the field in host memory ---------------------------------------------------
+// The field comes in by ky chunks (nz rows of nky (nx/2+1) modes each, one strided copy per
+// chunk on the copy stream) into `work`, and the entry pass (psi^ -> z-tiled psi^, A) runs
+// on each chunk as soon as it has arrived; the last step's z pass runs by the same chunks,
+// each copied back as soon as it is written.  Only the schedule that carries psi^ z-tiled
+// has chunked entry and last passes; others copy, step and copy back in order.
+pfc_status pfc_step_host(pfc_ctx* ctx, const void* host_in, void* host_out, void* kpsi, int nsteps,
+                         const pfc_step_params* p) {
+    PFC_CHECK_CTX();
+    if (!host_in || !host_out || !kpsi || !p || nsteps < 0)
+        return fail(ctx, PFC_ERR_INVALID, "pfc_step_host: bad arguments");
+    const size_t S = ctx->state_bytes * ctx->batch;
+    constexpr int G = pfc_ctx::kHostChunks;
+    const bool chunked = ctx->tiled && ctx->z_carry && ctx->batch == 1 && nsteps >= 1 && ctx->ny % G == 0;
+    if (!chunked) {
+        PFC_CUDA(cudaMemcpyAsync(kpsi, host_in, S, cudaMemcpyHostToDevice, ctx->stream), "pfc_step_host copy in");
+        pfc_status st = pfc_step(ctx, kpsi, nsteps, p);
+        if (st != PFC_OK) return st;
+        PFC_CUDA(cudaMemcpyAsync(host_out, kpsi, S, cudaMemcpyDeviceToHost, ctx->stream), "pfc_step_host copy out");
+        PFC_CUDA(cudaStreamSynchronize(ctx->stream), "pfc_step_host sync");
+        return PFC_OK;
+    }
+    if (!ctx->copy_stream) {
+        PFC_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "pfc_step_host stream");
+        for (cudaEvent_t& e : ctx->host_ev) PFC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "pfc_step_host event");
+    }
+    cudaStream_t cs = ctx->copy_stream;
+    cudaEvent_t* ev_in = ctx->host_ev;           // chunk g has arrived
+    cudaEvent_t* ev_out = ctx->host_ev + G;      // chunk g of psi^' is written
+    cudaEvent_t ev_start = ctx->host_ev[2 * G], ev_done = ctx->host_ev[2 * G + 1];
+    const int cky = ctx->ny / G;
+    const size_t pitch = (size_t)ctx->nxh * ctx->ny * sizeof(float2), width = (size_t)ctx->nxh * cky * sizeof(float2);
+    ZPropArgs za = zargs(ctx, p);
+    PFC_CUDA(cudaMemsetAsync(ctx->flag, 0, 3 * sizeof(int), ctx->stream), "pfc_step_host flag");
+    // the copies start after the work already queued on the context's stream (work is free)
+    PFC_CUDA(cudaEventRecord(ev_start, ctx->stream), "pfc_step_host event");
+    PFC_CUDA(cudaStreamWaitEvent(cs, ev_start, 0), "pfc_step_host wait");
+    for (int g = 0; g < G; ++g) {
+        PFC_CUDA(cudaMemcpy2DAsync((char*)ctx->work + g * width, pitch, (const char*)host_in + g * width, pitch, width,
+                                   ctx->nz, cudaMemcpyHostToDevice, cs),
+                 "pfc_step_host copy in");
+        PFC_CUDA(cudaEventRecord(ev_in[g], cs), "pfc_step_host event");
+    }
+    for (int g = 0; g < G; ++g) {
+        PFC_CUDA(cudaStreamWaitEvent(ctx->stream, ev_in[g], 0), "pfc_step_host wait");
+        PFC_CUDA(traced(ctx, 0, g == 0 ? 3 : 2,
+                        [&] {
+                            cudaError_t e = g == 0 ? launch_k0_save(ctx, ctx->work) : cudaSuccess;
+                            if (!e) e = launch_relayout(ctx, ctx->work, ctx->work2, 1, g * cky, cky);
+                            if (!e) e = launch_zfft(ctx, 1, ctx->work2, kpsi, 1.0 / ctx->nz, kLayZ | kLayZ << 2, g * cky, cky);
+                            return e;
+                        }),
+                 "pfc_step_host entry");
+    }
+    for (int t = 0; t < nsteps; ++t) {
+        const bool last = t == nsteps - 1;
+        PFC_CUDA(step_xy(ctx, kpsi, p, last), "pfc_step_host xy");
+        za.counter = p->counter + (uint64_t)t;
+        za.final_step = last;
+        if (!last) {
+            PFC_CUDA(step_z(ctx, kpsi, za), "pfc_step_host z");
+            continue;
+        }
+        for (int g = 0; g < G; ++g) {
+            PFC_CUDA(traced(ctx, 2, 1,
+                            [&] { return launch_zcarry_tiled(ctx, ctx->work2, kpsi, kpsi, nullptr, za, g * cky, cky); }),
+                     "pfc_step_host z");
+            PFC_CUDA(cudaEventRecord(ev_out[g], ctx->stream), "pfc_step_host event");
+            PFC_CUDA(cudaStreamWaitEvent(cs, ev_out[g], 0), "pfc_step_host wait");
+            PFC_CUDA(cudaMemcpy2DAsync((char*)host_out + g * width, pitch, (const char*)kpsi + g * width, pitch, width,
+                                       ctx->nz, cudaMemcpyDeviceToHost, cs),
+                     "pfc_step_host copy out");
+        }
+    }
+    PFC_CUDA(cudaEventRecord(ev_done, cs), "pfc_step_host event");
+    PFC_CUDA(cudaStreamWaitEvent(ctx->stream, ev_done, 0), "pfc_step_host wait");
+    int flag[3] = {0, 0, 0};
+    PFC_CUDA(cudaMemcpyAsync(flag, ctx->flag, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream), "pfc_step_host flag");
+    PFC_CUDA(cudaStreamSynchronize(ctx->stream), "pfc_step_host sync");
+    if (flag[0] & kFlagWaitTimeout) return fail(ctx, PFC_ERR_CUDA, "pfc_step_host: a device wait timed out");
+    if (flag[0]) return fail(ctx, PFC_ERR_NONFINITE, "pfc_step_host: non-finite value in the state");
     return PFC_OK;
 }
 

@@ -195,6 +195,89 @@ struct ZArgsT {
     int ky0, nyg;                           // a ky-slab: the field's first row here and its row count
 };
 
+// The field of a batch this CTA steps (grid z): its noise counter and parameters.
+template <typename T>
+__device__ __forceinline__ void zmember(ZArgsT<T>& a) {
+    if (a.dev_counter) a.dev_counter += blockIdx.z;
+    if (a.margs) {
+        const MemberArgs m = a.margs[blockIdx.z];
+        a.eps = (T)m.eps;
+        a.namp_eff = (T)m.namp_eff;
+        a.seed = m.seed;
+    }
+}
+
+// The update of mode (kx, kyg, kz) from psi^ and N^ (the propagator PROP, conserved noise,
+// the FP64 k = 0 mode); k1 = the ky wavenumber, deps = 1 + C - eps.  The relaxations fold
+// |psi^' - psi^| into mc.
+template <typename T, int PROP>
+__device__ __forceinline__ cx<T> zmode(cx<T> psi, cx<T> nl, int kx, int kyg, int kz, int nx, int nz, T k1, T deps,
+                                       const ZArgsT<T>& a, const double2* __restrict__ k0, float& mc) {
+    const T kk0 = kwave<T>(kx, nx, a.lx), kk2 = kwave<T>(kz, nz, a.lz);
+    const T dopx = -kk0 * kk0 - k1 * k1 - kk2 * kk2;
+    cx<T> v;
+    if constexpr (PROP == kPropConserved) {
+        const T dopy = dopx * dopx;
+        const T denom = T(1) - a.dt * (deps * dopx + T(2) * dopy + dopx * dopy);
+        if (kx == 0 && kyg == 0 && kz == 0) psi = mkc<T>((T)k0->x, (T)k0->y);
+        const T f = a.dt * dopx;
+        cx<T> num = mkc<T>(psi.x + f * nl.x, psi.y + f * nl.y);
+        if (a.use_noise) {
+            const T kabs = sqrt(-dopx);
+            const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
+            const cx<T> xi = kspace_noise<T>(kx, kyg, kz, nx, a.nyg, nz, a.seed, ctr);
+            const T g = a.dt * a.namp_eff * kabs;
+            num.x += g * xi.x;
+            num.y += g * xi.y;
+        }
+        v = mkc<T>(num.x / denom, num.y / denom);
+    } else {
+        if (prop_conserved<PROP>() && kx == 0 && kyg == 0 && kz == 0) psi = mkc<T>((T)k0->x, (T)k0->y);
+        T ca, cb, cg;
+        prop_coef<PROP, T>(dopx, a.dt, deps, ca, cb, cg);
+        v = mkc<T>(ca * psi.x + cb * nl.x, ca * psi.y + cb * nl.y);
+        if (prop_conserved<PROP>() && a.use_noise) {
+            const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
+            const cx<T> xi = kspace_noise<T>(kx, kyg, kz, nx, a.nyg, nz, a.seed, ctr);
+            v.x += a.namp_eff * cg * xi.x;
+            v.y += a.namp_eff * cg * xi.y;
+        }
+        if (!prop_conserved<PROP>()) {
+            const T dx = v.x - psi.x, dy = v.y - psi.y;
+            mc = fmaxf(mc, (float)sqrt(dx * dx + dy * dy));
+        }
+    }
+    return v;
+}
+
+// The z pass of a field with nz = 1 (2D): no z transform, so the update of every mode in
+// place, one thread per mode of the columns [col0, col0 + ncols) of every ky row.
+template <typename T, int PROP>
+__global__ void __launch_bounds__(256) k_zflat(cx<T>* A, const cx<T>* __restrict__ B, int nx, int ny, ZArgsT<T> a,
+                                               const double2* __restrict__ k0, int* flag, int col0, int ncols,
+                                               int64_t ms) {
+    A += blockIdx.z * ms;
+    B += blockIdx.z * ms;
+    k0 += blockIdx.z;
+    zmember(a);
+    const int nxh = nx / 2 + 1;
+    const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = m < (int64_t)ncols * ny;
+    float mc = 0.f;
+    bool bad = false;
+    if (valid) {
+        const int ky = (int)(m / ncols), kx = col0 + (int)(m - (int64_t)ky * ncols);
+        const int64_t off = (int64_t)ky * nxh + kx;
+        const int kyg = ky + a.ky0;
+        const T k1 = kwave<T>(kyg, a.nyg, a.ly);
+        const cx<T> v = zmode<T, PROP>(A[off], B[off], kx, kyg, 0, nx, 1, k1, T(1) + a.C - a.eps, a, k0, mc);
+        bad = !isfinite(v.x) || !isfinite(v.y);
+        A[off] = v;
+    }
+    if (!prop_conserved<PROP>() && a.maxc) fold_max_change(mc, a.maxc);
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
 template <typename T, int PROP>
 __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict__ B, int nx, int ny, int nz,
                                                LinePlan p, const cx<T>* __restrict__ tw, int tile, ZArgsT<T> a,
@@ -204,13 +287,7 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
     A += blockIdx.z * ms;
     B += blockIdx.z * ms;
     k0 += blockIdx.z;
-    if (a.dev_counter) a.dev_counter += blockIdx.z;
-    if (a.margs) {
-        const MemberArgs m = a.margs[blockIdx.z];
-        a.eps = (T)m.eps;
-        a.namp_eff = (T)m.namp_eff;
-        a.seed = m.seed;
-    }
+    zmember(a);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int bad;
     cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
@@ -240,42 +317,7 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
     for (int e = threadIdx.x; e < nt * n; e += blockDim.x) {
         const int i = e / n, kz = e - i * n;
         const int kx = i0 + i;
-        cx<T> psi = r[i * n + kz];
-        const cx<T> nl = r[(tile + i) * n + kz];
-        const T kk0 = kwave<T>(kx, nx, a.lx), kk2 = kwave<T>(kz, nz, a.lz);
-        const T dopx = -kk0 * kk0 - k1 * k1 - kk2 * kk2;
-        cx<T> v;
-        if constexpr (PROP == kPropConserved) {
-            const T dopy = dopx * dopx;
-            const T denom = T(1) - a.dt * (deps * dopx + T(2) * dopy + dopx * dopy);
-            if (kx == 0 && kyg == 0 && kz == 0) psi = mkc<T>((T)k0->x, (T)k0->y);
-            const T f = a.dt * dopx;
-            cx<T> num = mkc<T>(psi.x + f * nl.x, psi.y + f * nl.y);
-            if (a.use_noise) {
-                const T kabs = sqrt(-dopx);
-                const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
-                const cx<T> xi = kspace_noise<T>(kx, kyg, kz, nx, a.nyg, nz, a.seed, ctr);
-                const T g = a.dt * a.namp_eff * kabs;
-                num.x += g * xi.x;
-                num.y += g * xi.y;
-            }
-            v = mkc<T>(num.x / denom, num.y / denom);
-        } else {
-            if (prop_conserved<PROP>() && kx == 0 && kyg == 0 && kz == 0) psi = mkc<T>((T)k0->x, (T)k0->y);
-            T ca, cb, cg;
-            prop_coef<PROP, T>(dopx, a.dt, deps, ca, cb, cg);
-            v = mkc<T>(ca * psi.x + cb * nl.x, ca * psi.y + cb * nl.y);
-            if (prop_conserved<PROP>() && a.use_noise) {
-                const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
-                const cx<T> xi = kspace_noise<T>(kx, kyg, kz, nx, a.nyg, nz, a.seed, ctr);
-                v.x += a.namp_eff * cg * xi.x;
-                v.y += a.namp_eff * cg * xi.y;
-            }
-            if (!prop_conserved<PROP>()) {
-                const T dx = v.x - psi.x, dy = v.y - psi.y;
-                mc = fmaxf(mc, (float)sqrt(dx * dx + dy * dy));
-            }
-        }
+        const cx<T> v = zmode<T, PROP>(r[i * n + kz], r[(tile + i) * n + kz], kx, kyg, kz, nx, nz, k1, deps, a, k0, mc);
         if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
         r[i * n + kz] = v;
     }
@@ -399,6 +441,12 @@ void zprop_T(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int c
                 (T)a.lx,      (T)a.ly,     (T)a.lz,     a.seed,
                 a.counter,    a.dev_counter, a.use_noise, a.final_step,
                 a.maxc,       a.margs,     a.ky0,       a.ny_global > 0 ? a.ny_global : c->ny};
+    if (c->nz == 1) {
+        const int64_t modes = (int64_t)ncols * c->ny;
+        k_zflat<T, PROP><<<dim3((unsigned)((modes + 255) / 256), 1, c->batch), 256, 0, c->stream>>>(
+            (cx<T>*)A, (const cx<T>*)B, c->nx, c->ny, t, c->k0, c->flag, col0, ncols, c->mstride);
+        return;
+    }
     k_zprop<T, PROP><<<grid, 256, c->pzprop.smem, c->stream>>>((cx<T>*)A, (const cx<T>*)B, c->nx, c->ny, c->nz,
                                                                 c->pz.plan, (const cx<T>*)c->tw, tile, t, c->k0,
                                                                 c->flag, col0, col0 + ncols, c->mstride);

@@ -32,11 +32,11 @@ struct YCfg {
 template <class Y, int DIR, bool kZ>
 __global__ void __launch_bounds__(Y::T, Y::MINB)
     k_ycol(const float2* in, float2* out, int nxh, int ny, int nz, int lay, const float2* __restrict__ twg,
-           float scale, int64_t ms) {
-    // the columns of NY elements of kx tile blockIdx.x at plane blockIdx.y: y columns of
-    // z-plane blockIdx.y (kZ false) or z columns at ky = blockIdx.y (kZ); lay & 3: the
-    // layout of the input, lay >> 2: of the output (col_addr).  With the standard layout on
-    // both sides, in may equal out.  ms: elements between the fields of a batch (grid z).
+           float scale, int64_t ms, int q0) {
+    // the columns of NY elements of kx tile blockIdx.x at plane q0 + blockIdx.y: y columns of
+    // that z-plane (kZ false) or z columns at that ky (kZ); lay & 3: the layout of the input,
+    // lay >> 2: of the output (col_addr).  With the standard layout on both sides, in may
+    // equal out.  ms: elements between the fields of a batch (grid z).
     constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P, U = Y::U;
     in += blockIdx.z * ms;
     out += blockIdx.z * ms;
@@ -48,14 +48,15 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
     const int c = tid % TX, t = tid / TX;
     const int kx = blockIdx.x * TX + c;
     const bool valid = kx < nxh;
-    const ColAddr ai = col_addr(lay & 3, kZ, kx, blockIdx.y, nxh, ny, nz);
+    const int q = q0 + blockIdx.y;
+    const ColAddr ai = col_addr(lay & 3, kZ, kx, q, nxh, ny, nz);
     float2 v[E];
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = valid ? in[ai.base + (int64_t)(t + P * j) * ai.stride] : make_float2(0.f, 0.f);
     __syncthreads();
     fft_d1_to_d2<NY, E, TX, DIR, BarCta, Y::PADG>(v, t, c, xb, tw);
     if (valid) {
-        const ColAddr ao = col_addr(lay >> 2, kZ, kx, blockIdx.y, nxh, ny, nz);
+        const ColAddr ao = col_addr(lay >> 2, kZ, kx, q, nxh, ny, nz);
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
@@ -567,15 +568,15 @@ cudaError_t xattr() {
 // W_NY^m at tw_off
 template <class Y, bool kZ>
 cudaError_t collaunch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int planes, int lay,
-                      int tw_off) {
+                      int tw_off, int q0 = 0) {
     dim3 grid((c->nxh + Y::TX - 1) / Y::TX, planes, c->batch);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + tw_off;
     if (dir > 0)
         k_ycol<Y, 1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->ny, c->nz,
-                                                             lay, tw, (float)scale, c->mstride);
+                                                             lay, tw, (float)scale, c->mstride, q0);
     else
         k_ycol<Y, -1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->ny, c->nz,
-                                                              lay, tw, (float)scale, c->mstride);
+                                                              lay, tw, (float)scale, c->mstride, q0);
     return cudaGetLastError();
 }
 template <class Y>
@@ -583,8 +584,9 @@ cudaError_t ylaunch(const pfc_ctx* c, int dir, const void* in, void* out, double
     return collaunch<Y, false>(c, dir, in, out, scale, nzs, lay, c->ypass_tw_off);
 }
 template <class Y>
-cudaError_t zlaunch_fft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay) {
-    return collaunch<Y, true>(c, dir, in, out, scale, c->ny, lay, c->zfft_tw_off);
+cudaError_t zlaunch_fft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay, int ky0,
+                        int nky) {
+    return collaunch<Y, true>(c, dir, in, out, scale, nky, lay, c->zfft_tw_off, ky0);
 }
 template <class X, int MODE>
 cudaError_t xlaunch(const pfc_ctx* c, const void* in, void* out, const void* pot, double mul, double C, double mu,
@@ -716,12 +718,15 @@ int xkernel_variants(int nx, int dtype) {
 // k_xpair per 512^3 pass), else k_xrow
 int default_xkernel(int variants) { return (variants & 4) ? 2 : 0; }
 
-cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay) {
+cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay, int ky0,
+                        int nky) {
+    if (nky < 0) nky = c->ny - ky0;
+    if (ky0 < 0 || nky < 1 || ky0 + nky > c->ny) return cudaErrorInvalidValue;
     switch (c->fused_zfft) {
-        case 1: return zlaunch_fft<Y512>(c, dir, in, out, scale, lay);
-        case 2: return zlaunch_fft<Y256>(c, dir, in, out, scale, lay);
-        case 3: return zlaunch_fft<Y128>(c, dir, in, out, scale, lay);
-        case 4: return zlaunch_fft<Y64>(c, dir, in, out, scale, lay);
+        case 1: return zlaunch_fft<Y512>(c, dir, in, out, scale, lay, ky0, nky);
+        case 2: return zlaunch_fft<Y256>(c, dir, in, out, scale, lay, ky0, nky);
+        case 3: return zlaunch_fft<Y128>(c, dir, in, out, scale, lay, ky0, nky);
+        case 4: return zlaunch_fft<Y64>(c, dir, in, out, scale, lay, ky0, nky);
     }
     return cudaErrorNotSupported;
 }

@@ -243,28 +243,39 @@ __global__ void __launch_bounds__(kTX * kTY) k_peaks_mark(const T* __restrict__ 
 // The same stencil for FP32 3D fields with nx a multiple of 128 and ny of 16, at fewer
 // instructions per cell: a CTA of 18 warps owns 128 x 16 cells of kZC4 consecutive planes.
 // Warp w holds row y0 + w - 1 (w = 0 and 17 are the periodic halo rows), lane L the four
-// cells x0 + 4L .. 4L + 3 (one 16-byte load per plane).  In a plane each lane forms, per
-// cell, lr = max of its two x neighbours (the outer ones by warp shuffle, the warp's edges
-// loaded by lanes 0 and 31) and h = max(lr, psi); h goes to shared memory (double-buffered,
-// one barrier per plane), and the interior warps read the rows above and below:
-// M9 = max(h(y-1), h, h(y+1)), N8 = max(h(y-1), h(y+1), lr).  The 3D test and the NaN
+// cells x0 + 4L .. 4L + 3.  Planes stream through a ring of kStages4 slots in shared memory
+// by cp.async (each lane copies its own 16 bytes, lanes 0 and 31 also the cell beyond the
+// warp's edge, and reads back only what it copied: no barrier for the ring), kStages4 - 1
+// planes ahead of their use.  In a plane each lane forms, per cell, lr = max of its two x
+// neighbours (the outer ones by warp shuffle) and h = max(lr, psi); h goes to shared memory
+// (double-buffered, one barrier per plane), and the interior warps read the rows above and
+// below: M9 = max(h(y-1), h, h(y+1)), N8 = max(h(y-1), h(y+1), lr).  The 3D test and the NaN
 // semantics are k_peaks_mark's.  The four bits of a lane are OR-ed over the eight lanes of
-// a mask word by three shuffles.  Loads run two planes ahead of their use.
-constexpr int kZC4 = 32, kRows4 = 16;
+// a mask word by three shuffles.
+constexpr int kZC4 = 32, kRows4 = 16, kStages4 = 3;  // (static shared memory: 46 KB)
 
 __device__ __forceinline__ float4 nmax4(float4 a, float4 b) {
     return make_float4(nmax(a.x, b.x), nmax(a.y, b.y), nmax(a.z, b.z), nmax(a.w, b.w));
 }
-
-struct Plane4 {
-    float4 q;  // the lane's four cells
-    float e;   // lane 0: the cell left of the warp's row segment; lane 31: the cell right of it
-};
+__device__ __forceinline__ void cp_async16_cg(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_wait_group() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 __global__ void __launch_bounds__(32 * (kRows4 + 2), 2)
     k_peaks_mark4(const float* __restrict__ psi, int nx, int ny, int nz, float ths, uint32_t* __restrict__ mask,
                   int wpr) {
     __shared__ float4 H[2][kRows4 + 2][32];
+    __shared__ float4 Q[kStages4][kRows4 + 2][32];
+    __shared__ float EG[kStages4][kRows4 + 2][2];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int x0 = blockIdx.x * 128, y0 = blockIdx.y * kRows4, z0 = blockIdx.z * kZC4;
     const int zend = min(z0 + kZC4, nz);
@@ -274,27 +285,32 @@ __global__ void __launch_bounds__(32 * (kRows4 + 2), 2)
     // the edge cell of lanes 0 and 31, relative to rowp (periodic in x)
     const bool edge = lane == 0 || lane == 31;
     const int eoff = lane == 0 ? (x0 == 0 ? nx - 1 : -1) : (x0 + 128 == nx ? -x0 - 124 : 4);
+    float* eslot = &EG[0][w][lane == 0 ? 0 : 1];
     const int64_t plane = (int64_t)ny * nx;
-    auto load = [&](int zp) {
-        const int zz = zp < 0 ? zp + nz : (zp >= nz ? zp - nz : zp);
-        const float* p = rowp + zz * plane;
-        Plane4 o;
-        o.q = *reinterpret_cast<const float4*>(p);
-        o.e = edge ? p[eoff] : 0.f;
-        return o;
+    const int zfirst = z0 - 1, zlast = zend;
+    auto issue = [&](int zp) {
+        if (zp <= zlast) {
+            const int zz = zp < 0 ? zp + nz : (zp >= nz ? zp - nz : zp);
+            const float* p = rowp + zz * plane;
+            const int s = (zp - zfirst) % kStages4;
+            cp_async16_cg(&Q[s][w][lane], p);
+            if (edge) cp_async4(eslot + s * (kRows4 + 2) * 2, p + eoff);
+        }
+        cp_commit_group();  // (empty past the last plane: the group count stays regular)
     };
+#pragma unroll
+    for (int s = 0; s < kStages4 - 1; ++s) issue(zfirst + s);
     const bool interior = w >= 1 && w <= kRows4;
     float4 m9p = make_float4(0.f, 0.f, 0.f, 0.f), m9c = m9p, n8c = m9p, vc = m9p;
-    const int zfirst = z0 - 1, zlast = zend;
-    Plane4 a = load(zfirst), b = load(zfirst + 1);
     for (int zp = zfirst; zp <= zlast; ++zp) {
-        const Plane4 cur = a;
-        a = b;
-        if (zp + 2 <= zlast) b = load(zp + 2);
-        const float4 q = cur.q;
+        issue(zp + kStages4 - 1);  // into the slot of plane zp - 1, which this thread has read
+        cp_wait_group<kStages4 - 1>();
+        const int s = (zp - zfirst) % kStages4;
+        const float4 q = Q[s][w][lane];
+        const float e = edge ? eslot[s * (kRows4 + 2) * 2] : 0.f;
         float left = __shfl_up_sync(0xffffffffu, q.w, 1), right = __shfl_down_sync(0xffffffffu, q.x, 1);
-        if (lane == 0) left = cur.e;
-        if (lane == 31) right = cur.e;
+        if (lane == 0) left = e;
+        if (lane == 31) right = e;
         const float4 lr = make_float4(nmax(left, q.y), nmax(q.x, q.z), nmax(q.y, q.w), nmax(q.z, right));
         const float4 h = nmax4(lr, q);
         const int buf = (zp - zfirst) & 1;
@@ -321,6 +337,7 @@ __global__ void __launch_bounds__(32 * (kRows4 + 2), 2)
             vc = q;
         }
     }
+    cp_wait_group<0>();
 }
 
 // A chunk of kChunkWords mask words per block: warp w takes words [w 1024, (w + 1) 1024) of

@@ -485,12 +485,13 @@ __global__ void __launch_bounds__(Z::TH, Z::CMINB) k_zcarry(float2* kpsi, float2
 // kLast: B and psi^' in the standard layout (psi^' over B, in place), no A'.  Shared
 // memory: the exchange buffer, the stage [kz][c] (a warp's four modes per register have
 // two even and two odd kz: no bank conflicts), the tail.
-// kt0: the kx tile of blockIdx.x = 0 (a launch may cover only some tiles).
+// kt0, ky0: the kx tile and the ky of blockIdx.x = 0 and blockIdx.y = 0 (a launch may cover
+// only some tiles, or some ky).
 template <class Z, bool kLast, int PROP>
 __global__ void __launch_bounds__(Z::TH, 3) k_zcarry3(const float2* psi_in, const float2* B, float2* psi_out,
                                                        float2* A, int nx, int ny, ZArgsF a,
                                                        const double2* __restrict__ k0, int* flag,
-                                                       const float2* __restrict__ twg, int kt0, int64_t ms) {
+                                                       const float2* __restrict__ twg, int kt0, int ky0, int64_t ms) {
     constexpr int NZ = Z::NZ, E = Z::E, TX = Z::TX, P = Z::P, TH = Z::TH;
     static_assert(TX == kTileW, "the tiles of the z-tiled layout");
     psi_in += blockIdx.z * ms;  // fields of a batch (grid z)
@@ -507,7 +508,7 @@ __global__ void __launch_bounds__(Z::TH, 3) k_zcarry3(const float2* psi_in, cons
     const int c = tid % TX, t = tid / TX;
     const int kt = blockIdx.x + kt0;
     const int kx = kt * TX + c;
-    const int ky = blockIdx.y;
+    const int ky = blockIdx.y + ky0;
     const int nxh = nx / 2 + 1;
     const bool valid = kx < nxh;
     const ColAddr cp = zcol_addr<true>(kt, c, ky, nxh, ny, NZ);
@@ -647,9 +648,9 @@ __global__ void __launch_bounds__(Z::TH, 3) k_zbulk(float2* psi, float2* BA, int
 // Copy between the standard and the z-tiled layouts (col_addr layouts 0, 1): one kx tile
 // of the z columns at one ky per CTA of TX * 32 threads.
 __global__ void __launch_bounds__(256) k_relayout(const float2* __restrict__ in, float2* __restrict__ out, int nxh,
-                                                  int ny, int nz, int to_tiled) {
+                                                  int ny, int nz, int to_tiled, int ky0) {
     const int c = threadIdx.x % kTileW, t = threadIdx.x / kTileW;
-    const int kt = blockIdx.x, ky = blockIdx.y;
+    const int kt = blockIdx.x, ky = blockIdx.y + ky0;
     if (kt * kTileW + c >= nxh) return;
     const ColAddr s = to_tiled ? zcol_addr<false>(kt, c, ky, nxh, ny, nz) : zcol_addr<true>(kt, c, ky, nxh, ny, nz);
     const ColAddr d = to_tiled ? zcol_addr<true>(kt, c, ky, nxh, ny, nz) : zcol_addr<false>(kt, c, ky, nxh, ny, nz);
@@ -770,17 +771,19 @@ cudaError_t launch_zcarry(const pfc_ctx* c, void* kpsi, void* A, const void* B, 
 }
 
 cudaError_t launch_zcarry_tiled(const pfc_ctx* c, const void* psi_in, const void* B, void* psi_out, void* A,
-                                const ZPropArgs& a) {
+                                const ZPropArgs& a, int ky0, int nky) {
     if (c->fused_z != 6) return cudaErrorNotSupported;
+    if (nky < 0) nky = c->ny - ky0;
+    if (ky0 < 0 || nky < 1 || ky0 + nky > c->ny || (!a.final_step && nky != c->ny)) return cudaErrorInvalidValue;
     using Z = Z3_512;
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
     const ZArgsF za = zargs_f(a);
     const int ntx = (c->nxh + Z::TX - 1) / Z::TX;
     return by_prop(a.prop, [&](auto P) {
         if (a.final_step) {
-            k_zcarry3<Z, true, P.value><<<dim3(ntx, c->ny, c->batch), Z::TH, Z::SMEM_CARRY, c->stream>>>(
+            k_zcarry3<Z, true, P.value><<<dim3(ntx, nky, c->batch), Z::TH, Z::SMEM_CARRY, c->stream>>>(
                 (const float2*)psi_in, (const float2*)B, (float2*)psi_out, (float2*)A, c->nx, c->ny, za, c->k0,
-                c->flag, tw, 0, c->mstride);
+                c->flag, tw, 0, ky0, c->mstride);
             return cudaGetLastError();
         }
         // whole tiles with bulk copies (psi^ in place, A' over B); the partial last tile with
@@ -793,15 +796,17 @@ cudaError_t launch_zcarry_tiled(const pfc_ctx* c, const void* psi_in, const void
         if (full < ntx)
             k_zcarry3<Z, false, P.value><<<dim3(ntx - full, c->ny, c->batch), Z::TH, Z::SMEM_CARRY, c->stream>>>(
                 (const float2*)psi_in, (const float2*)B, (float2*)psi_out, (float2*)A, c->nx, c->ny, za, c->k0,
-                c->flag, tw, full, c->mstride);
+                c->flag, tw, full, 0, c->mstride);
         return cudaGetLastError();
     });
 }
 
-cudaError_t launch_relayout(const pfc_ctx* c, const void* in, void* out, int to_tiled) {
+cudaError_t launch_relayout(const pfc_ctx* c, const void* in, void* out, int to_tiled, int ky0, int nky) {
     if (c->dtype != PFC_F32 || in == out) return cudaErrorNotSupported;
-    dim3 grid((c->nxh + kTileW - 1) / kTileW, c->ny);
-    k_relayout<<<grid, 256, 0, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->ny, c->nz, to_tiled);
+    if (nky < 0) nky = c->ny - ky0;
+    if (ky0 < 0 || nky < 1 || ky0 + nky > c->ny) return cudaErrorInvalidValue;
+    dim3 grid((c->nxh + kTileW - 1) / kTileW, nky);
+    k_relayout<<<grid, 256, 0, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->ny, c->nz, to_tiled, ky0);
     return cudaGetLastError();
 }
 

@@ -84,6 +84,11 @@ struct pfc_ctx {
     size_t ev_used = 0;
     struct Span { int family; size_t from, to; };     // elapsed time between two pool events
     std::vector<Span> ev_pending;
+    // pfc_step_host: the copy stream and the events that order the field's ky chunks between
+    // it and the context's stream (created by the first call)
+    static constexpr int kHostChunks = 8;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t host_ev[2 * kHostChunks + 2] = {};
 };
 
 namespace pfc {
@@ -149,7 +154,9 @@ cudaError_t launch_xrows_c2r(const pfc_ctx* c, const void* in_cmpl, void* out_re
 int fused_zfft_variant(int nz, int dtype);
 cudaError_t set_zfft_attributes(const pfc_ctx* c);
 // (lay as launch_ypass)
-cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay = 0);
+// (ky0, nky: the z columns of ky in [ky0, ky0 + nky) only; nky < 0: to ny)
+cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay = 0, int ky0 = 0,
+                        int nky = -1);
 
 // ---- spectral low-pass post-processing (kern_lowpass.cu) ----
 cudaError_t launch_gaussian_init(const pfc_ctx* c, void* g, double lx, double ly, double lz, double hx, double hy,
@@ -173,10 +180,11 @@ cudaError_t launch_zcol(const pfc_ctx* c, const void* A, const void* B, void* O,
 cudaError_t launch_zcarry(const pfc_ctx* c, void* kpsi, void* A, const void* B, const ZPropArgs& a);
 // the same on the z-tiled layout (nz = 512): psi^ z-tiled (psi_out may be psi_in); B and A
 // z-tiled (A may be B), or on the last step B and psi_out standard (psi_out may be B), no A
+// (ky0, nky: the last step's z pass over ky in [ky0, ky0 + nky) only; nky < 0: to ny)
 cudaError_t launch_zcarry_tiled(const pfc_ctx* c, const void* psi_in, const void* B, void* psi_out, void* A,
-                                const ZPropArgs& a);
+                                const ZPropArgs& a, int ky0 = 0, int nky = -1);
 // FP32 field copy between the standard and the z-tiled layout (out of place)
-cudaError_t launch_relayout(const pfc_ctx* c, const void* in, void* out, int to_tiled);
+cudaError_t launch_relayout(const pfc_ctx* c, const void* in, void* out, int to_tiled, int ky0 = 0, int nky = -1);
 
 // ---- pointwise kernels, noise and reductions (kern_point.cu) ----
 cudaError_t launch_update_eom(const pfc_ctx* c, void* kpsi, const void* knl, const void* knoise,

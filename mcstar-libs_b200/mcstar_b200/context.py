@@ -220,6 +220,14 @@ class Context:
                    ctypes.byref(m))
         return m.value
 
+    def step_host(self, host_in, host_out, kpsi, nsteps, dt, eps, lens, mu=0.0, C=1.0, namp=0.0, seed=0, counter=0):
+        """pfc_step_host: psi^ from host_in (a CPU tensor, pinned for overlap) through the
+        device buffer kpsi, nsteps fused steps, the final psi^ into host_out."""
+        p = PfcStepParams(float(dt), float(eps), float(mu), float(C), float(namp), float(lens[0]),
+                          float(lens[1]), float(lens[2]), int(seed), int(counter))
+        self._call("pfc_step_host", ctypes.c_void_p(host_in.data_ptr()), ctypes.c_void_p(host_out.data_ptr()),
+                   _ptr(kpsi), int(nsteps), ctypes.byref(p))
+
     # -- reverse mode --------------------------------------------------------------------
     def adjoint_workspace(self):
         """Device workspace of pfc_adjoint_step (two states)."""

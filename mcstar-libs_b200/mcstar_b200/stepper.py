@@ -103,6 +103,13 @@ class Stepper:
         self.counter += int(nsteps)
         return m
 
+    def step_host(self, host_in, host_out, nsteps):
+        """nsteps fused steps of the field held in host memory (pfc_step_host): psi^ from
+        host_in through this stepper's device state, the final psi^ into host_out."""
+        self.ctx.step_host(host_in, host_out, self.kpsi, nsteps, self.dt, self.eps, self.lens, mu=self.mu, C=self.C,
+                           namp=self.namp, seed=self.seed, counter=self.counter)
+        self.counter += int(nsteps)
+
     def free_energy(self):
         return self.ctx.free_energy(self.kpsi, self.eps, self.lens, self.hh)
 

@@ -165,6 +165,29 @@ def test_resume_is_bit_exact(shape):
     np.testing.assert_array_equal(a.kspace(), b.kspace())
 
 
+@pytest.mark.parametrize("shape,nsteps,namp", [((64, 64, 512), 3, 0.05), ((64, 64, 512), 1, 0.0),
+                                               ((128, 64, 512), 2, 0.0), ((32, 24, 20), 3, 0.05)])
+def test_step_host_equals_device_step(shape, nsteps, namp):
+    """pfc_step_host (the field in pinned host memory, copies by ky chunks overlapped with the
+    entry pass and the last z pass; in order where the schedule has no chunked passes) gives
+    the bits of copy in + pfc_step + copy out, with host_out distinct from or equal to host_in."""
+    a = stepper(shape, F32, namp=namp, seed=4)
+    b = stepper(shape, F32, namp=namp, seed=4)
+    rng = np.random.default_rng(8)
+    a.set_real(-0.2 + 0.05 * rng.uniform(-1, 1, shape[::-1]))
+    host_in = a.kpsi.cpu().pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    a.step(nsteps)
+    want = a.kpsi.cpu()
+    b.step_host(host_in, host_out, nsteps)
+    assert torch.equal(host_out, want)
+    assert torch.equal(b.kpsi.cpu(), want)
+    b.kpsi.zero_()
+    b.counter = 0
+    b.step_host(host_in, host_in, nsteps)  # in place on the host
+    assert torch.equal(host_in, want)
+
+
 @pytest.mark.parametrize("dtype,shape,nsteps", [(F64, (64, 64, 1), 20), (F64, (16, 16, 16), 20),
                                                  (F32, (64, 64, 64), 20), (F64, (36, 30, 20), 10)])
 def test_step_vs_reference_cufft(dtype, shape, nsteps):
