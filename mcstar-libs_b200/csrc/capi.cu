@@ -595,6 +595,7 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
     if (e == cudaSuccess && c->fused_z) e = set_zcol_attributes(c);
     if (e == cudaSuccess && c->fused_y) e = set_pass_attributes(c);
     if (e == cudaSuccess && c->fused_zfft) e = set_zfft_attributes(c);
+    if (e == cudaSuccess) e = set_peak_attributes();
     if (e != cudaSuccess) {
         free_ctx(c);
         return PFC_ERR_CUDA;

@@ -400,23 +400,26 @@ __global__ void __launch_bounds__(X::T, 4) k_xpair(float2* g, int nrows, const f
 // P = 16 lanes per row: 512).  Lane t of a row holds modes kx = t + P j (j < E = P), the
 // four-step transforms' D1 = D2 distribution, so nothing is staged through shared memory
 // but the transposes of the two transforms:
-//  - load: mode kx and its split partner nx/2 - kx straight from global memory (the
-//    partner's lines are the ones another j of the same row loads, served by L1);
+//  - load: the lane's modes straight from global memory; the split partner of mode kx,
+//    nx/2 - kx, is register 15 - j of lane 16 - t (lane 0: its own register 16 - j, and
+//    mode nx/2 itself), fetched by warp shuffle;
 //  - C2R: c2r_pre_f, the nx/2-point inverse FFT (one transpose), cubic term, forward FFT
 //    (one transpose), all exchanges within the half-warp (__syncwarp only);
 //  - store: the R2C merge partner Y[(nx/2 - kx) mod nx/2] is register 15 - j of lane 16 - t
-//    (lane 0: its own register (16 - j) mod 16), fetched by warp shuffle; the merged modes go
+//    (lane 0: its own register (16 - j) mod 16), by warp shuffle; the merged modes go
 //    straight to global memory.
-// Exchange slots of a row: (a, b) -> a (P + 1) + b, so both the writes (b = t) and the reads
-// (a = t) of a half-warp fall on 16 distinct 8-byte bank pairs.  The stage twiddles W^{t k1}
-// sit in a [k1][t] table (a half-warp reads 16 consecutive entries).  A CTA holds 16 rows:
-// one 1 KB block of each kx tile of the row-tiled field.
+// The split/merge twiddle W_nx^(t + P j) is W_nx^t (one table read per lane) times the
+// compile-time constant W_(nx/P)^j.  Exchange slots of a row: (a, b) -> a (P + 1) + b, so
+// both the writes (b = t) and the reads (a = t) of a half-warp fall on 16 distinct 8-byte
+// bank pairs.  The stage twiddles W^{t k1} sit in a [k1][t] table (a half-warp reads 16
+// consecutive entries).  A CTA holds 16 rows: one 1 KB block of each kx tile of the
+// row-tiled field.
 template <int NX_>
 struct XLCfg {
     static constexpr int NX = NX_, M = NX / 2, P = 16, E = M / P, R = 16, T = R * P;
     static constexpr int LDA = P + 1, LDG = E * LDA;  // exchange: a stride, row stride
     static constexpr int XB = R * LDG;
-    static constexpr size_t SMEM = (size_t)(XB + E * P + M + 1) * sizeof(float2);
+    static constexpr size_t SMEM = (size_t)(XB + E * P) * sizeof(float2);
     static_assert(E == P && M % kTileW == 0 && P == 2 * kTileW, "shape");
 };
 
@@ -427,25 +430,39 @@ __global__ void __launch_bounds__(X::T, 3) k_xlane(float2* g, int nrows, const f
     g += blockIdx.z * ms;  // fields of a batch (grid z)
     extern __shared__ __align__(16) float2 sm[];
     float2* tw2 = sm + X::XB;  // [k1][t]: W_M^{t k1}
-    float2* twP = tw2 + E * P; // W_NX^k, k <= M
     const int tid = threadIdx.x;
     for (int i = tid; i < E * P; i += X::T) tw2[i] = twg[(i % P) * (i / P)];
-    for (int i = tid; i <= M; i += X::T) twP[i] = twg[M + i];
     const int t = tid % P, rl = tid / P;
+    // the split/merge twiddle of mode t + P j: W_NX^t W_{NX/P}^j (the second a constant)
+    const float2 wt = twg[M + t];
     float2* xr = sm + rl * X::LDG;
     const int64_t ts = (int64_t)kTileW * nrows;  // elements between tiles
     const int64_t rowoff = (int64_t)(blockIdx.x * R + rl) * kTileW;
     float2* gl = g + rowoff + (t & (kTileW - 1)) + (t / kTileW) * ts;  // mode t of the row
     float2* gnyq = g + FT * ts + blockIdx.x * R + rl;                   // mode M (tile of width 1)
-    __syncthreads();
+    const int src = (threadIdx.x & 31 & ~(P - 1)) | ((P - t) & (P - 1));  // the lane of mode M - t
     float2 v[E];
 #pragma unroll
-    for (int j = 0; j < E; ++j) {
-        const int k = t + P * j, km = M - k;  // km in [1, M]
-        const float2 xk = gl[(2 * j) * ts];
-        const float2 xm = km == M ? *gnyq : g[(km / kTileW) * ts + rowoff + (km & (kTileW - 1))];
-        v[j] = c2r_pre_f(xk, xm, twP[k]);
-    }
+    for (int j = 0; j < E; ++j) v[j] = gl[(2 * j) * ts];
+    __syncthreads();
+    // split: X[k] with X[M - k], which lane 16 - t holds at register 15 - j (lane 0: its own
+    // register 16 - j, and X[M] for j = 0), register pairs (j, 15 - j) at a time; lane 0's
+    // partner of register j is the original of register 16 - j, rewritten by the previous
+    // pair, so it is carried over
+    float2 carry = t == 0 ? *gnyq : make_float2(0.f, 0.f);
+    sfor<0, E / 2>([&](auto jj) {
+        constexpr int lo = decltype(jj)::value, hi = E - 1 - lo;
+        const float2 vl = v[lo], vh = v[hi];
+        float2 a = make_float2(__shfl_sync(0xffffffffu, vh.x, src), __shfl_sync(0xffffffffu, vh.y, src));
+        float2 b = make_float2(__shfl_sync(0xffffffffu, vl.x, src), __shfl_sync(0xffffffffu, vl.y, src));
+        if (t == 0) {
+            a = carry;
+            b = v[lo + 1];
+        }
+        carry = vh;
+        v[lo] = c2r_pre_f(vl, a, twmul<X::NX / P, lo, -1>(wt));
+        v[hi] = c2r_pre_f(vh, b, twmul<X::NX / P, hi, -1>(wt));
+    });
     // inverse transform, D1 -> D2 (thread t: pair n = t + P k2 at register k2)
     RF<E, 1>::run(v);
 #pragma unroll
@@ -477,14 +494,13 @@ __global__ void __launch_bounds__(X::T, 3) k_xlane(float2* g, int nrows, const f
     for (int n1 = 0; n1 < E; ++n1) v[n1] = xr[n1 * LDA + t];
     RF<E, -1>::run(v);
     // merge and store: Y[k] here, Y[(M - k) mod M] from lane 16 - t (lane 0: itself)
-    const int src = (threadIdx.x & 31 & ~(P - 1)) | ((P - t) & (P - 1));
-#pragma unroll
-    for (int j = 0; j < E; ++j) {
+    sfor<0, E>([&](auto jj) {
+        constexpr int j = decltype(jj)::value;
         const float2 s = v[E - 1 - j];
         float2 ym = make_float2(__shfl_sync(0xffffffffu, s.x, src), __shfl_sync(0xffffffffu, s.y, src));
         if (t == 0) ym = v[(E - j) & (E - 1)];
-        gl[(2 * j) * ts] = r2c_post_f(v[j], ym, twP[t + P * j]);
-    }
+        gl[(2 * j) * ts] = r2c_post_f(v[j], ym, twmul<X::NX / P, j, -1>(wt));
+    });
     if (t == 0) *gnyq = make_float2(v[0].x - v[0].y, 0.f);
 }
 
@@ -714,7 +730,7 @@ int xkernel_variants(int nx, int dtype) {
     if (dtype != PFC_F32) return 1;
     return 1 | (nx == 512 || nx == 128 ? 2 : 0) | (nx == 512 ? 4 : 0);
 }
-// k_xlane where the length has it (512: 0.309 against 0.338 ms for k_xrow and 0.348 for
+// k_xlane where the length has it (512: 0.288 against 0.338 ms for k_xrow and 0.348 for
 // k_xpair per 512^3 pass), else k_xrow
 int default_xkernel(int variants) { return (variants & 4) ? 2 : 0; }
 

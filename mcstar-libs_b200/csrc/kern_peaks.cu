@@ -252,7 +252,10 @@ __global__ void __launch_bounds__(kTX * kTY) k_peaks_mark(const T* __restrict__ 
 // below: M9 = max(h(y-1), h, h(y+1)), N8 = max(h(y-1), h(y+1), lr).  The 3D test and the NaN
 // semantics are k_peaks_mark's.  The four bits of a lane are OR-ed over the eight lanes of
 // a mask word by three shuffles.
-constexpr int kZC4 = 32, kRows4 = 16, kStages4 = 3;  // (static shared memory: 46 KB)
+constexpr int kZC4 = 32, kRows4 = 16, kStages4 = 8;
+// dynamic shared memory of k_peaks_mark4: the ring, the h rows, the edge cells
+constexpr size_t kMark4Smem = (size_t)(kStages4 + 2) * (kRows4 + 2) * 32 * sizeof(float4) +
+                              (size_t)kStages4 * (kRows4 + 2) * 2 * sizeof(float);
 
 __device__ __forceinline__ float4 nmax4(float4 a, float4 b) {
     return make_float4(nmax(a.x, b.x), nmax(a.y, b.y), nmax(a.z, b.z), nmax(a.w, b.w));
@@ -273,9 +276,11 @@ template <int N> __device__ __forceinline__ void cp_wait_group() {
 __global__ void __launch_bounds__(32 * (kRows4 + 2), 2)
     k_peaks_mark4(const float* __restrict__ psi, int nx, int ny, int nz, float ths, uint32_t* __restrict__ mask,
                   int wpr) {
-    __shared__ float4 H[2][kRows4 + 2][32];
-    __shared__ float4 Q[kStages4][kRows4 + 2][32];
-    __shared__ float EG[kStages4][kRows4 + 2][2];
+    extern __shared__ __align__(16) float4 sm4[];
+    float4 (*H)[kRows4 + 2][32] = reinterpret_cast<float4 (*)[kRows4 + 2][32]>(sm4);
+    float4 (*Q)[kRows4 + 2][32] = reinterpret_cast<float4 (*)[kRows4 + 2][32]>(sm4 + 2 * (kRows4 + 2) * 32);
+    float (*EG)[kRows4 + 2][2] =
+        reinterpret_cast<float (*)[kRows4 + 2][2]>(sm4 + (kStages4 + 2) * (kRows4 + 2) * 32);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int x0 = blockIdx.x * 128, y0 = blockIdx.y * kRows4, z0 = blockIdx.z * kZC4;
     const int zend = min(z0 + kZC4, nz);
@@ -435,8 +440,9 @@ cudaError_t peaks_ctx(const pfc_ctx* c, const void* psi, double ths, void* out, 
     dim3 grid(wpr, (c->ny + kTY - 1) / kTY, d3 ? (c->nz + kZC - 1) / kZC : 1);
     if (std::is_same<T, float>::value && d3 && c->nx % 128 == 0 && c->ny % kRows4 == 0 &&
         ((uintptr_t)psi & 15) == 0)
-        k_peaks_mark4<<<dim3(c->nx / 128, c->ny / kRows4, (c->nz + kZC4 - 1) / kZC4), 32 * (kRows4 + 2), 0,
-                        c->stream>>>((const float*)psi, c->nx, c->ny, c->nz, (float)ths, c->peak_mask, wpr);
+        k_peaks_mark4<<<dim3(c->nx / 128, c->ny / kRows4, (c->nz + kZC4 - 1) / kZC4), 32 * (kRows4 + 2),
+                        kMark4Smem, c->stream>>>((const float*)psi, c->nx, c->ny, c->nz, (float)ths, c->peak_mask,
+                                                 wpr);
     else if (d3)
         k_peaks_mark<T, true><<<grid, dim3(kTX, kTY), 0, c->stream>>>((const T*)psi, c->nx, c->ny, c->nz, (T)ths,
                                                                        c->peak_mask, wpr);
@@ -452,6 +458,10 @@ cudaError_t peaks_ctx(const pfc_ctx* c, const void* psi, double ths, void* out, 
 }
 
 }  // namespace
+
+cudaError_t set_peak_attributes() {
+    return cudaFuncSetAttribute(k_peaks_mark4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMark4Smem);
+}
 
 int64_t peak_mask_words(int nx, int ny, int nz) { return (int64_t)nz * ny * ((nx + 31) / 32); }
 int peak_chunks(int nx, int ny, int nz) {

@@ -172,6 +172,7 @@ int write_lowpass_file(const pfc_ctx* c, const void* spectrum, double lx, double
 // ---- register-resident z pass (kern_zcol.cu) ----
 int fused_z_variant(int nx, int nz, int dtype);
 cudaError_t set_zcol_attributes(const pfc_ctx* c);
+cudaError_t set_peak_attributes();
 // reads A and B, writes A' (or psi^' on the last step) to O; lay bits 0, 1, 2: A, B, O
 // z-tiled (col_addr layout 1; standard otherwise).  O may be A or B when it has the same
 // layout.
