@@ -52,6 +52,7 @@ bool make_plan(int n, LinePlan& p, std::vector<std::complex<double>>& tab, int o
     std::memset(&p, 0, sizeof(p));
     p.n = n;
     p.nst = (int)rs.size();
+    p.by_n = make_fastdiv(n);
     int Ns = 1;
     for (int s = 0; s < p.nst; ++s) {
         const int R = rs[s];
@@ -65,6 +66,8 @@ bool make_plan(int n, LinePlan& p, std::vector<std::complex<double>>& tab, int o
                 tab.emplace_back(std::cos(ang), std::sin(ang));
             }
         p.rtoff[s] = (int)tab.size();
+        p.by_m[s] = make_fastdiv(n / R);
+        p.by_ns[s] = make_fastdiv(Ns);
         if (R > 5)
             for (int q = 0; q < R; ++q) {
                 const double ang = -2.0 * M_PI * (double)q / (double)R;

@@ -22,17 +22,18 @@ __global__ void __launch_bounds__(256) k_cols(const cx<T>* __restrict__ in, cx<T
     cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
     const int n = p.n;
     cx<T>* b1 = b0 + (size_t)tile * n;
+    const int tile_lg = __ffs(tile) - 1;  // tile: a power of two
     const int i0 = blockIdx.x * tile;
     const int nt = min(tile, ni - i0);
     const int64_t base = (int64_t)blockIdx.y * os + i0;
     for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
-        const int i = e % tile, k = e / tile;
+        const int i = e & (tile - 1), k = e >> tile_lg;
         if (i < nt) b0[i * n + k] = in[base + i + k * es];
     }
     __syncthreads();
     cx<T>* r = stockham_lines<T, DIR>(b0, b1, nt, n, p, tw);
     for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
-        const int i = e % tile, k = e / tile;
+        const int i = e & (tile - 1), k = e >> tile_lg;
         if (i < nt) out[base + i + k * es] = r[i * n + k] * scale;
     }
 }
@@ -69,16 +70,17 @@ __global__ void __launch_bounds__(256) k_rows_r2c(const T* __restrict__ in, cx<T
     const int row0 = blockIdx.x * rpc;
     const int nr = min(rpc, nrows - row0);
     const int nxh = nx / 2 + 1;
+    const FastDiv by_nxh = make_fastdiv(nxh);
     const bool even = (nx & 1) == 0;
     for (int e = threadIdx.x; e < nr * L; e += blockDim.x) {
-        const int r = e / L, m = e - r * L;
+        const int r = fdiv(e, p.by_n), m = e - r * L;
         const T* row = in + (int64_t)(row0 + r) * nx;
         b0[e] = even ? reinterpret_cast<const cx<T>*>(row)[m] : mkc<T>(row[m], T(0));
     }
     __syncthreads();
     cx<T>* z = stockham_lines<T, -1>(b0, b1, nr, L, p, tw);
     for (int e = threadIdx.x; e < nr * nxh; e += blockDim.x) {
-        const int r = e / nxh, k = e - r * nxh;
+        const int r = fdiv(e, by_nxh), k = e - r * nxh;
         const cx<T>* zr = z + (size_t)r * L;
         cx<T> v;
         if (even) v = r2c_post<T>(zr[k % L], zr[(L - k) % L], post[k]);
@@ -100,7 +102,7 @@ __global__ void __launch_bounds__(256) k_rows_c2r(const cx<T>* __restrict__ in, 
     const int nxh = nx / 2 + 1;
     const bool even = (nx & 1) == 0;
     for (int e = threadIdx.x; e < nr * L; e += blockDim.x) {
-        const int r = e / L, k = e - r * L;
+        const int r = fdiv(e, p.by_n), k = e - r * L;
         const cx<T>* row = in + (int64_t)(row0 + r) * nxh;
         cx<T> v;
         if (even) v = c2r_pre<T>(row[k], row[L - k], post[k]);
@@ -110,7 +112,7 @@ __global__ void __launch_bounds__(256) k_rows_c2r(const cx<T>* __restrict__ in, 
     __syncthreads();
     cx<T>* z = stockham_lines<T, 1>(b0, b1, nr, L, p, tw);
     for (int e = threadIdx.x; e < nr * L; e += blockDim.x) {
-        const int r = e / L, m = e - r * L;
+        const int r = fdiv(e, p.by_n), m = e - r * L;
         T* row = out + (int64_t)(row0 + r) * nx;
         if (even) reinterpret_cast<cx<T>*>(row)[m] = z[e];
         else row[m] = z[e].x;
@@ -138,9 +140,10 @@ __global__ void __launch_bounds__(256) k_rows_nonlin(cx<T>* buf, const T* __rest
     const int row0 = blockIdx.x * rpc;
     const int nr = min(rpc, nrows - row0);
     const int nxh = nx / 2 + 1;
+    const FastDiv by_nxh = make_fastdiv(nxh);
     const bool even = (nx & 1) == 0;
     for (int e = threadIdx.x; e < nr * L; e += blockDim.x) {
-        const int r = e / L, k = e - r * L;
+        const int r = fdiv(e, p.by_n), k = e - r * L;
         const cx<T>* row = buf + (int64_t)(row0 + r) * nxh;
         cx<T> v;
         if (even) v = c2r_pre<T>(row[k], row[L - k], post[k]);
@@ -151,7 +154,7 @@ __global__ void __launch_bounds__(256) k_rows_nonlin(cx<T>* buf, const T* __rest
     cx<T>* z = stockham_lines<T, 1>(b0, b1, nr, L, p, tw);
     cx<T>* other = (z == b0) ? b1 : b0;
     for (int e = threadIdx.x; e < nr * L; e += blockDim.x) {
-        const int r = e / L, m = e - r * L;
+        const int r = fdiv(e, p.by_n), m = e - r * L;
         const int64_t rowi = (int64_t)(row0 + r) * nx;
         cx<T> v = z[e];
         if (even) {
@@ -168,7 +171,7 @@ __global__ void __launch_bounds__(256) k_rows_nonlin(cx<T>* buf, const T* __rest
     __syncthreads();
     cx<T>* y = stockham_lines<T, -1>(z, other, nr, L, p, tw);
     for (int e = threadIdx.x; e < nr * nxh; e += blockDim.x) {
-        const int r = e / nxh, k = e - r * nxh;
+        const int r = fdiv(e, by_nxh), k = e - r * nxh;
         const cx<T>* yr = y + (size_t)r * L;
         cx<T> v;
         if (even) v = r2c_post<T>(yr[k % L], yr[(L - k) % L], post[k]);
@@ -293,13 +296,14 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
     cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
     const int n = nz;
     cx<T>* b1 = b0 + (size_t)2 * tile * n;
+    const int tile_lg = __ffs(tile) - 1;  // tile: a power of two
     const int nxh = nx / 2 + 1;
     const int i0 = col0 + blockIdx.x * tile;
     const int ky = blockIdx.y;
     const int nt = min(tile, col_end - i0);
     if (threadIdx.x == 0) bad = 0;
     for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
-        const int i = e % tile, k = e / tile;
+        const int i = e & (tile - 1), k = e >> tile_lg;
         if (i < nt) {
             const int64_t off = ((int64_t)k * ny + ky) * nxh + i0 + i;
             b0[i * n + k] = A[off];
@@ -315,7 +319,7 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
     const T deps = T(1) + a.C - a.eps;
     float mc = 0.f;
     for (int e = threadIdx.x; e < nt * n; e += blockDim.x) {
-        const int i = e / n, kz = e - i * n;
+        const int i = fdiv(e, p.by_n), kz = e - i * n;
         const int kx = i0 + i;
         const cx<T> v = zmode<T, PROP>(r[i * n + kz], r[(tile + i) * n + kz], kx, kyg, kz, nx, nz, k1, deps, a, k0, mc);
         if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
@@ -331,7 +335,7 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
         scale = T(1) / T(nz);
     }
     for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
-        const int i = e % tile, k = e / tile;
+        const int i = e & (tile - 1), k = e >> tile_lg;
         if (i < nt) A[((int64_t)k * ny + ky) * nxh + i0 + i] = outb[i * n + k] * scale;
     }
 }

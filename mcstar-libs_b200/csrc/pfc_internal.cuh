@@ -98,13 +98,35 @@ template <typename T, int DIR> struct Dft<T, DIR, 5> {
 // ---------------------------------------------------------------------------------
 constexpr int kMaxStages = 16;
 constexpr int kMaxOddRadix = 31;  // largest prime radix of the general stage
+
+// Division of a non-negative 31-bit n by a fixed d >= 1 as a multiply-high, an add and a
+// shift: with l = ceil(log2 d) and mul = floor(2^32 (2^l - d) / d) + 1 (below 2^32),
+// n / d = (umulhi(n, mul) + n) >> l for every n < 2^31 (the round-up method of Granlund and
+// Montgomery, "Division by invariant integers using multiplication", PLDI 1994).
+struct FastDiv {
+    uint32_t mul;
+    int shift;
+};
+__host__ __device__ inline FastDiv make_fastdiv(int d) {
+    int l = 0;
+    while ((1ll << l) < d) ++l;
+    const unsigned long long m = ((1ull << 32) * (((1ull << l) - (unsigned long long)d))) / (unsigned long long)d + 1;
+    return FastDiv{(uint32_t)m, l};
+}
+__device__ __forceinline__ int fdiv(int n, FastDiv f) {
+    return (int)((__umulhi((uint32_t)n, f.mul) + (uint32_t)n) >> f.shift);
+}
+
 struct LinePlan {
     int n;
     int nst;
     int radix[kMaxStages];
     int ns[kMaxStages];
     int twoff[kMaxStages];
-    int rtoff[kMaxStages];  // W_R^q, q < R, for radices without a hand-written DFT
+    int rtoff[kMaxStages];     // W_R^q, q < R, for radices without a hand-written DFT
+    FastDiv by_n;              // division by n
+    FastDiv by_m[kMaxStages];  // by n / R_s
+    FastDiv by_ns[kMaxStages]; // by Ns
 };
 
 // Stage of a prime radix R (7 <= R <= kMaxOddRadix): direct R-point DFT with the
@@ -112,9 +134,9 @@ struct LinePlan {
 template <typename T, int DIR>
 __device__ __forceinline__ void stockham_bfly_gen(const cx<T>* __restrict__ sl, cx<T>* __restrict__ dl, int j,
                                                   int m, int Ns, int R, const cx<T>* __restrict__ tws,
-                                                  const cx<T>* __restrict__ wr) {
+                                                  const cx<T>* __restrict__ wr, FastDiv by_ns) {
     cx<T> v[kMaxOddRadix];
-    const int jj = j % Ns;
+    const int jj = j - fdiv(j, by_ns) * Ns;
     for (int r = 0; r < R; ++r) {
         cx<T> a = sl[j + r * m];
         if (Ns > 1 && r > 0) {
@@ -143,11 +165,12 @@ __device__ __forceinline__ void stockham_bfly_gen(const cx<T>* __restrict__ sl, 
 
 template <typename T, int DIR, int R>
 __device__ __forceinline__ void stockham_bfly(const cx<T>* __restrict__ sl, cx<T>* __restrict__ dl,
-                                              int j, int m, int Ns, const cx<T>* __restrict__ tws) {
+                                              int j, int m, int Ns, const cx<T>* __restrict__ tws,
+                                              FastDiv by_ns) {
     cx<T> v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = sl[j + r * m];
-    const int jj = j % Ns;
+    const int jj = j - fdiv(j, by_ns) * Ns;
     if (Ns > 1) {
 #pragma unroll
         for (int r = 1; r < R; ++r) {
@@ -171,19 +194,20 @@ __device__ cx<T>* stockham_lines(cx<T>* a, cx<T>* b, int nlines, int ld, const L
     cx<T>* dst = b;
     for (int s = 0; s < p.nst; ++s) {
         const int R = p.radix[s], Ns = p.ns[s], m = p.n / R;
+        const FastDiv by_m = p.by_m[s], by_ns = p.by_ns[s];
         const cx<T>* tws = tw + p.twoff[s];
         const int total = nlines * m;
         for (int e = threadIdx.x; e < total; e += blockDim.x) {
-            const int line = e / m, j = e - line * m;
+            const int line = fdiv(e, by_m), j = e - line * m;
             const cx<T>* sl = src + (size_t)line * ld;
             cx<T>* dl = dst + (size_t)line * ld;
             switch (R) {
-                case 8: stockham_bfly<T, DIR, 8>(sl, dl, j, m, Ns, tws); break;
-                case 4: stockham_bfly<T, DIR, 4>(sl, dl, j, m, Ns, tws); break;
-                case 2: stockham_bfly<T, DIR, 2>(sl, dl, j, m, Ns, tws); break;
-                case 3: stockham_bfly<T, DIR, 3>(sl, dl, j, m, Ns, tws); break;
-                case 5: stockham_bfly<T, DIR, 5>(sl, dl, j, m, Ns, tws); break;
-                default: stockham_bfly_gen<T, DIR>(sl, dl, j, m, Ns, R, tws, tw + p.rtoff[s]); break;
+                case 8: stockham_bfly<T, DIR, 8>(sl, dl, j, m, Ns, tws, by_ns); break;
+                case 4: stockham_bfly<T, DIR, 4>(sl, dl, j, m, Ns, tws, by_ns); break;
+                case 2: stockham_bfly<T, DIR, 2>(sl, dl, j, m, Ns, tws, by_ns); break;
+                case 3: stockham_bfly<T, DIR, 3>(sl, dl, j, m, Ns, tws, by_ns); break;
+                case 5: stockham_bfly<T, DIR, 5>(sl, dl, j, m, Ns, tws, by_ns); break;
+                default: stockham_bfly_gen<T, DIR>(sl, dl, j, m, Ns, R, tws, tw + p.rtoff[s], by_ns); break;
             }
         }
         __syncthreads();
