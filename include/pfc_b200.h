@@ -267,6 +267,13 @@ pfc_status pfc_step(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params*
  *                           ((1 - k^2)^2 + C - eps)) -- kernel_update_el, el.hpp:3-45
  *   PFC_PROP_RELAX_EXP      its exponential form psi^' = E psi^ + Q N^, L = (1 - k^2)^2 +
  *                           C - eps -- el-exp.hpp:3-60
+ *   PFC_PROP_CONSERVED_POLY the conserved update with the polynomial correlation function,
+ *                           D = 1 + dt k^2 (C - eps - P(k^2)), P the degree-6 polynomial in
+ *                           k^2 of kernel_update_eom_py (eom.hpp:143-180)
+ *   PFC_PROP_CONSERVED_HPFC the conserved update with the anisotropic noise of
+ *                           kernel_update_eom_hpfcnoise (eom.hpp:16-58): three noise fields
+ *                           weighted by the wavevector, cut off above |k| = 1/4; 2D fields only
+ *                           (nz = 1, PFC_ERR_INVALID otherwise, as the reference exits)
  * The relaxations move the k = 0 mode and take no noise (namp must be 0); for them
  * *max_change (may be NULL) receives max_k |psi^'_k - psi^_k| of the last step, the value
  * call_kernel_update_el returns (el.hpp:23-45), as a float.  The exponentials are
@@ -275,7 +282,9 @@ typedef enum pfc_propagator {
     PFC_PROP_CONSERVED = 0,
     PFC_PROP_CONSERVED_EXP = 1,
     PFC_PROP_RELAX = 2,
-    PFC_PROP_RELAX_EXP = 3
+    PFC_PROP_RELAX_EXP = 3,
+    PFC_PROP_CONSERVED_POLY = 4,
+    PFC_PROP_CONSERVED_HPFC = 5
 } pfc_propagator;
 pfc_status pfc_step_prop(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_params* params, int propagator,
                          double* max_change);

@@ -110,6 +110,9 @@ void free_ctx(pfc_ctx* c) {
     for (cudaEvent_t e : c->host_ev)
         if (e) cudaEventDestroy(e);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->side_fork) cudaEventDestroy(c->side_fork);
+    if (c->side_join) cudaEventDestroy(c->side_join);
+    if (c->side_stream) cudaStreamDestroy(c->side_stream);
     void* ptrs[] = {c->tw,          c->work,         c->work2,        c->red,       c->k0,
                     c->flag,        c->peak_counts,  c->peak_offsets, c->bond_scratch, c->bond_pairs,
                     c->peak_mask};
@@ -547,13 +550,13 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
     c->px.smem = 2 * (size_t)c->px.tile * lx * csz;
     c->py.tile = shifted(fit(pow2_floor((64 * 1024) / (2 * (size_t)c->ny * csz), 16), (int64_t)c->nxh * c->nz),
                          o.tile_shift[1]);
-    c->py.smem = 2 * (size_t)c->py.tile * c->ny * csz;
+    c->py.smem = 2 * (size_t)c->py.tile * line_stride(c->ny) * csz;
     c->pz.tile = shifted(fit(pow2_floor((64 * 1024) / (2 * (size_t)c->nz * csz), 16), (int64_t)c->nxh * c->ny),
                          o.tile_shift[2]);
-    c->pz.smem = 2 * (size_t)c->pz.tile * c->nz * csz;
+    c->pz.smem = 2 * (size_t)c->pz.tile * line_stride(c->nz) * csz;
     c->pzprop.tile = shifted(fit(pow2_floor((96 * 1024) / (4 * (size_t)c->nz * csz), 8), (int64_t)c->nxh * c->ny),
                              o.tile_shift[3]);
-    c->pzprop.smem = 4 * (size_t)c->pzprop.tile * c->nz * csz;
+    c->pzprop.smem = 4 * (size_t)c->pzprop.tile * line_stride(c->nz) * csz;
     if (c->px.smem > kMaxDynSmem || c->py.smem > kMaxDynSmem || c->pz.smem > kMaxDynSmem ||
         c->pzprop.smem > kMaxDynSmem) {
         free_ctx(c);
@@ -599,6 +602,11 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
     if (e == cudaSuccess && c->fused_y) e = set_pass_attributes(c);
     if (e == cudaSuccess && c->fused_zfft) e = set_zfft_attributes(c);
     if (e == cudaSuccess) e = set_peak_attributes();
+    if (e == cudaSuccess && c->tiled && c->z_carry) {
+        e = cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking);
+        if (!e) e = cudaEventCreateWithFlags(&c->side_fork, cudaEventDisableTiming);
+        if (!e) e = cudaEventCreateWithFlags(&c->side_join, cudaEventDisableTiming);
+    }
     if (e != cudaSuccess) {
         free_ctx(c);
         return PFC_ERR_CUDA;
@@ -771,8 +779,10 @@ pfc_status pfc_step_prop(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_pa
                          double* max_change) {
     PFC_CHECK_CTX();
     if (!kpsi || !p || nsteps < 0) return fail(ctx, PFC_ERR_INVALID, "pfc_step: bad arguments");
-    if (propagator < PFC_PROP_CONSERVED || propagator > PFC_PROP_RELAX_EXP)
+    if (propagator < PFC_PROP_CONSERVED || propagator > PFC_PROP_CONSERVED_HPFC)
         return fail(ctx, PFC_ERR_INVALID, "pfc_step_prop: unknown propagator");
+    if (propagator == PFC_PROP_CONSERVED_HPFC && ctx->nz != 1)
+        return fail(ctx, PFC_ERR_INVALID, "pfc_step_prop: the hpfc noise is for 2D fields only (eom.hpp:16-58)");
     const bool relax = propagator == PFC_PROP_RELAX || propagator == PFC_PROP_RELAX_EXP;
     if (relax && p->namp != 0.0)
         return fail(ctx, PFC_ERR_INVALID, "pfc_step_prop: the relaxation propagators take no noise (el.hpp)");

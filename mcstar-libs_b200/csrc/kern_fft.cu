@@ -21,20 +21,21 @@ __global__ void __launch_bounds__(256) k_cols(const cx<T>* __restrict__ in, cx<T
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
     const int n = p.n;
-    cx<T>* b1 = b0 + (size_t)tile * n;
+    const int ld = line_stride(n);
+    cx<T>* b1 = b0 + (size_t)tile * ld;
     const int tile_lg = __ffs(tile) - 1;  // tile: a power of two
     const int i0 = blockIdx.x * tile;
     const int nt = min(tile, ni - i0);
     const int64_t base = (int64_t)blockIdx.y * os + i0;
     for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
         const int i = e & (tile - 1), k = e >> tile_lg;
-        if (i < nt) b0[i * n + k] = in[base + i + k * es];
+        if (i < nt) b0[i * ld + k] = in[base + i + k * es];
     }
     __syncthreads();
-    cx<T>* r = stockham_lines<T, DIR>(b0, b1, nt, n, p, tw);
+    cx<T>* r = stockham_lines<T, DIR>(b0, b1, nt, ld, p, tw);
     for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
         const int i = e & (tile - 1), k = e >> tile_lg;
-        if (i < nt) out[base + i + k * es] = r[i * n + k] * scale;
+        if (i < nt) out[base + i + k * es] = r[i * ld + k] * scale;
     }
 }
 
@@ -241,7 +242,9 @@ __device__ __forceinline__ cx<T> zmode(cx<T> psi, cx<T> nl, int kx, int kyg, int
         v = mkc<T>(ca * psi.x + cb * nl.x, ca * psi.y + cb * nl.y);
         if (prop_conserved<PROP>() && a.use_noise) {
             const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
-            const cx<T> xi = kspace_noise<T>(kx, kyg, kz, nx, a.nyg, nz, a.seed, ctr);
+            const cx<T> xi = PROP == kPropConservedHpfc
+                                 ? hpfc_noise<T>(kx, kyg, nx, a.nyg, kk0, k1, sqrt(-dopx), a.seed, ctr)
+                                 : kspace_noise<T>(kx, kyg, kz, nx, a.nyg, nz, a.seed, ctr);
             v.x += a.namp_eff * cg * xi.x;
             v.y += a.namp_eff * cg * xi.y;
         }
@@ -295,7 +298,8 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
     __shared__ int bad;
     cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
     const int n = nz;
-    cx<T>* b1 = b0 + (size_t)2 * tile * n;
+    const int ld = line_stride(n);
+    cx<T>* b1 = b0 + (size_t)2 * tile * ld;
     const int tile_lg = __ffs(tile) - 1;  // tile: a power of two
     const int nxh = nx / 2 + 1;
     const int i0 = col0 + blockIdx.x * tile;
@@ -306,12 +310,12 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
         const int i = e & (tile - 1), k = e >> tile_lg;
         if (i < nt) {
             const int64_t off = ((int64_t)k * ny + ky) * nxh + i0 + i;
-            b0[i * n + k] = A[off];
-            b0[(tile + i) * n + k] = B[off];
+            b0[i * ld + k] = A[off];
+            b0[(tile + i) * ld + k] = B[off];
         }
     }
     __syncthreads();
-    cx<T>* r = stockham_lines<T, -1>(b0, b1, 2 * tile, n, p, tw);
+    cx<T>* r = stockham_lines<T, -1>(b0, b1, 2 * tile, ld, p, tw);
     cx<T>* other = (r == b0) ? b1 : b0;
     // a ky-slab of a larger field: wavenumbers, the k = 0 mode and the noise keys of the field
     const int kyg = ky + a.ky0;
@@ -321,9 +325,9 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
     for (int e = threadIdx.x; e < nt * n; e += blockDim.x) {
         const int i = fdiv(e, p.by_n), kz = e - i * n;
         const int kx = i0 + i;
-        const cx<T> v = zmode<T, PROP>(r[i * n + kz], r[(tile + i) * n + kz], kx, kyg, kz, nx, nz, k1, deps, a, k0, mc);
+        const cx<T> v = zmode<T, PROP>(r[i * ld + kz], r[(tile + i) * ld + kz], kx, kyg, kz, nx, nz, k1, deps, a, k0, mc);
         if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
-        r[i * n + kz] = v;
+        r[i * ld + kz] = v;
     }
     if (!prop_conserved<PROP>() && a.maxc) fold_max_change(mc, a.maxc);
     __syncthreads();
@@ -331,12 +335,12 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
     cx<T>* outb = r;
     T scale = T(1);
     if (!a.final_step) {
-        outb = stockham_lines<T, 1>(r, other, nt, n, p, tw);
+        outb = stockham_lines<T, 1>(r, other, nt, ld, p, tw);
         scale = T(1) / T(nz);
     }
     for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
         const int i = e & (tile - 1), k = e >> tile_lg;
-        if (i < nt) A[((int64_t)k * ny + ky) * nxh + i0 + i] = outb[i * n + k] * scale;
+        if (i < nt) A[((int64_t)k * ny + ky) * nxh + i0 + i] = outb[i * ld + k] * scale;
     }
 }
 
@@ -354,6 +358,10 @@ cudaError_t set_attrs_T(const pfc_ctx* c) {
         return e;
     if ((e = cudaFuncSetAttribute(k_zprop<T, kPropRelax>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
     if ((e = cudaFuncSetAttribute(k_zprop<T, kPropRelaxExp>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
+    if ((e = cudaFuncSetAttribute(k_zprop<T, kPropConservedPoly>, cudaFuncAttributeMaxDynamicSharedMemorySize, m)))
+        return e;
+    if ((e = cudaFuncSetAttribute(k_zprop<T, kPropConservedHpfc>, cudaFuncAttributeMaxDynamicSharedMemorySize, m)))
+        return e;
     (void)c;
     return cudaSuccess;
 }
@@ -467,6 +475,8 @@ cudaError_t launch_zprop_cols(const pfc_ctx* c, void* A, const void* B, const ZP
         case kPropConservedExp: zprop_dt<kPropConservedExp>(c, A, B, a, col0, ncols); break;
         case kPropRelax: zprop_dt<kPropRelax>(c, A, B, a, col0, ncols); break;
         case kPropRelaxExp: zprop_dt<kPropRelaxExp>(c, A, B, a, col0, ncols); break;
+        case kPropConservedPoly: zprop_dt<kPropConservedPoly>(c, A, B, a, col0, ncols); break;
+        case kPropConservedHpfc: zprop_dt<kPropConservedHpfc>(c, A, B, a, col0, ncols); break;
         default: zprop_dt<kPropConserved>(c, A, B, a, col0, ncols);
     }
     return cudaGetLastError();

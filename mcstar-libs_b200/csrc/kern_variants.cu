@@ -142,18 +142,6 @@ __global__ void k_init_el_op(cx<T>* kop, Modes m, T dt, T eps, T lx, T ly, T lz)
     }
 }
 
-// the polynomial P(k^2) of eom.hpp:143-149 (the model's coefficients c12 .. c0, Horner)
-template <typename T> __device__ __forceinline__ T py_poly(T k2) {
-    T d = T(-0.293423255328944);
-    d = d * k2 + T(4.678065276755401);
-    d = d * k2 + T(-30.20985042718309);
-    d = d * k2 + T(100.6942650417575);
-    d = d * k2 + T(-181.1481995196213);
-    d = d * k2 + T(164.4074088310241);
-    d = d * k2 + T(-57.94636917114257);
-    return d;
-}
-
 template <typename T>
 __global__ void k_update_eom_py(cx<T>* kpsi, const cx<T>* __restrict__ knl, const cx<T>* __restrict__ knoise,
                                 Modes m, T namp_eff, T dt, T eps, T lx, T ly, T lz) {

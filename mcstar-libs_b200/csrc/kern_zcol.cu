@@ -670,6 +670,7 @@ cudaError_t by_prop(int prop, F&& f) {
         case kPropConservedExp: return f(std::integral_constant<int, kPropConservedExp>{});
         case kPropRelax: return f(std::integral_constant<int, kPropRelax>{});
         case kPropRelaxExp: return f(std::integral_constant<int, kPropRelaxExp>{});
+        case kPropConservedPoly: return f(std::integral_constant<int, kPropConservedPoly>{});
         default: return f(std::integral_constant<int, kPropConserved>{});
     }
 }
@@ -677,7 +678,7 @@ cudaError_t by_prop(int prop, F&& f) {
 template <class F>
 cudaError_t each_prop(F&& f) {
     cudaError_t e = cudaSuccess;
-    for (int p = 0; p < 4 && !e; ++p) e = by_prop(p, f);
+    for (int p = 0; p <= kPropConservedPoly && !e; ++p) e = by_prop(p, f);
     return e;
 }
 
@@ -787,17 +788,30 @@ cudaError_t launch_zcarry_tiled(const pfc_ctx* c, const void* psi_in, const void
             return cudaGetLastError();
         }
         // whole tiles with bulk copies (psi^ in place, A' over B); the partial last tile with
-        // per-thread accesses
+        // per-thread accesses, on the side stream beside them (the two write disjoint tiles)
         const int full = c->nxh / Z::TX;
         if (psi_in != psi_out || B != A) return cudaErrorNotSupported;
+        const bool side = full > 0 && full < ntx && c->side_stream;
+        cudaError_t e = cudaSuccess;
+        if (side) {
+            if ((e = cudaEventRecord(c->side_fork, c->stream))) return e;
+            if ((e = cudaStreamWaitEvent(c->side_stream, c->side_fork, 0))) return e;
+        }
+        if (full < ntx)
+            k_zcarry3<Z, false, P.value>
+                <<<dim3(ntx - full, c->ny, c->batch), Z::TH, Z::SMEM_CARRY, side ? c->side_stream : c->stream>>>(
+                    (const float2*)psi_in, (const float2*)B, (float2*)psi_out, (float2*)A, c->nx, c->ny, za, c->k0,
+                    c->flag, tw, full, 0, c->mstride);
+        if ((e = cudaGetLastError())) return e;
         if (full > 0)
             k_zbulk<Z, P.value><<<dim3(full, c->ny, c->batch), Z::TH, ZBulkCfg<Z>::SMEM, c->stream>>>(
                 (float2*)psi_out, (float2*)A, c->nx, c->ny, za, c->k0, c->flag, tw, c->mstride);
-        if (full < ntx)
-            k_zcarry3<Z, false, P.value><<<dim3(ntx - full, c->ny, c->batch), Z::TH, Z::SMEM_CARRY, c->stream>>>(
-                (const float2*)psi_in, (const float2*)B, (float2*)psi_out, (float2*)A, c->nx, c->ny, za, c->k0,
-                c->flag, tw, full, 0, c->mstride);
-        return cudaGetLastError();
+        if ((e = cudaGetLastError())) return e;
+        if (side) {
+            if ((e = cudaEventRecord(c->side_join, c->side_stream))) return e;
+            if ((e = cudaStreamWaitEvent(c->stream, c->side_join, 0))) return e;
+        }
+        return cudaSuccess;
     });
 }
 

@@ -87,6 +87,10 @@ struct pfc_ctx {
     // pfc_step_host: the copy stream and the events that order the field's ky chunks between
     // it and the context's stream (created by the first call)
     static constexpr int kHostChunks = 8;
+    // the z pass of the tiled psi^-carrying schedule: the last kx tile (one column) runs on
+    // this stream beside the bulk-copy kernel of the whole tiles (forked and joined by events)
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t side_fork = nullptr, side_join = nullptr;
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t host_ev[2 * kHostChunks + 2] = {};
 };

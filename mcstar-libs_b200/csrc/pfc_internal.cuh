@@ -117,6 +117,10 @@ __device__ __forceinline__ int fdiv(int n, FastDiv f) {
     return (int)((__umulhi((uint32_t)n, f.mul) + (uint32_t)n) >> f.shift);
 }
 
+// Shared-memory stride of the lines of a column tile: odd (in elements), so that the lanes
+// of a warp moving one element of each of consecutive lines hit distinct banks.
+__host__ __device__ constexpr int line_stride(int n) { return n | 1; }
+
 struct LinePlan {
     int n;
     int nst;
@@ -237,11 +241,38 @@ template <typename T> __device__ __forceinline__ T kwave(int i, int n, T len) {
 //                     dopy); a = 1/D, b = -dt / D; no noise
 //  kPropRelaxExp      its exponential form (el-exp.hpp:3-60): L = deps + 2 dopx + dopy,
 //                     E = exp(-L dt), Q = (E - 1)/L (-dt where L = 0); a = E, b = Q; no noise
+//  kPropConservedPoly the conserved update with the polynomial correlation function
+//                     (eom.hpp:143-180): D = 1 - dt dopx (deps - 1 - P(k^2)), P the model's
+//                     degree-6 polynomial in k^2; a = 1/D, b = dt dopx / D, g = dt |k| / D
+//  kPropConservedHpfc the conserved update with the anisotropic 2D noise of eom.hpp:16-58:
+//                     D as kPropConserved; a = 1/D, b = dt dopx / D, g = dt / D multiplies
+//                     (c1 kx^2 + c2 ky^2) xi1 + (c2 kx^2 + c1 ky^2) xi2 + 2 kx ky xi3 for
+//                     |k| <= 1/4, three independent noise fields (hpfc_noise)
 // The conserved propagators leave the k = 0 mode unchanged (the stepper restores it from
 // FP64); the relaxations move it.
-enum { kPropConserved = 0, kPropConservedExp = 1, kPropRelax = 2, kPropRelaxExp = 3 };
+enum {
+    kPropConserved = 0,
+    kPropConservedExp = 1,
+    kPropRelax = 2,
+    kPropRelaxExp = 3,
+    kPropConservedPoly = 4,
+    kPropConservedHpfc = 5
+};
 template <int PROP> __host__ __device__ constexpr bool prop_conserved() {
-    return PROP == kPropConserved || PROP == kPropConservedExp;
+    return PROP == kPropConserved || PROP == kPropConservedExp || PROP == kPropConservedPoly ||
+           PROP == kPropConservedHpfc;
+}
+
+// the polynomial P(k^2) of eom.hpp:143-149 (the model's coefficients c12 .. c0, Horner)
+template <typename T> __host__ __device__ __forceinline__ T py_poly(T k2) {
+    T d = T(-0.293423255328944);
+    d = d * k2 + T(4.678065276755401);
+    d = d * k2 + T(-30.20985042718309);
+    d = d * k2 + T(100.6942650417575);
+    d = d * k2 + T(-181.1481995196213);
+    d = d * k2 + T(164.4074088310241);
+    d = d * k2 + T(-57.94636917114257);
+    return d;
 }
 
 // Per-field parameters of a batch of fields stepped by one launch (grid z = field).
@@ -272,6 +303,19 @@ __device__ __forceinline__ void prop_coef(T dopx, T dt, T deps, T& a, T& b, T& g
         a = inv;
         b = -dt * inv;
         g = T(0);
+    } else if constexpr (PROP == kPropConservedPoly) {
+        // the polynomial and D in FP64: near the maximum of P (k^2 ~ 1.2 .. 4) its terms cancel
+        // to a few parts in 10^3 of their size, which costs an FP32 evaluation ~1e-3 of D
+        const double dd = 1.0 - (double)dt * (double)dopx * ((double)deps - 1.0 - py_poly<double>(-(double)dopx));
+        const T inv = T(1.0 / dd);
+        a = inv;
+        b = dt * dopx * inv;
+        g = dt * sqrt(-dopx) * inv;
+    } else if constexpr (PROP == kPropConservedHpfc) {
+        const T inv = T(1) / (T(1) - dt * (deps * dopx + T(2) * dopy + dopx * dopy));
+        a = inv;
+        b = dt * dopx * inv;
+        g = dt * inv;
     } else {
         const T lin = deps + T(2) * dopx + dopy;
         const T e = dev_exp<T>(-lin * dt);
@@ -314,6 +358,8 @@ __host__ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t
 
 constexpr uint32_t kKspaceDomain = 0x0u;
 constexpr uint32_t kRealDomain = 0x52454131u;
+constexpr uint32_t kHpfcDomain = 0x48504600u;  // + 1, 2, 3: the three fields of the hpfc noise
+
 
 // Two standard normals from counter (idx, counter) under key (seed, domain),
 // Box-Muller on uniforms strictly inside (0, 1) that are exact in T.
@@ -349,7 +395,7 @@ template <> __device__ __forceinline__ void philox_normal2<double>(uint64_t idx,
 // +-k pair and conjugated on the other member; self-conjugate modes are real.
 template <typename T>
 __device__ __forceinline__ cx<T> kspace_noise(int i0, int i1, int i2, int nx, int ny, int nz,
-                                              uint64_t seed, uint64_t counter) {
+                                              uint64_t seed, uint64_t counter, uint32_t domain = kKspaceDomain) {
     const int nxh = nx / 2 + 1;
     const int64_t lin = ((int64_t)i2 * ny + i1) * nxh + i0;
     int64_t canon = lin;
@@ -362,10 +408,28 @@ __device__ __forceinline__ cx<T> kspace_noise(int i0, int i1, int i2, int nx, in
         selfc = (part == lin);
     }
     T g1, g2;
-    philox_normal2<T>((uint64_t)canon, seed, counter, kKspaceDomain, g1, g2);
+    philox_normal2<T>((uint64_t)canon, seed, counter, domain, g1, g2);
     const T s = T(0.70710678118654752440);
     if (selfc) return mkc<T>(g1, T(0));
     return mkc<T>(g1 * s, conj ? -g2 * s : g2 * s);
+}
+
+// The anisotropic 2D noise of eom.hpp:16-58 at wavenumbers (k0, k1), |k| = kabs: the three
+// Hermitian-consistent fields (keyed like kspace_noise, domains kHpfcDomain + 1..3) weighted
+// by c1 = kappa / (2 c2), c2 = sqrt(1 + kappa/2 + sqrt(1 + kappa)), kappa = 4/3, and cut off
+// above |k| = 1/4.
+template <typename T>
+__device__ __forceinline__ cx<T> hpfc_noise(int i0, int i1, int nx, int ny, T k0, T k1, T kabs, uint64_t seed,
+                                            uint64_t counter) {
+    if (!(kabs <= T(0.25))) return mkc<T>(T(0), T(0));
+    const T kappa = T(4) / T(3);
+    const T c2 = sqrt(T(1) + kappa / T(2) + sqrt(T(1) + kappa));
+    const T c1 = kappa / c2 / T(2);
+    const cx<T> a = kspace_noise<T>(i0, i1, 0, nx, ny, 1, seed, counter, kHpfcDomain + 1u);
+    const cx<T> b = kspace_noise<T>(i0, i1, 0, nx, ny, 1, seed, counter, kHpfcDomain + 2u);
+    const cx<T> c = kspace_noise<T>(i0, i1, 0, nx, ny, 1, seed, counter, kHpfcDomain + 3u);
+    const T fa = c1 * k0 * k0 + c2 * k1 * k1, fb = c2 * k0 * k0 + c1 * k1 * k1, fc = T(2) * k0 * k1;
+    return mkc<T>(fa * a.x + fb * b.x + fc * c.x, fa * a.y + fb * b.y + fc * c.y);
 }
 
 }  // namespace pfc

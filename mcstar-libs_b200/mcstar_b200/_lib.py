@@ -34,7 +34,8 @@ EXPORTED = (
 )
 
 # pfc_propagator
-PROPAGATORS = {"conserved": 0, "conserved_exp": 1, "relax": 2, "relax_exp": 3}
+PROPAGATORS = {"conserved": 0, "conserved_exp": 1, "relax": 2, "relax_exp": 3, "conserved_poly": 4,
+               "conserved_hpfc": 5}
 
 
 class PfcError(RuntimeError):

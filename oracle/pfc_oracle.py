@@ -377,6 +377,7 @@ def _u01_f64(hi, lo):
 
 KSPACE_DOMAIN = 0x0          # key word-1 xor for k-space noise
 REAL_DOMAIN = 0x52454131     # key word-1 xor for real-space noise ("REA1")
+HPFC_DOMAIN = 0x48504600     # + 1, 2, 3: the three k-space fields of the anisotropic 2D noise
 
 
 def _normals(idx, seed, counter, domain, f64):
@@ -394,8 +395,9 @@ def _normals(idx, seed, counter, domain, f64):
     return rad * np.cos(2.0 * np.pi * u2), rad * np.sin(2.0 * np.pi * u2)
 
 
-def fill_kspace(shape_xyz, seed, counter, dtype=np.float32):
-    """Hermitian-consistent complex normal k-space noise, E|xi|^2 = 1 (see module doc)."""
+def fill_kspace(shape_xyz, seed, counter, dtype=np.float32, domain=KSPACE_DOMAIN):
+    """Hermitian-consistent complex normal k-space noise, E|xi|^2 = 1 (see module doc);
+    domain: the key word-1 xor of the stream."""
     nx, ny, nz = shape_xyz
     nxh = nx // 2 + 1
     f64 = np.dtype(dtype) == np.float64
@@ -406,7 +408,7 @@ def fill_kspace(shape_xyz, seed, counter, dtype=np.float32):
     canon = np.where(on_plane, np.minimum(lin, partner), lin)
     conj = on_plane & (lin > partner)
     selfc = on_plane & (lin == partner)
-    g1, g2 = _normals(canon.ravel(), seed, counter, KSPACE_DOMAIN, f64)
+    g1, g2 = _normals(canon.ravel(), seed, counter, domain, f64)
     g1 = g1.reshape(lin.shape)
     g2 = g2.reshape(lin.shape)
     s = 1.0 / math.sqrt(2.0)
@@ -426,6 +428,29 @@ def fill_real(n, sigma, seed, counter, dtype=np.float32):
 # ----------------------------------------------------------------------------------
 # the step
 # ----------------------------------------------------------------------------------
+def py_poly(k2):
+    """The degree-6 polynomial in k^2 of kernel_update_eom_py (eom.hpp:143-149), Horner."""
+    d = np.full_like(k2, PY_COEFFS[-1])
+    for ci in PY_COEFFS[-2::-1]:
+        d = d * k2 + ci
+    return d
+
+
+def hpfc_noise(fields, shape_xyz, lens):
+    """The anisotropic 2D noise of kernel_update_eom_hpfcnoise (eom.hpp:16-58) from three
+    k-space fields: (c1 kx^2 + c2 ky^2) xi1 + (c2 kx^2 + c1 ky^2) xi2 + 2 kx ky xi3, zero
+    for |k| > 1/4; kappa = 4/3, c2 = sqrt(1 + kappa/2 + sqrt(1 + kappa)), c1 = kappa/(2 c2)."""
+    nx, ny, nz = shape_xyz
+    kappa = 4.0 / 3.0
+    c2 = math.sqrt(1.0 + kappa / 2.0 + math.sqrt(1.0 + kappa))
+    c1 = kappa / c2 / 2.0
+    k0 = wavenumbers(nx, lens[0], half=True)[None, None, :]
+    k1 = wavenumbers(ny, lens[1])[None, :, None]
+    a, b, c = (f.astype(np.complex128) for f in fields)
+    out = (c1 * k0 ** 2 + c2 * k1 ** 2) * a + (c2 * k0 ** 2 + c1 * k1 ** 2) * b + 2.0 * k0 * k1 * c
+    return np.where(np.sqrt(kgrid(shape_xyz, lens)) <= 0.25, out, 0.0)
+
+
 def propagate(kpsi, knl, knoise, namp, dt, eps, lens, shape_xyz, C, propagator):
     """One update of the fused stepper's other propagators, in full precision (the fused
     kernels evaluate exp in the field's precision), with the stabilisation C
@@ -434,6 +459,10 @@ def propagate(kpsi, knl, knoise, namp, dt, eps, lens, shape_xyz, C, propagator):
                        L = -dop.x (deps + 2 dop.x + dop.y), E = exp(-L dt), Q = (E-1)/L (-dt at L = 0)
       "relax"          el.hpp:3-25         psi^' = (psi^ - dt N^) / (1 + dt (deps + 2 dop.x + dop.y))
       "relax_exp"      el-exp.hpp:3-40     psi^' = E psi^ + Q N^, L = deps + 2 dop.x + dop.y
+      "conserved_poly" eom.hpp:143-180     psi^' = (psi^ + dt dop.x N^ + dt namp sqrt(N) |k| xi^)
+                       / (1 - dt dop.x (C - eps - P(k^2)))
+      "conserved_hpfc" eom.hpp:16-58       the conserved update with the anisotropic noise of
+                       hpfc_noise (knoise: its three fields) in place of |k| xi^
     Returns (psi^', max_k |psi^' - psi^|)."""
     dx, dy = _dops(shape_xyz, lens)
     deps = 1.0 + C - eps
@@ -455,6 +484,20 @@ def propagate(kpsi, knl, knoise, namp, dt, eps, lens, shape_xyz, C, propagator):
         with np.errstate(invalid="ignore", divide="ignore"):
             q = (e - 1.0) / lin
         new = e * kpsi + np.where(np.isnan(q), -dt, q) * knl
+    elif propagator == "conserved_poly":
+        denom = 1.0 - dt * dx * (deps - 1.0 - py_poly(-dx))
+        new = kpsi + dt * dx * knl
+        if knoise is not None:
+            nx, ny, nz = shape_xyz
+            new = new + dt * namp * np.sqrt(float(nx * ny * nz)) * np.sqrt(-dx) * knoise
+        new = new / denom
+    elif propagator == "conserved_hpfc":
+        denom = 1.0 - dt * (deps * dx + 2.0 * dy + dx * dy)
+        new = kpsi + dt * dx * knl
+        if knoise is not None:
+            nx, ny, nz = shape_xyz
+            new = new + dt * namp * np.sqrt(float(nx * ny * nz)) * hpfc_noise(knoise, shape_xyz, lens)
+        new = new / denom
     else:
         raise ValueError(propagator)
     return new, float(np.max(np.abs(new - kpsi)))
@@ -479,7 +522,10 @@ def step(kpsi, nsteps, dt, eps, lens, shape_xyz, mu=0.0, C=1.0, namp=0.0,
         nl = psi3_split(psi, None, mu, norm=True, C=C).astype(real_t)
         knl = r2c(nl, workers=workers).astype(cmpl_t)
         knoise = None
-        if namp != 0.0:
+        if namp != 0.0 and propagator == "conserved_hpfc":
+            knoise = tuple(fill_kspace(shape_xyz, seed, counter0 + t, dtype=noise_t, domain=HPFC_DOMAIN + i)
+                           for i in (1, 2, 3))
+        elif namp != 0.0:
             knoise = fill_kspace(shape_xyz, seed, counter0 + t, dtype=noise_t)
         if propagator == "conserved":
             new = update_eom(kpsi, knl, knoise, namp, dt, eps, lens, shape_xyz, C=C, ref_float_sqrt=ref_float_sqrt)

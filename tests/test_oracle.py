@@ -160,3 +160,27 @@ def test_peaks_on_gaussian_lattice():
     idx, val = O.findpeaks3d(f, 0.5)
     got = sorted(map(tuple, idx.tolist()))
     assert got == sorted(sites)
+
+
+def test_fused_forms_of_the_polynomial_and_hpfc_updates_equal_their_kernel_mirrors():
+    """The oracle's propagate() forms of kernel_update_eom_py and kernel_update_eom_hpfcnoise
+    (the stabilisation constant C in place of the reference's 1) equal its direct mirrors of
+    the two kernels at C = 1, with and without noise."""
+    rng = np.random.default_rng(0)
+    shape, lens = (32, 16, 8), (32 * 0.78, 16 * 0.78, 8 * 0.78)
+    k = O.r2c(rng.standard_normal(shape[::-1]))
+    n = O.r2c(rng.standard_normal(shape[::-1]))
+    xi = O.fill_kspace(shape, 3, 1, np.float64)
+    # (the mirrors take sqrt(N) and |k| in single precision, as the reference's sqrtf)
+    for noise, namp, tol in ((None, 0.0, 1e-12), (xi, 0.02, 1e-6)):
+        a, _ = O.propagate(k, n, noise, namp, 0.5, 0.3, lens, shape, 1.0, "conserved_poly")
+        b = O.update_eom_py(k, n, noise, namp, 0.5, 0.3, lens, shape)
+        assert np.abs(a - b).max() <= tol * np.abs(b).max()
+    s2, l2 = (64, 48, 1), (64 * 0.5, 48 * 0.5, 0.5)
+    k = O.r2c(rng.standard_normal(s2[::-1]))
+    n = O.r2c(rng.standard_normal(s2[::-1]))
+    f = [O.fill_kspace(s2, 3, 1, np.float64, domain=O.HPFC_DOMAIN + i) for i in (1, 2, 3)]
+    a, _ = O.propagate(k, n, tuple(f), 0.01, 0.5, 0.3, l2, s2, 1.0, "conserved_hpfc")
+    b = O.update_eom_hpfcnoise(k, n, *f, 0.01, 0.5, 0.3, l2, s2)
+    assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max()
+    assert not np.allclose(f[0], f[1])  # three independent streams
