@@ -175,7 +175,8 @@ def smooth_field(shape, seed, dtype):
 
 
 @pytest.mark.parametrize("dtype", [F32, F64])
-@pytest.mark.parametrize("shape", [(32, 24, 20), (17, 13, 11), (64, 48, 1), (128, 32, 20), (256, 48, 40)])
+@pytest.mark.parametrize("shape", [(32, 24, 20), (17, 13, 11), (64, 48, 1), (128, 32, 20), (256, 48, 40),
+                                   (256, 24, 12)])
 def test_findpeaks_bit_exact(shape, dtype):
     ctx = mk(shape, dtype)
     f = smooth_field(shape, 2, dtype)
@@ -194,14 +195,15 @@ def test_findpeaks_bit_exact(shape, dtype):
     np.testing.assert_array_equal(got["field"], val.astype(np.float32))
 
 
-@pytest.mark.parametrize("shape", [(32, 24, 20), (128, 32, 36)])
+@pytest.mark.parametrize("shape", [(32, 24, 20), (128, 32, 36), (256, 16, 20)])
 def test_findpeaks_nan_neighbourhoods(shape):
     """A NaN cell is no peak and makes none of its 26 neighbours one (each comparison with
     NaN is false in the reference's stencil), at grid edges (periodic wrap) too."""
     ctx = mk(shape, F32)
     f = smooth_field(shape, 7, F32)
     nx, ny, nz = shape
-    for (z, y, x) in [(0, 0, 0), (nz - 1, ny // 2, nx - 1), (nz // 2, ny - 1, nx // 2), (5, 3, 127 % nx)]:
+    for (z, y, x) in [(0, 0, 0), (nz - 1, ny // 2, nx - 1), (nz // 2, ny - 1, nx // 2), (5, 3, 127 % nx), (7, 9 % ny, 255 % nx),
+                      (3, 5, 8)]:
         f[z, y, x] = np.nan
     n, rec = ctx.findpeaks(up_r(ctx, f), -10.0)
     from mcstar_b200 import records_to_host
