@@ -437,9 +437,13 @@ __global__ void __launch_bounds__(X::T, 3) k_xlane(float2* g, int nrows, const f
     const float2 wt = twg[M + t];
     float2* xr = sm + rl * X::LDG;
     const int64_t ts = (int64_t)kTileW * nrows;  // elements between tiles
-    const int64_t rowoff = (int64_t)(blockIdx.x * R + rl) * kTileW;
+    // row blocks in descending order: the y pass before this one wrote the last planes last,
+    // so they are read while still in L2, and the first planes, which the y pass after this
+    // one reads first, are written last
+    const int blk = gridDim.x - 1 - blockIdx.x;
+    const int64_t rowoff = (int64_t)(blk * R + rl) * kTileW;
     float2* gl = g + rowoff + (t & (kTileW - 1)) + (t / kTileW) * ts;  // mode t of the row
-    float2* gnyq = g + FT * ts + blockIdx.x * R + rl;                   // mode M (tile of width 1)
+    float2* gnyq = g + FT * ts + blk * R + rl;                          // mode M (tile of width 1)
     const int src = (threadIdx.x & 31 & ~(P - 1)) | ((P - t) & (P - 1));  // the lane of mode M - t
     float2 v[E];
 #pragma unroll

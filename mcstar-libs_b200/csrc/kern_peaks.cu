@@ -378,7 +378,7 @@ __global__ void __launch_bounds__(256) k_words_count(const uint32_t* __restrict_
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t w0 = (int64_t)blockIdx.x * kChunkWords + warp * 1024 + lane;
     int c = 0;
-#pragma unroll 8
+#pragma unroll
     for (int it = 0; it < 32; ++it) {
         const int64_t w = w0 + it * 32;
         if (w < nwords) c += __popc(mask[w]);
@@ -399,13 +399,21 @@ __global__ void __launch_bounds__(256) k_peaks_emit(const T* __restrict__ psi, c
                                                     const int* __restrict__ offsets, MaxRec<T>* __restrict__ out,
                                                     int capacity) {
     __shared__ int ws[8];
+    __shared__ uint32_t words[8][32][32];  // the warps' words, kept for the emit pass
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t w0 = (int64_t)blockIdx.x * kChunkWords + warp * 1024 + lane;
-    int c = 0;
-#pragma unroll 8
+    // the warp's 1024 words, all loads in flight at once
+    uint32_t wv[32];
+#pragma unroll
     for (int it = 0; it < 32; ++it) {
         const int64_t w = w0 + it * 32;
-        if (w < nwords) c += __popc(mask[w]);
+        wv[it] = w < nwords ? mask[w] : 0u;
+    }
+    int c = 0;
+#pragma unroll
+    for (int it = 0; it < 32; ++it) {
+        c += __popc(wv[it]);
+        words[warp][it][lane] = wv[it];
     }
     c = warp_sum(c);
     if (lane == 0) ws[warp] = c;
@@ -415,7 +423,7 @@ __global__ void __launch_bounds__(256) k_peaks_emit(const T* __restrict__ psi, c
     for (int w = 0; w < warp; ++w) base += ws[w];
     for (int it = 0; it < 32; ++it) {
         const int64_t w = w0 + it * 32;
-        const uint32_t word = w < nwords ? mask[w] : 0u;
+        const uint32_t word = words[warp][it][lane];
         const int n = __popc(word);
         const int incl = warp_incl_scan(n, lane);
         int pos = base + incl - n;
