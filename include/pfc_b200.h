@@ -201,6 +201,19 @@ pfc_status pfc_noise_fill(pfc_ctx* ctx, void* arr, double sigma, uint64_t seed, 
 pfc_status pfc_findpeaks(pfc_ctx* ctx, const void* psi, double ths,
                          void* out_maxima, int capacity, int* n_found);
 
+/* The peak finder with its records going straight to host memory while the caller keeps
+ * stepping -- the overlap of findpeaks.hpp:37-53's copy and text output with the run.  The
+ * search starts when the work already queued on the context's stream is done (psi is
+ * ready), runs on the context's copy stream, writes the records into host_out (pinned host
+ * memory mapped into the device's address space, e.g. cudaHostAlloc / cudaMallocHost; else
+ * PFC_ERR_INVALID) and the count into *host_count, and the call returns at once.  psi, the
+ * records and the count belong to the search until pfc_findpeaks_wait(ctx, &n) returns it
+ * (n: the count; PFC_ERR_CAPACITY if it exceeded capacity, as pfc_findpeaks).  One search in
+ * flight per context; a pfc_findpeaks call on the context waits for it on the device. */
+pfc_status pfc_findpeaks_async(pfc_ctx* ctx, const void* psi, double ths, void* host_out, int capacity,
+                               int* host_count);
+pfc_status pfc_findpeaks_wait(pfc_ctx* ctx, int* n_found);
+
 /* The same peak finder for callers that must not allocate device memory -- no
  * counterpart in mcstar-libs.  A simulation whose device memory is reserved up front
  * by its own pool, or a driver that cannot afford the device-wide synchronisation a

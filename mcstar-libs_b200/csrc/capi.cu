@@ -109,6 +109,7 @@ void free_ctx(pfc_ctx* c) {
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : c->host_ev)
         if (e) cudaEventDestroy(e);
+    if (c->peaks_done) cudaEventDestroy(c->peaks_done);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->side_fork) cudaEventDestroy(c->side_fork);
     if (c->side_join) cudaEventDestroy(c->side_join);
@@ -547,7 +548,7 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
     };
     const int64_t nyz = (int64_t)c->ny * c->nz;
     c->px.tile = shifted(fit(pow2_floor((64 * 1024) / (2 * (size_t)lx * csz), 16), nyz), o.tile_shift[0]);
-    c->px.smem = 2 * (size_t)c->px.tile * lx * csz;
+    c->px.smem = 2 * (size_t)c->px.tile * line_stride(lx) * csz;
     c->py.tile = shifted(fit(pow2_floor((64 * 1024) / (2 * (size_t)c->ny * csz), 16), (int64_t)c->nxh * c->nz),
                          o.tile_shift[1]);
     c->py.smem = 2 * (size_t)c->py.tile * line_stride(c->ny) * csz;
@@ -728,13 +729,66 @@ pfc_status pfc_findpeaks(pfc_ctx* ctx, const void* psi, double ths, void* out, i
         return fail(ctx, PFC_ERR_INVALID, "pfc_findpeaks: bad arguments");
     if (ctx->nz == 1 && !(ctx->nx > 1 && ctx->ny > 1))
         return fail(ctx, PFC_ERR_INVALID, "pfc_findpeaks: input not a 2d array");
-    PFC_CUDA(launch_findpeaks(ctx, psi, ths, out, capacity), "pfc_findpeaks");
+    if (ctx->async_pending)  // the scratch of a search still in flight on the copy stream
+        PFC_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->peaks_done, 0), "pfc_findpeaks wait");
+    PFC_CUDA(launch_findpeaks(ctx, psi, ths, out, capacity, ctx->stream), "pfc_findpeaks");
     int total = 0;
     PFC_CUDA(cudaMemcpyAsync(&total, ctx->peak_offsets + ctx->n_peak_blocks, sizeof(int), cudaMemcpyDeviceToHost,
                              ctx->stream), "pfc_findpeaks copy");
     PFC_CUDA(cudaStreamSynchronize(ctx->stream), "pfc_findpeaks sync");
     *n_found = total;
     if (total > capacity) return fail(ctx, PFC_ERR_CAPACITY, "pfc_findpeaks: more peaks than capacity");
+    return PFC_OK;
+}
+
+namespace {
+// the copy stream and its events (created by the first call that needs them)
+cudaError_t ensure_copy_stream(pfc_ctx* ctx) {
+    if (ctx->copy_stream) return cudaSuccess;
+    cudaError_t e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
+    for (cudaEvent_t& ev : ctx->host_ev)
+        if (!e) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (!e) e = cudaEventCreateWithFlags(&ctx->peaks_done, cudaEventDisableTiming);
+    return e;
+}
+}  // namespace
+
+pfc_status pfc_findpeaks_async(pfc_ctx* ctx, const void* psi, double ths, void* host_out, int capacity,
+                               int* host_count) {
+    PFC_CHECK_CTX();
+    if (!psi || !host_count || capacity < 0 || (capacity > 0 && !host_out))
+        return fail(ctx, PFC_ERR_INVALID, "pfc_findpeaks_async: bad arguments");
+    if (ctx->nz == 1 && !(ctx->nx > 1 && ctx->ny > 1))
+        return fail(ctx, PFC_ERR_INVALID, "pfc_findpeaks_async: input not a 2d array");
+    void* dout = nullptr;
+    if (capacity > 0 && cudaHostGetDevicePointer(&dout, host_out, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, PFC_ERR_INVALID, "pfc_findpeaks_async: host_out is not pinned host memory mapped to the device");
+    }
+    PFC_CUDA(ensure_copy_stream(ctx), "pfc_findpeaks_async stream");
+    // the search starts when the work queued on the context's stream (which wrote psi) is done
+    cudaEvent_t ready = ctx->host_ev[2 * pfc_ctx::kHostChunks];
+    PFC_CUDA(cudaEventRecord(ready, ctx->stream), "pfc_findpeaks_async event");
+    PFC_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ready, 0), "pfc_findpeaks_async wait");
+    PFC_CUDA(launch_findpeaks(ctx, psi, ths, dout, capacity, ctx->copy_stream), "pfc_findpeaks_async");
+    PFC_CUDA(cudaMemcpyAsync(host_count, ctx->peak_offsets + ctx->n_peak_blocks, sizeof(int), cudaMemcpyDeviceToHost,
+                             ctx->copy_stream),
+             "pfc_findpeaks_async count");
+    PFC_CUDA(cudaEventRecord(ctx->peaks_done, ctx->copy_stream), "pfc_findpeaks_async event");
+    ctx->async_count = host_count;
+    ctx->async_capacity = capacity;
+    ctx->async_pending = true;
+    return PFC_OK;
+}
+
+pfc_status pfc_findpeaks_wait(pfc_ctx* ctx, int* n_found) {
+    PFC_CHECK_CTX();
+    if (!ctx->async_pending) return fail(ctx, PFC_ERR_INVALID, "pfc_findpeaks_wait: no search in flight");
+    PFC_CUDA(cudaEventSynchronize(ctx->peaks_done), "pfc_findpeaks_wait");
+    ctx->async_pending = false;
+    const int total = *ctx->async_count;
+    if (n_found) *n_found = total;
+    if (total > ctx->async_capacity) return fail(ctx, PFC_ERR_CAPACITY, "pfc_findpeaks_async: more peaks than capacity");
     return PFC_OK;
 }
 
@@ -835,10 +889,7 @@ pfc_status pfc_step_host(pfc_ctx* ctx, const void* host_in, void* host_out, void
         PFC_CUDA(cudaStreamSynchronize(ctx->stream), "pfc_step_host sync");
         return PFC_OK;
     }
-    if (!ctx->copy_stream) {
-        PFC_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "pfc_step_host stream");
-        for (cudaEvent_t& e : ctx->host_ev) PFC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "pfc_step_host event");
-    }
+    PFC_CUDA(ensure_copy_stream(ctx), "pfc_step_host stream");
     cudaStream_t cs = ctx->copy_stream;
     cudaEvent_t* ev_in = ctx->host_ev;           // chunk g has arrived
     cudaEvent_t* ev_out = ctx->host_ev + G;      // chunk g of psi^' is written

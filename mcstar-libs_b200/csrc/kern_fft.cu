@@ -29,13 +29,13 @@ __global__ void __launch_bounds__(256) k_cols(const cx<T>* __restrict__ in, cx<T
     const int64_t base = (int64_t)blockIdx.y * os + i0;
     for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
         const int i = e & (tile - 1), k = e >> tile_lg;
-        if (i < nt) b0[i * ld + k] = in[base + i + k * es];
+        if (i < nt) b0[i * ld + lpad(k)] = in[base + i + k * es];
     }
     __syncthreads();
     cx<T>* r = stockham_lines<T, DIR>(b0, b1, nt, ld, p, tw);
     for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
         const int i = e & (tile - 1), k = e >> tile_lg;
-        if (i < nt) out[base + i + k * es] = r[i * ld + k] * scale;
+        if (i < nt) out[base + i + k * es] = r[i * ld + lpad(k)] * scale;
     }
 }
 
@@ -66,8 +66,8 @@ __global__ void __launch_bounds__(256) k_rows_r2c(const T* __restrict__ in, cx<T
                                                   const cx<T>* __restrict__ post, int rpc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
-    const int L = p.n;
-    cx<T>* b1 = b0 + (size_t)rpc * L;
+    const int L = p.n, ld = line_stride(L);
+    cx<T>* b1 = b0 + (size_t)rpc * ld;
     const int row0 = blockIdx.x * rpc;
     const int nr = min(rpc, nrows - row0);
     const int nxh = nx / 2 + 1;
@@ -76,16 +76,16 @@ __global__ void __launch_bounds__(256) k_rows_r2c(const T* __restrict__ in, cx<T
     for (int e = threadIdx.x; e < nr * L; e += blockDim.x) {
         const int r = fdiv(e, p.by_n), m = e - r * L;
         const T* row = in + (int64_t)(row0 + r) * nx;
-        b0[e] = even ? reinterpret_cast<const cx<T>*>(row)[m] : mkc<T>(row[m], T(0));
+        b0[r * ld + lpad(m)] = even ? reinterpret_cast<const cx<T>*>(row)[m] : mkc<T>(row[m], T(0));
     }
     __syncthreads();
-    cx<T>* z = stockham_lines<T, -1>(b0, b1, nr, L, p, tw);
+    cx<T>* z = stockham_lines<T, -1>(b0, b1, nr, ld, p, tw);
     for (int e = threadIdx.x; e < nr * nxh; e += blockDim.x) {
         const int r = fdiv(e, by_nxh), k = e - r * nxh;
-        const cx<T>* zr = z + (size_t)r * L;
+        const cx<T>* zr = z + (size_t)r * ld;
         cx<T> v;
-        if (even) v = r2c_post<T>(zr[k % L], zr[(L - k) % L], post[k]);
-        else v = zr[k];
+        if (even) v = r2c_post<T>(zr[lpad(k % L)], zr[lpad((L - k) % L)], post[k]);
+        else v = zr[lpad(k)];
         out[(int64_t)(row0 + r) * nxh + k] = v;
     }
 }
@@ -96,8 +96,8 @@ __global__ void __launch_bounds__(256) k_rows_c2r(const cx<T>* __restrict__ in, 
                                                   const cx<T>* __restrict__ post, int rpc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
-    const int L = p.n;
-    cx<T>* b1 = b0 + (size_t)rpc * L;
+    const int L = p.n, ld = line_stride(L);
+    cx<T>* b1 = b0 + (size_t)rpc * ld;
     const int row0 = blockIdx.x * rpc;
     const int nr = min(rpc, nrows - row0);
     const int nxh = nx / 2 + 1;
@@ -108,15 +108,15 @@ __global__ void __launch_bounds__(256) k_rows_c2r(const cx<T>* __restrict__ in, 
         cx<T> v;
         if (even) v = c2r_pre<T>(row[k], row[L - k], post[k]);
         else v = k < nxh ? row[k] : cconj(row[nx - k]);
-        b0[e] = v;
+        b0[r * ld + lpad(k)] = v;
     }
     __syncthreads();
-    cx<T>* z = stockham_lines<T, 1>(b0, b1, nr, L, p, tw);
+    cx<T>* z = stockham_lines<T, 1>(b0, b1, nr, ld, p, tw);
     for (int e = threadIdx.x; e < nr * L; e += blockDim.x) {
         const int r = fdiv(e, p.by_n), m = e - r * L;
         T* row = out + (int64_t)(row0 + r) * nx;
-        if (even) reinterpret_cast<cx<T>*>(row)[m] = z[e];
-        else row[m] = z[e].x;
+        if (even) reinterpret_cast<cx<T>*>(row)[m] = z[r * ld + lpad(m)];
+        else row[m] = z[r * ld + lpad(m)].x;
     }
 }
 
@@ -136,8 +136,8 @@ __global__ void __launch_bounds__(256) k_rows_nonlin(cx<T>* buf, const T* __rest
     buf += blockIdx.z * ms;  // fields of a batch (grid z; no potential then)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* b0 = reinterpret_cast<cx<T>*>(smem_raw);
-    const int L = p.n;
-    cx<T>* b1 = b0 + (size_t)rpc * L;
+    const int L = p.n, ld = line_stride(L);
+    cx<T>* b1 = b0 + (size_t)rpc * ld;
     const int row0 = blockIdx.x * rpc;
     const int nr = min(rpc, nrows - row0);
     const int nxh = nx / 2 + 1;
@@ -149,15 +149,15 @@ __global__ void __launch_bounds__(256) k_rows_nonlin(cx<T>* buf, const T* __rest
         cx<T> v;
         if (even) v = c2r_pre<T>(row[k], row[L - k], post[k]);
         else v = k < nxh ? row[k] : cconj(row[nx - k]);
-        b0[e] = v;
+        b0[r * ld + lpad(k)] = v;
     }
     __syncthreads();
-    cx<T>* z = stockham_lines<T, 1>(b0, b1, nr, L, p, tw);
+    cx<T>* z = stockham_lines<T, 1>(b0, b1, nr, ld, p, tw);
     cx<T>* other = (z == b0) ? b1 : b0;
     for (int e = threadIdx.x; e < nr * L; e += blockDim.x) {
         const int r = fdiv(e, p.by_n), m = e - r * L;
         const int64_t rowi = (int64_t)(row0 + r) * nx;
-        cx<T> v = z[e];
+        cx<T> v = z[r * ld + lpad(m)];
         if (even) {
             T a = cubic<T>(v.x, mul, C, mu), b = cubic<T>(v.y, mul, C, mu);
             if (pot) { a += pot[rowi + 2 * m]; b += pot[rowi + 2 * m + 1]; }
@@ -167,16 +167,16 @@ __global__ void __launch_bounds__(256) k_rows_nonlin(cx<T>* buf, const T* __rest
             if (pot) a += pot[rowi + m];
             v = mkc<T>(a, T(0));
         }
-        z[e] = v;
+        z[r * ld + lpad(m)] = v;
     }
     __syncthreads();
-    cx<T>* y = stockham_lines<T, -1>(z, other, nr, L, p, tw);
+    cx<T>* y = stockham_lines<T, -1>(z, other, nr, ld, p, tw);
     for (int e = threadIdx.x; e < nr * nxh; e += blockDim.x) {
         const int r = fdiv(e, by_nxh), k = e - r * nxh;
-        const cx<T>* yr = y + (size_t)r * L;
+        const cx<T>* yr = y + (size_t)r * ld;
         cx<T> v;
-        if (even) v = r2c_post<T>(yr[k % L], yr[(L - k) % L], post[k]);
-        else v = yr[k];
+        if (even) v = r2c_post<T>(yr[lpad(k % L)], yr[lpad((L - k) % L)], post[k]);
+        else v = yr[lpad(k)];
         buf[(int64_t)(row0 + r) * nxh + k] = v;
     }
 }
@@ -310,8 +310,8 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
         const int i = e & (tile - 1), k = e >> tile_lg;
         if (i < nt) {
             const int64_t off = ((int64_t)k * ny + ky) * nxh + i0 + i;
-            b0[i * ld + k] = A[off];
-            b0[(tile + i) * ld + k] = B[off];
+            b0[i * ld + lpad(k)] = A[off];
+            b0[(tile + i) * ld + lpad(k)] = B[off];
         }
     }
     __syncthreads();
@@ -325,9 +325,10 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
     for (int e = threadIdx.x; e < nt * n; e += blockDim.x) {
         const int i = fdiv(e, p.by_n), kz = e - i * n;
         const int kx = i0 + i;
-        const cx<T> v = zmode<T, PROP>(r[i * ld + kz], r[(tile + i) * ld + kz], kx, kyg, kz, nx, nz, k1, deps, a, k0, mc);
+        const cx<T> v =
+            zmode<T, PROP>(r[i * ld + lpad(kz)], r[(tile + i) * ld + lpad(kz)], kx, kyg, kz, nx, nz, k1, deps, a, k0, mc);
         if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
-        r[i * ld + kz] = v;
+        r[i * ld + lpad(kz)] = v;
     }
     if (!prop_conserved<PROP>() && a.maxc) fold_max_change(mc, a.maxc);
     __syncthreads();
@@ -340,7 +341,7 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
     }
     for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
         const int i = e & (tile - 1), k = e >> tile_lg;
-        if (i < nt) A[((int64_t)k * ny + ky) * nxh + i0 + i] = outb[i * ld + k] * scale;
+        if (i < nt) A[((int64_t)k * ny + ky) * nxh + i0 + i] = outb[i * ld + lpad(k)] * scale;
     }
 }
 

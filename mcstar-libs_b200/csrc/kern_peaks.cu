@@ -451,7 +451,7 @@ __global__ void __launch_bounds__(256) k_peaks_emit(const T* __restrict__ psi, c
 }
 
 template <typename T>
-cudaError_t peaks_ctx(const pfc_ctx* c, const void* psi, double ths, void* out, int capacity) {
+cudaError_t peaks_ctx(const pfc_ctx* c, const void* psi, double ths, void* out, int capacity, cudaStream_t st) {
     const bool d3 = c->nz > 1;
     const int wpr = (c->nx + 31) / 32;
     const int64_t nwords = (int64_t)c->nz * c->ny * wpr;
@@ -460,18 +460,18 @@ cudaError_t peaks_ctx(const pfc_ctx* c, const void* psi, double ths, void* out, 
     if (std::is_same<T, float>::value && d3 && c->nx % 128 == 0 && c->ny % kRows4 == 0 &&
         ((uintptr_t)psi & 15) == 0)
         k_peaks_mark4<<<dim3(c->nx / 128, c->ny / kRows4, (c->nz + kZC4 - 1) / kZC4), 32 * (kRows4 + 2),
-                        kMark4Smem, c->stream>>>((const float*)psi, c->nx, c->ny, c->nz, (float)ths, c->peak_mask,
+                        kMark4Smem, st>>>((const float*)psi, c->nx, c->ny, c->nz, (float)ths, c->peak_mask,
                                                  wpr);
     else if (d3)
-        k_peaks_mark<T, true><<<grid, dim3(kTX, kTY), 0, c->stream>>>((const T*)psi, c->nx, c->ny, c->nz, (T)ths,
+        k_peaks_mark<T, true><<<grid, dim3(kTX, kTY), 0, st>>>((const T*)psi, c->nx, c->ny, c->nz, (T)ths,
                                                                        c->peak_mask, wpr);
     else
-        k_peaks_mark<T, false><<<grid, dim3(kTX, kTY), 0, c->stream>>>((const T*)psi, c->nx, c->ny, c->nz, (T)ths,
+        k_peaks_mark<T, false><<<grid, dim3(kTX, kTY), 0, st>>>((const T*)psi, c->nx, c->ny, c->nz, (T)ths,
                                                                         c->peak_mask, wpr);
-    k_words_count<<<nchunks, 256, 0, c->stream>>>(c->peak_mask, nwords, c->peak_counts);
-    k_scan<<<1, 1024, 0, c->stream>>>(c->peak_counts, nchunks, c->peak_offsets);
+    k_words_count<<<nchunks, 256, 0, st>>>(c->peak_mask, nwords, c->peak_counts);
+    k_scan<<<1, 1024, 0, st>>>(c->peak_counts, nchunks, c->peak_offsets);
     if (capacity > 0 && out)
-        k_peaks_emit<T><<<nchunks, 256, 0, c->stream>>>((const T*)psi, c->peak_mask, nwords, c->nx, c->ny, wpr,
+        k_peaks_emit<T><<<nchunks, 256, 0, st>>>((const T*)psi, c->peak_mask, nwords, c->nx, c->ny, wpr,
                                                         c->peak_offsets, (MaxRec<T>*)out, capacity);
     return cudaGetLastError();
 }
@@ -487,9 +487,10 @@ int peak_chunks(int nx, int ny, int nz) {
     return (int)((peak_mask_words(nx, ny, nz) + kChunkWords - 1) / kChunkWords);
 }
 
-cudaError_t launch_findpeaks(const pfc_ctx* c, const void* psi, double ths, void* out, int capacity) {
-    return c->dtype == PFC_F64 ? peaks_ctx<double>(c, psi, ths, out, capacity)
-                               : peaks_ctx<float>(c, psi, ths, out, capacity);
+cudaError_t launch_findpeaks(const pfc_ctx* c, const void* psi, double ths, void* out, int capacity,
+                             cudaStream_t st) {
+    return c->dtype == PFC_F64 ? peaks_ctx<double>(c, psi, ths, out, capacity, st)
+                               : peaks_ctx<float>(c, psi, ths, out, capacity, st);
 }
 
 }  // namespace pfc

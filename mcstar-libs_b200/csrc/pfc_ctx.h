@@ -93,6 +93,12 @@ struct pfc_ctx {
     cudaEvent_t side_fork = nullptr, side_join = nullptr;
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t host_ev[2 * kHostChunks + 2] = {};
+    // pfc_findpeaks_async: its completion event (on the copy stream), the caller's count and
+    // capacity; pending until pfc_findpeaks_wait
+    cudaEvent_t peaks_done = nullptr;
+    int* async_count = nullptr;
+    int async_capacity = 0;
+    bool async_pending = false;
 };
 
 namespace pfc {
@@ -212,7 +218,9 @@ cudaError_t launch_reduce_final(const pfc_ctx* c, int slot, double scale);
 // ---- peaks (kern_peaks.cu) ----
 int64_t peak_mask_words(int nx, int ny, int nz);
 int peak_chunks(int nx, int ny, int nz);
-cudaError_t launch_findpeaks(const pfc_ctx* c, const void* psi, double ths, void* out, int capacity);
+// (on stream st: the context's, or the copy stream of pfc_findpeaks_async)
+cudaError_t launch_findpeaks(const pfc_ctx* c, const void* psi, double ths, void* out, int capacity,
+                             cudaStream_t st);
 
 // ---- bond order (kern_bond.cu) ----
 size_t bond_scratch_bytes(int max_atoms);

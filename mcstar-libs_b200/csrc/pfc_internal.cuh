@@ -117,9 +117,13 @@ __device__ __forceinline__ int fdiv(int n, FastDiv f) {
     return (int)((__umulhi((uint32_t)n, f.mul) + (uint32_t)n) >> f.shift);
 }
 
-// Shared-memory stride of the lines of a column tile: odd (in elements), so that the lanes
-// of a warp moving one element of each of consecutive lines hit distinct banks.
-__host__ __device__ constexpr int line_stride(int n) { return n | 1; }
+// Lines of the Stockham engine in shared memory: element k of a line sits at lpad(k) (one
+// pad element after every 32), so that the strided writes of the early stages (R apart) and
+// the reads of later ones spread over the banks; lines are line_stride(n) elements apart, an
+// odd number, so that the lanes of a warp moving one element of each of consecutive lines
+// hit distinct banks too.
+__host__ __device__ __forceinline__ constexpr int lpad(int k) { return k + (k >> 5); }
+__host__ __device__ constexpr int line_stride(int n) { return (n + (n >> 5) + 1) | 1; }
 
 struct LinePlan {
     int n;
@@ -142,7 +146,7 @@ __device__ __forceinline__ void stockham_bfly_gen(const cx<T>* __restrict__ sl, 
     cx<T> v[kMaxOddRadix];
     const int jj = j - fdiv(j, by_ns) * Ns;
     for (int r = 0; r < R; ++r) {
-        cx<T> a = sl[j + r * m];
+        cx<T> a = sl[lpad(j + r * m)];
         if (Ns > 1 && r > 0) {
             cx<T> w = tws[jj * (R - 1) + r - 1];
             if (DIR > 0) w.y = -w.y;
@@ -163,7 +167,7 @@ __device__ __forceinline__ void stockham_bfly_gen(const cx<T>* __restrict__ sl, 
             acc.x += p.x;
             acc.y += p.y;
         }
-        dl[od + k * Ns] = acc;
+        dl[lpad(od + k * Ns)] = acc;
     }
 }
 
@@ -173,7 +177,7 @@ __device__ __forceinline__ void stockham_bfly(const cx<T>* __restrict__ sl, cx<T
                                               FastDiv by_ns) {
     cx<T> v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = sl[j + r * m];
+    for (int r = 0; r < R; ++r) v[r] = sl[lpad(j + r * m)];
     const int jj = j - fdiv(j, by_ns) * Ns;
     if (Ns > 1) {
 #pragma unroll
@@ -186,7 +190,7 @@ __device__ __forceinline__ void stockham_bfly(const cx<T>* __restrict__ sl, cx<T
     Dft<T, DIR, R>::run(v);
     const int od = (j - jj) * R + jj;
 #pragma unroll
-    for (int r = 0; r < R; ++r) dl[od + r * Ns] = v[r];
+    for (int r = 0; r < R; ++r) dl[lpad(od + r * Ns)] = v[r];
 }
 
 // FFT of nlines lines, line l at a[l*ld .. l*ld+n).  Ping-pongs between a and b and

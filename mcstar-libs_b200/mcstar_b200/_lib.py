@@ -30,7 +30,7 @@ EXPORTED = (
     "pfc_update_el", "pfc_init_el_op", "pfc_update_el_exp", "pfc_update_eom_py", "pfc_update_eom_hpfcnoise",
     "pfc_gaussian_init", "pfc_kmult_real", "pfc_kmult_imag", "pfc_square", "pfc_write_lowpass_2d",
     "pfc_amplitude_lowpass", "pfc_bond_reserve", "pfc_default_options", "pfc_create_with", "pfc_get_options",
-    "pfc_tune", "pfc_step_prop", "pfc_step_host", "pfc_slab_zinv", "pfc_slab_xy", "pfc_slab_zpass",
+    "pfc_tune", "pfc_step_prop", "pfc_step_host", "pfc_findpeaks_async", "pfc_findpeaks_wait", "pfc_slab_zinv", "pfc_slab_xy", "pfc_slab_zpass",
 )
 
 # pfc_propagator
@@ -120,6 +120,8 @@ _SIGS = {
     "pfc_step": ([_P, _P, _I, ctypes.POINTER(PfcStepParams)], _I),
     "pfc_step_prop": ([_P, _P, _I, ctypes.POINTER(PfcStepParams), _I, ctypes.POINTER(_D)], _I),
     "pfc_step_host": ([_P, _P, _P, _P, _I, ctypes.POINTER(PfcStepParams)], _I),
+    "pfc_findpeaks_async": ([_P, _P, _D, _P, _I, ctypes.POINTER(_I)], _I),
+    "pfc_findpeaks_wait": ([_P, ctypes.POINTER(_I)], _I),
     "pfc_slab_zinv": ([_P, _P, _P, _I], _I),
     "pfc_slab_xy": ([_P, _P, _P, _D, _D], _I),
     "pfc_slab_zpass": ([_P, _P, _P, ctypes.POINTER(PfcStepParams), _I, _I, _I], _I),

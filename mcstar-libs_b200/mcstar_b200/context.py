@@ -196,6 +196,24 @@ class Context:
         self._call("pfc_findpeaks", _ptr(psi), float(ths), _ptr(out), int(capacity), ctypes.byref(n))
         return n.value, out[: n.value * rec]
 
+    def findpeaks_async(self, psi, ths, host_out):
+        """Starts a peak search whose records go to host_out (a pinned CPU uint8 tensor of
+        Maximum<F> records, e.g. torch.empty(..., dtype=torch.uint8).pin_memory()) while the
+        caller keeps stepping; returns at once.  findpeaks_wait() gives the count."""
+        rec = 16 if self.code == _lib.PFC_F32 else 32
+        self._async_count = torch.zeros(1, dtype=torch.int32).pin_memory()
+        self._async_out = host_out
+        self._call("pfc_findpeaks_async", _ptr(psi), float(ths), ctypes.c_void_p(host_out.data_ptr()),
+                   int(host_out.numel() // rec), ctypes.cast(ctypes.c_void_p(self._async_count.data_ptr()),
+                                                             ctypes.POINTER(ctypes.c_int)))
+
+    def findpeaks_wait(self):
+        """Waits for the search of findpeaks_async; returns (n_found, records on the host)."""
+        rec = 16 if self.code == _lib.PFC_F32 else 32
+        n = ctypes.c_int()
+        self._call("pfc_findpeaks_wait", ctypes.byref(n))
+        return n.value, self._async_out[: n.value * rec]
+
     def bond_order(self, maxima, n, h, ths, boxsize, rlim, capacity=None):
         capacity = max(1, n) if capacity is None else capacity
         rows = torch.empty(capacity * _lib.PFC_BOND_NCOL, dtype=torch.float64, device="cuda")

@@ -213,6 +213,36 @@ def test_findpeaks_nan_neighbourhoods(shape):
     np.testing.assert_array_equal(np.stack([got["i0"], got["i1"], got["i2"]], 1).astype(np.int64), idx)
 
 
+@pytest.mark.parametrize("shape", [(64, 64, 64), (256, 48, 40)])
+def test_findpeaks_async_while_stepping(shape):
+    """pfc_findpeaks_async: the records go to pinned host memory while the stepper keeps
+    stepping on the context's stream; after pfc_findpeaks_wait they equal pfc_findpeaks's.
+    Too small a buffer gives PFC_ERR_CAPACITY at the wait; pageable memory is refused."""
+    from mcstar_b200 import PfcError, Stepper
+    st = Stepper(shape, math.pi / 4, 0.5, 0.3, dtype=F32)
+    st.set_real(smooth_field(shape, 5, F32))
+    field = st.real_device().contiguous().clone()
+    n_sync, rec_sync = st.ctx.findpeaks(field, 0.0)
+    assert n_sync > 0
+    host = torch.empty(n_sync * 16 + 4096, dtype=torch.uint8).pin_memory()
+    st.ctx.findpeaks_async(field, 0.0, host)
+    st.step(5)  # the step's kernels on the context's stream, the search on the copy stream
+    n, rec = st.ctx.findpeaks_wait()
+    assert n == n_sync
+    assert torch.equal(rec, rec_sync.cpu())
+    small = torch.empty(16, dtype=torch.uint8).pin_memory()
+    st.ctx.findpeaks_async(field, 0.0, small)
+    with pytest.raises(PfcError) as e:
+        st.ctx.findpeaks_wait()
+    assert e.value.status == 5
+    with pytest.raises(PfcError) as e:
+        st.ctx.findpeaks_async(field, 0.0, torch.empty(4096, dtype=torch.uint8))
+    assert e.value.status == 1
+    with pytest.raises(PfcError) as e:
+        st.ctx.findpeaks_wait()  # nothing in flight
+    assert e.value.status == 1
+
+
 def test_findpeaks_plateau_and_capacity():
     from mcstar_b200 import PfcError
     shape = (16, 16, 16)
