@@ -511,7 +511,7 @@ def run_b200(args, ws, rank, local):
                 "h2d_bytes_per_step": S / args.steps, "d2h_bytes_per_step": S / args.steps,
                 "note": "per K-step run, one C-ABI call (pfc_step_host): the initial half spectrum from "
                         "pinned host memory, K steps, the final half spectrum back to pinned host memory; "
-                        "the copies run by ky chunks overlapped with the entry pass and the last z pass"},
+                        "the copy in runs by ky chunks overlapped with the entry pass"},
         "gpu_launches": prof["launches"],
         "roofline": roof,
         "clocks": clk,

@@ -306,8 +306,7 @@ pfc_status pfc_step_prop(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_pa
  * holds psi^ (state layout, pfc_state_bytes(ctx) bytes; pinned memory for the copies to
  * overlap), kpsi is the device state buffer (it holds psi^ at the end, as after pfc_step),
  * host_out receives the final psi^ (may be host_in).  The copy in runs by ky chunks
- * overlapped with the step's entry pass, the copy out by ky chunks overlapped with the last
- * step's z pass.  Returns when host_out is written. */
+ * overlapped with the step's entry pass.  Returns when host_out is written. */
 pfc_status pfc_step_host(pfc_ctx* ctx, const void* host_in, void* host_out, void* kpsi, int nsteps,
                          const pfc_step_params* params);
 

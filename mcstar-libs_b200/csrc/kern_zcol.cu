@@ -772,19 +772,17 @@ cudaError_t launch_zcarry(const pfc_ctx* c, void* kpsi, void* A, const void* B, 
 }
 
 cudaError_t launch_zcarry_tiled(const pfc_ctx* c, const void* psi_in, const void* B, void* psi_out, void* A,
-                                const ZPropArgs& a, int ky0, int nky) {
+                                const ZPropArgs& a) {
     if (c->fused_z != 6) return cudaErrorNotSupported;
-    if (nky < 0) nky = c->ny - ky0;
-    if (ky0 < 0 || nky < 1 || ky0 + nky > c->ny || (!a.final_step && nky != c->ny)) return cudaErrorInvalidValue;
     using Z = Z3_512;
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->zcol_tw_off;
     const ZArgsF za = zargs_f(a);
     const int ntx = (c->nxh + Z::TX - 1) / Z::TX;
     return by_prop(a.prop, [&](auto P) {
         if (a.final_step) {
-            k_zcarry3<Z, true, P.value><<<dim3(ntx, nky, c->batch), Z::TH, Z::SMEM_CARRY, c->stream>>>(
+            k_zcarry3<Z, true, P.value><<<dim3(ntx, c->ny, c->batch), Z::TH, Z::SMEM_CARRY, c->stream>>>(
                 (const float2*)psi_in, (const float2*)B, (float2*)psi_out, (float2*)A, c->nx, c->ny, za, c->k0,
-                c->flag, tw, 0, ky0, c->mstride);
+                c->flag, tw, 0, 0, c->mstride);
             return cudaGetLastError();
         }
         // whole tiles with bulk copies (psi^ in place, A' over B); the partial last tile with

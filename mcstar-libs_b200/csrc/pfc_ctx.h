@@ -191,9 +191,8 @@ cudaError_t launch_zcol(const pfc_ctx* c, const void* A, const void* B, void* O,
 cudaError_t launch_zcarry(const pfc_ctx* c, void* kpsi, void* A, const void* B, const ZPropArgs& a);
 // the same on the z-tiled layout (nz = 512): psi^ z-tiled (psi_out may be psi_in); B and A
 // z-tiled (A may be B), or on the last step B and psi_out standard (psi_out may be B), no A
-// (ky0, nky: the last step's z pass over ky in [ky0, ky0 + nky) only; nky < 0: to ny)
 cudaError_t launch_zcarry_tiled(const pfc_ctx* c, const void* psi_in, const void* B, void* psi_out, void* A,
-                                const ZPropArgs& a, int ky0 = 0, int nky = -1);
+                                const ZPropArgs& a);
 // FP32 field copy between the standard and the z-tiled layout (out of place)
 cudaError_t launch_relayout(const pfc_ctx* c, const void* in, void* out, int to_tiled, int ky0 = 0, int nky = -1);
 
