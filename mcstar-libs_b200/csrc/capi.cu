@@ -210,12 +210,16 @@ ZPropArgs zargs(const pfc_ctx* c, const pfc_step_params* p) {
 constexpr int kLayZ = 1, kLayRow = 2;
 
 // Where the stepper's mixed-grid field A = IFFT_z(psi^)/nz lives: in work2 beside the
-// carried psi^ (z_carry) or z-tiled (tiled), in the psi^ buffer when tiled with psi^
-// carried z-tiled in work2, else in place of psi^.
+// carried psi^ (z_carry) or z-tiled (tiled), in work when tiled with psi^ carried z-tiled in
+// work2 (the psi^ buffer then holds the row-tiled field of the x pass), else in place of
+// psi^.
 void* carried_A(pfc_ctx* ctx, void* kpsi) {
-    if (ctx->tiled) return ctx->z_carry ? kpsi : ctx->work2;
+    if (ctx->tiled) return ctx->z_carry ? ctx->work : ctx->work2;
     return ctx->z_carry ? ctx->work2 : kpsi;
 }
+// The row-tiled field of the x pass (tiled schedules): the psi^ buffer when psi^ is carried
+// in work2 and A in work, else work.
+void* row_field(pfc_ctx* ctx, void* kpsi) { return ctx->z_carry ? kpsi : ctx->work; }
 
 // psi^ -> A = IFFT_z(psi^)/nz; the k = 0 mode is kept in FP64
 // complex FFT along z of a half-spectrum field: the register column kernel where the
@@ -233,10 +237,11 @@ cudaError_t ycols(const pfc_ctx* ctx, int dir, const void* in, void* out) {
 
 cudaError_t step_entry(pfc_ctx* ctx, void* kpsi) {
     if (ctx->tiled && ctx->z_carry)
-        return traced(ctx, 0, 3, [&] {
+        // one pass: the z columns of psi^ (standard layout) read once, A = IFFT_z/nz into work
+        // and psi^ itself into work2, both z-tiled
+        return traced(ctx, 0, 2, [&] {
             cudaError_t e = launch_k0_save(ctx, kpsi);
-            if (!e) e = launch_relayout(ctx, kpsi, ctx->work2, 1);
-            if (!e) e = zcols(ctx, 1, ctx->work2, kpsi, 1.0 / ctx->nz, kLayZ | kLayZ << 2);
+            if (!e) e = launch_zfft(ctx, 1, kpsi, ctx->work, 1.0 / ctx->nz, kLayZ << 2, 0, -1, ctx->work2);
             return e;
         });
     return traced(ctx, 0, ctx->nz > 1 ? 2 : 1, [&] {
@@ -259,19 +264,23 @@ cudaError_t step_exit(pfc_ctx* ctx, void* kpsi) {
     });
 }
 
-// B = FFT_xy(cubic term of IFFT_xy(A)) on the mixed grid.  Tiled: A (work2, z-tiled) ->
-// work (row-tiled), the x pass in place, then B into the psi^ buffer (free while A
-// carries the state): z-tiled, or on the last step in the standard layout, where the z
-// pass then writes psi^' in place.
+// B = FFT_xy(cubic term of IFFT_xy(A)) on the mixed grid.  Tiled: A (z-tiled) -> the
+// row-tiled field, the x pass in place, then B z-tiled (or, on the last step, in the
+// standard layout): with psi^ carried, A and B in work and the row-tiled field in the psi^
+// buffer; with A carried (in work2), the row-tiled field in work and B in the psi^ buffer,
+// where the last z pass then writes psi^' in place.
 cudaError_t step_xy(pfc_ctx* ctx, void* kpsi, const pfc_step_params* p, bool last) {
     const void* A = carried_A(ctx, kpsi);
     void* B = ctx->work;
     const double mul = 1.0 / ((double)ctx->nx * (double)ctx->ny);
-    if (ctx->tiled)
+    if (ctx->tiled) {
+        void* R = row_field(ctx, kpsi);
+        void* Bt = ctx->z_carry ? ctx->work : kpsi;
         return traced_xy3(
-            ctx, [&] { return launch_ypass(ctx, 1, A, B, 1.0, ctx->nz, kLayZ | kLayRow << 2); },
-            [&] { return launch_xpass(ctx, B, nullptr, mul, p->C, p->mu, ctx->nz, kLayRow); },
-            [&] { return launch_ypass(ctx, -1, B, kpsi, 1.0, ctx->nz, kLayRow | (last ? 0 : kLayZ << 2)); });
+            ctx, [&] { return launch_ypass(ctx, 1, A, R, 1.0, ctx->nz, kLayZ | kLayRow << 2); },
+            [&] { return launch_xpass(ctx, R, nullptr, mul, p->C, p->mu, ctx->nz, kLayRow); },
+            [&] { return launch_ypass(ctx, -1, R, Bt, 1.0, ctx->nz, kLayRow | (last ? 0 : kLayZ << 2)); });
+    }
     if (ctx->xy_mode == 2)
         return traced_xy3(
             ctx, [&] { return launch_ypass(ctx, 1, A, B, 1.0, ctx->nz); },
@@ -287,14 +296,16 @@ cudaError_t step_xy(pfc_ctx* ctx, void* kpsi, const pfc_step_params* p, bool las
     });
 }
 
-// the z pass with the semi-implicit update.  Tiled: B is in the psi^ buffer; A' stays
-// z-tiled in work2, and the last step writes psi^' over B (standard layout, in place).
+// the z pass with the semi-implicit update.  Tiled, psi^ carried: psi^ in work2 and B in
+// work -> psi^' (work2) and A' (work); the last step writes psi^' into the psi^ buffer
+// (standard layout).  Tiled, A carried: B is in the psi^ buffer; A' stays z-tiled in work2,
+// and the last step writes psi^' over B (standard layout, in place).
 cudaError_t step_z(pfc_ctx* ctx, void* kpsi, const ZPropArgs& za) {
     void* B = ctx->work;
     if (ctx->tiled && ctx->z_carry)
         return traced(ctx, 2, 1, [&] {
-            return launch_zcarry_tiled(ctx, ctx->work2, kpsi, za.final_step ? kpsi : ctx->work2,
-                                       za.final_step ? nullptr : kpsi, za);
+            return launch_zcarry_tiled(ctx, ctx->work2, ctx->work, za.final_step ? kpsi : ctx->work2,
+                                       za.final_step ? nullptr : ctx->work, za);
         });
     if (ctx->tiled) {
         void* A = ctx->work2;
@@ -869,8 +880,8 @@ pfc_status pfc_step_prop(pfc_ctx* ctx, void* kpsi, int nsteps, const pfc_step_pa
 
 // ---- the step with the field in host memory ---------------------------------------------------
 // The field comes in by ky chunks (nz rows of nky (nx/2+1) modes each, one strided copy per
-// chunk on the copy stream) into `work`, and the entry pass (psi^ -> z-tiled psi^, A) runs
-// on each chunk as soon as it has arrived; the final psi^ goes back in one copy.  Only the
+// chunk on the copy stream) into the psi^ buffer, and the entry pass (psi^ -> z-tiled psi^
+// and A) runs on each chunk as soon as it has arrived; the final psi^ goes back in one copy.  Only the
 // schedule that carries psi^ z-tiled has a chunked entry pass; others copy, step and copy
 // back in order.
 pfc_status pfc_step_host(pfc_ctx* ctx, const void* host_in, void* host_out, void* kpsi, int nsteps,
@@ -901,18 +912,19 @@ pfc_status pfc_step_host(pfc_ctx* ctx, const void* host_in, void* host_out, void
     PFC_CUDA(cudaEventRecord(ev_start, ctx->stream), "pfc_step_host event");
     PFC_CUDA(cudaStreamWaitEvent(cs, ev_start, 0), "pfc_step_host wait");
     for (int g = 0; g < G; ++g) {
-        PFC_CUDA(cudaMemcpy2DAsync((char*)ctx->work + g * width, pitch, (const char*)host_in + g * width, pitch, width,
+        PFC_CUDA(cudaMemcpy2DAsync((char*)kpsi + g * width, pitch, (const char*)host_in + g * width, pitch, width,
                                    ctx->nz, cudaMemcpyHostToDevice, cs),
                  "pfc_step_host copy in");
         PFC_CUDA(cudaEventRecord(ev_in[g], cs), "pfc_step_host event");
     }
     for (int g = 0; g < G; ++g) {
         PFC_CUDA(cudaStreamWaitEvent(ctx->stream, ev_in[g], 0), "pfc_step_host wait");
-        PFC_CUDA(traced(ctx, 0, g == 0 ? 3 : 2,
+        PFC_CUDA(traced(ctx, 0, g == 0 ? 2 : 1,
                         [&] {
-                            cudaError_t e = g == 0 ? launch_k0_save(ctx, ctx->work) : cudaSuccess;
-                            if (!e) e = launch_relayout(ctx, ctx->work, ctx->work2, 1, g * cky, cky);
-                            if (!e) e = launch_zfft(ctx, 1, ctx->work2, kpsi, 1.0 / ctx->nz, kLayZ | kLayZ << 2, g * cky, cky);
+                            cudaError_t e = g == 0 ? launch_k0_save(ctx, kpsi) : cudaSuccess;
+                            if (!e)
+                                e = launch_zfft(ctx, 1, kpsi, ctx->work, 1.0 / ctx->nz, kLayZ << 2, g * cky, cky,
+                                                ctx->work2);
                             return e;
                         }),
                  "pfc_step_host entry");
@@ -1301,7 +1313,11 @@ pfc_status pfc_ensemble_run(pfc_ensemble* e, int nsteps, void* stream) {
             pfc_ctx* c = e->ctx[i];
             c->stream = st;
             ce = step_entry(c, e->kpsi[i]);
-            if (!ce) ce = cudaMemcpyAsync((char*)k.state + q * S, e->kpsi[i], S, cudaMemcpyDeviceToDevice, st);
+            // A: in the psi^ buffer, or in work for the tiled psi^-carrying schedule
+            const bool awork = c->tiled && c->z_carry;
+            if (!ce)
+                ce = cudaMemcpyAsync((char*)(awork ? k.cc->work : k.state) + q * S, awork ? c->work : e->kpsi[i], S,
+                                     cudaMemcpyDeviceToDevice, st);
             if (!ce) ce = cudaMemcpyAsync((char*)k.cc->work2 + q * S, c->work2, S, cudaMemcpyDeviceToDevice, st);
             if (!ce) ce = cudaMemcpyAsync(k.cc->k0 + q, c->k0, sizeof(double2), cudaMemcpyDeviceToDevice, st);
             if (!ce) ce = launch_counter(st, k.ctr + q, e->p[i].counter, 1);
@@ -1315,7 +1331,9 @@ pfc_status pfc_ensemble_run(pfc_ensemble* e, int nsteps, void* stream) {
         for (int q = 0; q < (int)k.members.size() && !ce; ++q) {
             const int i = k.members[q];
             pfc_ctx* c = e->ctx[i];
-            ce = cudaMemcpyAsync(e->kpsi[i], (char*)k.state + q * S, S, cudaMemcpyDeviceToDevice, st);
+            const bool awork = c->tiled && c->z_carry;  // (psi^ is in work2 then: A is not needed)
+            ce = awork ? cudaSuccess
+                       : cudaMemcpyAsync(e->kpsi[i], (char*)k.state + q * S, S, cudaMemcpyDeviceToDevice, st);
             if (!ce) ce = cudaMemcpyAsync(c->work2, (char*)k.cc->work2 + q * S, S, cudaMemcpyDeviceToDevice, st);
             if (!ce) ce = step_exit(c, e->kpsi[i]);
         }

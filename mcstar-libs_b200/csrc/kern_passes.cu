@@ -32,11 +32,12 @@ struct YCfg {
 template <class Y, int DIR, bool kZ>
 __global__ void __launch_bounds__(Y::T, Y::MINB)
     k_ycol(const float2* in, float2* out, int nxh, int ny, int nz, int lay, const float2* __restrict__ twg,
-           float scale, int64_t ms, int q0) {
+           float scale, int64_t ms, int q0, float2* copy) {
     // the columns of NY elements of kx tile blockIdx.x at plane q0 + blockIdx.y: y columns of
     // that z-plane (kZ false) or z columns at that ky (kZ); lay & 3: the layout of the input,
     // lay >> 2: of the output (col_addr).  With the standard layout on both sides, in may
-    // equal out.  ms: elements between the fields of a batch (grid z).
+    // equal out.  ms: elements between the fields of a batch (grid z).  copy (or null): the
+    // input columns as read, written in the output's layout (a relayout fused with the FFT).
     constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P, U = Y::U;
     in += blockIdx.z * ms;
     out += blockIdx.z * ms;
@@ -53,6 +54,12 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
     float2 v[E];
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = valid ? in[ai.base + (int64_t)(t + P * j) * ai.stride] : make_float2(0.f, 0.f);
+    if (copy && valid) {
+        copy += blockIdx.z * ms;
+        const ColAddr ac = col_addr(lay >> 2, kZ, kx, q, nxh, ny, nz);
+#pragma unroll
+        for (int j = 0; j < E; ++j) copy[ac.base + (int64_t)(t + P * j) * ac.stride] = v[j];
+    }
     __syncthreads();
     fft_d1_to_d2<NY, E, TX, DIR, BarCta, Y::PADG>(v, t, c, xb, tw);
     if (valid) {
@@ -588,15 +595,15 @@ cudaError_t xattr() {
 // W_NY^m at tw_off
 template <class Y, bool kZ>
 cudaError_t collaunch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int planes, int lay,
-                      int tw_off, int q0 = 0) {
+                      int tw_off, int q0 = 0, void* copy = nullptr) {
     dim3 grid((c->nxh + Y::TX - 1) / Y::TX, planes, c->batch);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + tw_off;
     if (dir > 0)
         k_ycol<Y, 1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->ny, c->nz,
-                                                             lay, tw, (float)scale, c->mstride, q0);
+                                                             lay, tw, (float)scale, c->mstride, q0, (float2*)copy);
     else
         k_ycol<Y, -1, kZ><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->ny, c->nz,
-                                                              lay, tw, (float)scale, c->mstride, q0);
+                                                              lay, tw, (float)scale, c->mstride, q0, (float2*)copy);
     return cudaGetLastError();
 }
 template <class Y>
@@ -605,8 +612,8 @@ cudaError_t ylaunch(const pfc_ctx* c, int dir, const void* in, void* out, double
 }
 template <class Y>
 cudaError_t zlaunch_fft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay, int ky0,
-                        int nky) {
-    return collaunch<Y, true>(c, dir, in, out, scale, nky, lay, c->zfft_tw_off, ky0);
+                        int nky, void* copy) {
+    return collaunch<Y, true>(c, dir, in, out, scale, nky, lay, c->zfft_tw_off, ky0, copy);
 }
 template <class X, int MODE>
 cudaError_t xlaunch(const pfc_ctx* c, const void* in, void* out, const void* pot, double mul, double C, double mu,
@@ -739,14 +746,14 @@ int xkernel_variants(int nx, int dtype) {
 int default_xkernel(int variants) { return (variants & 4) ? 2 : 0; }
 
 cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay, int ky0,
-                        int nky) {
+                        int nky, void* copy) {
     if (nky < 0) nky = c->ny - ky0;
     if (ky0 < 0 || nky < 1 || ky0 + nky > c->ny) return cudaErrorInvalidValue;
     switch (c->fused_zfft) {
-        case 1: return zlaunch_fft<Y512>(c, dir, in, out, scale, lay, ky0, nky);
-        case 2: return zlaunch_fft<Y256>(c, dir, in, out, scale, lay, ky0, nky);
-        case 3: return zlaunch_fft<Y128>(c, dir, in, out, scale, lay, ky0, nky);
-        case 4: return zlaunch_fft<Y64>(c, dir, in, out, scale, lay, ky0, nky);
+        case 1: return zlaunch_fft<Y512>(c, dir, in, out, scale, lay, ky0, nky, copy);
+        case 2: return zlaunch_fft<Y256>(c, dir, in, out, scale, lay, ky0, nky, copy);
+        case 3: return zlaunch_fft<Y128>(c, dir, in, out, scale, lay, ky0, nky, copy);
+        case 4: return zlaunch_fft<Y64>(c, dir, in, out, scale, lay, ky0, nky, copy);
     }
     return cudaErrorNotSupported;
 }

@@ -164,9 +164,10 @@ cudaError_t launch_xrows_c2r(const pfc_ctx* c, const void* in_cmpl, void* out_re
 int fused_zfft_variant(int nz, int dtype);
 cudaError_t set_zfft_attributes(const pfc_ctx* c);
 // (lay as launch_ypass)
-// (ky0, nky: the z columns of ky in [ky0, ky0 + nky) only; nky < 0: to ny)
+// (ky0, nky: the z columns of ky in [ky0, ky0 + nky) only; nky < 0: to ny; copy, or null:
+// the input columns as read, written in the output's layout -- a relayout fused with the FFT)
 cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int lay = 0, int ky0 = 0,
-                        int nky = -1);
+                        int nky = -1, void* copy = nullptr);
 
 // ---- spectral low-pass post-processing (kern_lowpass.cu) ----
 cudaError_t launch_gaussian_init(const pfc_ctx* c, void* g, double lx, double ly, double lz, double hx, double hy,
