@@ -77,6 +77,10 @@ pfc_status  pfc_destroy(pfc_ctx* ctx);
  *                and 2 only, 2 the odd radices first
  *   tile_shift   the general passes' lines per CTA halved this many times (0..4), for the
  *                x rows, the y columns, the z columns and the stepper's z pass
+ *   y_kernel     the register y pass between the kx-tiled layouts (ny = 512): 0 per-thread
+ *                loads and stores, 1 the TMA unit moving whole tiles (bulk copies of the
+ *                row-tiled blocks, tensor-map tile copies of the z-tiled pieces); -1 the
+ *                library's choice
  * A choice the shape has no kernel for is PFC_ERR_UNSUPPORTED at creation.
  * pfc_tune times the step (pfc_step, FP32 or FP64 per desc) under candidate options on
  * the current device -- a coordinate search, one option at a time from the library's
@@ -90,6 +94,7 @@ typedef struct pfc_options {
     int tiled;
     int radix_order;
     int tile_shift[4];
+    int y_kernel;
 } pfc_options;
 pfc_status  pfc_default_options(pfc_options* opts);
 pfc_status  pfc_create_with(const pfc_desc* desc, const pfc_options* opts, pfc_ctx** out);

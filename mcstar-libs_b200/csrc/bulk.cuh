@@ -1,5 +1,6 @@
-// One-dimensional bulk asynchronous copies between global and shared memory (the TMA
-// unit's untiled form, cp.async.bulk), for kernels whose tiles are contiguous blocks.
+// Bulk asynchronous copies between global and shared memory (the TMA unit): the untiled
+// one-dimensional form (cp.async.bulk) for kernels whose tiles are contiguous blocks, and
+// the tiled tensor form for boxes of strided blocks.
 //
 //  loads   one elected thread arms an mbarrier with the byte count and issues the copy;
 //          every consumer waits on the barrier's phase (bounded: a wait that runs out
@@ -65,6 +66,26 @@ __device__ __forceinline__ void bulk_store(void* gdst, const void* smem_src, uns
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 // the issuing thread waits until every committed store has read its shared memory
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
+// Tiled tensor copies (cp.async.bulk.tensor) of one box of a five-dimensional tensor map
+// passed as a __grid_constant__ kernel parameter; c0 is the innermost coordinate (kept a
+// multiple of 16 bytes by the callers: always 0 here).  No multicast form.
+__device__ __forceinline__ void tma_load5(void* smem_dst, const void* tmap, int c0, int c1, int c2, int c3, int c4,
+                                          uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5, %6}], [%7];" ::"r"(smem_u32(smem_dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_store5(const void* tmap, const void* smem_src, int c0, int c1, int c2, int c3,
+                                           int c4) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];" ::"l"(
+            reinterpret_cast<uint64_t>(tmap)),
+        "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(smem_src))
+        : "memory");
+}
 
 // Polls of mbar_wait before a device wait counts as lost (each poll may suspend for up
 // to about a microsecond: seconds in total, far beyond any copy's latency).

@@ -369,7 +369,8 @@ bool same_class(const pfc_ctx* a, const pfc_step_params& pa, const pfc_ctx* b, c
     const pfc_options &oa = a->opt, &ob = b->opt;
     return a->nx == b->nx && a->ny == b->ny && a->nz == b->nz && a->dtype == b->dtype && oa.z_carry == ob.z_carry &&
            oa.x_kernel == ob.x_kernel && oa.tiled == ob.tiled && oa.radix_order == ob.radix_order &&
-           std::memcmp(oa.tile_shift, ob.tile_shift, sizeof(oa.tile_shift)) == 0 && pa.dt == pb.dt && pa.C == pb.C &&
+           std::memcmp(oa.tile_shift, ob.tile_shift, sizeof(oa.tile_shift)) == 0 && oa.y_kernel == ob.y_kernel &&
+           pa.dt == pb.dt && pa.C == pb.C &&
            pa.mu == pb.mu && pa.lx == pb.lx && pa.ly == pb.ly && pa.lz == pb.lz && (pa.namp != 0.0) == (pb.namp != 0.0);
 }
 
@@ -421,6 +422,7 @@ pfc_status pfc_default_options(pfc_options* o) {
     o->tiled = -1;
     o->radix_order = 0;
     for (int i = 0; i < 4; ++i) o->tile_shift[i] = 0;
+    o->y_kernel = -1;
     return PFC_OK;
 }
 
@@ -439,7 +441,7 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
     pfc_default_options(&o);
     if (opts) o = *opts;
     if (o.z_carry < -1 || o.z_carry > 1 || o.x_kernel < -1 || o.x_kernel > 2 || o.tiled < -1 || o.tiled > 1 ||
-        o.radix_order < 0 || o.radix_order > 2)
+        o.radix_order < 0 || o.radix_order > 2 || o.y_kernel < -1 || o.y_kernel > 1)
         return PFC_ERR_INVALID;
     for (int i = 0; i < 4; ++i)
         if (o.tile_shift[i] < 0 || o.tile_shift[i] > 4) return PFC_ERR_INVALID;
@@ -543,6 +545,16 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
     }
     c->z_carry = carry && (!c->tiled || c->fused_z == 6);
     if (!c->tiled && c->z_carry && c->fused_z == 6) c->fused_z = 1;
+    // the y pass between the tiled layouts: per-thread accesses (0) or the TMA unit (1),
+    // for the y lengths that have the latter (used when the layout is tiled)
+    {
+        const bool tma = ybulk_available(c);
+        if (o.y_kernel == 1 && !tma) {
+            free_ctx(c);
+            return PFC_ERR_UNSUPPORTED;
+        }
+        c->ykern = o.y_kernel >= 0 ? o.y_kernel : (tma ? 1 : 0);
+    }
     {
         int dev = 0;
         c->num_sms = 148;
@@ -627,6 +639,7 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
     c->opt = o;
     c->opt.z_carry = c->z_carry ? 1 : 0;
     c->opt.x_kernel = c->xkern;
+    c->opt.y_kernel = c->ykern;
     c->opt.tiled = c->tiled ? 1 : 0;
     *out = c;
     return PFC_OK;

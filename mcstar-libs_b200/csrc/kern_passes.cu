@@ -10,6 +10,9 @@
 // A y pass, the x pass and a y pass replace the general y/x/y passes of the step;
 // they stream whole tiles (contiguous rows for x, 64-byte column segments for y)
 // and keep every FFT in registers with one shared-memory transpose per transform.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include "bulk.cuh"
 #include "pfc_ctx.h"
 #include "regfft.cuh"
 
@@ -120,6 +123,106 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
             const int k = p + E * d3_k2<E>(r, h);
             out[ao.base + (int64_t)k * ao.stride] = make_float2(v[r].x * scale, v[r].y * scale);
         }
+    }
+}
+
+// The y pass between the two kx-tiled layouts with the TMA unit moving every whole tile:
+// per CTA (kx tile kt, z-plane blockIdx.y) the 512 y values of the tile's TX columns are
+// one contiguous 32 KB block in the row-tiled layout ([z][y][c]) and 512 pieces of 64
+// bytes, nz TX elements apart, in the z-tiled layout ([ky][z][c]).  The row-tiled side
+// moves by one 1-D bulk copy; the z-tiled side by tiled tensor copies of boxes of
+// 16 x 1 x 256 floats over the map (floats of a tile row, z, ky, whole tile, field).  One
+// elected thread arms the mbarrier and issues the loads; the stage then serves as the
+// transform's exchange buffer and as the output stage, which one thread stores after a
+// proxy fence.  The last, partial tile (nxh % TX columns) moves by per-thread accesses in
+// the same launch.  LIN / LOUT: the layouts of in / out (1 z-tiled, 2 row-tiled).
+template <class Y>
+struct YBulkCfg {
+    static constexpr int NY = Y::NY, TX = Y::TX;
+    static constexpr int BOX = 256;                     // ky per tensor box (the box limit)
+    static constexpr size_t SMEM = Y::SMEM + 16;        // exchange/stage, twiddles, mbarrier
+    static_assert(Y::XB >= NY * TX && NY % BOX == 0 && TX == kTileW, "stage");
+};
+
+template <class Y, int DIR, int LIN, int LOUT>
+__global__ void __launch_bounds__(Y::T, Y::MINB)
+    k_ybulk(const float2* in, float2* out, int nxh, int nz, const __grid_constant__ CUtensorMap tmap,
+            const float2* __restrict__ twg, float scale, int64_t ms, int* flag) {
+    static_assert((LIN == 1 && LOUT == 2) || (LIN == 2 && LOUT == 1), "between the tiled layouts");
+    using C = YBulkCfg<Y>;
+    constexpr int NY = Y::NY, E = Y::E, TX = Y::TX, P = Y::P;
+    constexpr unsigned kBlockBytes = NY * TX * sizeof(float2);
+    in += blockIdx.z * ms;  // fields of a batch (grid z)
+    out += blockIdx.z * ms;
+    extern __shared__ __align__(128) float2 sm[];
+    float2* xb = sm;
+    float2* tw = sm + Y::XB;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tw + Y::TW);
+    const int tid = threadIdx.x;
+    const int c = tid % TX, t = tid / TX;
+    const int kt = blockIdx.x, z = blockIdx.y;
+    const bool whole = (kt + 1) * TX <= nxh;
+    // the row-tiled block of (kt, z) (whole tiles)
+    const int64_t rblk = ((int64_t)kt * nz + z) * (NY * TX);
+    if (whole && tid == 0) {
+        mbar_init(bar, 1);
+        mbar_init_fence();
+        mbar_arrive_expect_tx(bar, kBlockBytes);
+        if (LIN == 2) bulk_load(xb, in + rblk, kBlockBytes, bar);
+        else
+#pragma unroll
+            for (int h = 0; h < NY / C::BOX; ++h)
+                tma_load5(xb + h * C::BOX * TX, &tmap, 0, z, h * C::BOX, kt, blockIdx.z, bar);
+    }
+    for (int i = tid; i < NY; i += Y::T) {
+        const float2 w = twg[i];
+        tw[i] = w;
+        if (Y::BAL) tw[NY + i] = make_float2(-w.x, -w.y);
+    }
+    float2 v[E];
+    const int kx = kt * TX + c;
+    const bool valid = kx < nxh;
+    if (!whole) {
+        const ColAddr ai = col_addr(LIN, false, kx, z, nxh, NY, nz);
+#pragma unroll
+        for (int j = 0; j < E; ++j)
+            v[j] = valid ? in[ai.base + (int64_t)(t + P * j) * ai.stride] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();  // the twiddles, and the barrier's initialisation
+    if (whole) {
+        if (!mbar_wait(bar, 0, kWaitPolls)) {
+            if (tid == 0) atomicOr(flag, kFlagWaitTimeout);
+            return;
+        }
+#pragma unroll
+        for (int j = 0; j < E; ++j) v[j] = xb[(t + P * j) * TX + c];
+    }
+    // (fft_d1_to_d3 synchronises before its first write to xb)
+    fft_d1_to_d3<NY, E, TX, DIR, BarCta, Y::BAL>(v, t, c, xb, tw);
+    const int p = t >> 1, h = t & 1;
+    if (!whole) {
+        if (valid) {
+            const ColAddr ao = col_addr(LOUT, false, kx, z, nxh, NY, nz);
+#pragma unroll
+            for (int r = 0; r < E; ++r)
+                out[ao.base + (int64_t)(p + E * d3_k2<E>(r, h)) * ao.stride] =
+                    make_float2(v[r].x * scale, v[r].y * scale);
+        }
+        return;
+    }
+    __syncthreads();  // every thread's last exchange reads are done
+#pragma unroll
+    for (int r = 0; r < E; ++r) xb[(p + E * d3_k2<E>(r, h)) * TX + c] = make_float2(v[r].x * scale, v[r].y * scale);
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+        if (LOUT == 2) bulk_store(out + rblk, xb, kBlockBytes);
+        else
+#pragma unroll
+            for (int h2 = 0; h2 < NY / C::BOX; ++h2)
+                tma_store5(&tmap, xb + h2 * C::BOX * TX, 0, z, h2 * C::BOX, kt, blockIdx.z);
+        bulk_commit();
+        bulk_wait_read();  // shared memory stays valid until the stores have read it
     }
 }
 
@@ -551,13 +654,67 @@ using Y512q = YCfg3<512, 16, 8, 4, false>;  // the y pass: 16 values per thread,
 template <class Y>
 cudaError_t y3attr() {
     cudaError_t e = cudaFuncSetAttribute(k_ycol3<Y, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Y::SMEM);
-    if (e) return e;
-    return cudaFuncSetAttribute(k_ycol3<Y, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Y::SMEM);
+    if (!e) e = cudaFuncSetAttribute(k_ycol3<Y, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Y::SMEM);
+    constexpr int kB = (int)YBulkCfg<Y>::SMEM;
+    if (!e) e = cudaFuncSetAttribute(k_ybulk<Y, 1, 1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kB);
+    if (!e) e = cudaFuncSetAttribute(k_ybulk<Y, -1, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kB);
+    return e;
 }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against the
+// driver library); null when the driver does not offer it.
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// The tensor map of the whole kx tiles of a z-tiled field (or batch of fields) at base:
+// dimensions (the 2 kTileW floats of a tile row, z, ky, tile, field), boxes of
+// 2 kTileW x 1 x box_ky x 1 x 1.  false when the shape has no such map (strides not
+// multiples of 16 bytes, or no whole tile).
+bool ztiled_map(const pfc_ctx* c, const void* base, int box_ky, CUtensorMap* m) {
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+    const int full = c->nxh / kTileW;
+    if (!enc || full < 1 || c->ny % box_ky) return false;
+    const cuuint64_t row = kTileW * sizeof(float2);
+    const cuuint64_t tile = row * (cuuint64_t)c->nz * (cuuint64_t)c->ny;
+    const cuuint64_t field = c->batch > 1 ? (cuuint64_t)c->mstride * sizeof(float2) : tile * full;
+    if (field % 16) return false;
+    const cuuint64_t dims[5] = {2 * kTileW, (cuuint64_t)c->nz, (cuuint64_t)c->ny, (cuuint64_t)full,
+                                (cuuint64_t)c->batch};
+    const cuuint64_t strides[4] = {row, row * (cuuint64_t)c->nz, tile, field};
+    const cuuint32_t box[5] = {2 * kTileW, 1, (cuuint32_t)box_ky, 1, 1};
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, const_cast<void*>(base), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <class Y>
 cudaError_t y3launch(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs, int lay) {
     dim3 grid((c->nxh + Y::TX - 1) / Y::TX, nzs, c->batch);
     const float2* tw = reinterpret_cast<const float2*>(c->tw) + c->ypass_tw_off;
+    // between the tiled layouts: the TMA kernel, the z-tiled side through a tensor map
+    const bool inv_tiled = dir > 0 && lay == (1 | 2 << 2), fwd_tiled = dir < 0 && lay == (2 | 1 << 2);
+    CUtensorMap m;
+    if (c->ykern == 1 && (inv_tiled || fwd_tiled) &&
+        ztiled_map(c, inv_tiled ? in : out, YBulkCfg<Y>::BOX, &m)) {
+        constexpr size_t kB = YBulkCfg<Y>::SMEM;
+        if (inv_tiled)
+            k_ybulk<Y, 1, 1, 2><<<grid, Y::T, kB, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->nz, m, tw,
+                                                              (float)scale, c->mstride, c->flag);
+        else
+            k_ybulk<Y, -1, 2, 1><<<grid, Y::T, kB, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->nz, m,
+                                                               tw, (float)scale, c->mstride, c->flag);
+        return cudaGetLastError();
+    }
     if (dir > 0)
         k_ycol3<Y, 1><<<grid, Y::T, Y::SMEM, c->stream>>>((const float2*)in, (float2*)out, c->nxh, c->nz, lay, tw,
                                                           (float)scale, c->mstride);
@@ -672,6 +829,8 @@ cudaError_t set_pass_attributes(const pfc_ctx* c) {
     if (!e && c->xkern == 2) e = xlattr<XL512>();
     return e;
 }
+
+bool ybulk_available(const pfc_ctx* c) { return c->fused_y == 7 && tmap_encoder() != nullptr; }
 
 cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, double scale, int nzs, int lay) {
     if (lay && nzs != c->nz) return cudaErrorNotSupported;  // tiled: whole fields

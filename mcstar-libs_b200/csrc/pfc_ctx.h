@@ -73,6 +73,7 @@ struct pfc_ctx {
     int ypass_tw_off;             // W_ny^m
     int xpass_tw_off;             // W_{nx/2}^m, then W_nx^k (k <= nx/2)
     int xkern;                    // the row-tiled x pass: 0 k_xrow, 1 k_xpair (row pairs), 2 k_xlane
+    int ykern;                    // the y pass between the tiled layouts: 0 k_ycol3, 1 k_ybulk (TMA)
     int xpair_tw_off;             // W_nx^m, m < nx
     int xy_mode;                  // 0 general passes, 2 register y/x/y passes
     // tracing (pfc_profile_enable / pfc_profile_read)
@@ -147,6 +148,9 @@ int fused_y_variant(int ny, int dtype);
 int fused_x_variant(int nx, int dtype);
 // the row-tiled x kernels this nx has (bit i: x kernel i; bit 0 always) and the default among them
 int xkernel_variants(int nx, int dtype);
+// whether the y pass has its TMA kernel for this context's y length (and the driver offers
+// tensor maps)
+bool ybulk_available(const pfc_ctx* c);
 int default_xkernel(int variants);
 cudaError_t set_pass_attributes(const pfc_ctx* c);
 // y FFT of nzs consecutive planes starting at in / out (in may equal out); lay & 3 / lay

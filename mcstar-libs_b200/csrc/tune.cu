@@ -48,7 +48,8 @@ std::string options_json(const pfc_options& o, double ms) {
     std::ostringstream s;
     s << "{\"z_carry\": " << o.z_carry << ", \"x_kernel\": " << o.x_kernel << ", \"tiled\": " << o.tiled
       << ", \"radix_order\": " << o.radix_order << ", \"tile_shift\": [" << o.tile_shift[0] << ", " << o.tile_shift[1]
-      << ", " << o.tile_shift[2] << ", " << o.tile_shift[3] << "], \"ms_per_step\": " << ms << "}";
+      << ", " << o.tile_shift[2] << ", " << o.tile_shift[3] << "], \"y_kernel\": " << o.y_kernel
+      << ", \"ms_per_step\": " << ms << "}";
     return s.str();
 }
 
@@ -104,6 +105,7 @@ bool parse_entry(const std::string& obj, pfc_options* o, double* ms) {
         std::sscanf(obj.c_str() + p + 13, " [%d, %d, %d, %d]", &o->tile_shift[0], &o->tile_shift[1], &o->tile_shift[2],
                     &o->tile_shift[3]) != 4)
         return false;
+    field_int(obj, "y_kernel", &o->y_kernel);  // (absent from older entries: the library's choice)
     const size_t m = obj.find("\"ms_per_step\":");
     double t = 0.0;
     if (m != std::string::npos) std::sscanf(obj.c_str() + m + 14, " %lf", &t);
@@ -181,7 +183,7 @@ extern "C" pfc_status pfc_tune(const pfc_desc* d, const char* cache_path, pfc_op
     // which options touch a kernel of this shape: ask a context with the library's choice
     pfc_options cur;
     pfc_default_options(&cur);
-    bool general = false, zreg = false, tiled_ok = false;
+    bool general = false, zreg = false, tiled_ok = false, ytma = false;
     int xks = 1;
     {
         pfc_ctx* c = nullptr;
@@ -191,6 +193,7 @@ extern "C" pfc_status pfc_tune(const pfc_desc* d, const char* cache_path, pfc_op
         zreg = c->fused_z != 0;
         xks = c->fused_x ? pfc::xkernel_variants(c->nx, c->dtype) : 1;
         tiled_ok = c->fused_z && c->fused_zfft && c->xy_mode == 2 && c->fused_y;
+        ytma = tiled_ok && c->fused_y && pfc::ybulk_available(c);
         pfc_get_options(c, &cur);  // the library's choices, explicit
         pfc_destroy(c);
     }
@@ -211,6 +214,7 @@ extern "C" pfc_status pfc_tune(const pfc_desc* d, const char* cache_path, pfc_op
         knobs.push_back(k);
     }
     if (tiled_ok) knobs.push_back({"tiled", &cur.tiled, {0, 1}});
+    if (ytma) knobs.push_back({"y_kernel", &cur.y_kernel, {0, 1}});
     if (general) {
         knobs.push_back({"radix_order", &cur.radix_order, {0, 1, 2}});
         for (int i = 0; i < 4; ++i) knobs.push_back({"tile_shift", &cur.tile_shift[i], {0, 1, 2}});

@@ -58,17 +58,17 @@ class PfcStepParams(ctypes.Structure):
 
 class PfcOptions(ctypes.Structure):
     _fields_ = [("z_carry", ctypes.c_int), ("x_kernel", ctypes.c_int), ("tiled", ctypes.c_int),
-                ("radix_order", ctypes.c_int), ("tile_shift", ctypes.c_int * 4)]
+                ("radix_order", ctypes.c_int), ("tile_shift", ctypes.c_int * 4), ("y_kernel", ctypes.c_int)]
 
     def to_dict(self):
         return {"z_carry": self.z_carry, "x_kernel": self.x_kernel, "tiled": self.tiled,
-                "radix_order": self.radix_order, "tile_shift": list(self.tile_shift)}
+                "radix_order": self.radix_order, "tile_shift": list(self.tile_shift), "y_kernel": self.y_kernel}
 
     @classmethod
     def from_dict(cls, d):
         o = cls()
         lib().pfc_default_options(ctypes.byref(o))
-        for k in ("z_carry", "x_kernel", "tiled", "radix_order"):
+        for k in ("z_carry", "x_kernel", "tiled", "radix_order", "y_kernel"):
             if k in d:
                 setattr(o, k, int(d[k]))
         if "tile_shift" in d:

@@ -34,7 +34,7 @@ class Context:
 
     def __init__(self, shape, dtype=np.float32, options=None):
         """options: None (the library's choices) or a dict of pfc_options fields (the
-        kernel schedules: z_carry, x_kernel, tiled, radix_order, tile_shift), e.g. the
+        kernel schedules: z_carry, x_kernel, tiled, radix_order, tile_shift, y_kernel), e.g. the
         result of ``tune``."""
         nx, ny, nz = (int(v) for v in shape)
         self.shape = (nx, ny, nz)

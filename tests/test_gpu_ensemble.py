@@ -21,7 +21,8 @@ def _members():
             mk((64, 64, 1), 0.4, -0.2, 17, 0.05), mk((32, 32, 32), 0.2, -0.25, 18, 0.02),
             mk((48, 40, 30), 0.35, -0.2, 19, 0.0), mk((64, 64, 64), 0.2, -0.3, 20, 0.0),
             mk((64, 64, 64), 0.25, -0.22, 21, 0.02), mk((32, 16, 512), 0.3, -0.2, 22, 0.01),
-            mk((32, 16, 512), 0.25, -0.25, 23, 0.02)]
+            mk((32, 16, 512), 0.25, -0.25, 23, 0.02), mk((64, 512, 64), 0.3, -0.2, 24, 0.0),
+            mk((64, 512, 64), 0.25, -0.22, 25, 0.02)]
 
 
 @pytest.mark.parametrize("spg", [1, 3])

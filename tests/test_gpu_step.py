@@ -56,9 +56,10 @@ def test_step_matches_oracle(shape, dtype, namp):
 
 VARIANT_SHAPES = [((64, 64, 64), 0.02), ((128, 128, 16), 0.0), ((32, 16, 128), 0.05), ((256, 256, 8), 0.0),
                   ((512, 512, 4), 0.0), ((16, 16, 512), 0.03), ((16, 8, 512), 0.0), ((64, 64, 512), 0.02),
-                  ((128, 64, 512), 0.0), ((512, 64, 64), 0.02), ((512, 128, 64), 0.0), ((48, 40, 30), 0.02), ((96, 80, 1), 0.0)]
+                  ((128, 64, 512), 0.0), ((512, 64, 64), 0.02), ((512, 128, 64), 0.0), ((128, 512, 64), 0.02),
+                  ((48, 40, 30), 0.02), ((96, 80, 1), 0.0)]
 OPTIONS = [dict(z_carry=1), dict(z_carry=0), dict(tiled=0), dict(x_kernel=0), dict(x_kernel=1), dict(x_kernel=2),
-           dict(x_kernel=2, z_carry=0), dict(z_carry=1, tiled=0),
+           dict(x_kernel=2, z_carry=0), dict(z_carry=1, tiled=0), dict(y_kernel=0),
            dict(radix_order=1), dict(radix_order=2), dict(tile_shift=[1, 2, 1, 2]), dict(tile_shift=[3, 3, 4, 3])]
 
 
@@ -86,6 +87,26 @@ def test_step_kernel_schedules_match_oracle(options):
         assert rel_l2(st.kspace(), want) < 2e-6, (shape, options, st.ctx.options)
         st.ctx.close()
     assert tried >= 3
+
+
+@pytest.mark.parametrize("y_kernel", [0, 1])
+@pytest.mark.parametrize("shape,namp", [((128, 512, 64), 0.02), ((64, 512, 512), 0.0), ((64, 512, 512), 0.03),
+                                        ((512, 512, 4), 0.0)])
+def test_y_pass_kernels_match_oracle(shape, namp, y_kernel):
+    """The two y-pass kernels between the kx-tiled layouts (ny = 512): per-thread accesses
+    and the TMA form (a bulk copy of the row-tiled block, tensor-map tiles of the z-tiled
+    pieces, the partial last kx tile by per-thread accesses), under the A-carrying
+    (nz = 64) and the psi^-carrying (nz = 512) schedules; a shape that is not tiled takes
+    the option and runs its own passes."""
+    from mcstar_b200 import Stepper
+    st = Stepper(shape, math.pi / 4, 0.5, 0.3, dtype=F32, namp=namp, seed=9, options=dict(y_kernel=y_kernel))
+    assert st.ctx.options["y_kernel"] == y_kernel
+    nx, ny, nz = shape
+    k = O.r2c(-0.2 + 0.1 * np.random.default_rng(8).uniform(-1, 1, (nz, ny, nx)))
+    st.set_kspace(k.astype(np.complex64))
+    st.step(3)
+    want = O.step(k, 3, 0.5, 0.3, st.lens, shape, namp=namp, seed=9, noise_dtype=F32)
+    assert rel_l2(st.kspace(), want) < 2e-6
 
 
 @pytest.mark.parametrize("shape,dtype,z_mode", [((64, 64, 64), F32, 3), ((64, 64, 512), F32, 4),
