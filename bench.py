@@ -129,7 +129,7 @@ def ncu_traffic(kernel, size):
 X_KERNELS = {0: "k_xrow", 1: "k_xpair", 2: "k_xlane"}
 
 
-def kernel_table(prof, S, steps, x_kernel=0):
+def kernel_table(prof, S, steps, x_kernel=0, y_kernel=0):
     """Per-kernel device time of the timed region (the library's CUDA-event brackets on
     its stream) with the algorithmic HBM bytes of one launch, S = bytes of one
     half-spectrum field: every pass reads each input field once and writes each output
@@ -143,8 +143,10 @@ def kernel_table(prof, S, steps, x_kernel=0):
                        "bytes_per_launch": bytes_per_launch}
 
     if prof["xy_mode"] == 2 and prof["calls"][3]:
-        # y-inverse A -> B, y-forward B -> B
-        add("k_ycol3" if prof.get("y_variant") in (6, 7, 8) else "k_ycol", 3, 2.0 * S)
+        # y-inverse and y-forward between the tiled layouts (the TMA kernel k_ybulk, or
+        # k_ycol3); the last step's y-forward into the standard layout is k_ycol3
+        y3 = prof.get("y_variant") in (6, 7, 8)
+        add(("k_ybulk" if y_kernel == 1 else "k_ycol3") if y3 else "k_ycol", 3, 2.0 * S)
         add(X_KERNELS.get(x_kernel, "k_xrow"), 4, 2.0 * S)  # C2R, cubic term, R2C of every row, in place
     elif prof["xy_mode"] == 2:
         add("k_ycol+k_xrow+k_ycol (z slabs)", 1, 6.0 * S)
@@ -475,7 +477,7 @@ def run_b200(args, ws, rank, local):
     cells = n ** 3
     # ---- roofline of the dominant kernel family -------------------------------------------------
     peak, peak_kind = measured_peak()
-    kern = kernel_table(prof, S, args.steps, ctx.options.get("x_kernel", 0))
+    kern = kernel_table(prof, S, args.steps, ctx.options.get("x_kernel", 0), ctx.options.get("y_kernel", 0))
     dom = max(kern, key=lambda k: kern[k]["ms_total"])
     d = kern[dom]
     achieved = d["bytes_per_launch"] / (d["ms_per_launch"] / 1e3) / 1e9
