@@ -26,7 +26,7 @@ def _smooth_field(shape, seed, dtype):
     ky = np.fft.fftfreq(ny)[None, :, None]
     kx = np.fft.rfftfreq(nx)[None, None, :]
     k *= np.exp(-(kx ** 2 + ky ** 2 + kz ** 2) * 60.0)
-    return np.fft.irfftn(k, s=(nz, ny, nx)).astype(dtype)
+    return np.fft.irfftn(k, s=(nz, ny, nx), axes=(0, 1, 2)).astype(dtype)
 
 
 def _static_call(field_dev, shape, dtype, ths, capacity):
