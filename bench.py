@@ -154,9 +154,10 @@ def kernel_table(prof, S, steps, x_kernel=0, y_kernel=0):
         add("k_plane_xy", 1, 2.0 * S)
     else:
         add("k_cols+k_rows_nonlin+k_cols", 1, 6.0 * S)
-    if prof["z_mode"] in (2, 4):
+    if prof["z_mode"] in (2, 4, 5):
         # psi^ and B read, psi^' and A' written; the last step of a run writes psi^' only
-        add("k_zbulk" if prof["z_mode"] == 4 else "k_zcarry", 2, (4.0 * (steps - 1) + 3.0) / steps * S)
+        name = {4: "k_zbulk", 2: "k_zcarry", 5: "k_zprop (psi^ carried)"}[prof["z_mode"]]
+        add(name, 2, (4.0 * (steps - 1) + 3.0) / steps * S)
     else:
         name = "k_zprop" if prof["z_mode"] == 0 else ("k_zcol3" if prof.get("z_variant") == 6 else "k_zcol")
         add(name, 2, 3.0 * S)

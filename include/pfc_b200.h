@@ -402,12 +402,14 @@ typedef struct pfc_profile {
                                                     fused plane kernel in use        */
     int xy_mode;                                 /* 0 general passes, 1 cluster plane
                                                     kernel, 2 register y/x/y passes  */
-    int z_mode;                                  /* 0 general z pass, 1 register z pass
-                                                    carrying A = IFFT_z(psi^)/nz, 2
-                                                    register z pass carrying psi^, 3
-                                                    register z pass carrying A in the
-                                                    kx-tiled layout, 4 carrying psi^
-                                                    in the kx-tiled layout           */
+    int z_mode;                                  /* 0 general z pass carrying A =
+                                                    IFFT_z(psi^)/nz, 1 register z pass
+                                                    carrying A, 2 register z pass
+                                                    carrying psi^, 3 register z pass
+                                                    carrying A in the kx-tiled layout,
+                                                    4 carrying psi^ in the kx-tiled
+                                                    layout, 5 general z pass carrying
+                                                    psi^                             */
     int z_variant;                               /* register z kernel (0: none): 1-4
                                                     square split for nz 512, 256, 128,
                                                     64; 5: 16-column tiles; 6: 16

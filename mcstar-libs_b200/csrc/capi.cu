@@ -312,6 +312,8 @@ cudaError_t step_z(pfc_ctx* ctx, void* kpsi, const ZPropArgs& za) {
         if (za.final_step) return traced(ctx, 2, 1, [&] { return launch_zcol(ctx, A, kpsi, kpsi, za, 1); });
         return traced(ctx, 2, 1, [&] { return launch_zcol(ctx, A, kpsi, A, za, 7); });
     }
+    if (ctx->z_carry && !ctx->fused_z)
+        return traced(ctx, 2, 1, [&] { return launch_zprop_carry(ctx, kpsi, B, ctx->work2, za); });
     if (ctx->z_carry) return traced(ctx, 2, 1, [&] { return launch_zcarry(ctx, kpsi, ctx->work2, B, za); });
     if (ctx->fused_z) return traced(ctx, 2, 1, [&] { return launch_zcol(ctx, kpsi, B, kpsi, za); });
     return traced(ctx, 2, 1, [&] { return launch_zprop(ctx, kpsi, B, za); });
@@ -513,9 +515,9 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
     // xy part of a step: the register y/x/y passes where the y and x lengths have them,
     // else the general passes
     c->xy_mode = c->fused_y ? 2 : 0;
-    // the register z pass carries A = IFFT_z(psi^)/nz (three z transforms, three field
-    // sweeps) or psi^ itself (two transforms, four sweeps)
-    if (o.z_carry == 1 && !c->fused_z) {
+    // the z pass carries A = IFFT_z(psi^)/nz (three z transforms, three field sweeps) or
+    // psi^ itself (two transforms, four sweeps); a field with nz = 1 has no z transforms
+    if (o.z_carry == 1 && !c->fused_z && c->nz == 1) {
         free_ctx(c);
         return PFC_ERR_UNSUPPORTED;
     }
@@ -532,7 +534,11 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
     // (two z transforms; 0.344 against 0.447 ms at 512^3) and no FP32 round trip of the state
     // through IFFT_z / FFT_z each step (its FP32 error against FP64 is the reference cuFFT
     // path's or lower at 1, 10, 100, 1000 steps); elsewhere A.
-    const bool carry = c->fused_z && (o.z_carry == 1 || (o.z_carry == -1 && c->tiled && c->fused_z == 6));
+    // The general (Stockham) z pass carries psi^ too unless the options ask for A: one
+    // transform fewer per column, the kernels being issue-bound at the lengths they serve.
+    const bool gen_carry = !c->fused_z && c->nz > 1 && o.z_carry != 0;
+    const bool carry =
+        gen_carry || (c->fused_z && (o.z_carry == 1 || (o.z_carry == -1 && c->tiled && c->fused_z == 6)));
     // psi^ carried: tiled, with the 16-values-per-thread kernel (nz 512); standard layout,
     // with the square split.  A tiled context whose z length has no tiled psi^-carrying
     // kernel carries A unless the options ask for psi^ (then the layout is standard).
@@ -1399,7 +1405,7 @@ pfc_status pfc_profile_read(pfc_ctx* ctx, pfc_profile* out) {
     out->launches = ctx->launches;
     out->xy_variant = 0;
     out->xy_mode = ctx->xy_mode;
-    out->z_mode = ctx->z_carry ? (ctx->tiled ? 4 : 2) : (ctx->tiled ? 3 : (ctx->fused_z ? 1 : 0));
+    out->z_mode = ctx->z_carry ? (ctx->tiled ? 4 : (ctx->fused_z ? 2 : 5)) : (ctx->tiled ? 3 : (ctx->fused_z ? 1 : 0));
     out->z_variant = ctx->fused_z;
     out->y_variant = ctx->xy_mode == 2 ? ctx->fused_y : 0;
     for (int f = 0; f < PFC_PROFILE_FAMILIES; ++f) { out->calls[f] = ctx->prof_calls[f]; out->ms[f] = ctx->prof_ms[f]; }

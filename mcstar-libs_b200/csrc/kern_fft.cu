@@ -284,14 +284,20 @@ __global__ void __launch_bounds__(256) k_zflat(cx<T>* A, const cx<T>* __restrict
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
-template <typename T, int PROP>
+// The z pass of the general-length stepper over the reference layout, a tile of z columns
+// per CTA.  CARRY false: A = IFFT_z(psi^)/nz is carried; psi^ = FFT_z(A) and N^ = FFT_z(B),
+// the update, A' = IFFT_z(psi^')/nz over A (three transforms).  CARRY true: psi^ itself is
+// carried in A; N^ = FFT_z(B), the update writes psi^' over psi^, and A' = IFFT_z(psi^')/nz
+// goes to anext (two transforms; none after the update on the final step).
+template <typename T, int PROP, bool CARRY>
 __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict__ B, int nx, int ny, int nz,
                                                LinePlan p, const cx<T>* __restrict__ tw, int tile, ZArgsT<T> a,
                                                const double2* __restrict__ k0, int* flag, int col0, int col_end,
-                                               int64_t ms) {
+                                               int64_t ms, cx<T>* anext) {
     // fields of a batch (grid z): their own state, k0, noise counter and parameters
     A += blockIdx.z * ms;
     B += blockIdx.z * ms;
+    if (CARRY && anext) anext += blockIdx.z * ms;
     k0 += blockIdx.z;
     zmember(a);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -315,7 +321,11 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
         }
     }
     __syncthreads();
-    cx<T>* r = stockham_lines<T, -1>(b0, b1, 2 * tile, ld, p, tw);
+    // CARRY: only the B lines are transformed (lines tile.. of both buffers); psi^ stays in b0
+    cx<T>* rb = stockham_lines<T, -1>(CARRY ? b0 + (size_t)tile * ld : b0, CARRY ? b1 + (size_t)tile * ld : b1,
+                                      CARRY ? tile : 2 * tile, ld, p, tw);
+    cx<T>* r = CARRY ? b0 : rb;
+    cx<T>* nl = CARRY ? rb : rb + (size_t)tile * ld;
     cx<T>* other = (r == b0) ? b1 : b0;
     // a ky-slab of a larger field: wavenumbers, the k = 0 mode and the noise keys of the field
     const int kyg = ky + a.ky0;
@@ -326,22 +336,45 @@ __global__ void __launch_bounds__(256) k_zprop(cx<T>* A, const cx<T>* __restrict
         const int i = fdiv(e, p.by_n), kz = e - i * n;
         const int kx = i0 + i;
         const cx<T> v =
-            zmode<T, PROP>(r[i * ld + lpad(kz)], r[(tile + i) * ld + lpad(kz)], kx, kyg, kz, nx, nz, k1, deps, a, k0, mc);
+            zmode<T, PROP>(r[i * ld + lpad(kz)], nl[i * ld + lpad(kz)], kx, kyg, kz, nx, nz, k1, deps, a, k0, mc);
         if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
         r[i * ld + lpad(kz)] = v;
     }
     if (!prop_conserved<PROP>() && a.maxc) fold_max_change(mc, a.maxc);
     __syncthreads();
     if (threadIdx.x == 0 && bad) atomicOr(flag, 1);
+    if (CARRY) {
+        // psi^' over psi^; A' = IFFT_z(psi^')/nz into anext unless this is the last step
+        for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
+            const int i = e & (tile - 1), k = e >> tile_lg;
+            if (i < nt) A[((int64_t)k * ny + ky) * nxh + i0 + i] = r[i * ld + lpad(k)];
+        }
+        if (a.final_step || !anext) return;
+    }
     cx<T>* outb = r;
     T scale = T(1);
     if (!a.final_step) {
+        // (CARRY: the b1 lines below tile held nothing)
         outb = stockham_lines<T, 1>(r, other, nt, ld, p, tw);
         scale = T(1) / T(nz);
     }
+    cx<T>* dst = CARRY ? anext : A;
     for (int e = threadIdx.x; e < tile * n; e += blockDim.x) {
         const int i = e & (tile - 1), k = e >> tile_lg;
-        if (i < nt) A[((int64_t)k * ny + ky) * nxh + i0 + i] = outb[i * ld + lpad(k)] * scale;
+        if (i < nt) dst[((int64_t)k * ny + ky) * nxh + i0 + i] = outb[i * ld + lpad(k)] * scale;
+    }
+}
+
+// f(std::integral_constant<int, PROP>) for a run-time propagator
+template <class F>
+cudaError_t by_zprop(int prop, F&& f) {
+    switch (prop) {
+        case kPropConservedExp: return f(std::integral_constant<int, kPropConservedExp>{});
+        case kPropRelax: return f(std::integral_constant<int, kPropRelax>{});
+        case kPropRelaxExp: return f(std::integral_constant<int, kPropRelaxExp>{});
+        case kPropConservedPoly: return f(std::integral_constant<int, kPropConservedPoly>{});
+        case kPropConservedHpfc: return f(std::integral_constant<int, kPropConservedHpfc>{});
+        default: return f(std::integral_constant<int, kPropConserved>{});
     }
 }
 
@@ -354,15 +387,14 @@ cudaError_t set_attrs_T(const pfc_ctx* c) {
     if ((e = cudaFuncSetAttribute(k_rows_r2c<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
     if ((e = cudaFuncSetAttribute(k_rows_c2r<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
     if ((e = cudaFuncSetAttribute(k_rows_nonlin<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
-    if ((e = cudaFuncSetAttribute(k_zprop<T, kPropConserved>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
-    if ((e = cudaFuncSetAttribute(k_zprop<T, kPropConservedExp>, cudaFuncAttributeMaxDynamicSharedMemorySize, m)))
-        return e;
-    if ((e = cudaFuncSetAttribute(k_zprop<T, kPropRelax>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
-    if ((e = cudaFuncSetAttribute(k_zprop<T, kPropRelaxExp>, cudaFuncAttributeMaxDynamicSharedMemorySize, m))) return e;
-    if ((e = cudaFuncSetAttribute(k_zprop<T, kPropConservedPoly>, cudaFuncAttributeMaxDynamicSharedMemorySize, m)))
-        return e;
-    if ((e = cudaFuncSetAttribute(k_zprop<T, kPropConservedHpfc>, cudaFuncAttributeMaxDynamicSharedMemorySize, m)))
-        return e;
+    for (int prop = 0; prop <= kPropConservedHpfc && !e; ++prop)
+        e = by_zprop(prop, [&](auto P) {
+            cudaError_t r = cudaFuncSetAttribute(k_zprop<T, P.value, false>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+            if (!r) r = cudaFuncSetAttribute(k_zprop<T, P.value, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+            return r;
+        });
+    if (e) return e;
     (void)c;
     return cudaSuccess;
 }
@@ -447,7 +479,8 @@ cudaError_t launch_rows_nonlin(const pfc_ctx* c, void* buf, const void* pot, dou
 }
 
 template <typename T, int PROP>
-void zprop_T(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int col0, int ncols) {
+void zprop_T(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int col0, int ncols, void* anext,
+             bool carry) {
     const int tile = c->pzprop.tile;
     dim3 grid((ncols + tile - 1) / tile, c->ny, c->batch);
     ZArgsT<T> t{(T)a.dt,      (T)a.eps,    (T)a.C,      (T)a.namp_eff,
@@ -460,31 +493,33 @@ void zprop_T(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int c
             (cx<T>*)A, (const cx<T>*)B, c->nx, c->ny, t, c->k0, c->flag, col0, ncols, c->mstride);
         return;
     }
-    k_zprop<T, PROP><<<grid, 256, c->pzprop.smem, c->stream>>>((cx<T>*)A, (const cx<T>*)B, c->nx, c->ny, c->nz,
-                                                                c->pz.plan, (const cx<T>*)c->tw, tile, t, c->k0,
-                                                                c->flag, col0, col0 + ncols, c->mstride);
+    if (carry)
+        k_zprop<T, PROP, true><<<grid, 256, c->pzprop.smem, c->stream>>>(
+            (cx<T>*)A, (const cx<T>*)B, c->nx, c->ny, c->nz, c->pz.plan, (const cx<T>*)c->tw, tile, t, c->k0, c->flag,
+            col0, col0 + ncols, c->mstride, (cx<T>*)anext);
+    else
+        k_zprop<T, PROP, false><<<grid, 256, c->pzprop.smem, c->stream>>>(
+            (cx<T>*)A, (const cx<T>*)B, c->nx, c->ny, c->nz, c->pz.plan, (const cx<T>*)c->tw, tile, t, c->k0, c->flag,
+            col0, col0 + ncols, c->mstride, nullptr);
 }
 
-template <int PROP>
-void zprop_dt(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int col0, int ncols) {
-    if (c->dtype == PFC_F64) zprop_T<double, PROP>(c, A, B, a, col0, ncols);
-    else zprop_T<float, PROP>(c, A, B, a, col0, ncols);
-}
-
-cudaError_t launch_zprop_cols(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int col0, int ncols) {
-    switch (a.prop) {
-        case kPropConservedExp: zprop_dt<kPropConservedExp>(c, A, B, a, col0, ncols); break;
-        case kPropRelax: zprop_dt<kPropRelax>(c, A, B, a, col0, ncols); break;
-        case kPropRelaxExp: zprop_dt<kPropRelaxExp>(c, A, B, a, col0, ncols); break;
-        case kPropConservedPoly: zprop_dt<kPropConservedPoly>(c, A, B, a, col0, ncols); break;
-        case kPropConservedHpfc: zprop_dt<kPropConservedHpfc>(c, A, B, a, col0, ncols); break;
-        default: zprop_dt<kPropConserved>(c, A, B, a, col0, ncols);
-    }
+cudaError_t launch_zprop_cols(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int col0, int ncols,
+                              void* anext, bool carry) {
+    if (carry && c->nz == 1) return cudaErrorNotSupported;
+    by_zprop(a.prop, [&](auto P) {
+        if (c->dtype == PFC_F64) zprop_T<double, P.value>(c, A, B, a, col0, ncols, anext, carry);
+        else zprop_T<float, P.value>(c, A, B, a, col0, ncols, anext, carry);
+        return cudaSuccess;
+    });
     return cudaGetLastError();
 }
 
 cudaError_t launch_zprop(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a) {
     return launch_zprop_cols(c, A, B, a, 0, c->nxh);
+}
+
+cudaError_t launch_zprop_carry(const pfc_ctx* c, void* kpsi, const void* B, void* anext, const ZPropArgs& a) {
+    return launch_zprop_cols(c, kpsi, B, a, 0, c->nxh, anext, true);
 }
 
 }  // namespace pfc

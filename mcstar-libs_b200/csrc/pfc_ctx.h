@@ -140,8 +140,12 @@ struct ZPropArgs {
     int ky0, ny_global;
 };
 cudaError_t launch_zprop(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a);
-// the general z pass over the kx columns [col0, col0 + ncols)
-cudaError_t launch_zprop_cols(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int col0, int ncols);
+// the general z pass over the kx columns [col0, col0 + ncols); carry: A holds psi^ itself
+// (updated in place) and A' = IFFT_z(psi^')/nz goes to anext (not on the final step)
+cudaError_t launch_zprop_cols(const pfc_ctx* c, void* A, const void* B, const ZPropArgs& a, int col0, int ncols,
+                              void* anext = nullptr, bool carry = false);
+// the psi^-carrying general z pass over the whole field (nz > 1)
+cudaError_t launch_zprop_carry(const pfc_ctx* c, void* kpsi, const void* B, void* anext, const ZPropArgs& a);
 
 // ---- register-resident y and x passes (kern_passes.cu) ----
 int fused_y_variant(int ny, int dtype);

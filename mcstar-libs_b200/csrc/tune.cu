@@ -183,14 +183,14 @@ extern "C" pfc_status pfc_tune(const pfc_desc* d, const char* cache_path, pfc_op
     // which options touch a kernel of this shape: ask a context with the library's choice
     pfc_options cur;
     pfc_default_options(&cur);
-    bool general = false, zreg = false, tiled_ok = false, ytma = false;
+    bool general = false, zcarry_ok = false, tiled_ok = false, ytma = false;
     int xks = 1;
     {
         pfc_ctx* c = nullptr;
         pfc_status s = pfc_create_with(d, &cur, &c);
         if (s != PFC_OK) return s;
         general = c->xy_mode != 2 || (c->nz > 1 && !c->fused_z);
-        zreg = c->fused_z != 0;
+        zcarry_ok = c->nz > 1;  // (both z passes carry either state)
         xks = c->fused_x ? pfc::xkernel_variants(c->nx, c->dtype) : 1;
         tiled_ok = c->fused_z && c->fused_zfft && c->xy_mode == 2 && c->fused_y;
         ytma = tiled_ok && c->fused_y && pfc::ybulk_available(c);
@@ -206,7 +206,7 @@ extern "C" pfc_status pfc_tune(const pfc_desc* d, const char* cache_path, pfc_op
         return PFC_ERR_CUDA;
     }
     std::vector<Knob> knobs;
-    if (zreg) knobs.push_back({"z_carry", &cur.z_carry, {0, 1}});
+    if (zcarry_ok) knobs.push_back({"z_carry", &cur.z_carry, {0, 1}});
     if (xks > 1) {
         Knob k{"x_kernel", &cur.x_kernel, {}};
         for (int v = 0; v < 3; ++v)

@@ -110,12 +110,13 @@ def test_y_pass_kernels_match_oracle(shape, namp, y_kernel):
 
 
 @pytest.mark.parametrize("shape,dtype,z_mode", [((64, 64, 64), F32, 3), ((64, 64, 512), F32, 4),
-                                                 ((512, 512, 4), F32, 0), ((16, 16, 512), F32, 1),
-                                                 ((16, 12, 10), F64, 0)])
+                                                 ((512, 512, 4), F32, 5), ((16, 16, 512), F32, 1),
+                                                 ((16, 12, 10), F64, 5), ((96, 80, 1), F32, 0)])
 def test_stepper_layout_mode(shape, dtype, z_mode):
     """FP32 grids with register y, x and z passes run kx-tiled: nz = 512 carries psi^ through
     the bulk-copy z pass (z_mode 4), other lengths carry A (3); the register z pass alone
-    keeps the standard layout (1); other shapes use the general z pass (0)."""
+    keeps the standard layout (1); other shapes use the general z pass carrying psi^ (5),
+    and 2D fields (no z transforms) its flat form (0)."""
     assert stepper(shape, dtype).ctx.profile_read()["z_mode"] == z_mode
 
 
