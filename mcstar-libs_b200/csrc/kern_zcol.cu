@@ -43,7 +43,10 @@ struct ZCfg {
     static constexpr int P = NZ / E, U = E / P;
     static constexpr int TH = TX * P;  // threads per field
     static constexpr int T = 2 * TH;
-    static constexpr int MINB = T <= 256 ? 2 : 1;  // k_zcol CTAs per SM its register cap allows
+    // k_zcol CTAs per SM its register cap allows: with up to 16 values per thread, 6 (128
+    // threads, 85 registers) or 3 (256 threads) fit without spilling and hide the latency of
+    // the update's noise; 32 values per thread keep 128 registers
+    static constexpr int MINB = E > 16 ? (T <= 256 ? 2 : 1) : (T <= 128 ? 6 : (T <= 256 ? 3 : 1));
     static constexpr int PADG = TX / U;  // exchange padding: the 32/TX t-groups of a warp hit distinct banks
     static constexpr int REG = E * (P * TX + PADG);
     static constexpr int STG = NZ * TX;  // staging of one field tile, [z][c]
