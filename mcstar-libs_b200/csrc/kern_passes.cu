@@ -21,15 +21,22 @@ namespace {
 
 constexpr int cmaxi(int a, int b) { return a > b ? a : b; }
 
-template <int NY_, int E_, int TX_>
+// Exchange padding of the four-step transforms of TX interleaved columns whose reads take
+// U rows per thread: successive rows of a read are U (P TX) + U PADG slots apart, and
+// with E even the 32 / TX thread groups of a warp land in alternate bank halves when
+// U PADG = TX (mod 2 TX): PADG = TX / gcd(U, TX) (TX / U for powers of two).
+constexpr int gcdi(int a, int b) { return b == 0 ? a : gcdi(b, a % b); }
+constexpr int exch_pad(int tx, int u) { return tx / gcdi(u, tx); }
+
+template <int NY_, int E_, int TX_, int MINB_ = 0>
 struct YCfg {
     static constexpr int NY = NY_, E = E_, TX = TX_;
     static constexpr int P = NY / E, U = E / P, T = TX * P;
-    static constexpr int PADG = TX < 32 ? TX / U : 0;
+    static constexpr int PADG = TX < 32 ? exch_pad(TX, U) : 0;
     static constexpr int XB = E * (P * TX + PADG);
     static constexpr size_t SMEM = (size_t)(XB + NY) * sizeof(float2);
-    static constexpr int MINB = T <= 128 ? 4 : 2;
-    static_assert(P * E == NY && U * P == E && (TX >= 32 || (32 % TX == 0 && TX % U == 0)), "shape");
+    static constexpr int MINB = MINB_ ? MINB_ : (T <= 128 ? 4 : 2);
+    static_assert(P * E == NY && U * P == E && E % 2 == 0 && (TX >= 32 || 32 % TX == 0), "shape");
 };
 
 template <class Y, int DIR, bool kZ>
@@ -226,14 +233,14 @@ __global__ void __launch_bounds__(Y::T, Y::MINB)
     }
 }
 
-template <int NX_, int E_, int T_>
+template <int NX_, int E_, int T_, int MINB_ = 0>
 struct XCfg {
     static constexpr int NX = NX_, M = NX / 2, NXH = M + 1, E = E_, T = T_;
     static constexpr int P = M / E, U = E / P, R = T / P;
     static constexpr int LDR = NXH;  // odd: a warp over 32 rows at one k is conflict-free
     static constexpr int BUF = cmaxi(R * LDR, E * P * R);
     static constexpr size_t SMEM = (size_t)(BUF + M + M + 1) * sizeof(float2);
-    static constexpr int MINB = E <= 16 ? 3 : 2;
+    static constexpr int MINB = MINB_ ? MINB_ : (E <= 16 ? 3 : 2);
     static_assert(P * E == M && U * P == E && (R % 32 == 0 || R == 16) && R * P == T, "shape");
 };
 
@@ -298,7 +305,7 @@ __device__ __forceinline__ void row_tiles_r2c(const float2* rb, const float2* tw
 #pragma unroll
         for (int k = 0; k < FT / TSTEP; ++k) {
             const int kx = (kt0 + k * TSTEP) * kTileW + c;
-            *gp = r2c_post_f(row[kx], row[(M - kx) & (M - 1)], twP[kx]);
+            *gp = r2c_post_f(row[kx], row[kx == 0 ? 0 : M - kx], twP[kx]);  // Y[(M - kx) mod M]
             gp += TSTEP * ts;
         }
     }
@@ -399,7 +406,7 @@ __global__ void __launch_bounds__(X::T, X::MINB)
         const int k = t + P * j;
         const float2 yk = v[j];
         if (k == 0) xm_last = make_float2(yk.x - yk.y, 0.f);  // X[nx/2]
-        v[j] = r2c_post_f(yk, rb[r * LDR + ((M - k) & (M - 1))], twP[k]);
+        v[j] = r2c_post_f(yk, rb[r * LDR + (k == 0 ? 0 : M - k)], twP[k]);  // Y[(M - k) mod M]
     }
     __syncthreads();
 #pragma unroll
@@ -730,6 +737,12 @@ using X512h = XCfg<512, 16, 256>;  // 16 rows per CTA, 16 values per thread: thr
 using X256 = XCfg<256, 16, 256>;
 using X128 = XCfg<128, 16, 128>;
 using X64 = XCfg<64, 8, 128>;
+// 3 2^k lengths: 24 (or 12) values per thread over P = 8 or 4 threads per column or row,
+// the first stage a radix-3 step (RF); small CTAs, so more of them per SM
+using Y192 = YCfg<192, 24, 8, 12>;  // P 8, U 3: 64 threads, 80 registers
+using Y96 = YCfg<96, 24, 8, 20>;   // P 4, U 6: 32 threads, 96 registers
+using X192 = XCfg<192, 24, 128, 5>;  // M 96 = 24 x 4, 32 rows per CTA, 96 registers
+using X96 = XCfg<96, 12, 128, 6>;   // M 48 = 12 x 4, 32 rows per CTA
 
 template <class Y, bool kZ>
 cudaError_t yattr() {
@@ -796,6 +809,8 @@ int fused_y_variant(int ny, int dtype) {
         case 256: return 2;
         case 128: return 3;
         case 64: return 4;
+        case 192: return 10;
+        case 96: return 11;
     }
     return 0;
 }
@@ -806,6 +821,8 @@ int fused_x_variant(int nx, int dtype) {
         case 256: return 2;
         case 128: return 3;
         case 64: return 4;
+        case 192: return 10;
+        case 96: return 11;
     }
     return 0;
 }
@@ -817,6 +834,8 @@ cudaError_t set_pass_attributes(const pfc_ctx* c) {
         case 3: e = yattr<Y128, false>(); break;
         case 4: e = yattr<Y64, false>(); break;
         case 7: e = y3attr<Y512q>(); break;
+        case 10: e = yattr<Y192, false>(); break;
+        case 11: e = yattr<Y96, false>(); break;
     }
     if (e) return e;
     switch (c->fused_x) {
@@ -824,6 +843,8 @@ cudaError_t set_pass_attributes(const pfc_ctx* c) {
         case 3: e = xattr<X128>(); break;
         case 4: e = xattr<X64>(); break;
         case 5: e = xattr<X512h>(); break;
+        case 10: e = xattr<X192>(); break;
+        case 11: e = xattr<X96>(); break;
     }
     if (!e && c->xkern == 1) e = c->nx == 512 ? xpattr<XP512>() : xpattr<XP128>();
     if (!e && c->xkern == 2) e = xlattr<XL512>();
@@ -839,6 +860,8 @@ cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, d
         case 3: return ylaunch<Y128>(c, dir, in, out, scale, nzs, lay);
         case 4: return ylaunch<Y64>(c, dir, in, out, scale, nzs, lay);
         case 7: return y3launch<Y512q>(c, dir, in, out, scale, nzs, lay);
+        case 10: return ylaunch<Y192>(c, dir, in, out, scale, nzs, lay);
+        case 11: return ylaunch<Y96>(c, dir, in, out, scale, nzs, lay);
     }
     return cudaErrorNotSupported;
 }
@@ -851,6 +874,8 @@ cudaError_t xdispatch(const pfc_ctx* c, const void* in, void* out, const void* p
         case 3: return xlaunch<X128, MODE>(c, in, out, pot, mul, C, mu, nrows);
         case 4: return xlaunch<X64, MODE>(c, in, out, pot, mul, C, mu, nrows);
         case 5: return xlaunch<X512h, MODE>(c, in, out, pot, mul, C, mu, nrows);
+        case 10: return xlaunch<X192, MODE>(c, in, out, pot, mul, C, mu, nrows);
+        case 11: return xlaunch<X96, MODE>(c, in, out, pot, mul, C, mu, nrows);
     }
     return cudaErrorNotSupported;
 }
@@ -883,6 +908,8 @@ int fused_zfft_variant(int nz, int dtype) {
         case 256: return 2;
         case 128: return 3;
         case 64: return 4;
+        case 192: return 10;
+        case 96: return 11;
     }
     return 0;
 }
@@ -892,6 +919,8 @@ cudaError_t set_zfft_attributes(const pfc_ctx* c) {
         case 2: return yattr<Y256, true>();
         case 3: return yattr<Y128, true>();
         case 4: return yattr<Y64, true>();
+        case 10: return yattr<Y192, true>();
+        case 11: return yattr<Y96, true>();
     }
     return cudaSuccess;
 }
@@ -913,6 +942,8 @@ cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, do
         case 2: return zlaunch_fft<Y256>(c, dir, in, out, scale, lay, ky0, nky, copy);
         case 3: return zlaunch_fft<Y128>(c, dir, in, out, scale, lay, ky0, nky, copy);
         case 4: return zlaunch_fft<Y64>(c, dir, in, out, scale, lay, ky0, nky, copy);
+        case 10: return zlaunch_fft<Y192>(c, dir, in, out, scale, lay, ky0, nky, copy);
+        case 11: return zlaunch_fft<Y96>(c, dir, in, out, scale, lay, ky0, nky, copy);
     }
     return cudaErrorNotSupported;
 }

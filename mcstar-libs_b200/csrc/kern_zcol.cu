@@ -37,7 +37,9 @@ __device__ __forceinline__ void take_member(ZArgsF& a) {
     }
 }
 
-template <int NZ_, int E_, int TX_>
+constexpr int zgcd(int a, int b) { return b == 0 ? a : zgcd(b, a % b); }
+
+template <int NZ_, int E_, int TX_, int MINB_ = 0>
 struct ZCfg {
     static constexpr int NZ = NZ_, E = E_, TX = TX_;
     static constexpr int P = NZ / E, U = E / P;
@@ -46,8 +48,10 @@ struct ZCfg {
     // k_zcol CTAs per SM its register cap allows: with up to 16 values per thread, 6 (128
     // threads, 85 registers) or 3 (256 threads) fit without spilling and hide the latency of
     // the update's noise; 32 values per thread keep 128 registers
-    static constexpr int MINB = E > 16 ? (T <= 256 ? 2 : 1) : (T <= 128 ? 6 : (T <= 256 ? 3 : 1));
-    static constexpr int PADG = TX / U;  // exchange padding: the 32/TX t-groups of a warp hit distinct banks
+    static constexpr int MINB =
+        MINB_ ? MINB_ : (E > 16 ? (T <= 256 ? 2 : 1) : (T <= 128 ? 6 : (T <= 256 ? 3 : 1)));
+    // exchange padding: the 32/TX t-groups of a warp hit distinct banks (U PADG = TX mod 2 TX)
+    static constexpr int PADG = TX / zgcd(U, TX);
     static constexpr int REG = E * (P * TX + PADG);
     static constexpr int STG = NZ * TX;  // staging of one field tile, [z][c]
     // every kernel ends its shared memory with the twiddles W_NZ^m (NZ float2) and the
@@ -58,7 +62,7 @@ struct ZCfg {
     static constexpr size_t SMEM_CARRY = (size_t)(REG + STG + TAIL) * sizeof(float2);  // TH threads, one field
     // resident CTAs of k_zcarry the shared memory allows (228 KB per SM): its register cap
     static constexpr int CMINB = 4 * (SMEM_CARRY + 1024) <= 228 * 1024 ? 4 : 3;
-    static_assert(TH % 32 == 0 && U * P == E && TX % U == 0 && 32 % TX == 0, "shape");
+    static_assert(TH % 32 == 0 && U * P == E && E % 2 == 0 && 32 % TX == 0, "shape");
 };
 
 // Row of mode kz in a [row][c] tile of modes (TX = 8 float2 per row: the N^ hand-over
@@ -665,6 +669,7 @@ using Z3_512 = Z3Cfg<512, 16, 8>;  // 16 values per thread (k_zcol3)
 using Z256 = ZCfg<256, 16, 8>;
 using Z128 = ZCfg<128, 16, 8>;
 using Z64 = ZCfg<64, 8, 8>;
+using Z192 = ZCfg<192, 24, 8, 6>;  // P 8, U 3 (the first stage a radix-3 step); 80 registers
 
 // The propagator of a launch as a compile-time constant: f(std::integral_constant<int, PROP>).
 template <class F>
@@ -690,9 +695,12 @@ cudaError_t zattr() {
     return each_prop([](auto P) {
         cudaError_t e = cudaFuncSetAttribute(k_zcol<Z, P.value>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)Z::SMEM);
-        if (e) return e;
-        return cudaFuncSetAttribute(k_zcarry<Z, P.value>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)Z::SMEM_CARRY);
+        if constexpr (Z::U == 1 || Z::U == 2) {  // (k_zcarry: U of 1 or 2 only)
+            if (e) return e;
+            return cudaFuncSetAttribute(k_zcarry<Z, P.value>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)Z::SMEM_CARRY);
+        }
+        return e;
     });
 }
 
@@ -730,13 +738,20 @@ cudaError_t zlaunch(const pfc_ctx* c, const void* A, const void* B, void* O, con
 // Register z kernels by length: 6 (nz = 512) 16 values per thread over 32 threads per
 // column (fft_d1_to_d3); 1-4 the square split for 512 (psi^-carrying, standard layout
 // only), 256, 128, 64.
+// whether the register z pass of variant v has the psi^-carrying form in the reference
+// layout (k_zcarry: U of 1 or 2)
+bool zcarry_available(int v) { return v >= 1 && v <= 4; }
+
 int fused_z_variant(int nx, int nz, int dtype) {
     if (dtype != PFC_F32 || nx < 16 || (nx / 2) % 8 != 0 || nx % 2 != 0) return 0;
+    // (nz = 96: 4 threads per column leave too few warps for the update's noise; the
+    // general z pass is faster there)
     switch (nz) {
         case 512: return 6;
         case 256: return 2;
         case 128: return 3;
         case 64: return 4;
+        case 192: return 10;
     }
     return 0;
 }
@@ -747,6 +762,7 @@ cudaError_t set_zcol_attributes(const pfc_ctx* c) {
         case 2: return zattr<Z256>();
         case 3: return zattr<Z128>();
         case 4: return zattr<Z64>();
+        case 10: return zattr<Z192>();
         case 6:
             return each_prop([](auto P) {
                 using Z = Z3_512;
@@ -843,6 +859,7 @@ cudaError_t launch_zcol(const pfc_ctx* c, const void* A, const void* B, void* O,
         case 2: return zlaunch<Z256>(c, A, B, O, a, lay);
         case 3: return zlaunch<Z128>(c, A, B, O, a, lay);
         case 4: return zlaunch<Z64>(c, A, B, O, a, lay);
+        case 10: return zlaunch<Z192>(c, A, B, O, a, lay);
     }
     return cudaErrorNotSupported;
 }

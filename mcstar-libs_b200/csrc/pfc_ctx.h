@@ -189,6 +189,7 @@ int write_lowpass_file(const pfc_ctx* c, const void* spectrum, double lx, double
                        cudaError_t* cuda_err);
 
 // ---- register-resident z pass (kern_zcol.cu) ----
+bool zcarry_available(int fused_z);
 int fused_z_variant(int nx, int nz, int dtype);
 cudaError_t set_zcol_attributes(const pfc_ctx* c);
 cudaError_t set_peak_attributes();

@@ -83,7 +83,8 @@ template <int DIR> struct RF<1, DIR> { __device__ __forceinline__ static void ru
 template <int DIR> struct RF<2, DIR> { __device__ __forceinline__ static void run(float2* v) { Dft<float, DIR, 2>::run(v); } };
 template <int DIR> struct RF<4, DIR> { __device__ __forceinline__ static void run(float2* v) { Dft<float, DIR, 4>::run(v); } };
 template <int DIR> struct RF<8, DIR> { __device__ __forceinline__ static void run(float2* v) { Dft<float, DIR, 8>::run(v); } };
-template <int N, int DIR> struct RF {
+// Powers of two from 16 up: radix-4 steps down to the hand-written 8, 4, 2.
+template <int N, int DIR> struct RF4 {
     static_assert(N % 4 == 0 && N >= 16, "power of two");
     __device__ __forceinline__ static void run(float2* v) {
         constexpr int Q = N / 4;
@@ -108,6 +109,48 @@ template <int N, int DIR> struct RF {
         });
     }
 };
+
+// N = R Q with a radix R of 3 or 5 first (decimation in time): the R sub-sequences
+// v[R m + r] transformed (length Q), twiddled by W_N^(r k), and combined by R-point DFTs
+// into v[k + q Q].
+template <int N, int DIR, int R> struct RFR {
+    __device__ __forceinline__ static void run(float2* v);
+};
+// Lengths 2^a 3^b 5^c: powers of two by RF4, others by one radix-3 or radix-5 step first.
+template <int N, int DIR> struct RF {
+    __device__ __forceinline__ static void run(float2* v) {
+        if constexpr ((N & (N - 1)) == 0) {
+            RF4<N, DIR>::run(v);
+        } else if constexpr (N % 3 == 0) {
+            RFR<N, DIR, 3>::run(v);
+        } else {
+            static_assert(N % 5 == 0, "lengths 2^a 3^b 5^c");
+            RFR<N, DIR, 5>::run(v);
+        }
+    }
+};
+template <int N, int DIR, int R>
+__device__ __forceinline__ void RFR<N, DIR, R>::run(float2* v) {
+    constexpr int Q = N / R;
+    float2 s[R][Q];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int m = 0; m < Q; ++m) s[r][m] = v[R * m + r];
+#pragma unroll
+    for (int r = 0; r < R; ++r) RF<Q, DIR>::run(s[r]);
+    sfor<0, Q>([&](auto kk) {
+        constexpr int k = decltype(kk)::value;
+        float2 a[R];
+        sfor<0, R>([&](auto rr) {
+            constexpr int r = decltype(rr)::value;
+            a[r] = twmul<N, r * k, DIR>(s[r][k]);
+        });
+        Dft<float, DIR, R>::run(a);
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[k + q * Q] = a[q];
+    });
+}
 
 // Barrier policies of the exchanges: the whole CTA, or a named barrier over the
 // first COUNT threads (used when half of a CTA runs a transform alone).

@@ -37,6 +37,10 @@ CASES = [
     ((64, 64, 64), F32, 0.02),
     # the kx-tiled carry (register y, x and z passes; partial last tile of one column)
     ((64, 64, 512), F32, 0.02), ((128, 64, 256), F32, 0.0), ((64, 128, 128), F32, 0.03),
+    # the 3 2^k register kernels (radix-3 first stage; x, y, z lengths 96 and 192, mixed),
+    # tiled, and a 2D field through their y and x passes
+    ((192, 192, 192), F32, 0.02), ((96, 96, 96), F32, 0.0), ((96, 192, 96), F32, 0.03), ((192, 96, 192), F32, 0.0),
+    ((192, 192, 1), F32, 0.02), ((96, 96, 64), F32, 0.0),
 ]
 
 
@@ -111,7 +115,8 @@ def test_y_pass_kernels_match_oracle(shape, namp, y_kernel):
 
 @pytest.mark.parametrize("shape,dtype,z_mode", [((64, 64, 64), F32, 3), ((64, 64, 512), F32, 4),
                                                  ((512, 512, 4), F32, 5), ((16, 16, 512), F32, 1),
-                                                 ((16, 12, 10), F64, 5), ((96, 80, 1), F32, 0)])
+                                                 ((16, 12, 10), F64, 5), ((96, 80, 1), F32, 0),
+                                                 ((192, 192, 192), F32, 3), ((96, 96, 96), F32, 5)])
 def test_stepper_layout_mode(shape, dtype, z_mode):
     """FP32 grids with register y, x and z passes run kx-tiled: nz = 512 carries psi^ through
     the bulk-copy z pass (z_mode 4), other lengths carry A (3); the register z pass alone
