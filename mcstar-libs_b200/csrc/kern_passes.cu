@@ -743,6 +743,9 @@ using Y192 = YCfg<192, 24, 8, 12>;  // P 8, U 3: 64 threads, 80 registers
 using Y96 = YCfg<96, 24, 8, 20>;   // P 4, U 6: 32 threads, 96 registers
 using X192 = XCfg<192, 24, 128, 5>;  // M 96 = 24 x 4, 32 rows per CTA, 96 registers
 using X96 = XCfg<96, 12, 128, 6>;   // M 48 = 12 x 4, 32 rows per CTA
+// 5 2^k: 160 (the first stage a radix-5 step)
+using Y160 = YCfg<160, 40, 8, 12>;  // P 4, U 10: 32 threads
+using X160 = XCfg<160, 20, 128, 5>; // M 80 = 20 x 4, 32 rows per CTA
 
 template <class Y, bool kZ>
 cudaError_t yattr() {
@@ -811,6 +814,7 @@ int fused_y_variant(int ny, int dtype) {
         case 64: return 4;
         case 192: return 10;
         case 96: return 11;
+        case 160: return 12;
     }
     return 0;
 }
@@ -823,6 +827,7 @@ int fused_x_variant(int nx, int dtype) {
         case 64: return 4;
         case 192: return 10;
         case 96: return 11;
+        case 160: return 12;
     }
     return 0;
 }
@@ -836,6 +841,7 @@ cudaError_t set_pass_attributes(const pfc_ctx* c) {
         case 7: e = y3attr<Y512q>(); break;
         case 10: e = yattr<Y192, false>(); break;
         case 11: e = yattr<Y96, false>(); break;
+        case 12: e = yattr<Y160, false>(); break;
     }
     if (e) return e;
     switch (c->fused_x) {
@@ -845,6 +851,7 @@ cudaError_t set_pass_attributes(const pfc_ctx* c) {
         case 5: e = xattr<X512h>(); break;
         case 10: e = xattr<X192>(); break;
         case 11: e = xattr<X96>(); break;
+        case 12: e = xattr<X160>(); break;
     }
     if (!e && c->xkern == 1) e = c->nx == 512 ? xpattr<XP512>() : xpattr<XP128>();
     if (!e && c->xkern == 2) e = xlattr<XL512>();
@@ -862,6 +869,7 @@ cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, d
         case 7: return y3launch<Y512q>(c, dir, in, out, scale, nzs, lay);
         case 10: return ylaunch<Y192>(c, dir, in, out, scale, nzs, lay);
         case 11: return ylaunch<Y96>(c, dir, in, out, scale, nzs, lay);
+        case 12: return ylaunch<Y160>(c, dir, in, out, scale, nzs, lay);
     }
     return cudaErrorNotSupported;
 }
@@ -876,6 +884,7 @@ cudaError_t xdispatch(const pfc_ctx* c, const void* in, void* out, const void* p
         case 5: return xlaunch<X512h, MODE>(c, in, out, pot, mul, C, mu, nrows);
         case 10: return xlaunch<X192, MODE>(c, in, out, pot, mul, C, mu, nrows);
         case 11: return xlaunch<X96, MODE>(c, in, out, pot, mul, C, mu, nrows);
+        case 12: return xlaunch<X160, MODE>(c, in, out, pot, mul, C, mu, nrows);
     }
     return cudaErrorNotSupported;
 }
@@ -910,6 +919,7 @@ int fused_zfft_variant(int nz, int dtype) {
         case 64: return 4;
         case 192: return 10;
         case 96: return 11;
+        case 160: return 12;
     }
     return 0;
 }
@@ -921,6 +931,7 @@ cudaError_t set_zfft_attributes(const pfc_ctx* c) {
         case 4: return yattr<Y64, true>();
         case 10: return yattr<Y192, true>();
         case 11: return yattr<Y96, true>();
+        case 12: return yattr<Y160, true>();
     }
     return cudaSuccess;
 }
@@ -944,6 +955,7 @@ cudaError_t launch_zfft(const pfc_ctx* c, int dir, const void* in, void* out, do
         case 4: return zlaunch_fft<Y64>(c, dir, in, out, scale, lay, ky0, nky, copy);
         case 10: return zlaunch_fft<Y192>(c, dir, in, out, scale, lay, ky0, nky, copy);
         case 11: return zlaunch_fft<Y96>(c, dir, in, out, scale, lay, ky0, nky, copy);
+        case 12: return zlaunch_fft<Y160>(c, dir, in, out, scale, lay, ky0, nky, copy);
     }
     return cudaErrorNotSupported;
 }

@@ -37,10 +37,11 @@ CASES = [
     ((64, 64, 64), F32, 0.02),
     # the kx-tiled carry (register y, x and z passes; partial last tile of one column)
     ((64, 64, 512), F32, 0.02), ((128, 64, 256), F32, 0.0), ((64, 128, 128), F32, 0.03),
-    # the 3 2^k register kernels (radix-3 first stage; x, y, z lengths 96 and 192, mixed),
-    # tiled, and a 2D field through their y and x passes
+    # the 3 2^k and 5 2^k register kernels (radix-3 or radix-5 first stage; x, y, z lengths
+    # 96, 160 and 192, mixed), tiled, and 2D fields through their y and x passes
     ((192, 192, 192), F32, 0.02), ((96, 96, 96), F32, 0.0), ((96, 192, 96), F32, 0.03), ((192, 96, 192), F32, 0.0),
-    ((192, 192, 1), F32, 0.02), ((96, 96, 64), F32, 0.0),
+    ((192, 192, 1), F32, 0.02), ((96, 96, 64), F32, 0.0), ((160, 160, 160), F32, 0.02), ((160, 96, 192), F32, 0.0),
+    ((160, 160, 1), F32, 0.0),
 ]
 
 
