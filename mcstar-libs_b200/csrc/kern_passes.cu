@@ -746,6 +746,9 @@ using X96 = XCfg<96, 12, 128, 6>;   // M 48 = 12 x 4, 32 rows per CTA
 // 5 2^k: 160 (the first stage a radix-5 step)
 using Y160 = YCfg<160, 40, 8, 12>;  // P 4, U 10: 32 threads
 using X160 = XCfg<160, 20, 128, 5>; // M 80 = 20 x 4, 32 rows per CTA
+// 1024 (2D fields and y / x lengths beyond 512): 32 values per thread
+using Y1024 = YCfg<1024, 32, 8>;     // P 32, U 1: 256 threads
+using X1024 = XCfg<1024, 32, 256>;   // M 512 = 32 x 16, 16 rows per CTA
 
 template <class Y, bool kZ>
 cudaError_t yattr() {
@@ -815,6 +818,7 @@ int fused_y_variant(int ny, int dtype) {
         case 192: return 10;
         case 96: return 11;
         case 160: return 12;
+        case 1024: return 13;
     }
     return 0;
 }
@@ -828,6 +832,7 @@ int fused_x_variant(int nx, int dtype) {
         case 192: return 10;
         case 96: return 11;
         case 160: return 12;
+        case 1024: return 13;
     }
     return 0;
 }
@@ -842,6 +847,7 @@ cudaError_t set_pass_attributes(const pfc_ctx* c) {
         case 10: e = yattr<Y192, false>(); break;
         case 11: e = yattr<Y96, false>(); break;
         case 12: e = yattr<Y160, false>(); break;
+        case 13: e = yattr<Y1024, false>(); break;
     }
     if (e) return e;
     switch (c->fused_x) {
@@ -852,6 +858,7 @@ cudaError_t set_pass_attributes(const pfc_ctx* c) {
         case 10: e = xattr<X192>(); break;
         case 11: e = xattr<X96>(); break;
         case 12: e = xattr<X160>(); break;
+        case 13: e = xattr<X1024>(); break;
     }
     if (!e && c->xkern == 1) e = c->nx == 512 ? xpattr<XP512>() : xpattr<XP128>();
     if (!e && c->xkern == 2) e = xlattr<XL512>();
@@ -870,6 +877,7 @@ cudaError_t launch_ypass(const pfc_ctx* c, int dir, const void* in, void* out, d
         case 10: return ylaunch<Y192>(c, dir, in, out, scale, nzs, lay);
         case 11: return ylaunch<Y96>(c, dir, in, out, scale, nzs, lay);
         case 12: return ylaunch<Y160>(c, dir, in, out, scale, nzs, lay);
+        case 13: return ylaunch<Y1024>(c, dir, in, out, scale, nzs, lay);
     }
     return cudaErrorNotSupported;
 }
@@ -885,6 +893,7 @@ cudaError_t xdispatch(const pfc_ctx* c, const void* in, void* out, const void* p
         case 10: return xlaunch<X192, MODE>(c, in, out, pot, mul, C, mu, nrows);
         case 11: return xlaunch<X96, MODE>(c, in, out, pot, mul, C, mu, nrows);
         case 12: return xlaunch<X160, MODE>(c, in, out, pot, mul, C, mu, nrows);
+        case 13: return xlaunch<X1024, MODE>(c, in, out, pot, mul, C, mu, nrows);
     }
     return cudaErrorNotSupported;
 }

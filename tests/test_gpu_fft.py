@@ -98,10 +98,10 @@ def test_small_and_odd_shapes(nshape):
 
 @pytest.mark.parametrize("nshape", [(64, 64, 64), (128, 64, 256), (512, 64, 128), (8, 512, 512), (64, 32, 64),
                                     (256, 128, 512), (3, 256, 64), (96, 192, 96), (192, 96, 192), (16, 192, 192),
-                                    (192, 16, 16), (64, 160, 160), (160, 16, 16)], ids=lambda s: "x".join(map(str, s)))
+                                    (192, 16, 16), (64, 160, 160), (160, 16, 16), (2, 1024, 1024)], ids=lambda s: "x".join(map(str, s)))
 def test_register_transform_paths_fp32(nshape):
     """FP32 shapes: register x rows + y columns where nx and ny are in {64, 96, 128, 160,
-    192, 256, 512}, register z columns where nz is, general passes for the other axes."""
+    192, 256, 512, 1024}, register z columns where nz is, general passes for the other axes."""
     rng = np.random.default_rng(11)
     x = rng.standard_normal(nshape).astype(np.float32)
     want = np.fft.rfftn(x.astype(np.float64))

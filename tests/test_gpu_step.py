@@ -41,7 +41,7 @@ CASES = [
     # 96, 160 and 192, mixed), tiled, and 2D fields through their y and x passes
     ((192, 192, 192), F32, 0.02), ((96, 96, 96), F32, 0.0), ((96, 192, 96), F32, 0.03), ((192, 96, 192), F32, 0.0),
     ((192, 192, 1), F32, 0.02), ((96, 96, 64), F32, 0.0), ((160, 160, 160), F32, 0.02), ((160, 96, 192), F32, 0.0),
-    ((160, 160, 1), F32, 0.0),
+    ((160, 160, 1), F32, 0.0), ((1024, 1024, 1), F32, 0.02),
 ]
 
 
