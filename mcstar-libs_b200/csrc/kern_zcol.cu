@@ -120,11 +120,33 @@ __device__ __forceinline__ void watch(const float2 (&v)[Z::E], bool all, bool va
 // the transforming threads (bar) first, for a scratch that is an exchange buffer other
 // threads may still be reading.  The k = 0 mode (register 0 of thread t = 0 in column
 // kx = 0 at ky = 0, where D = 1 and the noise vanishes) is set to the FP64 value k0.
+// The noise term g(k) xi(k) of the update at mode kz of column (kx, ky): the conserved
+// dt namp sqrt(N) |k| / D(k), or the propagator's own gain; kxy = kx^2 + ky^2 in wavenumbers.
+template <class Z, int PROP>
+__device__ __forceinline__ void noise_gain_xi(int kz, int kx, int ky, float kxy, float deps, const float* kz_tab, int nx,
+                                              int ny, const ZArgsF& a, uint64_t ctr, float& g, float2& xi) {
+    const float k2z = kz_tab[kz_slot(kz)];
+    const float dopx = -kxy - k2z * k2z;
+    if constexpr (PROP == kPropConserved) {
+        const float dopy = dopx * dopx;
+        const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
+        g = a.dt * a.namp_eff * sqrtf(-dopx) * inv;
+    } else {
+        float ca, cb, cg;
+        prop_coef<PROP, float>(dopx, a.dt, deps, ca, cb, cg);
+        g = a.namp_eff * cg;
+    }
+    xi = kspace_noise<float>(kx, ky, kz, nx, ny, Z::NZ, a.seed, ctr);
+}
+
+// noise_modes: the thread's modes m < noise_modes (mode m: kz = (t U + m / P) + E (m % P),
+// register m) take their noise here; a caller that splits the noise with other threads
+// adds the rest.
 template <class Z, bool kPsiInV, bool kSync, int PROP, class Bar, class OTHER, class SLOT>
 __device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2* scratch, SLOT slot, const Bar& bar,
                                           const float* kz_tab, int kx, int ky, int t, int nx, int ny,
-                                          const ZArgsF& a, const double2* k0) {
-    constexpr int NZ = Z::NZ, E = Z::E, P = Z::P, U = Z::U;
+                                          const ZArgsF& a, const double2* k0, int noise_modes = Z::E) {
+    constexpr int E = Z::E, P = Z::P, U = Z::U;
     // wavenumbers K(i) = i' * 2 pi / L (common.hpp:27-28) with 2 pi / L precomputed
     const float k0x = (float)kx * a.ckx;
     const float k1y = (float)(ky < ny / 2 + 1 ? ky : ky - ny) * a.cky;
@@ -165,21 +187,11 @@ __device__ __forceinline__ void propagate(float2 (&v)[Z::E], OTHER other, float2
 #pragma unroll
             for (int k2 = 0; k2 < P; ++k2) scratch[slot((t * U + u) + E * k2)] = v[u * P + k2];
 #pragma unroll 1
-        for (int m = 0; m < E; ++m) {
+        for (int m = 0; m < noise_modes; ++m) {
             const int kz = (t * U + m / P) + E * (m % P);
-            const float k2z = kz_tab[kz_slot(kz)];
-            const float dopx = -kxy - k2z * k2z;
             float g;
-            if constexpr (PROP == kPropConserved) {
-                const float dopy = dopx * dopx;
-                const float inv = prop_inv(1.0f - a.dt * (deps * dopx + 2.0f * dopy + dopx * dopy));
-                g = a.dt * a.namp_eff * sqrtf(-dopx) * inv;
-            } else {
-                float ca, cb, cg;
-                prop_coef<PROP, float>(dopx, a.dt, deps, ca, cb, cg);
-                g = a.namp_eff * cg;
-            }
-            const float2 xi = kspace_noise<float>(kx, ky, kz, nx, ny, NZ, a.seed, ctr);
+            float2 xi;
+            noise_gain_xi<Z, PROP>(kz, kx, ky, kxy, deps, kz_tab, nx, ny, a, ctr, g, xi);
             float2 w = scratch[slot(kz)];
             w.x += g * xi.x;
             w.y += g * xi.y;
@@ -254,9 +266,41 @@ __global__ void __launch_bounds__(Z::T, Z::MINB) k_zcol(const float2* A, const f
             for (int k2 = 0; k2 < P; ++k2) regB[own((t * U + u) + E * k2)] = v[u * P + k2];
     }
     __syncthreads();
-    if (half != 0) return;
+    // With noise the B half draws the noise terms g(k) xi(k) of the upper half of the column's
+    // modes (m >= E/2 of the A thread with the same lt) into their slots of regA, which the A
+    // half leaves idle between its two transforms; the A half draws the lower half itself and
+    // adds the others after a barrier (a kernel-uniform condition: both halves take it).
+    constexpr int kSplit = E / 2;
+    if (half != 0) {
+        if (a.use_noise) {
+            const uint64_t ctr = a.dev_counter ? *a.dev_counter : a.counter;
+            const float k0x = (float)kx * a.ckx;
+            const float k1y = (float)(ky < ny / 2 + 1 ? ky : ky - ny) * a.cky;
+            const float kxy = k0x * k0x + k1y * k1y;
+            const float deps = 1.0f + a.C - a.eps;
+#pragma unroll 1
+            for (int m = kSplit; m < E; ++m) {
+                const int kz = (t * U + m / P) + E * (m % P);
+                float g;
+                float2 xi;
+                noise_gain_xi<Z, PROP>(kz, kx, ky, kxy, deps, kz_tab, nx, ny, a, ctr, g, xi);
+                regA[own(kz)] = make_float2(g * xi.x, g * xi.y);
+            }
+            __syncthreads();
+        }
+        return;
+    }
     propagate<Z, true, true, PROP>(v, [&](int kz) { return regB[own(kz)]; }, regB, own, bar, kz_tab, kx, ky, t, nx, ny,
-                                   a, k0);
+                                   a, k0, a.use_noise ? kSplit : E);
+    if (a.use_noise) {
+        __syncthreads();
+#pragma unroll
+        for (int m = kSplit; m < E; ++m) {
+            const float2 n = regA[own((t * U + m / P) + E * (m % P))];
+            v[m].x += n.x;
+            v[m].y += n.y;
+        }
+    }
     if (!a.final_step) fft_d2_to_d1<NZ, E, TX, 1, BarDyn, Z::PADG>(v, t, c, regA, tw, bar);
     watch<Z>(v, a.final_step, valid, flag);
     const ColAddr co = col_addr((lay & 4) ? 1 : 0, true, kx, ky, nxh, ny, NZ);
