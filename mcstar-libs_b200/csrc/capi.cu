@@ -551,7 +551,7 @@ pfc_status pfc_create_with(const pfc_desc* d, const pfc_options* opts, pfc_ctx**
     }
     c->z_carry = carry && (!c->tiled || c->fused_z == 6);
     if (!c->tiled && c->z_carry && c->fused_z == 6) c->fused_z = 1;
-    // the reference-layout psi^-carrying register z pass exists for the power-of-two lengths
+    // the reference-layout psi^-carrying register z pass exists for nz = 64, 128, 256, 512
     if (c->z_carry && !c->tiled && c->fused_z && !zcarry_available(c->fused_z)) {
         free_ctx(c);
         return PFC_ERR_UNSUPPORTED;

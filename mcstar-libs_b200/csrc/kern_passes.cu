@@ -1,4 +1,5 @@
-// Register-resident single-dimension passes of the FP32 stepper (power-of-two grids).
+// Register-resident single-dimension passes of the FP32 stepper (lengths 64, 96, 128, 160,
+// 192, 256, 512, 1024).
 //
 //  k_ycol  complex FFT along y (either direction, optional scale) of a tile of TX
 //          consecutive kx columns of one z-plane; in place or out of place.

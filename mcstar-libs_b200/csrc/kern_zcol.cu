@@ -1,4 +1,4 @@
-// The stepper's z pass for FP32 grids with nz in {64, 128, 256, 512}: register-resident
+// The stepper's z pass for FP32 grids with nz in {64, 128, 192, 256, 512}: register-resident
 // four-step FFTs along z on tiles of TX consecutive kx columns at one ky.
 //
 // Per tile: psi^ = FFT_z(A) (the carried state), N^ = FFT_z(B) (the nonlinear term),
@@ -7,7 +7,8 @@
 // itself on the last step.  Half of each CTA transforms A, the other half B.
 //
 //  k_zcol   one tile per CTA; both halves load and transform concurrently, N^ is
-//           handed over through shared memory, then the A half finishes alone.
+//           handed over through shared memory, both halves draw the update's noise, then
+//           the A half finishes alone.
 #include <type_traits>
 #include "bulk.cuh"
 #include "pfc_ctx.h"

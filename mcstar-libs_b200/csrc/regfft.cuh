@@ -1,7 +1,8 @@
 // Register-resident FFT building blocks of the fused plane and column kernels.
 //
-//  RF<N, DIR>::run(v)     N-point DFT (N a power of two <= 64) of v[0..N) held in
-//                         registers, natural order in and out: radix-4 decimation in
+//  RF<N, DIR>::run(v)     N-point DFT (N = 2^a 3^b 5^c, at most 64) of v[0..N) held in
+//                         registers, natural order in and out: a radix-3 or radix-5
+//                         step first where N has the factor, then radix-4 decimation in
 //                         time down to 8/4/2-point kernels; every twiddle is a
 //                         compile-time constant (trivial ones cost nothing).
 //  fft_d1_to_d2 / fft_d2_to_d1
