@@ -22,7 +22,12 @@ def _members():
             mk((48, 40, 30), 0.35, -0.2, 19, 0.0), mk((64, 64, 64), 0.2, -0.3, 20, 0.0),
             mk((64, 64, 64), 0.25, -0.22, 21, 0.02), mk((32, 16, 512), 0.3, -0.2, 22, 0.01),
             mk((32, 16, 512), 0.25, -0.25, 23, 0.02), mk((64, 512, 64), 0.3, -0.2, 24, 0.0),
-            mk((64, 512, 64), 0.25, -0.22, 25, 0.02)]
+            mk((64, 512, 64), 0.25, -0.22, 25, 0.02),
+            # batched classes through the 3 2^k / 5 2^k register passes: x 192 (tiled, z 64),
+            # 2D 160, and 96 beside the general z pass
+            mk((192, 64, 64), 0.3, -0.2, 26, 0.02), mk((192, 64, 64), 0.25, -0.25, 27, 0.0),
+            mk((160, 160, 1), 0.3, -0.2, 28, 0.03), mk((160, 160, 1), 0.2, -0.3, 29, 0.0),
+            mk((96, 96, 24), 0.3, -0.22, 30, 0.02), mk((96, 96, 24), 0.35, -0.2, 31, 0.0)]
 
 
 @pytest.mark.parametrize("spg", [1, 3])
